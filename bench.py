@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the plain Monte Carlo fault-tree path on B200.
+
+Workload (one "step" = one pass of the hot path over one batch): the 5,000
+basic-event / 3,000-gate synthetic tree (seed 11, 45% AND, 40% OR, 10%
+ATLEAST, 5% NOT/XOR, 20 layers, 30% of nodes with fan-out >= 2, p
+log-uniform in [1e-5, 1e-2]); 2^30 samples = 2^24 uint64 words per node per
+GPU; every gate tallied.  Each step is a new pass (iteration = step + 1),
+exactly like the reference's pass loop.  N GPUs shard the sample-word range
+(weak scaling: 2^24 words per GPU) and all-reduce the tallies after each pass.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line on rank 0.  The metric is gate-evals/s (gates x samples
+per second); sample-words/s (basic-event words per second) is reported next
+to it.  The CPU baseline and the reference arm run the reference-dataflow CPU
+implementation (oracle/_ref: the reference's own Philox header compiled from
+its sources, gate and tally loops restated) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "gate-evals/s"
+UNIT = "gate-evals/s"
+WORDS_PER_GPU = 1 << 24
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mcg", choices=["mcg", "reference"])
+    ap.add_argument("--words", type=int, default=WORDS_PER_GPU, help="sample words per GPU per step")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        load = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+
+def cpu_rate(g, target_seconds: float, reference: bool = True):
+    """Gate-evals/s of the CPU reference dataflow on a bounded sample of the
+    workload (pass 1, leading words), using every host thread."""
+    from oracle import oracle
+    oracle.build()
+    ref = reference and oracle.has_reference_build()
+    words = 512
+    t0 = time.perf_counter()
+    oracle.tallies(g, 1, 1, 0, words, reference=ref)
+    dt = time.perf_counter() - t0
+    words = int(min(1 << 20, max(512, words * target_seconds / max(dt, 1e-3))))
+    words = (words // 64) * 64 or 64
+    t0 = time.perf_counter()
+    oracle.tallies(g, 1, 1, 0, words, reference=ref)
+    dt = time.perf_counter() - t0
+    rate = g.n_gates * words * 64 / dt
+    kind = "reference" if ref else "port"
+    what = ("oracle/_ref/libref_mc.so: reference src/mc/prng/philox128.h compiled from its sources, "
+            "gate/tally loops restated from src/mc/kernel/gate.h and tally.h" if ref else
+            "oracle/liboracle.so: plain-C restatement of the reference dataflow")
+    return {"value": rate, "unit": UNIT, "cores": oracle.max_threads(), "kind": kind,
+            "sample": f"{words} words (pass 1, words [0, {words})) of the 5,000-event tree, "
+                      f"{g.n_gates} gates tallied, {dt:.2f} s; {what}",
+            "seconds": dt, "words": words}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    from mcscram_b200 import synth
+    from oracle import oracle
+    oracle.build()
+    g = synth.config2()
+    ref = oracle.has_reference_build()
+    # size one step to ~args.cpu_seconds / 2 of CPU work
+    probe = 512
+    t0 = time.perf_counter()
+    oracle.tallies(g, 1, 1, 0, probe, reference=ref)
+    dt = time.perf_counter() - t0
+    words = int(min(1 << 20, max(256, probe * (args.cpu_seconds / 2) / max(dt, 1e-3))))
+    for i in range(args.warmup):
+        oracle.tallies(g, 1 + i, 1, 0, min(words, 1024), reference=ref)
+    times = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.tallies(g, 1 + i, 1, 0, words, reference=ref)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = g.n_gates * words * 64 * args.steps / total
+    cores = oracle.max_threads()
+    kind = "reference" if ref else "port"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "plain MC, 5,000-event / 3,000-gate synthetic tree (seed 11), pass-sized sample",
+                   "samples_per_step": words * 64, "n_be": g.n_be, "n_gates": g.n_gates},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{words} words per step of the 5,000-event tree on {cores} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- GPU arm
+
+def traffic_from_profile():
+    """DRAM bytes per fused launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "k_fused_config2.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def main() -> int:
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from mcscram_b200 import _capi, synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    g = synth.config2()
+    W = args.words
+    word_begin = rank * W
+    if word_begin + W > (1 << 32):
+        raise SystemExit("word range exceeds the 32-bit sample counter")
+    stream = torch.cuda.current_stream()
+    eng = _capi.Engine(g, device=local, stream=stream.cuda_stream)
+    info = eng.program_info()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def allreduce_tallies():
+        if world == 1:
+            return
+        ones, total = eng.tallies()
+        t = torch.from_numpy(ones.astype(np.int64)).cuda()
+        dist.all_reduce(t)
+
+    # warm-up passes (iterations 1..W); then the timed passes continue the numbering
+    for i in range(args.warmup):
+        flush.zero_()
+        eng.run(i + 1, 1, word_begin, W)
+        allreduce_tallies()
+    torch.cuda.synchronize()
+    eng.reset_tallies()
+    launches0 = eng.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev_run = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        flush.zero_()
+        ev_run[i][0].record(stream)
+        eng.run(args.warmup + i + 1, 1, word_begin, W)
+        ev_run[i][1].record(stream)
+        allreduce_tallies()
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = eng.launch_count() - launches0
+    elapsed_ms = t_start.elapsed_time(t_end)
+    run_ms = sum(a.elapsed_time(b) for a, b in ev_run)
+    if world > 1:
+        t = torch.tensor([elapsed_ms, run_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, run_ms = float(t[0]), float(t[1])
+    ms_per_step = elapsed_ms / args.steps
+    samples = W * 64 * world
+    value = g.n_gates * samples / (ms_per_step * 1e-3)
+    be_words_per_s = g.n_be * W * world / (ms_per_step * 1e-3)
+
+    # roofline of the fused kernel: basic-event words per launch / launch time,
+    # against the register-only sampler measured on this GPU in this run
+    launches_per_step = max(launches // max(args.steps, 1), 1)
+    avg_launch_s = run_ms * 1e-3 / (args.steps * launches_per_step)
+    be_words_per_launch = g.n_be * W / launches_per_step
+    achieved = be_words_per_launch / avg_launch_s
+    peak = _capi.sampler_peak(n_events=256, n_words=1 << 22, repeats=3, device=local)
+    traffic = traffic_from_profile()
+
+    # end to end: host descriptor -> engine (tables to HBM) -> one pass -> tallies to host
+    e2e = None
+    if args.e2e_steps > 0:
+        ts = []
+        for i in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            with _capi.Engine(g, device=local, stream=stream.cuda_stream) as e2:
+                e2.run(1, 1, word_begin, W)
+                ones, total = e2.tallies()
+            ts.append(time.perf_counter() - t0)
+        if world > 1:
+            t = torch.tensor([max(ts)], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ts = [float(t[0])]
+        e2e_s = statistics.median(ts)
+        h2d = (info["n_ops"] * 16 + g.n_be * 16 + g.n_gates * 20 + g.inputs.size * 4 + g.tally_nodes.size * 4)
+        e2e = {"value": g.n_gates * samples / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(g.tally_nodes.size * 8), "seconds_per_step": e2e_s}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_rate(g, args.cpu_seconds, reference=True)
+
+    if rank == 0:
+        peaks_file = ROOT / "MEASURED_PEAKS.json"
+        hbm_peak = None
+        if peaks_file.exists():
+            hbm_peak = json.loads(peaks_file.read_text()).get("hbm_gbs")
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "plain MC pass, 5,000-event / 3,000-gate synthetic tree (seed 11)",
+                       "samples_per_gpu": W * 64, "words_per_gpu": W, "n_be": g.n_be, "n_gates": g.n_gates,
+                       "tallied_nodes": int(g.tally_nodes.size), "parallelism": f"word-range shards x{world}",
+                       "l2": "256 MB buffer written between steps", "mode": "fused"},
+            "sample_words_per_s": be_words_per_s,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "int-alu", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gword/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "register-only Philox sampler kernel measured in this run"},
+            "clocks": clk,
+            "program": info,
+        }
+        if traffic and hbm_peak:
+            line["roofline_hbm"] = {"achieved": traffic / avg_launch_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                                    "frac": traffic / avg_launch_s / 1e9 / hbm_peak}
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

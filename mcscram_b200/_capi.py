@@ -1,0 +1,279 @@
+"""ctypes bindings of libmcg.so (include/mcg.h).
+
+The shared library is loaded from this package directory.  If it is missing
+or cannot be loaded, ``load()`` raises: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from .graph import FlatGraph
+
+LIB_PATH = Path(__file__).resolve().parent / "libmcg.so"
+
+MCG_OK = 0
+MCG_ERR_INVALID = 1
+MCG_ERR_CUDA = 2
+MCG_ERR_OOM = 3
+MCG_ERR_TIMEOUT = 4
+MCG_ERR_STATE = 5
+MCG_ERR_NO_DEVICE = 6
+
+MODE_FUSED = 0
+MODE_LAYERED = 1
+
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_u64p = C.POINTER(C.c_uint64)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class GraphDesc(C.Structure):
+    _fields_ = [
+        ("n_be", C.c_uint32),
+        ("n_gates", C.c_uint32),
+        ("be_pdag_idx", _i32p),
+        ("be_event_idx", _u32p),
+        ("be_threshold", _u64p),
+        ("gate_pdag_idx", _i32p),
+        ("gate_op", _u8p),
+        ("gate_k", _u32p),
+        ("gate_in_begin", _u32p),
+        ("gate_in_count", _u32p),
+        ("gate_neg_count", _u32p),
+        ("inputs", _u32p),
+        ("n_inputs", C.c_uint64),
+        ("n_tally", C.c_uint32),
+        ("tally_nodes", _u32p),
+    ]
+
+
+class RunDesc(C.Structure):
+    _fields_ = [
+        ("mode", C.c_uint32),
+        ("device", C.c_int32),
+        ("stream", C.c_void_p),
+        ("block_threads", C.c_uint32),
+        ("smem_slots", C.c_uint32),
+        ("ctas_per_sm", C.c_uint32),
+        ("chunk_words", C.c_uint64),
+        ("layered_max_words", C.c_uint64),
+    ]
+
+
+class ProgramInfo(C.Structure):
+    _fields_ = [
+        ("n_ops", C.c_uint64),
+        ("smem_slots", C.c_uint32),
+        ("global_slots", C.c_uint32),
+        ("max_live", C.c_uint32),
+        ("block_threads", C.c_uint32),
+        ("grid_ctas", C.c_uint32),
+        ("scratch_bytes", C.c_uint64),
+        ("smem_bytes", C.c_uint32),
+        ("n_inline_be", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class McgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mcg error {code}: {msg}")
+        self.code = code
+
+
+_lib: Optional[C.CDLL] = None
+
+_SIGNATURES = {
+    "mcg_create": (C.c_int, [C.POINTER(GraphDesc), C.POINTER(RunDesc), C.POINTER(C.c_void_p)]),
+    "mcg_destroy": (C.c_int, [C.c_void_p]),
+    "mcg_run": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64]),
+    "mcg_synchronize": (C.c_int, [C.c_void_p]),
+    "mcg_read_tallies": (C.c_int, [C.c_void_p, _u64p, _u64p]),
+    "mcg_tally_device_ptr": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mcg_set_tallies": (C.c_int, [C.c_void_p, _u64p, C.c_uint64]),
+    "mcg_reset_tallies": (C.c_int, [C.c_void_p]),
+    "mcg_dump_words": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, _u64p]),
+    "mcg_program_info_get": (C.c_int, [C.c_void_p, C.POINTER(ProgramInfo)]),
+    "mcg_compile": (C.c_int, [C.POINTER(GraphDesc), C.c_uint32, C.POINTER(ProgramInfo), _u32p, C.c_uint64]),
+    "mcg_launch_count": (C.c_int, [C.c_void_p, _u64p]),
+    "mcg_time_runs": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
+    "mcg_sampler_peak": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
+    "mcg_last_error": (C.c_char_p, []),
+    "mcg_version": (C.c_char_p, []),
+}
+
+
+def load() -> C.CDLL:
+    """Loads libmcg.so (building it first if the toolkit is here and it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        from . import build as _build
+        _build.build()
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    for name, (res, args) in _EXTRA_SIGNATURES.items():
+        if hasattr(lib, name):
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+_EXTRA_SIGNATURES: dict = {}
+
+
+def register_signatures(sigs: dict) -> None:
+    """Lets other binding modules add their entry points before or after load()."""
+    _EXTRA_SIGNATURES.update(sigs)
+    if _lib is not None:
+        for name, (res, args) in sigs.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+
+
+def check(status: int) -> None:
+    if status != MCG_OK:
+        msg = load().mcg_last_error().decode(errors="replace")
+        raise McgError(status, msg)
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class GraphView:
+    """Keeps the numpy arrays of a FlatGraph alive while a GraphDesc points at them."""
+
+    def __init__(self, g: FlatGraph):
+        g.validate()
+        self.g = g
+        self._keep = [g.be_pdag_idx, g.be_event_idx, g.be_threshold, g.gate_pdag_idx, g.gate_op, g.gate_k,
+                      g.gate_in_begin, g.gate_in_count, g.gate_neg_count, g.inputs, g.tally_nodes]
+        self.desc = GraphDesc(
+            n_be=g.n_be, n_gates=g.n_gates,
+            be_pdag_idx=_ptr(g.be_pdag_idx, C.c_int32), be_event_idx=_ptr(g.be_event_idx, C.c_uint32),
+            be_threshold=_ptr(g.be_threshold, C.c_uint64), gate_pdag_idx=_ptr(g.gate_pdag_idx, C.c_int32),
+            gate_op=_ptr(g.gate_op, C.c_uint8), gate_k=_ptr(g.gate_k, C.c_uint32),
+            gate_in_begin=_ptr(g.gate_in_begin, C.c_uint32), gate_in_count=_ptr(g.gate_in_count, C.c_uint32),
+            gate_neg_count=_ptr(g.gate_neg_count, C.c_uint32), inputs=_ptr(g.inputs, C.c_uint32),
+            n_inputs=int(g.inputs.size), n_tally=int(g.tally_nodes.size),
+            tally_nodes=_ptr(g.tally_nodes, C.c_uint32))
+
+
+def compile_program(g: FlatGraph, smem_slot_budget: int = 64):
+    """Host-only compilation of the fused program: (info dict, ops array [n_ops, 4] uint32)."""
+    lib = load()
+    view = GraphView(g)
+    info = ProgramInfo()
+    check(lib.mcg_compile(C.byref(view.desc), smem_slot_budget, C.byref(info), None, 0))
+    ops = np.zeros((info.n_ops, 4), dtype=np.uint32)
+    check(lib.mcg_compile(C.byref(view.desc), smem_slot_budget, C.byref(info), _ptr(ops, C.c_uint32), info.n_ops))
+    return info.as_dict(), ops
+
+
+class Engine:
+    """One device engine over a flattened PDAG (wraps mcg_create ... mcg_destroy)."""
+
+    def __init__(self, g: FlatGraph, mode: int = MODE_FUSED, device: int = 0, stream: Optional[int] = None,
+                 smem_slots: int = 0, ctas_per_sm: int = 0, chunk_words: int = 0, layered_max_words: int = 0):
+        self.lib = load()
+        self.graph = g
+        self._view = GraphView(g)
+        run = RunDesc(mode=mode, device=device, stream=C.c_void_p(stream) if stream else None, block_threads=0,
+                      smem_slots=smem_slots, ctas_per_sm=ctas_per_sm, chunk_words=chunk_words,
+                      layered_max_words=layered_max_words)
+        h = C.c_void_p()
+        check(self.lib.mcg_create(C.byref(self._view.desc), C.byref(run), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mcg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def n_tally(self) -> int:
+        return int(self.graph.tally_nodes.size)
+
+    def run(self, iteration_first: int, n_iterations: int, word_begin: int, word_count: int) -> None:
+        check(self.lib.mcg_run(self.handle, iteration_first, n_iterations, word_begin, word_count))
+
+    def synchronize(self) -> None:
+        check(self.lib.mcg_synchronize(self.handle))
+
+    def tallies(self):
+        ones = np.zeros(max(self.n_tally, 1), dtype=np.uint64)
+        total = C.c_uint64()
+        check(self.lib.mcg_read_tallies(self.handle, _ptr(ones, C.c_uint64), C.byref(total)))
+        return ones[: self.n_tally], int(total.value)
+
+    def set_tallies(self, ones: np.ndarray, total_bits: int) -> None:
+        ones = np.ascontiguousarray(ones, dtype=np.uint64)
+        check(self.lib.mcg_set_tallies(self.handle, _ptr(ones, C.c_uint64), total_bits))
+
+    def tally_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(self.lib.mcg_tally_device_ptr(self.handle, C.byref(p)))
+        return int(p.value or 0)
+
+    def reset_tallies(self) -> None:
+        check(self.lib.mcg_reset_tallies(self.handle))
+
+    def dump_words(self, iteration: int, word_begin: int, n_words: int) -> np.ndarray:
+        out = np.zeros((self.graph.n_nodes, n_words), dtype=np.uint64)
+        check(self.lib.mcg_dump_words(self.handle, iteration, word_begin, n_words, _ptr(out, C.c_uint64)))
+        return out
+
+    def program_info(self) -> dict:
+        info = ProgramInfo()
+        check(self.lib.mcg_program_info_get(self.handle, C.byref(info)))
+        return info.as_dict()
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        check(self.lib.mcg_launch_count(self.handle, C.byref(n)))
+        return int(n.value)
+
+    def time_runs(self, iteration_first: int, word_begin: int, word_count: int, repeats: int) -> float:
+        ms = C.c_double()
+        check(self.lib.mcg_time_runs(self.handle, iteration_first, word_begin, word_count, repeats, C.byref(ms)))
+        return float(ms.value)
+
+
+def sampler_peak(n_events: int = 256, n_words: int = 1 << 21, repeats: int = 5, device: int = 0) -> float:
+    """Basic-event words per second of the register-only sampler kernel."""
+    lib = load()
+    r = C.c_double()
+    check(lib.mcg_sampler_peak(device, n_events, n_words, repeats, C.byref(r)))
+    return float(r.value)
+
+
+def version() -> str:
+    return load().mcg_version().decode()

@@ -1,0 +1,493 @@
+// engine.cu -- the mcg_* engine entry points of include/mcg.h.
+//
+// One engine = one flattened PDAG on one device and stream.  It owns the
+// device copies of the compiled fused program, the layered-mode tables, the
+// tally counters and the fused kernel's scratch.  Replaces the device-memory
+// ownership and pass submission of the reference's layer_manager
+// (src/mc/queue/layer_manager.tpp:203-301) and its queueables
+// (src/mc/queue/queueable.h:206-273, 725-731).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "error.hpp"
+#include "graph.hpp"
+#include "kernels.cuh"
+#include "mcg.h"
+#include "program.hpp"
+
+namespace {
+
+constexpr int kMulForm = 0;   // (uint64)a*b: IMAD.WIDE.U32
+constexpr int kPackForm = 0;  // compare-and-or nibbles
+constexpr int kFusedThreads = 256;
+constexpr uint64_t kDefaultChunkWords = 1ull << 21;
+
+#define MCG_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t err_ = (call);                                                              \
+        if (err_ != cudaSuccess) {                                                              \
+            return mcg::fail(err_ == cudaErrorMemoryAllocation ? MCG_ERR_OOM : MCG_ERR_CUDA,    \
+                             std::string(#call) + ": " + cudaGetErrorString(err_));             \
+        }                                                                                       \
+    } while (0)
+
+template <typename T>
+cudaError_t upload(T **dptr, const std::vector<T> &v) {
+    *dptr = nullptr;
+    if (v.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void **)dptr, v.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+struct mcg_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t mode = MCG_MODE_FUSED;
+    mcg::Graph graph;
+    mcg::Program prog;
+
+    // fused
+    uint4 *d_ops = nullptr;
+    uint64_t *d_scratch = nullptr;
+    uint64_t scratch_stride = 0;
+    uint32_t nt = kFusedThreads;
+    uint32_t grid = 0;
+    uint32_t smem_bytes = 0;
+    bool tally_in_smem = false;
+    uint64_t chunk_words = kDefaultChunkWords;
+
+    // tallies
+    unsigned long long *d_tally = nullptr;
+    uint64_t total_bits = 0;
+
+    // layered
+    uint4 *d_be = nullptr;
+    uint4 *d_meta = nullptr;
+    uint32_t *d_inputs = nullptr;
+    uint32_t *d_tally_nodes = nullptr;
+    uint32_t *d_layer_gates = nullptr;
+    std::vector<uint32_t> layer_offsets;  // into d_layer_gates, size n_layers + 1
+    uint64_t *d_buf = nullptr;
+    uint64_t buf_words = 0;
+    uint64_t layered_max_words = 0;
+
+    uint64_t launches = 0;
+};
+
+namespace {
+
+mcg_status build_layered_tables(mcg_engine *e) {
+    const mcg::Graph &g = e->graph;
+    std::vector<uint4> be(g.n_be);
+    for (uint32_t i = 0; i < g.n_be; ++i) {
+        be[i] = make_uint4((uint32_t)g.be_pdag_idx[i] + 1u, g.be_event_idx[i] + 1u, (uint32_t)g.be_threshold[i],
+                           (uint32_t)(g.be_threshold[i] >> 32));
+    }
+    std::vector<uint4> meta(g.n_gates);
+    std::vector<uint32_t> layer(g.n_gates, 1);
+    uint32_t n_layers = 0;
+    for (uint32_t i = 0; i < g.n_gates; ++i) {
+        meta[i] = make_uint4((uint32_t)g.gate_op[i] | ((g.gate_k[i] & 0xFFu) << 8), g.gate_in_begin[i],
+                             g.gate_in_count[i], g.gate_neg_count[i]);
+        uint32_t l = 1;
+        for (uint32_t j = 0; j < g.gate_in_count[i]; ++j) {
+            const uint32_t c = g.inputs[g.gate_in_begin[i] + j];
+            if (c >= g.n_be) l = std::max(l, layer[c - g.n_be] + 1);
+        }
+        layer[i] = l;
+        n_layers = std::max(n_layers, l);
+    }
+    // Gate ids grouped by layer (layer 1 .. n_layers), like the reference's
+    // LayeredTopologicalOrder depth (src/preprocessor.cc:130-171).
+    std::vector<uint32_t> counts(n_layers + 2, 0);
+    for (uint32_t i = 0; i < g.n_gates; ++i) counts[layer[i]]++;
+    e->layer_offsets.assign(n_layers + 1, 0);
+    for (uint32_t l = 1; l <= n_layers; ++l) e->layer_offsets[l] = e->layer_offsets[l - 1] + counts[l];
+    std::vector<uint32_t> cursor(e->layer_offsets.begin(), e->layer_offsets.end());
+    std::vector<uint32_t> order(g.n_gates);
+    for (uint32_t i = 0; i < g.n_gates; ++i) order[cursor[layer[i] - 1]++] = i;
+
+    MCG_CUDA(upload(&e->d_be, be));
+    MCG_CUDA(upload(&e->d_meta, meta));
+    MCG_CUDA(upload(&e->d_inputs, g.inputs));
+    MCG_CUDA(upload(&e->d_tally_nodes, g.tally_nodes));
+    MCG_CUDA(upload(&e->d_layer_gates, order));
+    return MCG_OK;
+}
+
+dim3 rows_grid(uint64_t words, uint32_t rows, uint32_t threads) {
+    const uint32_t bx = (uint32_t)((words + threads - 1) / threads);
+    uint32_t by = rows, bz = 1;
+    while (by > 65535u) {
+        bz *= 2;
+        by = (rows + bz - 1) / bz;
+    }
+    return dim3(bx, by, bz);
+}
+
+// Materialises every node's words for one pass over [word_begin, word_begin + W)
+// into d_buf (reference dataflow).
+mcg_status layered_eval(mcg_engine *e, uint32_t iteration, uint64_t word_begin, uint64_t W) {
+    const mcg::Graph &g = e->graph;
+    const uint64_t need = (uint64_t)g.n_nodes() * W;
+    if (need > e->buf_words) {
+        if (e->d_buf) cudaFree(e->d_buf);
+        e->d_buf = nullptr;
+        e->buf_words = 0;
+        MCG_CUDA(cudaMalloc((void **)&e->d_buf, std::max<uint64_t>(need, 1) * sizeof(uint64_t)));
+        e->buf_words = need;
+    }
+    const uint32_t t3 = (iteration + 1u) << 6;
+    if (g.n_be > 0) {
+        mcg::dev::k_layer_be<kMulForm, kPackForm><<<rows_grid(W, g.n_be, 256), 256, 0, e->stream>>>(
+            e->d_be, g.n_be, W, word_begin, t3, e->d_buf);
+        ++e->launches;
+    }
+    for (size_t l = 0; l + 1 < e->layer_offsets.size(); ++l) {
+        const uint32_t n = e->layer_offsets[l + 1] - e->layer_offsets[l];
+        if (n == 0) continue;
+        mcg::dev::k_layer_gates<<<rows_grid(W, n, 256), 256, 0, e->stream>>>(
+            e->d_meta, e->d_inputs, e->d_layer_gates + e->layer_offsets[l], n, g.n_be, W, e->d_buf);
+        ++e->launches;
+    }
+    MCG_CUDA(cudaGetLastError());
+    return MCG_OK;
+}
+
+mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
+    cudaDeviceProp prop;
+    MCG_CUDA(cudaGetDeviceProperties(&prop, e->device));
+    if (run.block_threads != 0 && run.block_threads != kFusedThreads)
+        return mcg::fail(MCG_ERR_INVALID, "block_threads must be 0 or 256");
+    e->nt = kFusedThreads;
+    const uint32_t ctas_per_sm = run.ctas_per_sm ? run.ctas_per_sm : 2u;
+    const size_t smem_cap = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / ctas_per_sm) -
+                            1024;  // per-CTA reserve
+    const uint64_t n_tally = e->graph.tally_nodes.size();
+    size_t tally_bytes = n_tally * sizeof(unsigned long long);
+    e->tally_in_smem = tally_bytes <= smem_cap / 2;
+    if (!e->tally_in_smem) tally_bytes = 0;
+    const size_t slot_bytes = (size_t)e->nt * sizeof(uint64_t);
+    uint32_t budget = (uint32_t)((smem_cap - tally_bytes) / slot_bytes);
+    if (run.smem_slots == MCG_SMEM_SLOTS_NONE) budget = 0;
+    else if (run.smem_slots) budget = std::min(budget, run.smem_slots);
+    const std::string err = mcg::compile_program(e->graph, budget, e->prog);
+    if (!err.empty()) return mcg::fail(MCG_ERR_INVALID, err);
+    e->smem_bytes = (uint32_t)(e->prog.smem_slots * slot_bytes + tally_bytes);
+    e->grid = (uint32_t)prop.multiProcessorCount * ctas_per_sm;
+    e->scratch_stride = (uint64_t)e->grid * e->nt;
+    e->chunk_words = run.chunk_words ? run.chunk_words : kDefaultChunkWords;
+
+    auto kern = mcg::dev::k_fused<kFusedThreads, kMulForm, kPackForm>;
+    MCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<uint32_t>(e->smem_bytes, 1)));
+    MCG_CUDA(upload(reinterpret_cast<mcg::Op **>(&e->d_ops), e->prog.ops));
+    if (e->prog.global_slots) {
+        MCG_CUDA(cudaMalloc((void **)&e->d_scratch, (size_t)e->prog.global_slots * e->scratch_stride * sizeof(uint64_t)));
+    }
+    return MCG_OK;
+}
+
+mcg_status launch_fused(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t word_begin, uint64_t count) {
+    mcg::dev::FusedArgs a;
+    a.ops = e->d_ops;
+    a.smem_slots = e->prog.smem_slots;
+    a.scratch = e->d_scratch;
+    a.scratch_stride = e->scratch_stride;
+    a.tally = e->d_tally;
+    a.n_tally = (uint32_t)e->graph.tally_nodes.size();
+    a.tally_in_smem = e->tally_in_smem ? 1u : 0u;
+    a.iteration_first = it_first;
+    a.n_iterations = n_it;
+    a.word_begin = word_begin;
+    a.word_count = count;
+    const uint64_t want = (count + e->nt - 1) / e->nt;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(e->grid, std::max<uint64_t>(want, 1));
+    mcg::dev::k_fused<kFusedThreads, kMulForm, kPackForm><<<grid, e->nt, e->smem_bytes, e->stream>>>(a);
+    ++e->launches;
+    MCG_CUDA(cudaGetLastError());
+    return MCG_OK;
+}
+
+void release(mcg_engine *e) {
+    cudaFree(e->d_ops);
+    cudaFree(e->d_scratch);
+    cudaFree(e->d_tally);
+    cudaFree(e->d_be);
+    cudaFree(e->d_meta);
+    cudaFree(e->d_inputs);
+    cudaFree(e->d_tally_nodes);
+    cudaFree(e->d_layer_gates);
+    cudaFree(e->d_buf);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, mcg_engine **out) {
+    mcg::clear_error();
+    if (!graph || !out) return mcg::fail(MCG_ERR_INVALID, "graph and out must not be NULL");
+    *out = nullptr;
+    mcg_run_desc run{};
+    if (run_in) run = *run_in;
+    if (run.mode > MCG_MODE_LAYERED) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
+    auto *e = new (std::nothrow) mcg_engine();
+    if (!e) return mcg::fail(MCG_ERR_OOM, "host allocation failed");
+    const std::string err = mcg::Graph::from_desc(*graph, e->graph);
+    if (!err.empty()) {
+        delete e;
+        return mcg::fail(MCG_ERR_INVALID, err);
+    }
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+        cudaGetLastError();
+        delete e;
+        return mcg::fail(MCG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (run.device < 0 || run.device >= n_dev) {
+        delete e;
+        return mcg::fail(MCG_ERR_INVALID, "device ordinal out of range");
+    }
+    e->device = run.device;
+    e->mode = run.mode;
+    e->layered_max_words = run.layered_max_words;
+    mcg_status st = MCG_OK;
+    do {
+        if (cudaSetDevice(e->device) != cudaSuccess) {
+            st = mcg::fail(MCG_ERR_CUDA, "cudaSetDevice failed");
+            break;
+        }
+        if (run.stream) {
+            e->stream = (cudaStream_t)run.stream;
+        } else {
+            if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+                st = mcg::fail(MCG_ERR_CUDA, "cudaStreamCreate failed");
+                break;
+            }
+            e->own_stream = true;
+        }
+        const size_t nt = std::max<size_t>(e->graph.tally_nodes.size(), 1);
+        if (cudaMalloc((void **)&e->d_tally, nt * sizeof(unsigned long long)) != cudaSuccess ||
+            cudaMemset(e->d_tally, 0, nt * sizeof(unsigned long long)) != cudaSuccess) {
+            st = mcg::fail(MCG_ERR_OOM, "tally allocation failed");
+            break;
+        }
+        st = build_layered_tables(e);
+        if (st != MCG_OK) break;
+        st = setup_fused(e, run);
+    } while (false);
+    if (st != MCG_OK) {
+        release(e);
+        delete e;
+        return st;
+    }
+    *out = e;
+    return MCG_OK;
+}
+
+mcg_status mcg_destroy(mcg_engine *e) {
+    mcg::clear_error();
+    if (!e) return MCG_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    release(e);
+    delete e;
+    return MCG_OK;
+}
+
+mcg_status mcg_run(mcg_engine *e, uint32_t iteration_first, uint32_t n_iterations, uint64_t word_begin,
+                   uint64_t word_count) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    if (word_begin + word_count > (1ull << 32) || word_begin + word_count < word_begin)
+        return mcg::fail(MCG_ERR_INVALID, "word range exceeds the 32-bit sample counter");
+    if ((uint64_t)iteration_first + n_iterations + 1 >= (1ull << 26))
+        return mcg::fail(MCG_ERR_INVALID, "iteration exceeds the 26-bit pass counter field");
+    if (n_iterations == 0 || word_count == 0) return MCG_OK;
+    MCG_CUDA(cudaSetDevice(e->device));
+    if (e->mode == MCG_MODE_FUSED) {
+        for (uint64_t off = 0; off < word_count; off += e->chunk_words) {
+            const uint64_t n = std::min<uint64_t>(e->chunk_words, word_count - off);
+            const mcg_status st = launch_fused(e, iteration_first, n_iterations, word_begin + off, n);
+            if (st != MCG_OK) return st;
+        }
+    } else {
+        const uint64_t nn = std::max<uint64_t>(e->graph.n_nodes(), 1);
+        uint64_t W = e->layered_max_words ? e->layered_max_words : std::max<uint64_t>((8ull << 30) / (nn * 8), 1024);
+        W = std::min<uint64_t>(W, word_count);
+        const uint32_t n_tally = (uint32_t)e->graph.tally_nodes.size();
+        for (uint32_t it = 0; it < n_iterations; ++it) {
+            for (uint64_t off = 0; off < word_count; off += W) {
+                const uint64_t n = std::min<uint64_t>(W, word_count - off);
+                mcg_status st = layered_eval(e, iteration_first + it, word_begin + off, n);
+                if (st != MCG_OK) return st;
+                if (n_tally) {
+                    const uint32_t bx = (uint32_t)std::min<uint64_t>((n + 255) / 256, 64);
+                    dim3 grid = rows_grid(1, n_tally, 256);
+                    grid.x = bx;
+                    mcg::dev::k_layer_tally<<<grid, 256, 0, e->stream>>>(e->d_tally_nodes, n_tally, n, e->d_buf,
+                                                                         e->d_tally);
+                    ++e->launches;
+                    MCG_CUDA(cudaGetLastError());
+                }
+            }
+        }
+    }
+    e->total_bits += (uint64_t)n_iterations * word_count * 64ull;
+    return MCG_OK;
+}
+
+mcg_status mcg_synchronize(mcg_engine *e) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    MCG_CUDA(cudaSetDevice(e->device));
+    MCG_CUDA(cudaStreamSynchronize(e->stream));
+    return MCG_OK;
+}
+
+mcg_status mcg_read_tallies(mcg_engine *e, uint64_t *ones, uint64_t *total_bits) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    MCG_CUDA(cudaSetDevice(e->device));
+    MCG_CUDA(cudaStreamSynchronize(e->stream));
+    if (ones && !e->graph.tally_nodes.empty()) {
+        MCG_CUDA(cudaMemcpy(ones, e->d_tally, e->graph.tally_nodes.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    }
+    if (total_bits) *total_bits = e->total_bits;
+    return MCG_OK;
+}
+
+mcg_status mcg_tally_device_ptr(mcg_engine *e, uint64_t **ones_dev) {
+    mcg::clear_error();
+    if (!e || !ones_dev) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    *ones_dev = reinterpret_cast<uint64_t *>(e->d_tally);
+    return MCG_OK;
+}
+
+mcg_status mcg_set_tallies(mcg_engine *e, const uint64_t *ones, uint64_t total_bits) {
+    mcg::clear_error();
+    if (!e || !ones) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    MCG_CUDA(cudaSetDevice(e->device));
+    MCG_CUDA(cudaStreamSynchronize(e->stream));
+    if (!e->graph.tally_nodes.empty())
+        MCG_CUDA(cudaMemcpy(e->d_tally, ones, e->graph.tally_nodes.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    e->total_bits = total_bits;
+    return MCG_OK;
+}
+
+mcg_status mcg_reset_tallies(mcg_engine *e) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    MCG_CUDA(cudaSetDevice(e->device));
+    MCG_CUDA(cudaMemsetAsync(e->d_tally, 0, std::max<size_t>(e->graph.tally_nodes.size(), 1) * sizeof(uint64_t),
+                             e->stream));
+    e->total_bits = 0;
+    return MCG_OK;
+}
+
+mcg_status mcg_dump_words(mcg_engine *e, uint32_t iteration, uint64_t word_begin, uint64_t n_words, uint64_t *out) {
+    mcg::clear_error();
+    if (!e || !out) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    if (word_begin + n_words > (1ull << 32)) return mcg::fail(MCG_ERR_INVALID, "word range exceeds the sample counter");
+    if (n_words == 0) return MCG_OK;
+    MCG_CUDA(cudaSetDevice(e->device));
+    mcg_status st = layered_eval(e, iteration, word_begin, n_words);
+    if (st != MCG_OK) return st;
+    MCG_CUDA(cudaStreamSynchronize(e->stream));
+    MCG_CUDA(cudaMemcpy(out, e->d_buf, (size_t)e->graph.n_nodes() * n_words * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    return MCG_OK;
+}
+
+mcg_status mcg_program_info_get(mcg_engine *e, mcg_program_info *info) {
+    mcg::clear_error();
+    if (!e || !info) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    info->n_ops = e->prog.ops.size();
+    info->smem_slots = e->prog.smem_slots;
+    info->global_slots = e->prog.global_slots;
+    info->max_live = e->prog.max_live;
+    info->block_threads = e->nt;
+    info->grid_ctas = e->grid;
+    info->scratch_bytes = (uint64_t)e->prog.global_slots * e->scratch_stride * sizeof(uint64_t);
+    info->smem_bytes = e->smem_bytes;
+    info->n_inline_be = e->prog.n_inline_be;
+    return MCG_OK;
+}
+
+mcg_status mcg_launch_count(mcg_engine *e, uint64_t *launches) {
+    mcg::clear_error();
+    if (!e || !launches) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    *launches = e->launches;
+    return MCG_OK;
+}
+
+mcg_status mcg_time_runs(mcg_engine *e, uint32_t iteration_first, uint64_t word_begin, uint64_t word_count,
+                         uint32_t repeats, double *ms_per_run) {
+    mcg::clear_error();
+    if (!e || !ms_per_run || repeats == 0) return mcg::fail(MCG_ERR_INVALID, "bad argument");
+    MCG_CUDA(cudaSetDevice(e->device));
+    cudaEvent_t a, b;
+    MCG_CUDA(cudaEventCreate(&a));
+    MCG_CUDA(cudaEventCreate(&b));
+    MCG_CUDA(cudaEventRecord(a, e->stream));
+    for (uint32_t r = 0; r < repeats; ++r) {
+        const mcg_status st = mcg_run(e, iteration_first + r, 1, word_begin, word_count);
+        if (st != MCG_OK) {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            return st;
+        }
+    }
+    MCG_CUDA(cudaEventRecord(b, e->stream));
+    MCG_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    MCG_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms_per_run = (double)ms / repeats;
+    return MCG_OK;
+}
+
+mcg_status mcg_sampler_peak(int32_t device, uint64_t n_events, uint64_t n_words, uint32_t repeats,
+                            double *words_per_second) {
+    mcg::clear_error();
+    if (!words_per_second || n_events == 0 || n_words == 0 || repeats == 0 || n_events > 0xFFFFFFFFull ||
+        n_words > 0xFFFFFFFFull)
+        return mcg::fail(MCG_ERR_INVALID, "bad argument");
+    MCG_CUDA(cudaSetDevice(device));
+    uint64_t *sink = nullptr;
+    MCG_CUDA(cudaMalloc((void **)&sink, n_words * sizeof(uint64_t)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const uint32_t blocks = (uint32_t)((n_words + 255) / 256);
+    // warm-up
+    mcg::dev::k_sampler_peak<kMulForm, kPackForm><<<blocks, 256>>>((uint32_t)n_events, n_words, 2u << 6, sink);
+    cudaEventRecord(a);
+    for (uint32_t r = 0; r < repeats; ++r)
+        mcg::dev::k_sampler_peak<kMulForm, kPackForm><<<blocks, 256>>>((uint32_t)n_events, n_words, (r + 2u) << 6, sink);
+    cudaEventRecord(b);
+    cudaError_t err = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (err != cudaSuccess) return mcg::fail(MCG_ERR_CUDA, cudaGetErrorString(err));
+    *words_per_second = (double)n_events * (double)n_words * repeats / (ms * 1e-3);
+    return MCG_OK;
+}
+
+const char *mcg_version(void) { return "mcg 0.1 (sm_100a)"; }
+
+}  // extern "C"

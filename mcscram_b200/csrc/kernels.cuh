@@ -1,0 +1,270 @@
+// kernels.cuh -- sm_100a kernels of the Monte Carlo engine.
+//
+//  k_fused       persistent interpreter: each thread owns one sample word per
+//                slab and walks the compiled node program (program_format.h):
+//                Philox sampling in registers, gates in an accumulator,
+//                shared-memory value slots, popcount tallies reduced per warp
+//                into shared-memory counters and flushed once per CTA.
+//  k_layer_be    reference dataflow, basic events: one word per thread
+//                (src/mc/kernel/basic_event.h:125-142)
+//  k_layer_gates reference dataflow, one layer of gates
+//                (src/mc/kernel/gate.h:299-362, ATLEAST 506-555)
+//  k_layer_tally reference dataflow, tallies (src/mc/kernel/tally.h:322-361)
+//  k_sampler_peak register-only sampler: the fused kernel's speed of light.
+#pragma once
+#include <cstdint>
+
+#include "mcg.h"
+#include "philox.cuh"
+#include "program_format.h"
+
+namespace mcg {
+namespace dev {
+
+constexpr uint64_t kAllOnes = ~0ull;
+
+// Bit-sliced 8-bit counters (mod 256, like the reference's uint8 count).
+struct SlicedCount {
+    uint64_t c[8];
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int b = 0; b < 8; ++b) c[b] = 0;
+    }
+    __device__ __forceinline__ void add(uint64_t v, uint32_t nbits) {
+        uint64_t carry = v;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            if ((uint32_t)b < nbits) {
+                const uint64_t t = c[b] & carry;
+                c[b] ^= carry;
+                carry = t;
+            }
+        }
+    }
+    // Per-lane (count >= k) for an 8-bit k.
+    __device__ __forceinline__ uint64_t ge(uint32_t k) const {
+        uint64_t gt = 0, eq = kAllOnes;
+#pragma unroll
+        for (int b = 7; b >= 0; --b) {
+            if ((k >> b) & 1u) {
+                eq &= c[b];
+            } else {
+                gt |= eq & c[b];
+                eq &= ~c[b];
+            }
+        }
+        return gt | eq;
+    }
+};
+
+__device__ __forceinline__ uint64_t load_slot(uint32_t ref, const uint64_t *my_slots, const uint64_t *my_scratch,
+                                              uint32_t nt, uint64_t stride) {
+    if (ref & kSlotGlobal) return my_scratch[(uint64_t)(ref & kSlotIndexMask) * stride];
+    return my_slots[(uint32_t)ref * nt];
+}
+
+__device__ __forceinline__ void store_slot(uint32_t ref, uint64_t v, uint64_t *my_slots, uint64_t *my_scratch,
+                                           uint32_t nt, uint64_t stride) {
+    if (ref == kNoSlot) return;
+    if (ref & kSlotGlobal) my_scratch[(uint64_t)(ref & kSlotIndexMask) * stride] = v;
+    else my_slots[(uint32_t)ref * nt] = v;
+}
+
+struct FusedArgs {
+    const uint4 *ops;
+    uint32_t smem_slots;
+    uint64_t *scratch;        // [global_slots][grid * NT]
+    uint64_t scratch_stride;  // grid * NT of the allocation
+    unsigned long long *tally;
+    uint32_t n_tally;
+    uint32_t tally_in_smem;
+    uint32_t iteration_first;
+    uint32_t n_iterations;
+    uint64_t word_begin;
+    uint64_t word_count;
+};
+
+template <int NT, int MF, int PF>
+__global__ void __launch_bounds__(NT, 2) k_fused(FusedArgs a) {
+    extern __shared__ __align__(16) uint64_t smem[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    unsigned long long *s_tally = reinterpret_cast<unsigned long long *>(smem + (size_t)a.smem_slots * NT);
+    if (a.tally_in_smem) {
+        for (uint32_t i = tid; i < a.n_tally; i += NT) s_tally[i] = 0ull;
+        __syncthreads();
+    }
+    unsigned long long *tally = a.tally_in_smem ? s_tally : a.tally;
+    const uint64_t gtid = (uint64_t)blockIdx.x * NT + tid;
+    const uint64_t total_threads = (uint64_t)gridDim.x * NT;
+    uint64_t *my_slots = smem + tid;
+    uint64_t *my_scratch = a.scratch + gtid;
+
+    for (uint32_t it = 0; it < a.n_iterations; ++it) {
+        const uint32_t t3 = (a.iteration_first + it + 1u) << 6;
+        for (uint64_t base = 0; base < a.word_count; base += total_threads) {
+            const uint64_t j = base + gtid;
+            const bool valid = j < a.word_count;
+            const WordCtx ctx = make_word_ctx<MF>((uint32_t)(a.word_begin + j));
+            uint64_t acc = 0, last = 0;
+            uint32_t conn = 0, kk = 0, nbits = 0;
+            SlicedCount cnt;
+            cnt.clear();
+            const uint4 *p = a.ops;
+            uint4 op = __ldg(p);
+            while (true) {
+                const uint4 nxt = __ldg(p + 1);
+                const uint32_t code = op.x & kOpMask;
+                if (code == kOpHalt) break;
+                // Value of the op: one sampler call site keeps the unrolled
+                // Philox body in the instruction cache once.
+                uint64_t v = 0;
+                if (code == kOpInBe || code == kOpBeDef) {
+                    v = be_word<MF, PF>(op.y, op.w, ctx, t3, op.z);
+                } else if (code == kOpInSlot) {
+                    v = load_slot(op.y, my_slots, my_scratch, NT, a.scratch_stride);
+                } else if (code == kOpInConst || code == kOpConstDef) {
+                    v = ((uint64_t)op.z << 32) | op.y;
+                }
+                if (code == kOpInBe || code == kOpInSlot || code == kOpInConst) {
+                    if (op.x & kNegBit) v = ~v;
+                    switch (conn) {
+                        case MCG_AND: case MCG_NAND: acc &= v; break;
+                        case MCG_OR: case MCG_NOR: acc |= v; break;
+                        case MCG_XOR: acc ^= v; break;
+                        case MCG_ATLEAST: cnt.add(v, nbits); break;
+                        default: acc = v; break;  // NOT, NULL: the last input wins
+                    }
+                } else if (code == kOpBeDef || code == kOpConstDef) {
+                    last = v;
+                    store_slot(op.x >> 8, last, my_slots, my_scratch, NT, a.scratch_stride);
+                } else if (code == kOpBegin) {
+                    conn = (op.x >> 8) & 0xFFu;
+                    kk = (op.x >> 16) & 0xFFu;
+                    nbits = (op.x >> 24) & 0xFu;
+                    acc = (conn == MCG_AND || conn == MCG_NAND) ? kAllOnes : 0ull;
+                    if (conn == MCG_ATLEAST) cnt.clear();
+                } else if (code == kOpEnd) {
+                    if (conn == MCG_ATLEAST) last = cnt.ge(kk);
+                    else if (conn == MCG_NAND || conn == MCG_NOR || conn == MCG_NOT) last = ~acc;
+                    else last = acc;
+                    store_slot(op.y, last, my_slots, my_scratch, NT, a.scratch_stride);
+                } else if (code == kOpTally) {
+                    uint32_t c = valid ? (uint32_t)__popcll(last) : 0u;
+                    c = __reduce_add_sync(0xFFFFFFFFu, c);
+                    if (lane == 0) atomicAdd(&tally[op.y], (unsigned long long)c);
+                }
+                op = nxt;
+                ++p;
+            }
+        }
+    }
+    if (a.tally_in_smem) {
+        __syncthreads();
+        for (uint32_t i = tid; i < a.n_tally; i += NT) {
+            const unsigned long long c = s_tally[i];
+            if (c) atomicAdd(&a.tally[i], c);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Reference dataflow (layered).  Node words live in buf[node * W + w].
+
+// Basic events: be[e] = {pdag_idx+1, event_idx+1, thr_lo, thr_hi}.
+template <int MF, int PF>
+__global__ void __launch_bounds__(256) k_layer_be(const uint4 *__restrict__ be, uint32_t n_be, uint64_t W,
+                                                  uint64_t word_begin, uint32_t t3, uint64_t *__restrict__ buf) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e = blockIdx.y + gridDim.y * blockIdx.z;
+    if (w >= W || e >= n_be) return;
+    const uint4 r = be[e];
+    const uint64_t thr = ((uint64_t)r.w << 32) | r.z;
+    uint64_t v;
+    if (thr == 0) v = 0;
+    else if (thr >= (1ull << 32)) v = kAllOnes;
+    else v = be_word<MF, PF>(r.x, r.y, make_word_ctx<MF>((uint32_t)(word_begin + w)), t3, (uint32_t)thr);
+    buf[(uint64_t)e * W + w] = v;
+}
+
+// One layer of gates; gate ids listed in layer_gates.  meta[g] = {op | k<<8, in_begin, in_count, neg_count}.
+// ATLEAST counts each bit lane with a uint8 counter, as the reference kernel does.
+__global__ void __launch_bounds__(256) k_layer_gates(const uint4 *__restrict__ meta, const uint32_t *__restrict__ inputs,
+                                                     const uint32_t *__restrict__ layer_gates, uint32_t n_layer,
+                                                     uint32_t n_be, uint64_t W, uint64_t *__restrict__ buf) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t li = blockIdx.y + gridDim.y * blockIdx.z;
+    if (w >= W || li >= n_layer) return;
+    const uint32_t gi = layer_gates[li];
+    const uint4 m = meta[gi];
+    const uint32_t op = m.x & 0xFFu;
+    const uint32_t n = m.z;
+    const uint32_t off = n - m.w;
+    const uint32_t *in = inputs + m.y;
+    uint64_t r;
+    if (op == MCG_ATLEAST) {
+        const uint8_t k = (uint8_t)(m.x >> 8);
+        r = 0;
+        for (uint32_t lane = 0; lane < 64; ++lane) {
+            const uint64_t mask = 1ull << lane;
+            uint8_t cnt = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                const uint64_t v = buf[(uint64_t)in[i] * W + w];
+                cnt += (uint8_t)((((i < off) ? v : ~v) & mask) ? 1 : 0);
+            }
+            if (cnt >= k) r |= mask;
+        }
+    } else {
+        r = (op == MCG_AND || op == MCG_NAND) ? kAllOnes : 0ull;
+        for (uint32_t i = 0; i < n; ++i) {
+            uint64_t v = buf[(uint64_t)in[i] * W + w];
+            if (i >= off) v = ~v;
+            if (op == MCG_OR || op == MCG_NOR) r |= v;
+            else if (op == MCG_AND || op == MCG_NAND) r &= v;
+            else if (op == MCG_XOR) r ^= v;
+            else r = v;
+        }
+        if (op == MCG_NAND || op == MCG_NOR || op == MCG_NOT) r = ~r;
+    }
+    buf[(uint64_t)(n_be + gi) * W + w] = r;
+}
+
+// Tallies: popcount, block reduction, one atomic per block and node.
+__global__ void __launch_bounds__(256) k_layer_tally(const uint32_t *__restrict__ tally_nodes, uint32_t n_tally,
+                                                     uint64_t W, const uint64_t *__restrict__ buf,
+                                                     unsigned long long *__restrict__ ones) {
+    __shared__ uint32_t warp_sums[8];
+    const uint32_t t = blockIdx.y + gridDim.y * blockIdx.z;
+    if (t >= n_tally) return;
+    uint32_t c = 0;
+    const uint64_t *row = buf + (uint64_t)tally_nodes[t] * W;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < W; w += (uint64_t)gridDim.x * blockDim.x)
+        c += (uint32_t)__popcll(row[w]);
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31u) == 0) warp_sums[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) s += warp_sums[i];
+        if (s) atomicAdd(&ones[t], s);
+    }
+}
+
+// Register-only sampler: thread w generates words (e, w) for n_events events
+// and xors them together; one store per thread keeps the work alive.
+template <int MF, int PF>
+__global__ void __launch_bounds__(256) k_sampler_peak(uint32_t n_events, uint64_t n_words, uint32_t t3,
+                                                      uint64_t *__restrict__ sink) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_words) return;
+    const WordCtx ctx = make_word_ctx<MF>((uint32_t)w);
+    uint64_t x = 0;
+    for (uint32_t e = 0; e < n_events; ++e) {
+        const uint32_t thr = 0x01000000u + (e * 0x9E3779B9u >> 8);  // spread of probabilities
+        x ^= be_word<MF, PF>(e + 3u, e + 1u, ctx, t3, thr);
+    }
+    sink[w] = x;
+}
+
+}  // namespace dev
+}  // namespace mcg

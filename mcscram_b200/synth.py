@@ -1,0 +1,327 @@
+"""Seeded synthetic fault trees in the shapes of the benchmark configurations.
+
+The reference measures on the Aralia fault-tree set; synthetic trees with
+the benchmark's stated sizes, gate mixes and probability ranges stand in for
+it here.  The generator builds a single-top DAG bottom-up in depth layers:
+
+* gate layer sizes grow geometrically from the top (1 gate) downwards and
+  level off, so every gate at depth d >= 2 gets one input from depth d - 1
+  (fixing the number of layers) and every non-top gate has a parent;
+* every basic event is used; a chosen fraction of basic events (or of all
+  nodes) gets a second parent, which makes the graph a DAG;
+* AND/OR fan-in is drawn uniformly from its range and then nudged, one input
+  at a time and never outside the range, until the input slots match the
+  edges needed to cover every node and the requested sharing;
+* ATLEAST gates take n uniform in their range and k uniform in [2, n - 1];
+  XOR gates have two inputs, NOT gates one;
+* probabilities are log-uniform in the given range.
+
+The top gate is an OR gate.  Basic events get PDAG indices 2, 3, ...
+(core::Pdag::kVariableStartIndex, mcSCRAM src/pdag.h:804) and gates the
+indices after them.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+
+from .graph import AND, ATLEAST, NOT, OR, XOR, FlatGraph, probability_threshold
+
+
+@dataclass
+class TreeSpec:
+    n_be: int
+    n_gates: int
+    mix: Dict[int, float]                      # connective -> fraction of gates
+    p_range: Tuple[float, float]
+    seed: int
+    n_layers: Optional[int] = None
+    fanin: Tuple[int, int] = (2, 4)            # AND/OR fan-in range
+    atleast_n: Tuple[int, int] = (3, 8)
+    atleast_k_max_offset: int = 1              # k in [2, n - offset]
+    share_be_frac: float = 0.0                 # basic events given >= 2 parents
+    share_node_frac: float = 0.0               # nodes (events and gates) given >= 2 parents
+    name: str = "tree"
+    extra: dict = field(default_factory=dict)
+
+
+def _layer_sizes(n_gates: int, n_layers: int) -> np.ndarray:
+    """Sizes for depths 1..n_layers (index 0 = depth 1); top (last) is 1,
+    non-increasing with depth, growth at most x2 per layer."""
+    if n_layers < 1:
+        raise ValueError("n_layers must be >= 1")
+    if n_gates < n_layers:
+        raise ValueError("need at least one gate per layer")
+    # ramp[i] for depth n_layers - i
+    lo, hi = 1, n_gates
+    while lo < hi:  # smallest cap with sum(min(2^i, cap)) >= n_gates
+        cap = (lo + hi) // 2
+        s = sum(min(1 << min(i, 40), cap) for i in range(n_layers))
+        if s >= n_gates:
+            hi = cap
+        else:
+            lo = cap + 1
+    cap = lo
+    ramp = [min(1 << min(i, 40), cap) for i in range(n_layers)]
+    excess = sum(ramp) - n_gates
+    i = n_layers - 1
+    while excess > 0:  # trim the bottom layers, keep non-increasing towards the top
+        floor_i = ramp[i - 1] if i > 0 else 1
+        can = ramp[i] - floor_i
+        take = min(can, excess)
+        ramp[i] -= take
+        excess -= take
+        i -= 1
+        if i < 0:
+            i = n_layers - 1
+    deficit = n_gates - sum(ramp)  # only when 2^n_layers - 1 < n_gates
+    j = n_layers - 1
+    while deficit > 0:  # widen the bottom layers
+        ramp[j] += 1
+        deficit -= 1
+        j = j - 1 if j > max(0, n_layers - 3) else n_layers - 1
+    sizes = np.array(ramp[::-1], dtype=np.int64)  # depth 1 first
+    assert sizes.sum() == n_gates and sizes[-1] == 1
+    return sizes
+
+
+def _default_layers(n_gates: int, fanin_mean: float) -> int:
+    # depth of a balanced tree of n_gates gates with the mean fan-in, plus a margin
+    d = int(np.ceil(np.log(max(n_gates, 2)) / np.log(max(fanin_mean, 1.5)))) + 2
+    return max(2, min(d, n_gates))
+
+
+def generate(spec: TreeSpec) -> FlatGraph:
+    rng = np.random.default_rng(spec.seed)
+    G, B = spec.n_gates, spec.n_be
+    if G < 1 or B < 1:
+        raise ValueError("need at least one gate and one basic event")
+    L = spec.n_layers or _default_layers(G, (spec.fanin[0] + spec.fanin[1]) / 2)
+    sizes = _layer_sizes(G, L)
+    depth = np.repeat(np.arange(1, L + 1), sizes)  # gate j (topological) -> depth
+
+    # Connectives: the mix over all gates, top forced to OR.
+    kinds = []
+    for op, frac in sorted(spec.mix.items()):
+        kinds += [op] * int(round(frac * G))
+    while len(kinds) < G:
+        kinds.append(max(spec.mix, key=spec.mix.get))
+    kinds = np.array(kinds[:G], dtype=np.int64)
+    rng.shuffle(kinds)
+    top = G - 1
+    if kinds[top] != OR:
+        swap = np.nonzero(kinds == OR)[0]
+        if swap.size:
+            kinds[swap[0]] = kinds[top]
+        kinds[top] = OR
+    # NOT gates at depth >= 2 take their one input from depth - 1, which is fine;
+    # a NOT at depth 1 takes a basic event.
+
+    # Fan-in.
+    fanin = np.zeros(G, dtype=np.int64)
+    kvals = np.zeros(G, dtype=np.int64)
+    flexible = np.zeros(G, dtype=bool)
+    for j in range(G):
+        op = kinds[j]
+        if op in (AND, OR):
+            fanin[j] = rng.integers(spec.fanin[0], spec.fanin[1] + 1)
+            flexible[j] = True
+        elif op == ATLEAST:
+            n = int(rng.integers(spec.atleast_n[0], spec.atleast_n[1] + 1))
+            fanin[j] = n
+            kvals[j] = int(rng.integers(2, max(2, n - spec.atleast_k_max_offset) + 1))
+        elif op == XOR:
+            fanin[j] = 2
+        elif op == NOT:
+            fanin[j] = 1
+        else:
+            raise ValueError(f"unsupported connective {op} in generator")
+
+    # Which nodes get a second parent.
+    share_be = np.zeros(B, dtype=bool)
+    share_gate = np.zeros(G, dtype=bool)
+    if spec.share_node_frac > 0:
+        n_share = int(round(spec.share_node_frac * (B + G)))
+        pick = rng.choice(B + G - 1, size=min(n_share, B + G - 1), replace=False)  # top excluded
+        for x in pick:
+            if x < B:
+                share_be[x] = True
+            else:
+                share_gate[x - B] = True
+    if spec.share_be_frac > 0:
+        n_share = int(round(spec.share_be_frac * B))
+        share_be[rng.choice(B, size=n_share, replace=False)] = True
+    # gates sharing must have a possible second parent above them
+    share_gate[depth >= L - 1] = False
+    need_be = 1 + share_be.astype(np.int64)
+    need_gate = np.where(np.arange(G) == top, 0, 1 + share_gate.astype(np.int64))
+    demand = int(need_be.sum() + need_gate.sum())
+
+    # Match supply (sum of fan-in) to demand within the AND/OR ranges.
+    supply = int(fanin.sum())
+    flex_idx = np.nonzero(flexible)[0]
+    guard = 0
+    while supply != demand:
+        guard += 1
+        if guard > 50 * (G + B) or flex_idx.size == 0:
+            raise ValueError(f"cannot match fan-in supply {supply} to demand {demand} within ranges")
+        j = int(flex_idx[rng.integers(flex_idx.size)])
+        if supply < demand and fanin[j] < spec.fanin[1]:
+            fanin[j] += 1
+            supply += 1
+        elif supply > demand and fanin[j] > spec.fanin[0]:
+            fanin[j] -= 1
+            supply -= 1
+
+    children = [[] for _ in range(G)]
+    free = fanin.copy()
+    rem_gate = need_gate.copy()
+    by_depth = [np.nonzero(depth == d)[0] for d in range(L + 1)]
+
+    # A: depth edges, distinct children from the layer below.
+    for d in range(L, 1, -1):
+        parents = by_depth[d]
+        below = by_depth[d - 1].copy()
+        rng.shuffle(below)
+        for i, p in enumerate(parents):
+            c = int(below[i % below.size])
+            children[p].append(B + c)
+            free[p] -= 1
+            rem_gate[c] -= 1
+
+    # B: remaining gate requirements, the highest (most constrained) layers first.
+    above_cache = {}
+    widened = 0
+    for d in range(L - 1, 0, -1):
+        for c in by_depth[d]:
+            while rem_gate[c] > 0:
+                cand = above_cache.get(d)
+                if cand is None:
+                    cand = np.nonzero(depth > d)[0]
+                    above_cache[d] = cand
+                ok = cand[(free[cand] > 0)]
+                ok = np.array([p for p in ok if (B + c) not in children[p]], dtype=np.int64)
+                if ok.size == 0:
+                    # Widen an AND/OR gate above by one input and narrow another
+                    # AND/OR gate with a free slot, so the totals still match.
+                    grow = [p for p in cand if flexible[p] and (B + c) not in children[p]]
+                    shrink = [q for q in np.nonzero(flexible & (free > 0) & (fanin > spec.fanin[0]))[0]]
+                    if not grow or not shrink:
+                        raise ValueError("generator ran out of parent slots for gates; adjust layers/fan-in")
+                    p = int(grow[rng.integers(len(grow))])
+                    q = int(shrink[rng.integers(len(shrink))])
+                    fanin[p] += 1
+                    free[p] += 1
+                    fanin[q] -= 1
+                    free[q] -= 1
+                    widened += 1
+                    continue
+                w = free[ok].astype(np.float64)
+                p = int(rng.choice(ok, p=w / w.sum()))
+                children[p].append(B + int(c))
+                free[p] -= 1
+                rem_gate[c] -= 1
+
+    # C: basic events into the remaining slots.
+    be_req = np.repeat(np.arange(B), need_be)
+    rng.shuffle(be_req)
+    slots = np.repeat(np.arange(G), free)
+    rng.shuffle(slots)
+    if slots.size != be_req.size:
+        raise ValueError(f"slot/requirement mismatch {slots.size} vs {be_req.size}")
+    # assign avoiding duplicate children; repair collisions by swapping
+    assign = slots.copy()
+    child_sets = [set(ch) for ch in children]
+    pending = []
+    for i, e in enumerate(be_req):
+        p = int(assign[i])
+        if int(e) in child_sets[p]:
+            pending.append(i)
+        else:
+            child_sets[p].add(int(e))
+    for i in pending:
+        e = int(be_req[i])
+        placed = False
+        for _ in range(200):
+            k = int(rng.integers(be_req.size))
+            if k == i:
+                continue
+            p, q = int(assign[i]), int(assign[k])
+            ek = int(be_req[k])
+            # swap parents of i and k if both stay duplicate-free
+            if e not in child_sets[q] and (ek == e or ek not in child_sets[p]) and k not in pending:
+                child_sets[q].discard(ek)
+                child_sets[q].add(e)
+                child_sets[p].add(ek)
+                assign[i], assign[k] = q, p
+                placed = True
+                break
+        if not placed:
+            raise ValueError("could not place a basic event without duplicate inputs")
+    for i, e in enumerate(be_req):
+        children[int(assign[i])].append(int(e))
+
+    # Flatten.
+    inputs, in_begin, in_count = [], [], []
+    for j in range(G):
+        ch = sorted(children[j], key=lambda x: (x < B, x))  # gate inputs first, then events
+        in_begin.append(len(inputs))
+        in_count.append(len(ch))
+        inputs.extend(ch)
+    lo, hi = spec.p_range
+    p = np.exp(rng.uniform(np.log(lo), np.log(hi), size=B))
+    fg = FlatGraph(
+        be_pdag_idx=np.arange(B, dtype=np.int32) + 2,
+        be_event_idx=np.arange(B, dtype=np.uint32),
+        be_threshold=probability_threshold(p),
+        gate_op=kinds.astype(np.uint8),
+        gate_k=kvals.astype(np.uint32),
+        gate_in_begin=np.array(in_begin, dtype=np.uint32),
+        gate_in_count=np.array(in_count, dtype=np.uint32),
+        gate_neg_count=np.zeros(G, dtype=np.uint32),
+        inputs=np.array(inputs, dtype=np.uint32),
+        tally_nodes=np.arange(B, B + G, dtype=np.uint32),
+        gate_pdag_idx=np.arange(G, dtype=np.int32) + 2 + B,
+        be_prob=p,
+        root=B + G - 1,
+        name=spec.name,
+        meta={"seed": spec.seed, "n_layers": L, "fanin_widened": widened},
+    )
+    fg.validate()
+    return fg
+
+
+# --- benchmark configurations ------------------------------------------------
+
+def config1(seed: int = 372) -> FlatGraph:
+    """200 basic events, 100 gates (50/50 AND/OR), fan-in 2-4, 20% of events
+    shared by >= 2 gates, p log-uniform in [1e-3, 1e-1]."""
+    return generate(TreeSpec(n_be=200, n_gates=100, mix={AND: 0.5, OR: 0.5}, p_range=(1e-3, 1e-1), seed=seed,
+                             n_layers=7, share_be_frac=0.2, name="config1-200be-100g"))
+
+
+def config2(seed: int = 11) -> FlatGraph:
+    """5,000 basic events, 3,000 gates (45% AND, 40% OR, 10% ATLEAST k-of-n with
+    n in 3-8, k in [2, n-1], 5% NOT/XOR), 20 layers, 30% of nodes with fan-out
+    >= 2, p log-uniform in [1e-5, 1e-2]."""
+    return generate(TreeSpec(n_be=5000, n_gates=3000, mix={AND: 0.45, OR: 0.40, ATLEAST: 0.10, NOT: 0.025, XOR: 0.025},
+                             p_range=(1e-5, 1e-2), seed=seed, n_layers=20, share_node_frac=0.30,
+                             name="config2-5000be-3000g"))
+
+
+def config4(seed: int = 4) -> FlatGraph:
+    """2,000 basic events, 1,200 gates (60% AND, 30% OR, 10% ATLEAST 2-of-3 ..
+    3-of-5), p log-uniform in [1e-6, 1e-3]."""
+    return generate(TreeSpec(n_be=2000, n_gates=1200, mix={AND: 0.6, OR: 0.3, ATLEAST: 0.1}, p_range=(1e-6, 1e-3),
+                             seed=seed, n_layers=12, atleast_n=(3, 5), share_be_frac=0.1,
+                             name="config4-2000be-1200g"))
+
+
+def small_tree(seed: int, n_be: int = 24, n_gates: int = 12, mix=None, p_range=(0.05, 0.5), n_layers=4,
+               share_node_frac: float = 0.2, atleast_n=(3, 5)) -> FlatGraph:
+    """A small random DAG with every connective the generator knows, for tests."""
+    mix = mix or {AND: 0.3, OR: 0.3, ATLEAST: 0.2, XOR: 0.1, NOT: 0.1}
+    return generate(TreeSpec(n_be=n_be, n_gates=n_gates, mix=mix, p_range=p_range, seed=seed, n_layers=n_layers,
+                             share_node_frac=share_node_frac, atleast_n=atleast_n, name=f"small-{seed}"))

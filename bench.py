@@ -47,6 +47,10 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="fused kernel CTAs per SM (0 = engine default)")
+    ap.add_argument("--peak-words", type=int, default=1 << 22, help="words per register-only sampler launch")
+    ap.add_argument("--mode", default="staged", choices=["fused", "staged", "layered"])
+    ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")
     return ap.parse_args()
 
 
@@ -180,9 +184,10 @@ def run_reference(args, rank: int, world: int):
 
 # ----------------------------------------------------------------------------- GPU arm
 
-def traffic_from_profile():
-    """DRAM bytes per fused launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "k_fused_config2.txt"
+def traffic_from_profile(kernel: str):
+    """DRAM bytes per launch of `kernel` at the bench's launch size, from the
+    committed ncu summary (profiles/<kernel>_config2.txt), if present."""
+    p = ROOT / "profiles" / f"{kernel}_config2.txt"
     if not p.exists():
         return None
     for ln in p.read_text().splitlines():
@@ -217,8 +222,12 @@ def main() -> int:
     word_begin = rank * W
     if word_begin + W > (1 << 32):
         raise SystemExit("word range exceeds the 32-bit sample counter")
-    stream = torch.cuda.current_stream()
-    eng = _capi.Engine(g, device=local, stream=stream.cuda_stream)
+    # one dedicated stream for the engine and for every torch op and event here
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng_kw = dict(device=local, stream=stream.cuda_stream, ctas_per_sm=args.ctas_per_sm, mode=_capi.MODES[args.mode],
+                  layered_max_words=args.chunk_words)
+    eng = _capi.Engine(g, **eng_kw)
     info = eng.program_info()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
@@ -236,6 +245,8 @@ def main() -> int:
         allreduce_tallies()
     torch.cuda.synchronize()
     eng.reset_tallies()
+    if args.mode == "staged":
+        eng.profile_sampler(True)  # events around every sampler-phase launch
     launches0 = eng.launch_count()
     if world > 1:
         dist.barrier()
@@ -269,14 +280,23 @@ def main() -> int:
     value = g.n_gates * samples / (ms_per_step * 1e-3)
     be_words_per_s = g.n_be * W * world / (ms_per_step * 1e-3)
 
-    # roofline of the fused kernel: basic-event words per launch / launch time,
-    # against the register-only sampler measured on this GPU in this run
-    launches_per_step = max(launches // max(args.steps, 1), 1)
-    avg_launch_s = run_ms * 1e-3 / (args.steps * launches_per_step)
-    be_words_per_launch = g.n_be * W / launches_per_step
+    # Roofline of the dominant kernel: basic-event words per launch / its mean
+    # launch duration (CUDA events on its own stream), against the
+    # register-only sampler measured on this GPU in this run.
+    if args.mode == "staged":
+        kernel = "k_stage_be"
+        n_a, ms_a = eng.profile_sampler_read()
+        eng.profile_sampler(False)
+        kernel_launches = max(n_a, 1)
+        avg_launch_s = ms_a * 1e-3 / kernel_launches
+    else:
+        kernel = "k_fused" if args.mode == "fused" else "k_layer_be"
+        kernel_launches = max(launches, 1) if args.mode == "fused" else args.steps
+        avg_launch_s = run_ms * 1e-3 / kernel_launches
+    be_words_per_launch = g.n_be * W * args.steps / kernel_launches
     achieved = be_words_per_launch / avg_launch_s
-    peak = _capi.sampler_peak(n_events=256, n_words=1 << 22, repeats=3, device=local)
-    traffic = traffic_from_profile()
+    peak = _capi.sampler_peak(n_events=256, n_words=args.peak_words, repeats=3, device=local)
+    traffic = traffic_from_profile(kernel)
 
     # end to end: host descriptor -> engine (tables to HBM) -> one pass -> tallies to host
     e2e = None
@@ -285,7 +305,7 @@ def main() -> int:
         for i in range(args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            with _capi.Engine(g, device=local, stream=stream.cuda_stream) as e2:
+            with _capi.Engine(g, **eng_kw) as e2:
                 e2.run(1, 1, word_begin, W)
                 ones, total = e2.tallies()
             ts.append(time.perf_counter() - t0)
@@ -314,12 +334,15 @@ def main() -> int:
             "config": {"workload": "plain MC pass, 5,000-event / 3,000-gate synthetic tree (seed 11)",
                        "samples_per_gpu": W * 64, "words_per_gpu": W, "n_be": g.n_be, "n_gates": g.n_gates,
                        "tallied_nodes": int(g.tally_nodes.size), "parallelism": f"word-range shards x{world}",
-                       "l2": "256 MB buffer written between steps", "mode": "fused"},
+                       "l2": "256 MB buffer written between steps", "mode": args.mode},
             "sample_words_per_s": be_words_per_s,
             "gpu_launches": int(launches),
-            "roofline": {"bound": "int-alu", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gword/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": "register-only Philox sampler kernel measured in this run"},
+            "roofline": {"bound": "int-alu", "kernel": kernel, "achieved": achieved / 1e9, "peak": peak / 1e9,
+                         "unit": "Gword/s", "frac": achieved / peak, "traffic": traffic,
+                         "launches": kernel_launches, "avg_launch_ms": avg_launch_s * 1e3,
+                         "peak_source": "register-only Philox sampler kernel (k_sampler_peak) measured in this run",
+                         "work_unit": "basic-event word = 16 Philox4x32-10 calls"},
+            "pipeline": {"be_words_per_s": be_words_per_s, "frac_of_peak": be_words_per_s / world / peak},
             "clocks": clk,
             "program": info,
         }

@@ -46,7 +46,10 @@ enum mcg_connective {
 /* Evaluation strategies for mcg_run. */
 enum mcg_mode {
     MCG_MODE_FUSED = 0,   /* one persistent kernel per launch chunk: sample, gates, tallies fused */
-    MCG_MODE_LAYERED = 1  /* reference dataflow: materialised node words, one launch per layer */
+    MCG_MODE_LAYERED = 1, /* reference dataflow: materialised node words, one launch per layer */
+    MCG_MODE_STAGED = 2   /* two-phase pipeline: a pure sampler kernel writes basic-event words to
+                             HBM, per-layer gate kernels with fused tallies read them; chunks are
+                             double buffered on two streams so the phases overlap */
 };
 
 /* Flattened PDAG handed to the engine.  All arrays are host memory, copied
@@ -83,7 +86,7 @@ typedef struct mcg_run_desc {
                                  MCG_SMEM_SLOTS_NONE = keep every value in global scratch */
     uint32_t ctas_per_sm;     /* fused kernel persistent CTAs per SM; 0 = auto */
     uint64_t chunk_words;     /* words per launch in one mcg_run; 0 = auto */
-    uint64_t layered_max_words; /* layered mode: words materialised per chunk; 0 = auto */
+    uint64_t layered_max_words; /* layered/staged modes: words materialised per chunk; 0 = auto */
 } mcg_run_desc;
 
 typedef struct mcg_engine mcg_engine;
@@ -164,6 +167,13 @@ mcg_status mcg_launch_count(mcg_engine *engine, uint64_t *launches);
  * are left accumulated. */
 mcg_status mcg_time_runs(mcg_engine *engine, uint32_t iteration_first, uint64_t word_begin,
                          uint64_t word_count, uint32_t repeats, double *ms_per_run);
+
+/* Staged mode: when enabled, every sampler-phase (k_stage_be) launch is
+ * bracketed by CUDA events on its stream; mcg_profile_sampler_read returns
+ * the number of timed launches since enabling and their summed duration.
+ * For measurement only (adds two event records per launch). */
+mcg_status mcg_profile_sampler(mcg_engine *engine, int32_t enable);
+mcg_status mcg_profile_sampler_read(mcg_engine *engine, uint64_t *launches, double *total_ms);
 
 /* Register-only sampler rate: basic-event words generated per second by a
  * kernel that only runs the Philox sampler (no memory traffic besides one

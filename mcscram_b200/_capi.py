@@ -26,6 +26,8 @@ MCG_ERR_NO_DEVICE = 6
 
 MODE_FUSED = 0
 MODE_LAYERED = 1
+MODE_STAGED = 2
+MODES = {"fused": MODE_FUSED, "layered": MODE_LAYERED, "staged": MODE_STAGED}
 
 _u32p = C.POINTER(C.c_uint32)
 _i32p = C.POINTER(C.c_int32)
@@ -106,6 +108,8 @@ _SIGNATURES = {
     "mcg_launch_count": (C.c_int, [C.c_void_p, _u64p]),
     "mcg_time_runs": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
     "mcg_sampler_peak": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
+    "mcg_profile_sampler": (C.c_int, [C.c_void_p, C.c_int32]),
+    "mcg_profile_sampler_read": (C.c_int, [C.c_void_p, _u64p, C.POINTER(C.c_double)]),
     "mcg_last_error": (C.c_char_p, []),
     "mcg_version": (C.c_char_p, []),
 }
@@ -260,6 +264,15 @@ class Engine:
         n = C.c_uint64()
         check(self.lib.mcg_launch_count(self.handle, C.byref(n)))
         return int(n.value)
+
+    def profile_sampler(self, enable: bool = True) -> None:
+        check(self.lib.mcg_profile_sampler(self.handle, 1 if enable else 0))
+
+    def profile_sampler_read(self):
+        n = C.c_uint64()
+        ms = C.c_double()
+        check(self.lib.mcg_profile_sampler_read(self.handle, C.byref(n), C.byref(ms)))
+        return int(n.value), float(ms.value)
 
     def time_runs(self, iteration_first: int, word_begin: int, word_count: int, repeats: int) -> float:
         ms = C.c_double()

@@ -23,8 +23,10 @@
 
 namespace {
 
-constexpr int kMulForm = 0;   // (uint64)a*b: IMAD.WIDE.U32
-constexpr int kPackForm = 0;  // compare-and-or nibbles
+// Sampler code form: separate high/low multiplies and the carry-chain bit
+// packing measured fastest of the four forms on B200 (register-only sampler).
+constexpr int kMulForm = 1;
+constexpr int kPackForm = 1;
 constexpr int kFusedThreads = 256;
 constexpr uint64_t kDefaultChunkWords = 1ull << 21;
 
@@ -61,6 +63,7 @@ struct mcg_engine {
     uint64_t *d_scratch = nullptr;
     uint64_t scratch_stride = 0;
     uint32_t nt = kFusedThreads;
+    uint32_t ctas_per_sm = 2;
     uint32_t grid = 0;
     uint32_t smem_bytes = 0;
     bool tally_in_smem = false;
@@ -80,6 +83,22 @@ struct mcg_engine {
     uint64_t *d_buf = nullptr;
     uint64_t buf_words = 0;
     uint64_t layered_max_words = 0;
+
+    // staged
+    uint4 *d_smeta = nullptr;           // gate meta with counter bits for the bit-sliced ATLEAST
+    uint2 *d_gate_tally = nullptr;      // per gate {offset, count} into d_gate_tally_list
+    uint32_t *d_gate_tally_list = nullptr;
+    uint32_t *d_be_tally_nodes = nullptr;  // tallied basic events
+    uint32_t *d_be_tally_idx = nullptr;
+    uint32_t n_be_tally = 0;
+    uint64_t *d_stage[2] = {nullptr, nullptr};
+    uint64_t stage_words = 0;           // words per chunk the stage buffers hold
+    cudaStream_t s_a = nullptr, s_b = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_a[2] = {nullptr, nullptr}, ev_b[2] = {nullptr, nullptr};
+    cudaEvent_t ev_join_a = nullptr, ev_join_b = nullptr;
+    bool profile_a = false;                   // time every sampler-phase launch
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+    size_t prof_used = 0;
 
     uint64_t launches = 0;
 };
@@ -116,6 +135,39 @@ mcg_status build_layered_tables(mcg_engine *e) {
     std::vector<uint32_t> cursor(e->layer_offsets.begin(), e->layer_offsets.end());
     std::vector<uint32_t> order(g.n_gates);
     for (uint32_t i = 0; i < g.n_gates; ++i) order[cursor[layer[i] - 1]++] = i;
+
+    // staged-mode tables
+    std::vector<uint4> smeta(g.n_gates);
+    for (uint32_t i = 0; i < g.n_gates; ++i) {
+        uint32_t nbits = 0;
+        while (nbits < 8 && (g.gate_in_count[i] >> nbits) != 0) ++nbits;
+        if (nbits == 0) nbits = 1;
+        smeta[i] = make_uint4((uint32_t)g.gate_op[i] | ((g.gate_k[i] & 0xFFu) << 8) | (nbits << 16),
+                              g.gate_in_begin[i], g.gate_in_count[i], g.gate_neg_count[i]);
+    }
+    std::vector<std::vector<uint32_t>> per_gate(g.n_gates);
+    std::vector<uint32_t> be_nodes, be_idx;
+    for (uint32_t t = 0; t < (uint32_t)g.tally_nodes.size(); ++t) {
+        const uint32_t v = g.tally_nodes[t];
+        if (v < g.n_be) {
+            be_nodes.push_back(v);
+            be_idx.push_back(t);
+        } else {
+            per_gate[v - g.n_be].push_back(t);
+        }
+    }
+    std::vector<uint2> gate_tally(g.n_gates);
+    std::vector<uint32_t> gate_tally_list;
+    for (uint32_t i = 0; i < g.n_gates; ++i) {
+        gate_tally[i] = make_uint2((uint32_t)gate_tally_list.size(), (uint32_t)per_gate[i].size());
+        gate_tally_list.insert(gate_tally_list.end(), per_gate[i].begin(), per_gate[i].end());
+    }
+    e->n_be_tally = (uint32_t)be_nodes.size();
+    MCG_CUDA(upload(&e->d_smeta, smeta));
+    MCG_CUDA(upload(&e->d_gate_tally, gate_tally));
+    MCG_CUDA(upload(&e->d_gate_tally_list, gate_tally_list));
+    MCG_CUDA(upload(&e->d_be_tally_nodes, be_nodes));
+    MCG_CUDA(upload(&e->d_be_tally_idx, be_idx));
 
     MCG_CUDA(upload(&e->d_be, be));
     MCG_CUDA(upload(&e->d_meta, meta));
@@ -164,6 +216,18 @@ mcg_status layered_eval(mcg_engine *e, uint32_t iteration, uint64_t word_begin, 
     return MCG_OK;
 }
 
+using FusedKernel = void (*)(mcg::dev::FusedArgs);
+
+// Register budget follows the CTAs wanted per SM (65536 / (256 * n) per thread).
+FusedKernel fused_kernel(uint32_t ctas_per_sm) {
+    switch (ctas_per_sm) {
+        case 1: return mcg::dev::k_fused<kFusedThreads, 1, kMulForm, kPackForm>;
+        case 3: return mcg::dev::k_fused<kFusedThreads, 3, kMulForm, kPackForm>;
+        case 4: return mcg::dev::k_fused<kFusedThreads, 4, kMulForm, kPackForm>;
+        default: return mcg::dev::k_fused<kFusedThreads, 2, kMulForm, kPackForm>;
+    }
+}
+
 mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
     cudaDeviceProp prop;
     MCG_CUDA(cudaGetDeviceProperties(&prop, e->device));
@@ -171,6 +235,8 @@ mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
         return mcg::fail(MCG_ERR_INVALID, "block_threads must be 0 or 256");
     e->nt = kFusedThreads;
     const uint32_t ctas_per_sm = run.ctas_per_sm ? run.ctas_per_sm : 2u;
+    if (ctas_per_sm < 1 || ctas_per_sm > 4) return mcg::fail(MCG_ERR_INVALID, "ctas_per_sm must be 1..4");
+    e->ctas_per_sm = ctas_per_sm;
     const size_t smem_cap = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / ctas_per_sm) -
                             1024;  // per-CTA reserve
     const uint64_t n_tally = e->graph.tally_nodes.size();
@@ -188,12 +254,111 @@ mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
     e->scratch_stride = (uint64_t)e->grid * e->nt;
     e->chunk_words = run.chunk_words ? run.chunk_words : kDefaultChunkWords;
 
-    auto kern = mcg::dev::k_fused<kFusedThreads, kMulForm, kPackForm>;
-    MCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<uint32_t>(e->smem_bytes, 1)));
+    MCG_CUDA(cudaFuncSetAttribute(fused_kernel(e->ctas_per_sm), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max<uint32_t>(e->smem_bytes, 1)));
     MCG_CUDA(upload(reinterpret_cast<mcg::Op **>(&e->d_ops), e->prog.ops));
-    if (e->prog.global_slots) {
+    if (e->prog.global_slots && e->mode == MCG_MODE_FUSED) {
         MCG_CUDA(cudaMalloc((void **)&e->d_scratch, (size_t)e->prog.global_slots * e->scratch_stride * sizeof(uint64_t)));
     }
+    return MCG_OK;
+}
+
+constexpr uint32_t kStageEventsPerThread = 4;
+constexpr int kStageWordsPerThread = 4;
+
+mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
+    const uint64_t nn = std::max<uint64_t>(e->graph.n_nodes(), 1);
+    // two chunk buffers, together at most ~48 GB by default
+    uint64_t words = run.layered_max_words ? run.layered_max_words : (24ull << 30) / (nn * sizeof(uint64_t));
+    words = std::max<uint64_t>(256, std::min<uint64_t>(words, 1ull << 20));
+    words = (words + 255) / 256 * 256;
+    e->stage_words = words;
+    for (int i = 0; i < 2; ++i) MCG_CUDA(cudaMalloc((void **)&e->d_stage[i], nn * words * sizeof(uint64_t)));
+    // The gate phase of chunk k runs while chunk k+1 is sampled: giving its
+    // stream the higher priority lets its (memory-bound) blocks be scheduled
+    // in between the sampler's blocks instead of after all of them.
+    int prio_low = 0, prio_high = 0;
+    MCG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    MCG_CUDA(cudaStreamCreateWithPriority(&e->s_a, cudaStreamNonBlocking, prio_low));
+    MCG_CUDA(cudaStreamCreateWithPriority(&e->s_b, cudaStreamNonBlocking, prio_high));
+    for (cudaEvent_t *ev : {&e->ev_fork, &e->ev_a[0], &e->ev_a[1], &e->ev_b[0], &e->ev_b[1], &e->ev_join_a,
+                            &e->ev_join_b})
+        MCG_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    return MCG_OK;
+}
+
+// One chunk: phase A (sampling) on s_a into buffer `set`, phase B (gate layers
+// and tallies) on s_b once A is done.  A reuses a buffer only after the B that
+// read it (two chunks earlier) has finished.
+mcg_status staged_chunk(mcg_engine *e, uint64_t k, uint32_t iteration, uint64_t word_begin, uint64_t W) {
+    const mcg::Graph &g = e->graph;
+    const int set = (int)(k & 1);
+    uint64_t *buf = e->d_stage[set];
+    if (k >= 2) MCG_CUDA(cudaStreamWaitEvent(e->s_a, e->ev_b[set], 0));
+    const uint32_t t3 = (iteration + 1u) << 6;
+    if (g.n_be > 0) {
+        const uint32_t groups = (g.n_be + kStageEventsPerThread - 1) / kStageEventsPerThread;
+        cudaEvent_t p0 = nullptr, p1 = nullptr;
+        if (e->profile_a) {
+            if (e->prof_used == e->prof_events.size()) {
+                cudaEvent_t a, b;
+                MCG_CUDA(cudaEventCreate(&a));
+                MCG_CUDA(cudaEventCreate(&b));
+                e->prof_events.push_back({a, b});
+            }
+            p0 = e->prof_events[e->prof_used].first;
+            p1 = e->prof_events[e->prof_used].second;
+            ++e->prof_used;
+            MCG_CUDA(cudaEventRecord(p0, e->s_a));
+        }
+        mcg::dev::k_stage_be<kMulForm, kPackForm, kStageEventsPerThread>
+            <<<rows_grid(W, groups, 256), 256, 0, e->s_a>>>(e->d_be, g.n_be, W, word_begin, t3, buf);
+        ++e->launches;
+        if (p1) MCG_CUDA(cudaEventRecord(p1, e->s_a));
+    }
+    MCG_CUDA(cudaEventRecord(e->ev_a[set], e->s_a));
+    MCG_CUDA(cudaStreamWaitEvent(e->s_b, e->ev_a[set], 0));
+    const uint64_t words_per_block = 256ull * kStageWordsPerThread;
+    for (size_t l = 0; l + 1 < e->layer_offsets.size(); ++l) {
+        const uint32_t n = e->layer_offsets[l + 1] - e->layer_offsets[l];
+        if (n == 0) continue;
+        dim3 grid = rows_grid(1, n, 256);
+        grid.x = (uint32_t)((W + words_per_block - 1) / words_per_block);
+        mcg::dev::k_stage_gates<kStageWordsPerThread><<<grid, 256, 0, e->s_b>>>(
+            e->d_smeta, e->d_inputs, e->d_layer_gates + e->layer_offsets[l], n, g.n_be, W, buf, e->d_gate_tally,
+            e->d_gate_tally_list, e->d_tally);
+        ++e->launches;
+    }
+    if (e->n_be_tally) {
+        dim3 grid = rows_grid(1, e->n_be_tally, 256);
+        grid.x = (uint32_t)std::min<uint64_t>((W + 255) / 256, 64);
+        mcg::dev::k_layer_tally<<<grid, 256, 0, e->s_b>>>(e->d_be_tally_nodes, e->n_be_tally, W, buf, e->d_tally,
+                                                          e->d_be_tally_idx);
+        ++e->launches;
+    }
+    MCG_CUDA(cudaEventRecord(e->ev_b[set], e->s_b));
+    MCG_CUDA(cudaGetLastError());
+    return MCG_OK;
+}
+
+mcg_status run_staged(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t word_begin, uint64_t count) {
+    // fork from the engine stream so the chunks follow earlier work on it
+    MCG_CUDA(cudaEventRecord(e->ev_fork, e->stream));
+    MCG_CUDA(cudaStreamWaitEvent(e->s_a, e->ev_fork, 0));
+    MCG_CUDA(cudaStreamWaitEvent(e->s_b, e->ev_fork, 0));
+    uint64_t k = 0;
+    for (uint32_t it = 0; it < n_it; ++it) {
+        for (uint64_t off = 0; off < count; off += e->stage_words, ++k) {
+            const uint64_t n = std::min<uint64_t>(e->stage_words, count - off);
+            const mcg_status st = staged_chunk(e, k, it_first + it, word_begin + off, n);
+            if (st != MCG_OK) return st;
+        }
+    }
+    // join back into the engine stream
+    MCG_CUDA(cudaEventRecord(e->ev_join_a, e->s_a));
+    MCG_CUDA(cudaEventRecord(e->ev_join_b, e->s_b));
+    MCG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_join_a, 0));
+    MCG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_join_b, 0));
     return MCG_OK;
 }
 
@@ -212,7 +377,7 @@ mcg_status launch_fused(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_
     a.word_count = count;
     const uint64_t want = (count + e->nt - 1) / e->nt;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(e->grid, std::max<uint64_t>(want, 1));
-    mcg::dev::k_fused<kFusedThreads, kMulForm, kPackForm><<<grid, e->nt, e->smem_bytes, e->stream>>>(a);
+    fused_kernel(e->ctas_per_sm)<<<grid, e->nt, e->smem_bytes, e->stream>>>(a);
     ++e->launches;
     MCG_CUDA(cudaGetLastError());
     return MCG_OK;
@@ -228,6 +393,21 @@ void release(mcg_engine *e) {
     cudaFree(e->d_tally_nodes);
     cudaFree(e->d_layer_gates);
     cudaFree(e->d_buf);
+    cudaFree(e->d_smeta);
+    cudaFree(e->d_gate_tally);
+    cudaFree(e->d_gate_tally_list);
+    cudaFree(e->d_be_tally_nodes);
+    cudaFree(e->d_be_tally_idx);
+    cudaFree(e->d_stage[0]);
+    cudaFree(e->d_stage[1]);
+    for (cudaEvent_t ev : {e->ev_fork, e->ev_a[0], e->ev_a[1], e->ev_b[0], e->ev_b[1], e->ev_join_a, e->ev_join_b})
+        if (ev) cudaEventDestroy(ev);
+    for (auto &pe : e->prof_events) {
+        cudaEventDestroy(pe.first);
+        cudaEventDestroy(pe.second);
+    }
+    if (e->s_a) cudaStreamDestroy(e->s_a);
+    if (e->s_b) cudaStreamDestroy(e->s_b);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -241,7 +421,7 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
     *out = nullptr;
     mcg_run_desc run{};
     if (run_in) run = *run_in;
-    if (run.mode > MCG_MODE_LAYERED) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
+    if (run.mode > MCG_MODE_STAGED) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
     auto *e = new (std::nothrow) mcg_engine();
     if (!e) return mcg::fail(MCG_ERR_OOM, "host allocation failed");
     const std::string err = mcg::Graph::from_desc(*graph, e->graph);
@@ -286,6 +466,8 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
         st = build_layered_tables(e);
         if (st != MCG_OK) break;
         st = setup_fused(e, run);
+        if (st != MCG_OK) break;
+        if (e->mode == MCG_MODE_STAGED) st = setup_staged(e, run);
     } while (false);
     if (st != MCG_OK) {
         release(e);
@@ -316,7 +498,10 @@ mcg_status mcg_run(mcg_engine *e, uint32_t iteration_first, uint32_t n_iteration
         return mcg::fail(MCG_ERR_INVALID, "iteration exceeds the 26-bit pass counter field");
     if (n_iterations == 0 || word_count == 0) return MCG_OK;
     MCG_CUDA(cudaSetDevice(e->device));
-    if (e->mode == MCG_MODE_FUSED) {
+    if (e->mode == MCG_MODE_STAGED) {
+        const mcg_status st = run_staged(e, iteration_first, n_iterations, word_begin, word_count);
+        if (st != MCG_OK) return st;
+    } else if (e->mode == MCG_MODE_FUSED) {
         for (uint64_t off = 0; off < word_count; off += e->chunk_words) {
             const uint64_t n = std::min<uint64_t>(e->chunk_words, word_count - off);
             const mcg_status st = launch_fused(e, iteration_first, n_iterations, word_begin + off, n);
@@ -337,7 +522,7 @@ mcg_status mcg_run(mcg_engine *e, uint32_t iteration_first, uint32_t n_iteration
                     dim3 grid = rows_grid(1, n_tally, 256);
                     grid.x = bx;
                     mcg::dev::k_layer_tally<<<grid, 256, 0, e->stream>>>(e->d_tally_nodes, n_tally, n, e->d_buf,
-                                                                         e->d_tally);
+                                                                         e->d_tally, nullptr);
                     ++e->launches;
                     MCG_CUDA(cudaGetLastError());
                 }
@@ -485,6 +670,30 @@ mcg_status mcg_sampler_peak(int32_t device, uint64_t n_events, uint64_t n_words,
     cudaFree(sink);
     if (err != cudaSuccess) return mcg::fail(MCG_ERR_CUDA, cudaGetErrorString(err));
     *words_per_second = (double)n_events * (double)n_words * repeats / (ms * 1e-3);
+    return MCG_OK;
+}
+
+mcg_status mcg_profile_sampler(mcg_engine *e, int32_t enable) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    e->profile_a = enable != 0;
+    e->prof_used = 0;
+    return MCG_OK;
+}
+
+mcg_status mcg_profile_sampler_read(mcg_engine *e, uint64_t *launches, double *total_ms) {
+    mcg::clear_error();
+    if (!e || !launches || !total_ms) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    MCG_CUDA(cudaSetDevice(e->device));
+    MCG_CUDA(cudaStreamSynchronize(e->stream));
+    double sum = 0;
+    for (size_t i = 0; i < e->prof_used; ++i) {
+        float ms = 0;
+        MCG_CUDA(cudaEventElapsedTime(&ms, e->prof_events[i].first, e->prof_events[i].second));
+        sum += ms;
+    }
+    *launches = e->prof_used;
+    *total_ms = sum;
     return MCG_OK;
 }
 

@@ -84,8 +84,8 @@ struct FusedArgs {
     uint64_t word_count;
 };
 
-template <int NT, int MF, int PF>
-__global__ void __launch_bounds__(NT, 2) k_fused(FusedArgs a) {
+template <int NT, int MINB, int MF, int PF>
+__global__ void __launch_bounds__(NT, MINB) k_fused(FusedArgs a) {
     extern __shared__ __align__(16) uint64_t smem[];
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
@@ -230,9 +230,11 @@ __global__ void __launch_bounds__(256) k_layer_gates(const uint4 *__restrict__ m
 }
 
 // Tallies: popcount, block reduction, one atomic per block and node.
+// tally_idx (optional) maps row t of tally_nodes to its counter.
 __global__ void __launch_bounds__(256) k_layer_tally(const uint32_t *__restrict__ tally_nodes, uint32_t n_tally,
                                                      uint64_t W, const uint64_t *__restrict__ buf,
-                                                     unsigned long long *__restrict__ ones) {
+                                                     unsigned long long *__restrict__ ones,
+                                                     const uint32_t *__restrict__ tally_idx) {
     __shared__ uint32_t warp_sums[8];
     const uint32_t t = blockIdx.y + gridDim.y * blockIdx.z;
     if (t >= n_tally) return;
@@ -246,7 +248,100 @@ __global__ void __launch_bounds__(256) k_layer_tally(const uint32_t *__restrict_
     if (threadIdx.x == 0) {
         unsigned long long s = 0;
         for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) s += warp_sums[i];
-        if (s) atomicAdd(&ones[t], s);
+        if (s) atomicAdd(&ones[tally_idx ? tally_idx[t] : t], s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Staged pipeline.  Phase A samples basic-event words into buf rows
+// [0, n_be); phase B evaluates one layer of gates per launch into rows
+// n_be + g, with tallies fused.
+
+// Phase A: thread (w, group) samples word w of events [group * EPT, +EPT).
+template <int MF, int PF, int EPT>
+__global__ void __launch_bounds__(256) k_stage_be(const uint4 *__restrict__ be, uint32_t n_be, uint64_t W,
+                                                  uint64_t word_begin, uint32_t t3, uint64_t *__restrict__ buf) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e0 = (blockIdx.y + gridDim.y * blockIdx.z) * EPT;
+    if (w >= W || e0 >= n_be) return;
+    const WordCtx ctx = make_word_ctx<MF>((uint32_t)(word_begin + w));
+#pragma unroll 1
+    for (uint32_t i = 0; i < EPT; ++i) {
+        const uint32_t e = e0 + i;
+        if (e >= n_be) break;
+        const uint4 r = be[e];
+        uint64_t v;
+        if (r.w != 0) v = kAllOnes;           // threshold 2^32
+        else if (r.z == 0) v = 0;             // threshold 0
+        else v = be_word<MF, PF>(r.x, r.y, ctx, t3, r.z);
+        buf[(uint64_t)e * W + w] = v;
+    }
+}
+
+// Phase B: gate layer_gates[blockIdx.y] for words [blockIdx.x * 256 * WPT, ...),
+// WPT words per thread at stride 256 (coalesced).  meta[g] = {op | k << 8 |
+// nbits << 16, in_begin, in_count, neg_count}; gate_tally[g] = {offset, count}
+// into tally_list.  Each block adds its popcount once per tally entry.
+template <int WPT>
+__global__ void __launch_bounds__(256) k_stage_gates(const uint4 *__restrict__ meta, const uint32_t *__restrict__ inputs,
+                                                     const uint32_t *__restrict__ layer_gates, uint32_t n_layer,
+                                                     uint32_t n_be, uint64_t W, uint64_t *__restrict__ buf,
+                                                     const uint2 *__restrict__ gate_tally,
+                                                     const uint32_t *__restrict__ tally_list,
+                                                     unsigned long long *__restrict__ ones) {
+    __shared__ uint32_t warp_sums[8];
+    const uint32_t li = blockIdx.y + gridDim.y * blockIdx.z;
+    if (li >= n_layer) return;
+    const uint32_t gi = layer_gates[li];
+    const uint4 m = meta[gi];
+    const uint32_t op = m.x & 0xFFu;
+    const uint32_t kk = (m.x >> 8) & 0xFFu;
+    const uint32_t nbits = (m.x >> 16) & 0xFu;
+    const uint32_t n = m.z;
+    const uint32_t off = n - m.w;
+    const uint32_t *in = inputs + m.y;
+    uint64_t *out = buf + (uint64_t)(n_be + gi) * W;
+    uint32_t count = 0;
+    const uint64_t base = (uint64_t)blockIdx.x * 256 * WPT + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+        const uint64_t w = base + (uint64_t)k * 256;
+        if (w >= W) break;
+        uint64_t r;
+        if (op == MCG_ATLEAST) {
+            SlicedCount cnt;
+            cnt.clear();
+            for (uint32_t i = 0; i < n; ++i) {
+                uint64_t v = buf[(uint64_t)in[i] * W + w];
+                if (i >= off) v = ~v;
+                cnt.add(v, nbits);
+            }
+            r = cnt.ge(kk);
+        } else {
+            r = (op == MCG_AND || op == MCG_NAND) ? kAllOnes : 0ull;
+            for (uint32_t i = 0; i < n; ++i) {
+                uint64_t v = buf[(uint64_t)in[i] * W + w];
+                if (i >= off) v = ~v;
+                if (op == MCG_OR || op == MCG_NOR) r |= v;
+                else if (op == MCG_AND || op == MCG_NAND) r &= v;
+                else if (op == MCG_XOR) r ^= v;
+                else r = v;
+            }
+            if (op == MCG_NAND || op == MCG_NOR || op == MCG_NOT) r = ~r;
+        }
+        out[w] = r;
+        count += (uint32_t)__popcll(r);
+    }
+    const uint2 t = gate_tally[gi];
+    if (t.y == 0) return;  // uniform per block
+    count = __reduce_add_sync(0xFFFFFFFFu, count);
+    if ((threadIdx.x & 31u) == 0) warp_sums[threadIdx.x >> 5] = count;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (uint32_t i = 0; i < 8; ++i) s += warp_sums[i];
+        if (s)
+            for (uint32_t j = 0; j < t.y; ++j) atomicAdd(&ones[tally_list[t.x + j]], s);
     }
 }
 

@@ -32,10 +32,10 @@ def test_words_match_golden_fixtures(capi, gpu):
             assert np.array_equal(e.dump_words(3, (1 << 32) - 64, 64), npz[str(name) + "words_it3_whigh"])
 
 
-@pytest.mark.parametrize("mode", ["fused", "layered"])
+@pytest.mark.parametrize("mode", ["fused", "layered", "staged"])
 def test_small_tree_tallies_golden(capi, oracle_mod, gpu, mode):
     npz = np.load(GOLDEN / "small_trees.npz")
-    m = capi.MODE_FUSED if mode == "fused" else capi.MODE_LAYERED
+    m = capi.MODES[mode]
     for name in npz["names"]:
         g = load_graph(npz, str(name))
         g = g.with_tallies(np.arange(g.n_nodes))  # every node, basic events included
@@ -48,11 +48,11 @@ def test_small_tree_tallies_golden(capi, oracle_mod, gpu, mode):
             assert np.array_equal(ones, expect)
 
 
-@pytest.mark.parametrize("mode", ["fused", "layered"])
+@pytest.mark.parametrize("mode", ["fused", "layered", "staged"])
 def test_config1_golden_tallies(capi, gpu, mode):
     npz = np.load(GOLDEN / "config1_tallies.npz")
     g = load_graph(npz)
-    m = capi.MODE_FUSED if mode == "fused" else capi.MODE_LAYERED
+    m = capi.MODES[mode]
     with engine(capi, g, mode=m) as e:
         e.run(1, 1, 0, int(npz["words"]))
         ones, total = e.tallies()
@@ -75,10 +75,11 @@ def test_fused_any_slot_budget(capi, oracle_mod, gpu, slots):
         assert np.array_equal(ones, expect), (slots, it, wb, n)
 
 
-def test_multiple_passes_and_ranges(capi, oracle_mod, gpu):
+@pytest.mark.parametrize("mode", ["fused", "staged"])
+def test_multiple_passes_and_ranges(capi, oracle_mod, gpu, mode):
     g = synth.config1()
     expect = oracle_mod.tallies(g, 2, 3, 500, 3000)
-    with engine(capi, g) as e:
+    with engine(capi, g, mode=capi.MODES[mode], layered_max_words=1024) as e:
         e.run(2, 3, 500, 3000)
         ones, total = e.tallies()
         assert total == 3 * 3000 * 64
@@ -92,9 +93,10 @@ def test_multiple_passes_and_ranges(capi, oracle_mod, gpu):
         assert total2 == total and np.array_equal(ones2, expect)
 
 
-def test_config2_windows_bit_exact(capi, oracle_mod, gpu):
+@pytest.mark.parametrize("mode", ["fused", "staged"])
+def test_config2_windows_bit_exact(capi, oracle_mod, gpu, mode):
     g = synth.config2()
-    with engine(capi, g) as e:
+    with engine(capi, g, mode=capi.MODES[mode]) as e:
         for (wb, n) in [(0, 2048), ((1 << 24) - 2048, 2048), ((1 << 24) + 77, 513)]:
             expect = oracle_mod.tallies(g, 1, 1, wb, n)
             e.reset_tallies()
@@ -112,8 +114,11 @@ def test_config2_fused_equals_layered_large(capi, gpu):
     with engine(capi, g, mode=capi.MODE_LAYERED, layered_max_words=1 << 17) as l:
         l.run(1, 1, 0, W)
         b, tb = l.tallies()
-    assert ta == tb == W * 64
-    assert np.array_equal(a, b)
+    with engine(capi, g, mode=capi.MODE_STAGED, layered_max_words=1 << 17) as st:
+        st.run(1, 1, 0, W)
+        c, tc = st.tallies()
+    assert ta == tb == tc == W * 64
+    assert np.array_equal(a, b) and np.array_equal(a, c)
     assert a.sum() > 0
 
 
@@ -130,7 +135,7 @@ def test_edge_cases(capi, oracle_mod, gpu):
         tally_nodes=[5, 6, 7, 8, 9, 10, 11, 12, 0, 12, 2])
     expect = oracle_mod.tallies(g, 1, 1, 0, 4000)
     words = oracle_mod.eval_words(g, 1, 0, 64)
-    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED):
+    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED, capi.MODE_STAGED):
         with engine(capi, g, mode=mode) as e:
             e.run(1, 1, 0, 4000)
             ones, _ = e.tallies()
@@ -147,7 +152,7 @@ def test_atleast_uint8_wrap(capi, oracle_mod, gpu):
                   gate_in_count=[n, n, n], gate_neg_count=[0, 10, 0], inputs=np.arange(n),
                   tally_nodes=[n, n + 1, n + 2])
     expect = oracle_mod.tallies(g, 1, 1, 0, 2000)
-    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED):
+    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED, capi.MODE_STAGED):
         with engine(capi, g, mode=mode) as e:
             e.run(1, 1, 0, 2000)
             assert np.array_equal(e.tallies()[0], expect)

@@ -87,6 +87,8 @@ typedef struct mcg_run_desc {
     uint32_t ctas_per_sm;     /* fused kernel persistent CTAs per SM; 0 = auto */
     uint64_t chunk_words;     /* words per launch in one mcg_run; 0 = auto */
     uint64_t layered_max_words; /* layered/staged modes: words materialised per chunk; 0 = auto */
+    uint32_t sampler_blocks_per_sm; /* staged mode: sampler blocks resident per SM, which leaves
+                                       room for gate-phase blocks; 0 = 6, 8 = no cap */
 } mcg_run_desc;
 
 typedef struct mcg_engine mcg_engine;
@@ -156,8 +158,9 @@ mcg_status mcg_program_info_get(mcg_engine *engine, mcg_program_info *info);
  * fields stay 0) and, when ops is non-NULL, copies min(n_ops, ops_capacity)
  * ops of 4 uint32 words each.  For inspection and verification of the
  * program format; mcg_create compiles its own program. */
-mcg_status mcg_compile(const mcg_graph_desc *graph, uint32_t smem_slot_budget, mcg_program_info *info,
-                       uint32_t *ops, uint64_t ops_capacity);
+#define MCG_COMPILE_VARIABLE_THRESHOLDS 1u /* basic-event ops index a per-instance threshold table */
+mcg_status mcg_compile(const mcg_graph_desc *graph, uint32_t smem_slot_budget, uint32_t flags,
+                       mcg_program_info *info, uint32_t *ops, uint64_t ops_capacity);
 
 /* Number of fused/layered kernel launches the engine has issued so far. */
 mcg_status mcg_launch_count(mcg_engine *engine, uint64_t *launches);

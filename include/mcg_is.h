@@ -1,0 +1,84 @@
+/*
+ * mcg_is.h -- importance sampling for rare top events and the proposal MLP
+ * (libmcg.so).  No counterpart in the reference, whose Monte Carlo path only
+ * samples the nominal probabilities (src/mc/kernel/basic_event.h:125-142).
+ *
+ * A proposal q_i replaces p_i in the Bernoulli threshold, thr_i = q_i * 2^32,
+ * so sampling stays the bit-exact bit-packed Philox sampler and gate
+ * evaluation stays the same kernels.  For every sample where the top event
+ * fires, the likelihood ratio
+ *     log w = C + sum_i a_i x_i,  C = sum_i ln((1 - p_i) / (1 - q_i)),
+ *     a_i = ln(p_i / q_i) - ln((1 - p_i) / (1 - q_i))
+ * is accumulated in FP64, and so are sum w, sum w^2 (the estimator
+ * P = sum w / N and its variance) and, for the cross-entropy update,
+ * sum w x_i per basic event.  p_i and q_i are taken at their quantised
+ * values thr / 2^32, the probabilities the sampler actually draws.
+ */
+#ifndef MCG_IS_H
+#define MCG_IS_H
+
+#include "mcg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mcg_is mcg_is;
+
+typedef struct mcg_is_result {
+    uint64_t samples;      /* N */
+    uint64_t hits;         /* samples where the top event fired */
+    double sum_w;          /* sum over hits of w */
+    double sum_w2;         /* sum over hits of w^2 */
+    double estimate;       /* sum_w / N */
+    double std_err;        /* sqrt((sum_w2 / N - estimate^2) / (N - 1)) */
+    double rel_err;        /* std_err / estimate */
+    double ess;            /* (sum_w)^2 / sum_w2 */
+    double max_log_w;      /* largest log-weight seen */
+    double kernel_ms;      /* device time of the run (CUDA events) */
+} mcg_is_result;
+
+/* Engine over a flattened graph whose tally list holds exactly the top
+ * event.  Nominal thresholds come from graph->be_threshold.  Uses the
+ * staged kernels (layered_max_words = words per chunk). */
+mcg_status mcg_is_create(const mcg_graph_desc *graph, const mcg_run_desc *run, mcg_is **out);
+mcg_status mcg_is_destroy(mcg_is *is);
+
+/* Samples pass `iteration`, words [word_begin, word_begin + word_count),
+ * with proposal thresholds q_threshold[n_be] (host array; each in
+ * [1, 2^32 - 1] where the nominal threshold is in that range, else equal to
+ * it).  ce_num (host, n_be doubles, optional) receives sum over hits of
+ * w * x_i for the cross-entropy update. */
+mcg_status mcg_is_run(mcg_is *is, const uint64_t *q_threshold, uint32_t iteration, uint64_t word_begin,
+                      uint64_t word_count, mcg_is_result *result, double *ce_num);
+
+/* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
+ * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32
+ * accumulation), FP32 master weights and Adam state.  Parameter layout
+ * (5,313 floats): W1[16][64], b1[64], W2[64][64], b2[64], W3[64], b3. */
+typedef struct mcg_mlp mcg_mlp;
+#define MCG_MLP_IN 16
+#define MCG_MLP_HIDDEN 64
+#define MCG_MLP_PARAMS (16 * 64 + 64 + 64 * 64 + 64 + 64 + 1)
+
+mcg_status mcg_mlp_create(int32_t device, uint64_t seed, mcg_mlp **out);
+mcg_status mcg_mlp_destroy(mcg_mlp *m);
+mcg_status mcg_mlp_set_params(mcg_mlp *m, const float *params);
+mcg_status mcg_mlp_get_params(mcg_mlp *m, float *params);
+/* q_out[n] = sigmoid(MLP(features[n][16])). Host arrays. */
+mcg_status mcg_mlp_forward(mcg_mlp *m, const float *features, uint32_t n, float *q_out);
+/* Gradient of the weighted binary cross-entropy
+ *     L = sum_i w_i * -(t_i log q_i + (1 - t_i) log(1 - q_i)) / sum_i w_i
+ * with respect to every parameter (BF16 forward, FP32 accumulation).
+ * weights may be NULL (all 1). */
+mcg_status mcg_mlp_grad(mcg_mlp *m, const float *features, const float *targets, const float *weights, uint32_t n,
+                        float *grad_out, float *loss_out);
+/* `steps` Adam steps (lr, beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
+mcg_status mcg_mlp_train(mcg_mlp *m, const float *features, const float *targets, const float *weights, uint32_t n,
+                         uint32_t steps, float lr, float *loss_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCG_IS_H */

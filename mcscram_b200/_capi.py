@@ -65,6 +65,7 @@ class RunDesc(C.Structure):
         ("ctas_per_sm", C.c_uint32),
         ("chunk_words", C.c_uint64),
         ("layered_max_words", C.c_uint64),
+        ("sampler_blocks_per_sm", C.c_uint32),
     ]
 
 
@@ -104,7 +105,8 @@ _SIGNATURES = {
     "mcg_reset_tallies": (C.c_int, [C.c_void_p]),
     "mcg_dump_words": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, _u64p]),
     "mcg_program_info_get": (C.c_int, [C.c_void_p, C.POINTER(ProgramInfo)]),
-    "mcg_compile": (C.c_int, [C.POINTER(GraphDesc), C.c_uint32, C.POINTER(ProgramInfo), _u32p, C.c_uint64]),
+    "mcg_compile": (C.c_int, [C.POINTER(GraphDesc), C.c_uint32, C.c_uint32, C.POINTER(ProgramInfo), _u32p,
+                              C.c_uint64]),
     "mcg_launch_count": (C.c_int, [C.c_void_p, _u64p]),
     "mcg_time_runs": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
     "mcg_sampler_peak": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
@@ -179,14 +181,16 @@ class GraphView:
             tally_nodes=_ptr(g.tally_nodes, C.c_uint32))
 
 
-def compile_program(g: FlatGraph, smem_slot_budget: int = 64):
+def compile_program(g: FlatGraph, smem_slot_budget: int = 64, variable_thresholds: bool = False):
     """Host-only compilation of the fused program: (info dict, ops array [n_ops, 4] uint32)."""
     lib = load()
     view = GraphView(g)
     info = ProgramInfo()
-    check(lib.mcg_compile(C.byref(view.desc), smem_slot_budget, C.byref(info), None, 0))
+    flags = 1 if variable_thresholds else 0
+    check(lib.mcg_compile(C.byref(view.desc), smem_slot_budget, flags, C.byref(info), None, 0))
     ops = np.zeros((info.n_ops, 4), dtype=np.uint32)
-    check(lib.mcg_compile(C.byref(view.desc), smem_slot_budget, C.byref(info), _ptr(ops, C.c_uint32), info.n_ops))
+    check(lib.mcg_compile(C.byref(view.desc), smem_slot_budget, flags, C.byref(info), _ptr(ops, C.c_uint32),
+                          info.n_ops))
     return info.as_dict(), ops
 
 
@@ -194,13 +198,14 @@ class Engine:
     """One device engine over a flattened PDAG (wraps mcg_create ... mcg_destroy)."""
 
     def __init__(self, g: FlatGraph, mode: int = MODE_FUSED, device: int = 0, stream: Optional[int] = None,
-                 smem_slots: int = 0, ctas_per_sm: int = 0, chunk_words: int = 0, layered_max_words: int = 0):
+                 smem_slots: int = 0, ctas_per_sm: int = 0, chunk_words: int = 0, layered_max_words: int = 0,
+                 sampler_blocks_per_sm: int = 0):
         self.lib = load()
         self.graph = g
         self._view = GraphView(g)
         run = RunDesc(mode=mode, device=device, stream=C.c_void_p(stream) if stream else None, block_threads=0,
                       smem_slots=smem_slots, ctas_per_sm=ctas_per_sm, chunk_words=chunk_words,
-                      layered_max_words=layered_max_words)
+                      layered_max_words=layered_max_words, sampler_blocks_per_sm=sampler_blocks_per_sm)
         h = C.c_void_p()
         check(self.lib.mcg_create(C.byref(self._view.desc), C.byref(run), C.byref(h)))
         self.handle = h

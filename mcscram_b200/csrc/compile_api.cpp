@@ -7,15 +7,15 @@
 #include "mcg.h"
 #include "program.hpp"
 
-extern "C" mcg_status mcg_compile(const mcg_graph_desc *graph, uint32_t smem_slot_budget, mcg_program_info *info,
-                                  uint32_t *ops, uint64_t ops_capacity) {
+extern "C" mcg_status mcg_compile(const mcg_graph_desc *graph, uint32_t smem_slot_budget, uint32_t flags,
+                                  mcg_program_info *info, uint32_t *ops, uint64_t ops_capacity) {
     mcg::clear_error();
     if (!graph || !info) return mcg::fail(MCG_ERR_INVALID, "graph and info must not be NULL");
     mcg::Graph g;
     std::string err = mcg::Graph::from_desc(*graph, g);
     if (!err.empty()) return mcg::fail(MCG_ERR_INVALID, err);
     mcg::Program prog;
-    err = mcg::compile_program(g, smem_slot_budget, prog);
+    err = mcg::compile_program(g, smem_slot_budget, prog, (flags & MCG_COMPILE_VARIABLE_THRESHOLDS) != 0);
     if (!err.empty()) return mcg::fail(MCG_ERR_INVALID, err);
     std::memset(info, 0, sizeof(*info));
     info->n_ops = prog.ops.size();

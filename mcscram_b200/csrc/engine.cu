@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "engine_internal.hpp"
 #include "error.hpp"
 #include "graph.hpp"
 #include "kernels.cuh"
@@ -27,8 +28,8 @@ namespace {
 // packing measured fastest of the four forms on B200 (register-only sampler).
 constexpr int kMulForm = 1;
 constexpr int kPackForm = 1;
-constexpr int kFusedThreads = 256;
-constexpr uint64_t kDefaultChunkWords = 1ull << 21;
+using mcg::internal::kDefaultChunkWords;
+using mcg::internal::kFusedThreads;
 
 #define MCG_CUDA(call)                                                                          \
     do {                                                                                        \
@@ -49,59 +50,6 @@ cudaError_t upload(T **dptr, const std::vector<T> &v) {
 }
 
 }  // namespace
-
-struct mcg_engine {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    uint32_t mode = MCG_MODE_FUSED;
-    mcg::Graph graph;
-    mcg::Program prog;
-
-    // fused
-    uint4 *d_ops = nullptr;
-    uint64_t *d_scratch = nullptr;
-    uint64_t scratch_stride = 0;
-    uint32_t nt = kFusedThreads;
-    uint32_t ctas_per_sm = 2;
-    uint32_t grid = 0;
-    uint32_t smem_bytes = 0;
-    bool tally_in_smem = false;
-    uint64_t chunk_words = kDefaultChunkWords;
-
-    // tallies
-    unsigned long long *d_tally = nullptr;
-    uint64_t total_bits = 0;
-
-    // layered
-    uint4 *d_be = nullptr;
-    uint4 *d_meta = nullptr;
-    uint32_t *d_inputs = nullptr;
-    uint32_t *d_tally_nodes = nullptr;
-    uint32_t *d_layer_gates = nullptr;
-    std::vector<uint32_t> layer_offsets;  // into d_layer_gates, size n_layers + 1
-    uint64_t *d_buf = nullptr;
-    uint64_t buf_words = 0;
-    uint64_t layered_max_words = 0;
-
-    // staged
-    uint4 *d_smeta = nullptr;           // gate meta with counter bits for the bit-sliced ATLEAST
-    uint2 *d_gate_tally = nullptr;      // per gate {offset, count} into d_gate_tally_list
-    uint32_t *d_gate_tally_list = nullptr;
-    uint32_t *d_be_tally_nodes = nullptr;  // tallied basic events
-    uint32_t *d_be_tally_idx = nullptr;
-    uint32_t n_be_tally = 0;
-    uint64_t *d_stage[2] = {nullptr, nullptr};
-    uint64_t stage_words = 0;           // words per chunk the stage buffers hold
-    cudaStream_t s_a = nullptr, s_b = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_a[2] = {nullptr, nullptr}, ev_b[2] = {nullptr, nullptr};
-    cudaEvent_t ev_join_a = nullptr, ev_join_b = nullptr;
-    bool profile_a = false;                   // time every sampler-phase launch
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
-    size_t prof_used = 0;
-
-    uint64_t launches = 0;
-};
 
 namespace {
 
@@ -264,7 +212,10 @@ mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
 }
 
 constexpr uint32_t kStageEventsPerThread = 4;
-constexpr int kStageWordsPerThread = 4;
+// Gate-phase blocks are small (128 threads, 2 words each) so that they fit in
+// the registers and threads left next to the capped sampler blocks.
+constexpr int kStageGateThreads = 128;
+constexpr int kStageWordsPerThread = 2;
 
 mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
     const uint64_t nn = std::max<uint64_t>(e->graph.n_nodes(), 1);
@@ -274,6 +225,17 @@ mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
     words = (words + 255) / 256 * 256;
     e->stage_words = words;
     for (int i = 0; i < 2; ++i) MCG_CUDA(cudaMalloc((void **)&e->d_stage[i], nn * words * sizeof(uint64_t)));
+    MCG_CUDA(cudaMalloc((void **)&e->d_event_table,
+                        std::max<uint64_t>(e->graph.n_be, 1) * mcg::dev::kEventTableStride * sizeof(uint2)));
+    // Cap the resident sampler blocks per SM through their shared-memory
+    // footprint, so gate-phase blocks (memory bound) can run next to them.
+    cudaDeviceProp prop;
+    MCG_CUDA(cudaGetDeviceProperties(&prop, e->device));
+    const uint32_t blocks = run.sampler_blocks_per_sm ? run.sampler_blocks_per_sm : 6u;
+    if (blocks < 1 || blocks > 8) return mcg::fail(MCG_ERR_INVALID, "sampler_blocks_per_sm must be 1..8");
+    e->sampler_smem = blocks >= 8 ? 0u : (uint32_t)(prop.sharedMemPerMultiprocessor / blocks - 2048);
+    MCG_CUDA(cudaFuncSetAttribute(mcg::dev::k_stage_be<kMulForm, kPackForm, kStageEventsPerThread>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<uint32_t>(e->sampler_smem, 1)));
     // The gate phase of chunk k runs while chunk k+1 is sampled: giving its
     // stream the higher priority lets its (memory-bound) blocks be scheduled
     // in between the sampler's blocks instead of after all of them.
@@ -296,6 +258,15 @@ mcg_status staged_chunk(mcg_engine *e, uint64_t k, uint32_t iteration, uint64_t 
     uint64_t *buf = e->d_stage[set];
     if (k >= 2) MCG_CUDA(cudaStreamWaitEvent(e->s_a, e->ev_b[set], 0));
     const uint32_t t3 = (iteration + 1u) << 6;
+    const uint4 *be_tab = e->d_be_sample ? e->d_be_sample : e->d_be;
+    if (g.n_be > 0 && e->table_iteration != iteration) {
+        // s_a is in order: earlier sampler launches finish before the table changes
+        const uint64_t n = (uint64_t)g.n_be * mcg::dev::kEventTableStride;
+        mcg::dev::k_event_table<kMulForm><<<(uint32_t)((n + 255) / 256), 256, 0, e->s_a>>>(be_tab, g.n_be, t3,
+                                                                                           e->d_event_table);
+        ++e->launches;
+        e->table_iteration = iteration;
+    }
     if (g.n_be > 0) {
         const uint32_t groups = (g.n_be + kStageEventsPerThread - 1) / kStageEventsPerThread;
         cudaEvent_t p0 = nullptr, p1 = nullptr;
@@ -312,19 +283,20 @@ mcg_status staged_chunk(mcg_engine *e, uint64_t k, uint32_t iteration, uint64_t 
             MCG_CUDA(cudaEventRecord(p0, e->s_a));
         }
         mcg::dev::k_stage_be<kMulForm, kPackForm, kStageEventsPerThread>
-            <<<rows_grid(W, groups, 256), 256, 0, e->s_a>>>(e->d_be, g.n_be, W, word_begin, t3, buf);
+            <<<rows_grid(W, groups, 256), 256, e->sampler_smem, e->s_a>>>(be_tab, e->d_event_table, g.n_be, W,
+                                                                          word_begin, buf);
         ++e->launches;
         if (p1) MCG_CUDA(cudaEventRecord(p1, e->s_a));
     }
     MCG_CUDA(cudaEventRecord(e->ev_a[set], e->s_a));
     MCG_CUDA(cudaStreamWaitEvent(e->s_b, e->ev_a[set], 0));
-    const uint64_t words_per_block = 256ull * kStageWordsPerThread;
+    const uint64_t words_per_block = (uint64_t)kStageGateThreads * kStageWordsPerThread;
     for (size_t l = 0; l + 1 < e->layer_offsets.size(); ++l) {
         const uint32_t n = e->layer_offsets[l + 1] - e->layer_offsets[l];
         if (n == 0) continue;
         dim3 grid = rows_grid(1, n, 256);
         grid.x = (uint32_t)((W + words_per_block - 1) / words_per_block);
-        mcg::dev::k_stage_gates<kStageWordsPerThread><<<grid, 256, 0, e->s_b>>>(
+        mcg::dev::k_stage_gates<kStageGateThreads, kStageWordsPerThread><<<grid, kStageGateThreads, 0, e->s_b>>>(
             e->d_smeta, e->d_inputs, e->d_layer_gates + e->layer_offsets[l], n, g.n_be, W, buf, e->d_gate_tally,
             e->d_gate_tally_list, e->d_tally);
         ++e->launches;
@@ -336,12 +308,16 @@ mcg_status staged_chunk(mcg_engine *e, uint64_t k, uint32_t iteration, uint64_t 
                                                           e->d_be_tally_idx);
         ++e->launches;
     }
+    if (e->chunk_hook) {
+        const mcg_status st = e->chunk_hook(e->s_b, buf, W);
+        if (st != MCG_OK) return st;
+    }
     MCG_CUDA(cudaEventRecord(e->ev_b[set], e->s_b));
     MCG_CUDA(cudaGetLastError());
     return MCG_OK;
 }
 
-mcg_status run_staged(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t word_begin, uint64_t count) {
+mcg_status run_staged_impl(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t word_begin, uint64_t count) {
     // fork from the engine stream so the chunks follow earlier work on it
     MCG_CUDA(cudaEventRecord(e->ev_fork, e->stream));
     MCG_CUDA(cudaStreamWaitEvent(e->s_a, e->ev_fork, 0));
@@ -398,6 +374,7 @@ void release(mcg_engine *e) {
     cudaFree(e->d_gate_tally_list);
     cudaFree(e->d_be_tally_nodes);
     cudaFree(e->d_be_tally_idx);
+    cudaFree(e->d_event_table);
     cudaFree(e->d_stage[0]);
     cudaFree(e->d_stage[1]);
     for (cudaEvent_t ev : {e->ev_fork, e->ev_a[0], e->ev_a[1], e->ev_b[0], e->ev_b[1], e->ev_join_a, e->ev_join_b})
@@ -412,6 +389,14 @@ void release(mcg_engine *e) {
 }
 
 }  // namespace
+
+namespace mcg {
+namespace internal {
+mcg_status run_staged(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t word_begin, uint64_t count) {
+    return run_staged_impl(e, it_first, n_it, word_begin, count);
+}
+}  // namespace internal
+}  // namespace mcg
 
 extern "C" {
 
@@ -499,7 +484,7 @@ mcg_status mcg_run(mcg_engine *e, uint32_t iteration_first, uint32_t n_iteration
     if (n_iterations == 0 || word_count == 0) return MCG_OK;
     MCG_CUDA(cudaSetDevice(e->device));
     if (e->mode == MCG_MODE_STAGED) {
-        const mcg_status st = run_staged(e, iteration_first, n_iterations, word_begin, word_count);
+        const mcg_status st = run_staged_impl(e, iteration_first, n_iterations, word_begin, word_count);
         if (st != MCG_OK) return st;
     } else if (e->mode == MCG_MODE_FUSED) {
         for (uint64_t off = 0; off < word_count; off += e->chunk_words) {
@@ -651,22 +636,30 @@ mcg_status mcg_sampler_peak(int32_t device, uint64_t n_events, uint64_t n_words,
         return mcg::fail(MCG_ERR_INVALID, "bad argument");
     MCG_CUDA(cudaSetDevice(device));
     uint64_t *sink = nullptr;
+    uint2 *table = nullptr;
     MCG_CUDA(cudaMalloc((void **)&sink, n_words * sizeof(uint64_t)));
+    if (cudaMalloc((void **)&table, n_events * mcg::dev::kEventTableStride * sizeof(uint2)) != cudaSuccess) {
+        cudaFree(sink);
+        return mcg::fail(MCG_ERR_OOM, "sampler table allocation failed");
+    }
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
+    const uint64_t nt = n_events * mcg::dev::kEventTableStride;
+    mcg::dev::k_peak_table<kMulForm><<<(uint32_t)((nt + 255) / 256), 256>>>((uint32_t)n_events, 2u << 6, table);
     const uint32_t blocks = (uint32_t)((n_words + 255) / 256);
     // warm-up
-    mcg::dev::k_sampler_peak<kMulForm, kPackForm><<<blocks, 256>>>((uint32_t)n_events, n_words, 2u << 6, sink);
+    mcg::dev::k_sampler_peak<kMulForm, kPackForm><<<blocks, 256>>>((uint32_t)n_events, n_words, table, sink);
     cudaEventRecord(a);
     for (uint32_t r = 0; r < repeats; ++r)
-        mcg::dev::k_sampler_peak<kMulForm, kPackForm><<<blocks, 256>>>((uint32_t)n_events, n_words, (r + 2u) << 6, sink);
+        mcg::dev::k_sampler_peak<kMulForm, kPackForm><<<blocks, 256>>>((uint32_t)n_events, n_words, table, sink);
     cudaEventRecord(b);
     cudaError_t err = cudaEventSynchronize(b);
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    cudaFree(table);
     cudaFree(sink);
     if (err != cudaSuccess) return mcg::fail(MCG_ERR_CUDA, cudaGetErrorString(err));
     *words_per_second = (double)n_events * (double)n_words * repeats / (ms * 1e-3);

@@ -70,6 +70,75 @@ __device__ __forceinline__ void store_slot(uint32_t ref, uint64_t v, uint64_t *m
     else my_slots[(uint32_t)ref * nt] = v;
 }
 
+// Walks one node program for this thread's sample word.  With THR_TABLE the
+// basic-event ops carry an index into thr (a per-instance uint64 threshold
+// table) instead of the threshold itself.  tally(index, count) is called by
+// lane 0 of each warp with the warp's popcount sum for a TALLY op.
+template <int NT, int MF, int PF, bool THR_TABLE, class Tally>
+__device__ __forceinline__ void interpret(const uint4 *__restrict__ ops, const WordCtx &ctx, uint32_t t3, bool valid,
+                                          uint64_t *my_slots, uint64_t *my_scratch, uint64_t stride,
+                                          const uint64_t *__restrict__ thr, Tally &&tally) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint64_t acc = 0, last = 0;
+    uint32_t conn = 0, kk = 0, nbits = 0;
+    SlicedCount cnt;
+    cnt.clear();
+    const uint4 *p = ops;
+    uint4 op = __ldg(p);
+    while (true) {
+        const uint4 nxt = __ldg(p + 1);
+        const uint32_t code = op.x & kOpMask;
+        if (code == kOpHalt) break;
+        // Value of the op: one sampler call site keeps the unrolled Philox
+        // body in the instruction cache once.
+        uint64_t v = 0;
+        if (code == kOpInBe || code == kOpBeDef) {
+            if constexpr (THR_TABLE) {
+                const uint64_t t = thr[op.z];
+                if (t >= (1ull << 32)) v = kAllOnes;
+                else if (t == 0) v = 0;
+                else v = be_word<MF, PF>(op.y, op.w, ctx, t3, (uint32_t)t);
+            } else {
+                v = be_word<MF, PF>(op.y, op.w, ctx, t3, op.z);
+            }
+        } else if (code == kOpInSlot) {
+            v = load_slot(op.y, my_slots, my_scratch, NT, stride);
+        } else if (code == kOpInConst || code == kOpConstDef) {
+            v = ((uint64_t)op.z << 32) | op.y;
+        }
+        if (code == kOpInBe || code == kOpInSlot || code == kOpInConst) {
+            if (op.x & kNegBit) v = ~v;
+            switch (conn) {
+                case MCG_AND: case MCG_NAND: acc &= v; break;
+                case MCG_OR: case MCG_NOR: acc |= v; break;
+                case MCG_XOR: acc ^= v; break;
+                case MCG_ATLEAST: cnt.add(v, nbits); break;
+                default: acc = v; break;  // NOT, NULL: the last input wins
+            }
+        } else if (code == kOpBeDef || code == kOpConstDef) {
+            last = v;
+            store_slot(op.x >> 8, last, my_slots, my_scratch, NT, stride);
+        } else if (code == kOpBegin) {
+            conn = (op.x >> 8) & 0xFFu;
+            kk = (op.x >> 16) & 0xFFu;
+            nbits = (op.x >> 24) & 0xFu;
+            acc = (conn == MCG_AND || conn == MCG_NAND) ? kAllOnes : 0ull;
+            if (conn == MCG_ATLEAST) cnt.clear();
+        } else if (code == kOpEnd) {
+            if (conn == MCG_ATLEAST) last = cnt.ge(kk);
+            else if (conn == MCG_NAND || conn == MCG_NOR || conn == MCG_NOT) last = ~acc;
+            else last = acc;
+            store_slot(op.y, last, my_slots, my_scratch, NT, stride);
+        } else if (code == kOpTally) {
+            uint32_t c = valid ? (uint32_t)__popcll(last) : 0u;
+            c = __reduce_add_sync(0xFFFFFFFFu, c);
+            if (lane == 0) tally(op.y, c);
+        }
+        op = nxt;
+        ++p;
+    }
+}
+
 struct FusedArgs {
     const uint4 *ops;
     uint32_t smem_slots;
@@ -88,7 +157,6 @@ template <int NT, int MINB, int MF, int PF>
 __global__ void __launch_bounds__(NT, MINB) k_fused(FusedArgs a) {
     extern __shared__ __align__(16) uint64_t smem[];
     const uint32_t tid = threadIdx.x;
-    const uint32_t lane = tid & 31u;
     unsigned long long *s_tally = reinterpret_cast<unsigned long long *>(smem + (size_t)a.smem_slots * NT);
     if (a.tally_in_smem) {
         for (uint32_t i = tid; i < a.n_tally; i += NT) s_tally[i] = 0ull;
@@ -99,64 +167,15 @@ __global__ void __launch_bounds__(NT, MINB) k_fused(FusedArgs a) {
     const uint64_t total_threads = (uint64_t)gridDim.x * NT;
     uint64_t *my_slots = smem + tid;
     uint64_t *my_scratch = a.scratch + gtid;
+    auto add = [tally](uint32_t idx, uint32_t c) { atomicAdd(&tally[idx], (unsigned long long)c); };
 
     for (uint32_t it = 0; it < a.n_iterations; ++it) {
         const uint32_t t3 = (a.iteration_first + it + 1u) << 6;
         for (uint64_t base = 0; base < a.word_count; base += total_threads) {
             const uint64_t j = base + gtid;
-            const bool valid = j < a.word_count;
             const WordCtx ctx = make_word_ctx<MF>((uint32_t)(a.word_begin + j));
-            uint64_t acc = 0, last = 0;
-            uint32_t conn = 0, kk = 0, nbits = 0;
-            SlicedCount cnt;
-            cnt.clear();
-            const uint4 *p = a.ops;
-            uint4 op = __ldg(p);
-            while (true) {
-                const uint4 nxt = __ldg(p + 1);
-                const uint32_t code = op.x & kOpMask;
-                if (code == kOpHalt) break;
-                // Value of the op: one sampler call site keeps the unrolled
-                // Philox body in the instruction cache once.
-                uint64_t v = 0;
-                if (code == kOpInBe || code == kOpBeDef) {
-                    v = be_word<MF, PF>(op.y, op.w, ctx, t3, op.z);
-                } else if (code == kOpInSlot) {
-                    v = load_slot(op.y, my_slots, my_scratch, NT, a.scratch_stride);
-                } else if (code == kOpInConst || code == kOpConstDef) {
-                    v = ((uint64_t)op.z << 32) | op.y;
-                }
-                if (code == kOpInBe || code == kOpInSlot || code == kOpInConst) {
-                    if (op.x & kNegBit) v = ~v;
-                    switch (conn) {
-                        case MCG_AND: case MCG_NAND: acc &= v; break;
-                        case MCG_OR: case MCG_NOR: acc |= v; break;
-                        case MCG_XOR: acc ^= v; break;
-                        case MCG_ATLEAST: cnt.add(v, nbits); break;
-                        default: acc = v; break;  // NOT, NULL: the last input wins
-                    }
-                } else if (code == kOpBeDef || code == kOpConstDef) {
-                    last = v;
-                    store_slot(op.x >> 8, last, my_slots, my_scratch, NT, a.scratch_stride);
-                } else if (code == kOpBegin) {
-                    conn = (op.x >> 8) & 0xFFu;
-                    kk = (op.x >> 16) & 0xFFu;
-                    nbits = (op.x >> 24) & 0xFu;
-                    acc = (conn == MCG_AND || conn == MCG_NAND) ? kAllOnes : 0ull;
-                    if (conn == MCG_ATLEAST) cnt.clear();
-                } else if (code == kOpEnd) {
-                    if (conn == MCG_ATLEAST) last = cnt.ge(kk);
-                    else if (conn == MCG_NAND || conn == MCG_NOR || conn == MCG_NOT) last = ~acc;
-                    else last = acc;
-                    store_slot(op.y, last, my_slots, my_scratch, NT, a.scratch_stride);
-                } else if (code == kOpTally) {
-                    uint32_t c = valid ? (uint32_t)__popcll(last) : 0u;
-                    c = __reduce_add_sync(0xFFFFFFFFu, c);
-                    if (lane == 0) atomicAdd(&tally[op.y], (unsigned long long)c);
-                }
-                op = nxt;
-                ++p;
-            }
+            interpret<NT, MF, PF, false>(a.ops, ctx, t3, j < a.word_count, my_slots, my_scratch, a.scratch_stride,
+                                         nullptr, add);
         }
     }
     if (a.tally_in_smem) {
@@ -165,6 +184,53 @@ __global__ void __launch_bounds__(NT, MINB) k_fused(FusedArgs a) {
             const unsigned long long c = s_tally[i];
             if (c) atomicAdd(&a.tally[i], c);
         }
+    }
+}
+
+// Batched instances (uncertainty analysis): a persistent work queue over
+// (instance, slab) items; an instance runs its tree's program with its own
+// threshold table over words [0, words_per_instance) of pass `iteration`
+// and counts the ones of every TALLY op into inst_ones[instance].
+struct BatchArgs {
+    const uint4 *ops;                  // all tree programs, concatenated
+    const uint32_t *tree_op_offset;    // first op of each tree's program
+    const uint32_t *inst_tree;         // tree of each instance
+    const uint64_t *inst_thr_offset;   // first threshold of each instance
+    const uint64_t *thr;               // thresholds (uint64, 0 .. 2^32)
+    uint32_t n_instances;
+    uint32_t slabs_per_instance;
+    uint64_t words_per_instance;
+    uint32_t iteration;
+    uint32_t smem_slots;
+    uint64_t *scratch;
+    uint64_t scratch_stride;
+    unsigned int *queue;               // next item; zero before the launch
+    unsigned long long *inst_ones;
+};
+
+template <int NT, int MINB, int MF, int PF>
+__global__ void __launch_bounds__(NT, MINB) k_fused_batch(BatchArgs a) {
+    extern __shared__ __align__(16) uint64_t smem[];
+    __shared__ unsigned int s_item;
+    const uint32_t tid = threadIdx.x;
+    const uint64_t gtid = (uint64_t)blockIdx.x * NT + tid;
+    uint64_t *my_slots = smem + tid;
+    uint64_t *my_scratch = a.scratch + gtid;
+    const uint32_t t3 = (a.iteration + 1u) << 6;
+    const unsigned int n_items = a.n_instances * a.slabs_per_instance;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        const unsigned int item = s_item;
+        if (item >= n_items) break;
+        const uint32_t inst = item / a.slabs_per_instance;
+        const uint64_t j = (uint64_t)(item % a.slabs_per_instance) * NT + tid;
+        const WordCtx ctx = make_word_ctx<MF>((uint32_t)j);
+        unsigned long long *ones = a.inst_ones + inst;
+        auto add = [ones](uint32_t, uint32_t c) { atomicAdd(ones, (unsigned long long)c); };
+        interpret<NT, MF, PF, true>(a.ops + a.tree_op_offset[a.inst_tree[inst]], ctx, t3, j < a.words_per_instance,
+                                    my_slots, my_scratch, a.scratch_stride, a.thr + a.inst_thr_offset[inst], add);
     }
 }
 
@@ -189,7 +255,7 @@ __global__ void __launch_bounds__(256) k_layer_be(const uint4 *__restrict__ be, 
 
 // One layer of gates; gate ids listed in layer_gates.  meta[g] = {op | k<<8, in_begin, in_count, neg_count}.
 // ATLEAST counts each bit lane with a uint8 counter, as the reference kernel does.
-__global__ void __launch_bounds__(256) k_layer_gates(const uint4 *__restrict__ meta, const uint32_t *__restrict__ inputs,
+static __global__ void __launch_bounds__(256) k_layer_gates(const uint4 *__restrict__ meta, const uint32_t *__restrict__ inputs,
                                                      const uint32_t *__restrict__ layer_gates, uint32_t n_layer,
                                                      uint32_t n_be, uint64_t W, uint64_t *__restrict__ buf) {
     const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -231,7 +297,7 @@ __global__ void __launch_bounds__(256) k_layer_gates(const uint4 *__restrict__ m
 
 // Tallies: popcount, block reduction, one atomic per block and node.
 // tally_idx (optional) maps row t of tally_nodes to its counter.
-__global__ void __launch_bounds__(256) k_layer_tally(const uint32_t *__restrict__ tally_nodes, uint32_t n_tally,
+static __global__ void __launch_bounds__(256) k_layer_tally(const uint32_t *__restrict__ tally_nodes, uint32_t n_tally,
                                                      uint64_t W, const uint64_t *__restrict__ buf,
                                                      unsigned long long *__restrict__ ones,
                                                      const uint32_t *__restrict__ tally_idx) {
@@ -257,10 +323,24 @@ __global__ void __launch_bounds__(256) k_layer_tally(const uint32_t *__restrict_
 // [0, n_be); phase B evaluates one layer of gates per launch into rows
 // n_be + g, with tallies fused.
 
-// Phase A: thread (w, group) samples word w of events [group * EPT, +EPT).
+// Per-pass event table (philox.cuh): thread (e, g) fills entry g of event e.
+template <int MF>
+__global__ void __launch_bounds__(256) k_event_table(const uint4 *__restrict__ be, uint32_t n_be, uint32_t t3,
+                                                     uint2 *__restrict__ table) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)n_be * kEventTableStride) return;
+    const uint32_t e = (uint32_t)(i / kEventTableStride);
+    const int g = (int)(i % kEventTableStride);
+    event_table_entry<MF>(be[e].x, t3, g, table[i]);
+}
+
+// Phase A: thread (w, group) samples word w of events [group * EPT, +EPT)
+// using the pass's event table.  Launched with dynamic shared memory that
+// only caps the blocks per SM, leaving room for gate-phase blocks.
 template <int MF, int PF, int EPT>
-__global__ void __launch_bounds__(256) k_stage_be(const uint4 *__restrict__ be, uint32_t n_be, uint64_t W,
-                                                  uint64_t word_begin, uint32_t t3, uint64_t *__restrict__ buf) {
+__global__ void __launch_bounds__(256) k_stage_be(const uint4 *__restrict__ be, const uint2 *__restrict__ table,
+                                                  uint32_t n_be, uint64_t W, uint64_t word_begin,
+                                                  uint64_t *__restrict__ buf) {
     const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t e0 = (blockIdx.y + gridDim.y * blockIdx.z) * EPT;
     if (w >= W || e0 >= n_be) return;
@@ -273,23 +353,24 @@ __global__ void __launch_bounds__(256) k_stage_be(const uint4 *__restrict__ be, 
         uint64_t v;
         if (r.w != 0) v = kAllOnes;           // threshold 2^32
         else if (r.z == 0) v = 0;             // threshold 0
-        else v = be_word<MF, PF>(r.x, r.y, ctx, t3, r.z);
+        else v = be_word_tab<MF, PF>(r.y, ctx, table + (uint64_t)e * kEventTableStride, r.z);
         buf[(uint64_t)e * W + w] = v;
     }
 }
 
-// Phase B: gate layer_gates[blockIdx.y] for words [blockIdx.x * 256 * WPT, ...),
-// WPT words per thread at stride 256 (coalesced).  meta[g] = {op | k << 8 |
+// Phase B: gate layer_gates[blockIdx.y] for words [blockIdx.x * NT * WPT, ...),
+// WPT words per thread at stride NT (coalesced).  meta[g] = {op | k << 8 |
 // nbits << 16, in_begin, in_count, neg_count}; gate_tally[g] = {offset, count}
 // into tally_list.  Each block adds its popcount once per tally entry.
-template <int WPT>
-__global__ void __launch_bounds__(256) k_stage_gates(const uint4 *__restrict__ meta, const uint32_t *__restrict__ inputs,
+template <int NT, int WPT>
+__global__ void __launch_bounds__(NT) k_stage_gates(const uint4 *__restrict__ meta, const uint32_t *__restrict__ inputs,
                                                      const uint32_t *__restrict__ layer_gates, uint32_t n_layer,
                                                      uint32_t n_be, uint64_t W, uint64_t *__restrict__ buf,
                                                      const uint2 *__restrict__ gate_tally,
                                                      const uint32_t *__restrict__ tally_list,
                                                      unsigned long long *__restrict__ ones) {
-    __shared__ uint32_t warp_sums[8];
+    constexpr uint32_t kMaxIn = 8;  // inputs loaded up front (memory-level parallelism)
+    __shared__ uint32_t warp_sums[NT / 32];
     const uint32_t li = blockIdx.y + gridDim.y * blockIdx.z;
     if (li >= n_layer) return;
     const uint32_t gi = layer_gates[li];
@@ -301,36 +382,81 @@ __global__ void __launch_bounds__(256) k_stage_gates(const uint4 *__restrict__ m
     const uint32_t off = n - m.w;
     const uint32_t *in = inputs + m.y;
     uint64_t *out = buf + (uint64_t)(n_be + gi) * W;
+    const uint64_t base = (uint64_t)blockIdx.x * NT * WPT + threadIdx.x;
+    uint64_t r[WPT];
+    if (n <= kMaxIn) {
+        uint64_t v[kMaxIn][WPT];
+#pragma unroll
+        for (uint32_t i = 0; i < kMaxIn; ++i) {
+            if (i < n) {
+                const uint64_t *row = buf + (uint64_t)in[i] * W;
+#pragma unroll
+                for (int k = 0; k < WPT; ++k) {
+                    const uint64_t w = base + (uint64_t)k * NT;
+                    v[i][k] = (w < W) ? row[w] : 0ull;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < WPT; ++k) {
+            if (op == MCG_ATLEAST) {
+                SlicedCount cnt;
+                cnt.clear();
+#pragma unroll
+                for (uint32_t i = 0; i < kMaxIn; ++i)
+                    if (i < n) cnt.add(i >= off ? ~v[i][k] : v[i][k], nbits);
+                r[k] = cnt.ge(kk);
+            } else {
+                uint64_t a = (op == MCG_AND || op == MCG_NAND) ? kAllOnes : 0ull;
+#pragma unroll
+                for (uint32_t i = 0; i < kMaxIn; ++i) {
+                    if (i < n) {
+                        const uint64_t x = i >= off ? ~v[i][k] : v[i][k];
+                        if (op == MCG_OR || op == MCG_NOR) a |= x;
+                        else if (op == MCG_AND || op == MCG_NAND) a &= x;
+                        else if (op == MCG_XOR) a ^= x;
+                        else a = x;
+                    }
+                }
+                r[k] = (op == MCG_NAND || op == MCG_NOR || op == MCG_NOT) ? ~a : a;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < WPT; ++k) {
+            const uint64_t w = base + (uint64_t)k * NT;
+            r[k] = 0;
+            if (w >= W) continue;
+            if (op == MCG_ATLEAST) {
+                SlicedCount cnt;
+                cnt.clear();
+                for (uint32_t i = 0; i < n; ++i) {
+                    const uint64_t x = buf[(uint64_t)in[i] * W + w];
+                    cnt.add(i >= off ? ~x : x, nbits);
+                }
+                r[k] = cnt.ge(kk);
+            } else {
+                uint64_t a = (op == MCG_AND || op == MCG_NAND) ? kAllOnes : 0ull;
+                for (uint32_t i = 0; i < n; ++i) {
+                    uint64_t x = buf[(uint64_t)in[i] * W + w];
+                    if (i >= off) x = ~x;
+                    if (op == MCG_OR || op == MCG_NOR) a |= x;
+                    else if (op == MCG_AND || op == MCG_NAND) a &= x;
+                    else if (op == MCG_XOR) a ^= x;
+                    else a = x;
+                }
+                r[k] = (op == MCG_NAND || op == MCG_NOR || op == MCG_NOT) ? ~a : a;
+            }
+        }
+    }
     uint32_t count = 0;
-    const uint64_t base = (uint64_t)blockIdx.x * 256 * WPT + threadIdx.x;
 #pragma unroll
     for (int k = 0; k < WPT; ++k) {
-        const uint64_t w = base + (uint64_t)k * 256;
-        if (w >= W) break;
-        uint64_t r;
-        if (op == MCG_ATLEAST) {
-            SlicedCount cnt;
-            cnt.clear();
-            for (uint32_t i = 0; i < n; ++i) {
-                uint64_t v = buf[(uint64_t)in[i] * W + w];
-                if (i >= off) v = ~v;
-                cnt.add(v, nbits);
-            }
-            r = cnt.ge(kk);
-        } else {
-            r = (op == MCG_AND || op == MCG_NAND) ? kAllOnes : 0ull;
-            for (uint32_t i = 0; i < n; ++i) {
-                uint64_t v = buf[(uint64_t)in[i] * W + w];
-                if (i >= off) v = ~v;
-                if (op == MCG_OR || op == MCG_NOR) r |= v;
-                else if (op == MCG_AND || op == MCG_NAND) r &= v;
-                else if (op == MCG_XOR) r ^= v;
-                else r = v;
-            }
-            if (op == MCG_NAND || op == MCG_NOR || op == MCG_NOT) r = ~r;
+        const uint64_t w = base + (uint64_t)k * NT;
+        if (w < W) {
+            out[w] = r[k];
+            count += (uint32_t)__popcll(r[k]);
         }
-        out[w] = r;
-        count += (uint32_t)__popcll(r);
     }
     const uint2 t = gate_tally[gi];
     if (t.y == 0) return;  // uniform per block
@@ -339,26 +465,37 @@ __global__ void __launch_bounds__(256) k_stage_gates(const uint4 *__restrict__ m
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long s = 0;
-        for (uint32_t i = 0; i < 8; ++i) s += warp_sums[i];
+        for (uint32_t i = 0; i < NT / 32; ++i) s += warp_sums[i];
         if (s)
             for (uint32_t j = 0; j < t.y; ++j) atomicAdd(&ones[tally_list[t.x + j]], s);
     }
 }
 
 // Register-only sampler: thread w generates words (e, w) for n_events events
-// and xors them together; one store per thread keeps the work alive.
+// (event e: pdag_idx + 1 = e + 3, event_idx + 1 = e + 1, table row e) and
+// xors them together; one store per thread keeps the work alive.  Same
+// sampler code as the product's sampling kernel.
 template <int MF, int PF>
-__global__ void __launch_bounds__(256) k_sampler_peak(uint32_t n_events, uint64_t n_words, uint32_t t3,
-                                                      uint64_t *__restrict__ sink) {
+__global__ void __launch_bounds__(256) k_sampler_peak(uint32_t n_events, uint64_t n_words,
+                                                      const uint2 *__restrict__ table, uint64_t *__restrict__ sink) {
     const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n_words) return;
     const WordCtx ctx = make_word_ctx<MF>((uint32_t)w);
     uint64_t x = 0;
     for (uint32_t e = 0; e < n_events; ++e) {
         const uint32_t thr = 0x01000000u + (e * 0x9E3779B9u >> 8);  // spread of probabilities
-        x ^= be_word<MF, PF>(e + 3u, e + 1u, ctx, t3, thr);
+        x ^= be_word_tab<MF, PF>(e + 1u, ctx, table + (uint64_t)e * kEventTableStride, thr);
     }
     sink[w] = x;
+}
+
+// Event table for k_sampler_peak's synthetic events.
+template <int MF>
+__global__ void __launch_bounds__(256) k_peak_table(uint32_t n_events, uint32_t t3, uint2 *__restrict__ table) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)n_events * kEventTableStride) return;
+    const uint32_t e = (uint32_t)(i / kEventTableStride);
+    event_table_entry<MF>(e + 3u, t3, (int)(i % kEventTableStride), table[i]);
 }
 
 }  // namespace dev

@@ -67,7 +67,7 @@ Op make_op(uint32_t w0, uint32_t w1 = 0, uint32_t w2 = 0, uint32_t w3 = 0) {
 
 }  // namespace
 
-std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &out) {
+std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &out, bool variable_thresholds) {
     out = Program{};
     const uint32_t nb = g.n_be;
     const uint32_t nn = g.n_nodes();
@@ -105,7 +105,7 @@ std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &
     for (uint32_t e = 0; e < nb; ++e) {
         if (!needed[e]) continue;
         const uint64_t thr = g.be_threshold[e];
-        if (thr == 0 || thr >= kFullThreshold)
+        if (!variable_thresholds && (thr == 0 || thr >= kFullThreshold))
             kind[e] = BeKind::kConst;
         else if (uses[e] == 1 && tally_of[e].empty())
             kind[e] = BeKind::kInline;
@@ -150,8 +150,8 @@ std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &
             ops.push_back(make_op(kOpConstDef | (kNoSlot << 8), (uint32_t)val, (uint32_t)(val >> 32)));
         } else {
             const size_t at = ops.size();
-            ops.push_back(make_op(kOpBeDef, (uint32_t)g.be_pdag_idx[e] + 1u, (uint32_t)g.be_threshold[e],
-                                  g.be_event_idx[e] + 1u));
+            ops.push_back(make_op(kOpBeDef, (uint32_t)g.be_pdag_idx[e] + 1u,
+                                  variable_thresholds ? e : (uint32_t)g.be_threshold[e], g.be_event_idx[e] + 1u));
             if (uses[e] > 0) def_sites.push_back({at, e});
             else ops[at].w[0] |= (kNoSlot << 8);
         }
@@ -173,7 +173,7 @@ std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &
                 ops.push_back(make_op(kOpInConst | neg, (uint32_t)val, (uint32_t)(val >> 32)));
             } else if (c < nb && kind[c] == BeKind::kInline) {
                 ops.push_back(make_op(kOpInBe | neg, (uint32_t)g.be_pdag_idx[c] + 1u,
-                                      (uint32_t)g.be_threshold[c], g.be_event_idx[c] + 1u));
+                                      variable_thresholds ? c : (uint32_t)g.be_threshold[c], g.be_event_idx[c] + 1u));
                 ++out.n_inline_be;
                 ++out.n_be_sampled;
             } else {

@@ -24,6 +24,11 @@ struct Program {
 // evaluated.  smem_slot_budget bounds the shared-memory slots; values that do
 // not fit go to global scratch slots (linear-scan allocation that spills the
 // live value with the furthest last use).
-std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &out);
+//
+// With variable_thresholds the basic-event ops carry the event's node id in
+// place of its threshold (w2), for kernels that read thresholds from a
+// per-instance table, and no event is treated as a constant word.
+std::string compile_program(const Graph &g, uint32_t smem_slot_budget, Program &out,
+                            bool variable_thresholds = false);
 
 }  // namespace mcg

@@ -17,9 +17,10 @@ ALL = np.uint64(0xFFFFFFFFFFFFFFFF)
 AND, OR, ATLEAST, XOR, NOT, NAND, NOR, NULL = range(8)
 
 
-def emulate(ops: np.ndarray, g, words: np.ndarray, n_tally: int):
+def emulate(ops: np.ndarray, g, words: np.ndarray, n_tally: int, variable_thresholds: bool = False):
     """Returns (tally_values, ones): tally_values[i] is the word vector the
-    program counted for tally i (last TALLY wins), ones[i] its popcount sum."""
+    program counted for tally i (last TALLY wins), ones[i] its popcount sum.
+    With variable_thresholds the basic-event ops carry node ids in w2."""
     W = words.shape[1]
     by_counter = {}
     for e in range(g.n_be):
@@ -44,6 +45,10 @@ def emulate(ops: np.ndarray, g, words: np.ndarray, n_tally: int):
             smem[ref] = v.copy()
 
     def be_value(op):
+        if variable_thresholds:
+            e = int(op[2])
+            assert (int(g.be_pdag_idx[e]) + 1, int(g.be_event_idx[e]) + 1) == (int(op[1]), int(op[3]))
+            return words[e]
         key = (int(op[1]), int(op[3]), int(op[2]))
         return words[by_counter[key]]
 

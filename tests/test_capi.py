@@ -36,13 +36,6 @@ def test_version_and_error_strings(capi):
     assert capi.load().mcg_last_error() is not None
 
 
-def _bad(g, capi, msg_part):
-    with pytest.raises(capi.McgError) as ei:
-        capi.Engine(g)
-    assert ei.value.code == capi.MCG_ERR_INVALID
-    assert msg_part in str(ei.value)
-
-
 def _graph(**kw):
     base = dict(be_pdag_idx=[2, 3], be_event_idx=[0, 1], be_threshold=[1 << 30, 1 << 31], gate_op=[AND],
                 gate_k=[0], gate_in_begin=[0], gate_in_count=[2], gate_neg_count=[0], inputs=[0, 1],
@@ -64,8 +57,6 @@ def test_rejects_malformed_graphs(capi):
         (dict(gate_in_count=[5]), "inputs out of range"),
     ]:
         g = _graph(**kw)
-        view = capi.GraphView.__new__(capi.GraphView)
-        capi.GraphView.__init__.__wrapped__ if False else None
         # build the descriptor without python-side validation
         p = lambda a, t: a.ctypes.data_as(C.POINTER(t))
         keep = [g.be_pdag_idx, g.be_event_idx, g.be_threshold, g.gate_pdag_idx, g.gate_op, g.gate_k,
@@ -81,7 +72,7 @@ def test_rejects_malformed_graphs(capi):
         assert rc == capi.MCG_ERR_INVALID, (kw, rc)
         assert msg in lib.mcg_last_error().decode(), (kw, lib.mcg_last_error())
         info = capi.ProgramInfo()
-        assert lib.mcg_compile(C.byref(desc), 8, C.byref(info), None, 0) == capi.MCG_ERR_INVALID
+        assert lib.mcg_compile(C.byref(desc), 8, 0, C.byref(info), None, 0) == capi.MCG_ERR_INVALID
         del keep
 
 

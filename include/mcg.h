@@ -178,6 +178,39 @@ mcg_status mcg_time_runs(mcg_engine *engine, uint32_t iteration_first, uint64_t 
 mcg_status mcg_profile_sampler(mcg_engine *engine, int32_t enable);
 mcg_status mcg_profile_sampler_read(mcg_engine *engine, uint64_t *launches, double *total_ms);
 
+/* Fused Monte Carlo pass that allocates no device memory.  No counterpart in
+ * the reference, whose engine allocates every buffer it uses.
+ *
+ * For callers that cannot call cudaMalloc: work enqueued while a CUDA graph
+ * is being captured, processes whose device memory comes from their own
+ * pool or a fixed budget, and services that cannot afford the implicit
+ * synchronisation of cudaMalloc/cudaFree.  The caller compiles the program
+ * on the host with mcg_compile (flags 0), copies its n_ops ops (16 bytes
+ * each) to device memory it owns (d_ops, 16-byte aligned) and passes a
+ * device array d_ones of n_tally uint64 counters; smem_slots and
+ * global_slots are the program's own counts from mcg_compile's info.  The
+ * kernel adds each tallied node's ones over passes
+ * [iteration_first, iteration_first + n_iterations) and words
+ * [word_begin, word_begin + word_count) into d_ones (zero it first for fresh
+ * counts), asynchronously on `stream` (NULL = the default stream) of the
+ * current device.
+ *
+ * Values the program keeps outside shared memory go to one static device
+ * array of MCG_NOALLOC_SCRATCH_BYTES per device, which every GPU that loads
+ * the library holds until the process exits.  Programs whose global slots
+ * need more than that at full occupancy (global_slots x SMs x 2 CTAs x 256
+ * threads x 8 bytes) are rejected with MCG_ERR_INVALID; compile them with a
+ * larger shared-memory budget or use mcg_create / mcg_run.  All calls share
+ * the array, so calls that overlap on the GPU (concurrent streams, or
+ * another device context of the same process on the same GPU) race and give
+ * wrong counts; serialise them.  The first call on a device resolves the
+ * array's address and sets the kernel's shared-memory limit, so make that
+ * first call before any stream capture on that device. */
+#define MCG_NOALLOC_SCRATCH_BYTES (32ull << 20)
+mcg_status mcg_run_fused_noalloc(const void *d_ops, uint64_t n_ops, uint32_t smem_slots, uint32_t global_slots,
+                                 uint64_t *d_ones, uint32_t n_tally, uint32_t iteration_first, uint32_t n_iterations,
+                                 uint64_t word_begin, uint64_t word_count, void *stream);
+
 /* Register-only sampler rate: basic-event words generated per second by a
  * kernel that only runs the Philox sampler (no memory traffic besides one
  * store per thread).  The speed of light of the fused kernel. */

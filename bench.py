@@ -52,8 +52,13 @@ def parse_args():
     ap.add_argument("--mode", default="staged", choices=["fused", "staged", "layered"])
     ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")
     ap.add_argument("--sampler-blocks", type=int, default=0, help="staged: sampler blocks per SM (0 = default)")
-    ap.add_argument("--workload", default="plain", choices=["plain", "ua"],
-                    help="plain: the 5,000-event tree (headline); ua: batched uncertainty analysis")
+    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is"],
+                    help="plain: the 5,000-event tree (headline); ua: batched uncertainty analysis; "
+                         "is: GPU time to 5%% relative error on the 1e-8 tree, learned IS vs plain")
+    ap.add_argument("--is-rounds", type=int, default=5)
+    ap.add_argument("--is-round-words", type=int, default=1 << 20, help="words per CE round (2^26 samples)")
+    ap.add_argument("--is-batch-words", type=int, default=1 << 20)
+    ap.add_argument("--plain-words", type=int, default=1 << 23, help="words of the plain-MC rate measurement")
     ap.add_argument("--ua-trees", type=int, default=512)
     ap.add_argument("--ua-draws", type=int, default=16)
     ap.add_argument("--ua-words", type=int, default=1 << 16)
@@ -244,6 +249,67 @@ def run_ua(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
+def run_is(args, rank: int, world: int, local: int) -> int:
+    """GPU time to a 5% relative error (95% confidence) on the 2,000-event tree
+    whose exact top-event probability is ~1e-8: the learned-IS pipeline
+    (cross-entropy rounds with on-GPU MLP training, then IS batches until the
+    target) measured end to end, against the plain sampler's time derived
+    from its rate measured on the same tree."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    from mcscram_b200 import _capi, synth
+    from mcscram_b200.importance import ImportanceSampler, cross_entropy, estimate
+
+    torch.cuda.set_device(local)
+    g = synth.config4().with_tallies([])
+    g = g.with_tallies([g.root])
+    # plain sampler rate on this tree (staged pipeline, inputs resident)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    with _capi.Engine(g, device=local, stream=stream.cuda_stream, mode=_capi.MODE_STAGED) as e:
+        for i in range(args.warmup):
+            e.run(1 + i, 1, 0, 1 << 20)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e.run(100, 1, 0, args.plain_words)
+        b.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = a.elapsed_time(b)
+        ones, total = e.tallies()
+    plain_rate = args.plain_words * 64 / (plain_ms * 1e-3)  # samples / s
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    with ImportanceSampler(g, device=local) as s:
+        q, mlp, hist = cross_entropy(g, rounds=args.is_rounds, words_per_round=args.is_round_words, sampler=s,
+                                     device=local)
+        res = estimate(s, q, target_rel_err=0.05, words_per_batch=args.is_batch_words)
+    torch.cuda.synchronize()
+    is_wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    mlp.close()
+    p_hat = res["estimate"]
+    n_req = 1.959963984540054 ** 2 * (1 - p_hat) / (p_hat * 0.05 ** 2) if p_hat > 0 else float("inf")
+    plain_s = n_req / plain_rate
+    print(json.dumps({
+        "metric": "GPU time to 5% rel err at P_top~1e-8", "value": is_wall, "unit": "s", "n_gpus": 1,
+        "higher_is_better": False, "vs_baseline": None, "dtype": "u64 sampling, fp64 weights, bf16/fp32 MLP",
+        "data": "synthetic", "steps": 1, "warmup": args.warmup,
+        "config": {"workload": "2,000-event / 1,200-gate rare-event tree (seed 49), learned IS (CE rounds "
+                               f"{args.is_rounds} x {args.is_round_words * 64} samples) vs plain MC"},
+        "is": {"estimate": p_hat, "rel_err95": res["rel_err95"], "samples": res["samples"], "hits": res["hits"],
+               "ess": res["ess"], "fallback": res["fallback"], "wall_s": is_wall,
+               "gpu_s": (hist.gpu_ms + res["gpu_ms"]) * 1e-3, "ce_rounds": hist.rounds},
+        "plain": {"samples_per_s": plain_rate, "required_samples": n_req, "seconds": plain_s,
+                  "measured_words": args.plain_words, "measured_ms": plain_ms,
+                  "note": "time derived from the rate measured on this tree"},
+        "speedup": plain_s / is_wall, "clocks": clk}), flush=True)
+    return 0
+
+
 def main() -> int:
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -253,12 +319,14 @@ def main() -> int:
         return run_reference(args, rank, world)
     if args.workload == "ua":
         return run_ua(args, rank, world, local)
+    if args.workload == "is":
+        return run_is(args, rank, world, local)
 
     import numpy as np
     import torch
     import torch.distributed as dist
 
-    from mcscram_b200 import _capi, synth
+    from mcscram_b200 import _capi, parallel, synth
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -266,9 +334,7 @@ def main() -> int:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     g = synth.config2()
     W = args.words
-    word_begin = rank * W
-    if word_begin + W > (1 << 32):
-        raise SystemExit("word range exceeds the 32-bit sample counter")
+    word_begin, W = parallel.weak_shard(W, rank)  # weak scaling: W words per rank
     # one dedicated stream for the engine and for every torch op and event here
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -279,11 +345,11 @@ def main() -> int:
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     def allreduce_tallies():
+        # the one exchange of the multi-GPU path: sum of uint64 tallies over ranks (NCCL)
         if world == 1:
             return
         ones, total = eng.tallies()
-        t = torch.from_numpy(ones.astype(np.int64)).cuda()
-        dist.all_reduce(t)
+        parallel.allreduce_tallies(ones)
 
     # warm-up passes (iterations 1..W); then the timed passes continue the numbering
     for i in range(args.warmup):
@@ -319,9 +385,7 @@ def main() -> int:
     elapsed_ms = t_start.elapsed_time(t_end)
     run_ms = sum(a.elapsed_time(b) for a, b in ev_run)
     if world > 1:
-        t = torch.tensor([elapsed_ms, run_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms, run_ms = float(t[0]), float(t[1])
+        elapsed_ms, run_ms = parallel.allreduce_max([elapsed_ms, run_ms])
     ms_per_step = elapsed_ms / args.steps
     samples = W * 64 * world
     value = g.n_gates * samples / (ms_per_step * 1e-3)
@@ -357,9 +421,7 @@ def main() -> int:
                 ones, total = e2.tallies()
             ts.append(time.perf_counter() - t0)
         if world > 1:
-            t = torch.tensor([max(ts)], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ts = [float(t[0])]
+            ts = parallel.allreduce_max([max(ts)])
         e2e_s = statistics.median(ts)
         h2d = (info["n_ops"] * 16 + g.n_be * 16 + g.n_gates * 20 + g.inputs.size * 4 + g.tally_nodes.size * 4)
         e2e = {"value": g.n_gates * samples / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

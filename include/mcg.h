@@ -87,8 +87,8 @@ typedef struct mcg_run_desc {
     uint32_t ctas_per_sm;     /* fused kernel persistent CTAs per SM; 0 = auto */
     uint64_t chunk_words;     /* words per launch in one mcg_run; 0 = auto */
     uint64_t layered_max_words; /* layered/staged modes: words materialised per chunk; 0 = auto */
-    uint32_t sampler_blocks_per_sm; /* staged mode: sampler blocks resident per SM, which leaves
-                                       room for gate-phase blocks; 0 = 6, 8 = no cap */
+    uint32_t sampler_blocks_per_sm; /* staged mode: cap on sampler blocks per SM, to leave room for
+                                       gate-phase blocks; 0 or 8 = no cap (measured best) */
 } mcg_run_desc;
 
 typedef struct mcg_engine mcg_engine;

@@ -231,7 +231,7 @@ mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
     // footprint, so gate-phase blocks (memory bound) can run next to them.
     cudaDeviceProp prop;
     MCG_CUDA(cudaGetDeviceProperties(&prop, e->device));
-    const uint32_t blocks = run.sampler_blocks_per_sm ? run.sampler_blocks_per_sm : 6u;
+    const uint32_t blocks = run.sampler_blocks_per_sm ? run.sampler_blocks_per_sm : 8u;
     if (blocks < 1 || blocks > 8) return mcg::fail(MCG_ERR_INVALID, "sampler_blocks_per_sm must be 1..8");
     e->sampler_smem = blocks >= 8 ? 0u : (uint32_t)(prop.sharedMemPerMultiprocessor / blocks - 2048);
     MCG_CUDA(cudaFuncSetAttribute(mcg::dev::k_stage_be<kMulForm, kPackForm, kStageEventsPerThread>,

@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256) k_event_table(const uint4 *__restrict__ b
 // using the pass's event table.  Launched with dynamic shared memory that
 // only caps the blocks per SM, leaving room for gate-phase blocks.
 template <int MF, int PF, int EPT>
-__global__ void __launch_bounds__(256) k_stage_be(const uint4 *__restrict__ be, const uint2 *__restrict__ table,
+__global__ void __launch_bounds__(256, 6) k_stage_be(const uint4 *__restrict__ be, const uint2 *__restrict__ table,
                                                   uint32_t n_be, uint64_t W, uint64_t word_begin,
                                                   uint64_t *__restrict__ buf) {
     const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;

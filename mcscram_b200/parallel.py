@@ -1,0 +1,65 @@
+"""Multi-GPU plumbing: sample-word sharding and the tally all-reduce.
+
+Word w of a pass depends only on (pdag_idx, event_idx, w, pass) (mcSCRAM
+src/mc/kernel/basic_event.h:112-122), so any partition of the word range
+gives bit-identical words on every GPU, and tallies are plain sums.  Ranks
+take contiguous word ranges (or whole instances for batched work) and the
+only exchange is one all-reduce of the uint64 tallies per convergence step,
+over NCCL (NVLink / NVSwitch) on GPUs or gloo on CPUs.
+"""
+from __future__ import annotations
+
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+
+def shard_words(word_begin: int, word_count: int, world: int, rank: int) -> Tuple[int, int]:
+    """Contiguous, balanced share [begin, begin + count) of a word range for
+    `rank` of `world` (the first word_count % world ranks get one more)."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("rank must lie in [0, world)")
+    base, extra = divmod(word_count, world)
+    begin = word_begin + rank * base + min(rank, extra)
+    return begin, base + (1 if rank < extra else 0)
+
+
+def weak_shard(words_per_rank: int, rank: int, word_begin: int = 0) -> Tuple[int, int]:
+    """Fixed work per rank: rank r takes [begin + r * W, begin + (r + 1) * W)."""
+    b = word_begin + rank * words_per_rank
+    if b + words_per_rank > (1 << 32):
+        raise ValueError("word range exceeds the 32-bit sample counter")
+    return b, words_per_rank
+
+
+def shard_items(n_items: int, world: int, rank: int) -> List[int]:
+    """Round-robin assignment of independent items (trees, instances)."""
+    return list(range(rank, n_items, world))
+
+
+def allreduce_tallies(ones: np.ndarray, group=None, device: Optional[str] = None) -> np.ndarray:
+    """Sum of every rank's uint64 counters (tallies stay below 2^63)."""
+    import torch
+    import torch.distributed as dist
+
+    a = np.ascontiguousarray(ones, dtype=np.uint64)
+    if np.any(a >= np.uint64(1 << 63)):
+        raise OverflowError("tally does not fit a signed 64-bit reduction")
+    t = torch.from_numpy(a.astype(np.int64))
+    if device is None:
+        device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = t.to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy().astype(np.uint64)
+
+
+def allreduce_max(values: Sequence[float], group=None, device: Optional[str] = None) -> List[float]:
+    """Element-wise maximum over ranks (for timings: the slowest rank counts)."""
+    import torch
+    import torch.distributed as dist
+
+    if device is None:
+        device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return [float(x) for x in t.cpu()]

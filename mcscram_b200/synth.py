@@ -349,3 +349,101 @@ def config3(n_trees: int = 512, seed: int = 3) -> list:
                                        seed=int(rng.integers(1 << 31)), share_be_frac=0.2,
                                        name=f"config3-tree{t}-{b}be-{g}g")))
     return trees
+
+
+def read_once_probability(g: FlatGraph, p: Optional[np.ndarray] = None) -> np.ndarray:
+    """Exact probability of every node of a read-once tree (no node with more
+    than one parent): AND = prod p, OR = 1 - prod (1 - p), XOR of two, NOT,
+    ATLEAST k-of-n by the usual count recursion.  Used to calibrate generated
+    rare-event instances; raises for graphs with shared nodes."""
+    fanout = np.bincount(g.inputs, minlength=g.n_nodes)
+    if np.any(fanout > 1):
+        raise ValueError("read_once_probability needs a tree (a node has several parents)")
+    pr = np.zeros(g.n_nodes)
+    pr[: g.n_be] = g.quantised_probabilities() if p is None else p
+    from .graph import NAND, NOR, NULL
+    for gi in range(g.n_gates):
+        ins = g.gate_inputs(gi)
+        off = int(g.gate_in_count[gi] - g.gate_neg_count[gi])
+        v = np.array([pr[c] if i < off else 1.0 - pr[c] for i, c in enumerate(ins)])
+        op = int(g.gate_op[gi])
+        if op in (AND, NAND):
+            r = float(np.prod(v)) if v.size else 1.0
+        elif op in (OR, NOR):
+            r = 1.0 - float(np.prod(1.0 - v)) if v.size else 0.0
+        elif op == XOR:
+            r = 0.0
+            for x in v:
+                r = r * (1 - x) + (1 - r) * x
+        elif op == ATLEAST:
+            k = int(g.gate_k[gi]) & 0xFF
+            dist = np.zeros(v.size + 1)
+            dist[0] = 1.0
+            for x in v:
+                dist[1:] = dist[1:] * (1 - x) + dist[:-1] * x
+                dist[0] *= 1 - x
+            r = float(dist[k:].sum()) if k <= v.size else 0.0
+        else:  # NOT, NULL: the last input
+            r = float(v[-1]) if v.size else 0.0
+        if op in (NAND, NOR, NOT):
+            r = 1.0 - r
+        pr[g.n_be + gi] = r
+    return pr
+
+
+def calibrate_rare(g: FlatGraph, target: float, p_floor: float = 1e-9, p_cap: float = 0.5) -> FlatGraph:
+    """Rescales the basic-event probabilities of a read-once tree as
+    p -> clip(p^gamma, p_floor, p_cap), bisecting gamma until the exact top
+    probability (at the quantised thresholds) is within 1 % of `target`."""
+    base = np.clip(g.quantised_probabilities(), 1e-12, 1.0)
+
+    def top(gamma):
+        p = np.clip(base ** gamma, p_floor, p_cap)
+        thr = probability_threshold(p)
+        return read_once_probability(g, thr.astype(np.float64) / (1 << 32))[g.root], thr
+
+    lo, hi = 0.05, 20.0  # top probability decreases with gamma
+    t_lo, _ = top(lo)
+    t_hi, _ = top(hi)
+    if not (t_hi <= target <= t_lo):
+        raise ValueError(f"target {target:g} outside the reachable range [{t_hi:g}, {t_lo:g}]")
+    thr = None
+    for _ in range(200):
+        mid = np.sqrt(lo * hi)
+        t, thr = top(mid)
+        if t > 0 and abs(np.log(t / target)) < 0.01:
+            break
+        if t > target:
+            lo = mid
+        else:
+            hi = mid
+    out = g.with_thresholds(thr)
+    out.be_prob = thr.astype(np.float64) / (1 << 32)
+    out.meta = dict(g.meta, target_p_top=target, exact_p_top=float(t))
+    return out
+
+
+def config5(n_instances: int = 1024, seed: int = 5) -> list:
+    """Batched rare-event instances: basic events log-uniform in [50, 10,000]
+    (gates = events / 1.6), alternating AND-heavy (60/30/10 AND/OR/ATLEAST) and
+    ATLEAST-heavy (30/30/40) mixes, read-once trees whose base probabilities
+    (log-uniform [1e-6, 1e-3]) are rescaled so that the exact top-event
+    probability is a target drawn log-uniformly from [1e-10, 1e-5]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n_instances:
+        i = len(out)
+        nb = int(round(np.exp(rng.uniform(np.log(50), np.log(10000)))))
+        and_heavy = i % 2 == 0
+        mix = {AND: 0.6, OR: 0.3, ATLEAST: 0.1} if and_heavy else {AND: 0.3, OR: 0.3, ATLEAST: 0.4}
+        # a tree needs events + gates - 1 inputs; ATLEAST gates take 3-5, so that mix gets fewer gates
+        ng = max(4, int(round(nb / (1.6 if and_heavy else 2.0))))
+        target = float(np.exp(rng.uniform(np.log(1e-10), np.log(1e-5))))
+        try:
+            g = generate(TreeSpec(n_be=nb, n_gates=ng, mix=mix, p_range=(1e-6, 1e-3),
+                                  seed=int(rng.integers(1 << 31)), atleast_n=(3, 5), share_be_frac=0.0,
+                                  name=f"config5-{i}-{nb}be"))
+            out.append(calibrate_rare(g, target))
+        except ValueError:
+            continue  # infeasible draw or unreachable target: draw another
+    return out

@@ -52,6 +52,38 @@ mcg_status mcg_is_destroy(mcg_is *is);
 mcg_status mcg_is_run(mcg_is *is, const uint64_t *q_threshold, uint32_t iteration, uint64_t word_begin,
                       uint64_t word_count, mcg_is_result *result, double *ce_num);
 
+/* Batched form: many independent trees joined into one graph (no node read
+ * by two trees), sampled together in one staged pass per call.  Tree k owns
+ * basic events [be_begin[k], be_begin[k + 1]) (be_begin has n_tree + 1
+ * entries, from 0 to n_be) and its top event is graph->tally_nodes[k]
+ * (n_tally == n_tree); create rejects graphs where a gate reads two trees
+ * or a tallied node is not in its tree.  Each tree gets its own likelihood
+ * ratio (the C and a_i of its events) and its own sums. */
+typedef struct mcg_is_batch mcg_is_batch;
+
+mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_tree, const uint32_t *be_begin,
+                               const mcg_run_desc *run, mcg_is_batch **out);
+mcg_status mcg_is_batch_destroy(mcg_is_batch *b);
+
+/* Samples pass `iteration`, words [word_begin, word_begin + word_count) of
+ * every tree with proposal thresholds q_threshold[n_be] (rules as for
+ * mcg_is_run).  With a defensive proposal (q_defensive[n_be], words_defensive
+ * > 0) the first words_defensive words are drawn from q_defensive and the
+ * rest from q_threshold, and every sample is weighted by the balance
+ * heuristic of multiple importance sampling,
+ *     w = p(x) / (alpha q_defensive(x) + (1 - alpha) q(x)),
+ *     alpha = words_defensive / word_count,
+ * which stays unbiased and bounds the variance by 1 / alpha times that of
+ * the defensive proposal alone (a failure region the proposal misses is
+ * still sampled).  q_defensive may be NULL when words_defensive is 0.
+ * tree_sums (host, 4 * n_tree doubles) receives per tree {sum w, sum w^2,
+ * hits, max log w} over its word_count * 64 samples; ce_num (host, n_be
+ * doubles, optional) sum over hits of w * x_i; kernel_ms (optional) the
+ * device time of the call (CUDA events). */
+mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_threshold, const uint64_t *q_defensive,
+                            uint64_t words_defensive, uint32_t iteration, uint64_t word_begin, uint64_t word_count,
+                            double *tree_sums, double *ce_num, double *kernel_ms);
+
 /* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
  * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32
  * accumulation), FP32 master weights and Adam state.  Parameter layout

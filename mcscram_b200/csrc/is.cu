@@ -114,6 +114,159 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights(const uint64_t *_
     }
 }
 
+// Batched form: many independent trees in one graph, tree k owning basic
+// events [be_begin[k], be_begin[k + 1]) and tallied root root_row[k].
+// Work items are (tree, strip of 256 words), taken from a queue (a counter
+// zeroed before the launch) so that trees of very different size balance.
+// One thread per word: the buffer rows are read coalesced, and because
+// x_i & top is almost always zero under a proposal, the FP64 log-ratio of a
+// sample is only touched where event i fired in a sample where the tree's
+// top event fired.  acc[] (per-thread, local memory) holds the running
+// sum of a_i of sample b, later its weight.
+// With a defensive proposal (a_def != null) every sample is weighted by the
+// balance heuristic of multiple importance sampling,
+//     w = p(x) / (alpha q_def(x) + (1 - alpha) q(x)),
+//     log w = -logaddexp(ln alpha - log(p/q_def), ln(1 - alpha) - log(p/q)),
+// whichever of the two proposals drew it; accd[] holds log(p/q_def).
+struct IsBatchArgs {
+    const uint64_t *buf;
+    uint64_t W;
+    uint32_t n_inst;
+    uint32_t strips;               // ceil(W / kWeightThreads)
+    const uint32_t *be_begin;      // n_inst + 1
+    const uint32_t *root_row;      // n_inst
+    const double *a;               // per event
+    const double *C;               // per tree
+    const double *a_def;           // defensive proposal's terms, or null
+    const double *C_def;
+    double log_alpha, log_1m_alpha;  // share of the samples the defensive proposal draws
+    double *sums;                  // per tree: sum w, sum w^2, hits, max log w
+    double *ce;                    // per event, or null
+    unsigned long long *queue;
+};
+
+__global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs p) {
+    __shared__ unsigned long long s_item;
+    double acc[64], accd[64];
+    const bool mix = p.a_def != nullptr;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t items = (uint64_t)p.n_inst * p.strips;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1ull);
+        __syncthreads();
+        const uint64_t item = s_item;
+        __syncthreads();
+        if (item >= items) break;
+        const uint32_t k = (uint32_t)(item / p.strips);
+        const uint64_t w = (item % p.strips) * kWeightThreads + threadIdx.x;
+        const bool valid = w < p.W;
+        const uint64_t top = valid ? p.buf[(uint64_t)p.root_row[k] * p.W + w] : 0ull;
+        if (!__syncthreads_or(top != 0ull)) continue;
+        for (uint64_t m = top; m; m &= m - 1) {
+            acc[__ffsll((long long)m) - 1] = 0.0;
+            accd[__ffsll((long long)m) - 1] = 0.0;
+        }
+        const uint32_t b0 = p.be_begin[k], b1 = p.be_begin[k + 1];
+        const uint64_t *col = p.buf + w;
+        uint32_t i = b0;
+        for (; i + 4 <= b1; i += 4) {
+            uint64_t x[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) x[j] = valid ? col[(uint64_t)(i + j) * p.W] : 0ull;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                uint64_t m = x[j] & top;
+                if (m) {
+                    const double ai = p.a[i + j], di = mix ? p.a_def[i + j] : 0.0;
+                    do {
+                        const int b = __ffsll((long long)m) - 1;
+                        acc[b] += ai;
+                        accd[b] += di;
+                        m &= m - 1;
+                    } while (m);
+                }
+            }
+        }
+        for (; i < b1; ++i) {
+            uint64_t m = (valid ? col[(uint64_t)i * p.W] : 0ull) & top;
+            if (m) {
+                const double ai = p.a[i], di = mix ? p.a_def[i] : 0.0;
+                do {
+                    const int b = __ffsll((long long)m) - 1;
+                    acc[b] += ai;
+                    accd[b] += di;
+                    m &= m - 1;
+                } while (m);
+            }
+        }
+        const double C = p.C[k], Cd = mix ? p.C_def[k] : 0.0;
+        double lsum = 0.0, lsum2 = 0.0, lhits = 0.0, lmax = -INFINITY;
+        for (uint64_t m = top; m; m &= m - 1) {
+            const int b = __ffsll((long long)m) - 1;
+            double lw = C + acc[b];
+            if (mix) {
+                const double u1 = p.log_alpha - (Cd + accd[b]), u2 = p.log_1m_alpha - lw;
+                const double hi = fmax(u1, u2), lo = fmin(u1, u2);
+                lw = -(hi + log1p(exp(lo - hi)));
+            }
+            const double wv = exp(lw);
+            acc[b] = wv;
+            lsum += wv;
+            lsum2 += wv * wv;
+            lhits += 1.0;
+            lmax = fmax(lmax, lw);
+        }
+        if (p.ce) {
+            for (uint32_t e = b0; e < b1; ++e) {
+                uint64_t m = (valid ? col[(uint64_t)e * p.W] : 0ull) & top;
+                double c = 0.0;
+                for (; m; m &= m - 1) c += acc[__ffsll((long long)m) - 1];
+                if (__any_sync(0xFFFFFFFFu, c != 0.0)) {
+                    c = warp_sum(c);
+                    if (lane == 0 && c != 0.0) atomicAdd(&p.ce[e], c);
+                }
+            }
+        }
+        lsum = warp_sum(lsum);
+        lsum2 = warp_sum(lsum2);
+        lhits = warp_sum(lhits);
+        lmax = warp_max(lmax);
+        if (lane == 0 && lhits != 0.0) {
+            double *out = p.sums + 4ull * k;
+            atomicAdd(&out[0], lsum);
+            atomicAdd(&out[1], lsum2);
+            atomicAdd(&out[2], lhits);
+            atomic_max_double(&out[3], lmax);
+        }
+    }
+}
+
+// Proposal table and log-ratio terms at the quantised probabilities, for the
+// events [b0, b1): beq[i] (the sampler's layout), a[i], and the sum of the
+// constant terms over the range.  Returns false with `why` set on a bad q.
+bool ratio_terms(const mcg::Graph &g, const uint64_t *q_thr, uint32_t b0, uint32_t b1, uint4 *beq, double *a,
+                 double &C, std::string &why) {
+    const double two32 = 4294967296.0;
+    C = 0.0;
+    for (uint32_t i = b0; i < b1; ++i) {
+        const uint64_t tp = g.be_threshold[i], tq = q_thr[i];
+        const bool fixed = tp == 0 || tp >= (1ull << 32);
+        if (fixed ? tq != tp : (tq == 0 || tq >= (1ull << 32))) {
+            why = "proposal threshold " + std::to_string(i) +
+                  " must lie in [1, 2^32 - 1] (or equal a constant nominal one)";
+            return false;
+        }
+        beq[i] = make_uint4((uint32_t)g.be_pdag_idx[i] + 1u, g.be_event_idx[i] + 1u, (uint32_t)tq, (uint32_t)(tq >> 32));
+        a[i] = 0.0;
+        if (fixed) continue;
+        const double p = (double)tp / two32, q = (double)tq / two32;
+        const double l1 = std::log1p(-p) - std::log1p(-q);
+        a[i] = std::log(p) - std::log(q) - l1;
+        C += l1;
+    }
+    return true;
+}
+
 }  // namespace
 
 struct mcg_is {
@@ -191,20 +344,8 @@ mcg_status mcg_is_run(mcg_is *is, const uint64_t *q_thr, uint32_t iteration, uin
     std::vector<double> a(nb, 0.0);
     double C = 0.0;
     std::vector<uint4> beq(nb);
-    const double two32 = 4294967296.0;
-    for (uint32_t i = 0; i < nb; ++i) {
-        const uint64_t tp = g.be_threshold[i], tq = q_thr[i];
-        const bool fixed = tp == 0 || tp >= (1ull << 32);
-        if (fixed ? tq != tp : (tq == 0 || tq >= (1ull << 32)))
-            return mcg::fail(MCG_ERR_INVALID, "proposal threshold " + std::to_string(i) +
-                                                  " must lie in [1, 2^32 - 1] (or equal a constant nominal one)");
-        beq[i] = make_uint4((uint32_t)g.be_pdag_idx[i] + 1u, g.be_event_idx[i] + 1u, (uint32_t)tq, (uint32_t)(tq >> 32));
-        if (fixed) continue;
-        const double p = (double)tp / two32, q = (double)tq / two32;
-        const double l1 = std::log1p(-p) - std::log1p(-q);
-        a[i] = std::log(p) - std::log(q) - l1;
-        C += l1;
-    }
+    std::string why;
+    if (!ratio_terms(g, q_thr, 0, nb, beq.data(), a.data(), C, why)) return mcg::fail(MCG_ERR_INVALID, why);
     MCG_CUDA(cudaSetDevice(e->device));
     MCG_CUDA(cudaMemcpyAsync(is->d_be_q, beq.data(), nb * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
     MCG_CUDA(cudaMemcpyAsync(is->d_a, a.data(), nb * sizeof(double), cudaMemcpyHostToDevice, e->stream));
@@ -254,6 +395,259 @@ mcg_status mcg_is_run(mcg_is *is, const uint64_t *q_thr, uint32_t iteration, uin
     result->ess = sums[1] > 0 ? sums[0] * sums[0] / sums[1] : 0.0;
     result->max_log_w = sums[3];
     result->kernel_ms = ms;
+    return MCG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched importance sampling over many trees joined into one graph.
+
+struct mcg_is_batch {
+    mcg_engine *engine = nullptr;
+    uint32_t n_inst = 0;
+    std::vector<uint32_t> be_begin;
+    uint4 *d_be_q = nullptr;
+    uint4 *d_be_def = nullptr;
+    double *d_a = nullptr;
+    double *d_C = nullptr;
+    double *d_a_def = nullptr;
+    double *d_C_def = nullptr;
+    double *d_sums = nullptr;
+    double *d_ce = nullptr;
+    uint32_t *d_be_begin = nullptr;
+    uint32_t *d_root = nullptr;
+    unsigned long long *d_queue = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<uint4> beq, beq_def;
+    std::vector<double> a, C, a_def, C_def, init;
+};
+
+namespace {
+
+// Frees everything; keeps the error message a failed create has just set.
+void release_batch(mcg_is_batch *b) {
+    const std::string keep = mcg::last_error();
+    if (b->engine) {
+        cudaSetDevice(b->engine->device);
+        cudaStreamSynchronize(b->engine->stream);
+    }
+    cudaFree(b->d_be_q);
+    cudaFree(b->d_be_def);
+    cudaFree(b->d_a);
+    cudaFree(b->d_C);
+    cudaFree(b->d_a_def);
+    cudaFree(b->d_C_def);
+    cudaFree(b->d_sums);
+    cudaFree(b->d_ce);
+    cudaFree(b->d_be_begin);
+    cudaFree(b->d_root);
+    cudaFree(b->d_queue);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->engine) mcg_destroy(b->engine);
+    mcg::last_error() = keep;
+}
+
+// Every gate must read nodes of one tree only, and root k must belong to
+// tree k: the owner of each node is propagated from the event ranges.
+std::string check_partition(const mcg::Graph &g, const std::vector<uint32_t> &be_begin) {
+    const uint32_t n_inst = (uint32_t)be_begin.size() - 1;
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    std::vector<uint32_t> owner(g.n_nodes(), kNone);
+    for (uint32_t k = 0; k < n_inst; ++k)
+        for (uint32_t i = be_begin[k]; i < be_begin[k + 1]; ++i) owner[i] = k;
+    for (uint32_t j = 0; j < g.n_gates; ++j) {
+        uint32_t o = kNone;
+        for (uint32_t s = 0; s < g.gate_in_count[j]; ++s) {
+            const uint32_t x = owner[g.inputs[g.gate_in_begin[j] + s]];
+            if (x == kNone) continue;
+            if (o != kNone && x != o) return "gate " + std::to_string(j) + " reads nodes of two trees";
+            o = x;
+        }
+        owner[g.n_be + j] = o;
+    }
+    for (uint32_t k = 0; k < n_inst; ++k) {
+        const uint32_t r = g.tally_nodes[k];
+        if (owner[r] != k && !(owner[r] == kNone && be_begin[k] == be_begin[k + 1]))
+            return "tallied node " + std::to_string(k) + " is not a node of tree " + std::to_string(k);
+    }
+    return std::string();
+}
+
+}  // namespace
+
+extern "C" {
+
+mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_inst, const uint32_t *be_begin,
+                               const mcg_run_desc *run_in, mcg_is_batch **out) {
+    mcg::clear_error();
+    if (!graph || !be_begin || !out) return mcg::fail(MCG_ERR_INVALID, "graph, be_begin and out must not be NULL");
+    *out = nullptr;
+    if (n_inst == 0) return mcg::fail(MCG_ERR_INVALID, "no trees");
+    if (graph->n_tally != n_inst) return mcg::fail(MCG_ERR_INVALID, "the tally list must hold one top event per tree");
+    if (be_begin[0] != 0 || be_begin[n_inst] != graph->n_be)
+        return mcg::fail(MCG_ERR_INVALID, "be_begin must start at 0 and end at n_be");
+    for (uint32_t k = 0; k < n_inst; ++k)
+        if (be_begin[k + 1] < be_begin[k]) return mcg::fail(MCG_ERR_INVALID, "be_begin must not decrease");
+    mcg_run_desc run{};
+    if (run_in) run = *run_in;
+    run.mode = MCG_MODE_STAGED;
+    auto b = std::unique_ptr<mcg_is_batch, void (*)(mcg_is_batch *)>(new mcg_is_batch, [](mcg_is_batch *x) {
+        release_batch(x);
+        delete x;
+    });
+    b->n_inst = n_inst;
+    b->be_begin.assign(be_begin, be_begin + n_inst + 1);
+    mcg_status st = mcg_create(graph, &run, &b->engine);
+    if (st != MCG_OK) return st;
+    const mcg::Graph &g = b->engine->graph;
+    const std::string bad = check_partition(g, b->be_begin);
+    if (!bad.empty()) return mcg::fail(MCG_ERR_INVALID, bad);
+    const uint32_t nb = std::max<uint32_t>(g.n_be, 1);
+    MCG_CUDA(cudaSetDevice(b->engine->device));
+    MCG_CUDA(cudaMalloc((void **)&b->d_be_q, nb * sizeof(uint4)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_be_def, nb * sizeof(uint4)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_a_def, nb * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_C_def, n_inst * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_a, nb * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_ce, nb * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_C, n_inst * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_sums, 4ull * n_inst * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_be_begin, (n_inst + 1ull) * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_root, n_inst * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_queue, sizeof(unsigned long long)));
+    MCG_CUDA(cudaMemcpy(b->d_be_begin, be_begin, (n_inst + 1ull) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_root, g.tally_nodes.data(), n_inst * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaEventCreate(&b->ev0));
+    MCG_CUDA(cudaEventCreate(&b->ev1));
+    b->beq.resize(nb);
+    b->beq_def.resize(nb);
+    b->a.resize(nb);
+    b->a_def.resize(nb);
+    b->C.resize(n_inst);
+    b->C_def.resize(n_inst);
+    b->init.resize(4ull * n_inst);
+    for (uint32_t k = 0; k < n_inst; ++k) {
+        b->init[4ull * k] = b->init[4ull * k + 1] = b->init[4ull * k + 2] = 0.0;
+        b->init[4ull * k + 3] = -std::numeric_limits<double>::infinity();
+    }
+    *out = b.release();
+    return MCG_OK;
+}
+
+mcg_status mcg_is_batch_destroy(mcg_is_batch *b) {
+    mcg::clear_error();
+    if (!b) return MCG_OK;
+    release_batch(b);
+    delete b;
+    return MCG_OK;
+}
+
+mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, const uint64_t *q_def, uint64_t words_def,
+                            uint32_t iteration, uint64_t word_begin, uint64_t word_count, double *tree_sums,
+                            double *ce_num, double *kernel_ms) {
+    mcg::clear_error();
+    if (!b || !q_thr || !tree_sums) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    if (words_def > word_count) return mcg::fail(MCG_ERR_INVALID, "words_defensive exceeds word_count");
+    if (words_def > 0 && !q_def) return mcg::fail(MCG_ERR_INVALID, "words_defensive > 0 needs q_defensive");
+    mcg_engine *e = b->engine;
+    const mcg::Graph &g = e->graph;
+    if (word_begin + word_count > (1ull << 32) || word_begin + word_count < word_begin)
+        return mcg::fail(MCG_ERR_INVALID, "word range exceeds the 32-bit sample counter");
+    if ((uint64_t)iteration + 2 >= (1ull << 26))
+        return mcg::fail(MCG_ERR_INVALID, "iteration exceeds the 26-bit pass counter field");
+    const uint32_t n_inst = b->n_inst;
+    const bool mix = words_def > 0 && words_def < word_count;
+    const uint64_t *q_only = words_def == word_count && words_def ? q_def : q_thr;  // one proposal draws all
+    std::string why;
+    for (uint32_t k = 0; k < n_inst; ++k) {
+        if (!ratio_terms(g, q_only, b->be_begin[k], b->be_begin[k + 1], b->beq.data(), b->a.data(), b->C[k], why))
+            return mcg::fail(MCG_ERR_INVALID, why);
+        if (mix && !ratio_terms(g, q_def, b->be_begin[k], b->be_begin[k + 1], b->beq_def.data(), b->a_def.data(),
+                                b->C_def[k], why))
+            return mcg::fail(MCG_ERR_INVALID, why);
+    }
+    MCG_CUDA(cudaSetDevice(e->device));
+    if (g.n_be) {
+        MCG_CUDA(cudaMemcpyAsync(b->d_be_q, b->beq.data(), g.n_be * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
+        MCG_CUDA(cudaMemcpyAsync(b->d_a, b->a.data(), g.n_be * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        MCG_CUDA(cudaMemsetAsync(b->d_ce, 0, g.n_be * sizeof(double), e->stream));
+        if (mix) {
+            MCG_CUDA(cudaMemcpyAsync(b->d_be_def, b->beq_def.data(), g.n_be * sizeof(uint4), cudaMemcpyHostToDevice,
+                                     e->stream));
+            MCG_CUDA(cudaMemcpyAsync(b->d_a_def, b->a_def.data(), g.n_be * sizeof(double), cudaMemcpyHostToDevice,
+                                     e->stream));
+        }
+    }
+    MCG_CUDA(cudaMemcpyAsync(b->d_C, b->C.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (mix)
+        MCG_CUDA(cudaMemcpyAsync(b->d_C_def, b->C_def.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice,
+                                 e->stream));
+    MCG_CUDA(cudaMemcpyAsync(b->d_sums, b->init.data(), 4ull * n_inst * sizeof(double), cudaMemcpyHostToDevice,
+                             e->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    IsBatchArgs args{};
+    args.n_inst = n_inst;
+    args.be_begin = b->d_be_begin;
+    args.root_row = b->d_root;
+    args.a = b->d_a;
+    args.C = b->d_C;
+    if (mix) {
+        const double alpha = (double)words_def / (double)word_count;
+        args.a_def = b->d_a_def;
+        args.C_def = b->d_C_def;
+        args.log_alpha = std::log(alpha);
+        args.log_1m_alpha = std::log1p(-alpha);
+    }
+    args.sums = b->d_sums;
+    args.ce = ce_num ? b->d_ce : nullptr;
+    args.queue = b->d_queue;
+    e->chunk_hook = [=](cudaStream_t s, const uint64_t *buf, uint64_t W) -> mcg_status {
+        IsBatchArgs p = args;
+        p.buf = buf;
+        p.W = W;
+        p.strips = (uint32_t)((W + kWeightThreads - 1) / kWeightThreads);
+        const uint64_t items = (uint64_t)n_inst * p.strips;
+        const uint32_t blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sms * 8));
+        cudaError_t err = cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), s);
+        if (err == cudaSuccess) {
+            k_is_weights_batch<<<blocks, kWeightThreads, 0, s>>>(p);
+            err = cudaGetLastError();
+        }
+        if (err != cudaSuccess)
+            return mcg::fail(MCG_ERR_CUDA, std::string("k_is_weights_batch: ") + cudaGetErrorString(err));
+        return MCG_OK;
+    };
+    MCG_CUDA(cudaEventRecord(b->ev0, e->stream));
+    // the defensive proposal draws the first words_def words, the proposal the rest
+    mcg_status st = MCG_OK;
+    if (mix) {
+        e->d_be_sample = b->d_be_def;
+        e->table_iteration = 0xFFFFFFFFu;
+        st = mcg::internal::run_staged(e, iteration, 1, word_begin, words_def);
+    }
+    if (st == MCG_OK && word_count > (mix ? words_def : 0)) {
+        e->d_be_sample = b->d_be_q;
+        e->table_iteration = 0xFFFFFFFFu;
+        const uint64_t off = mix ? words_def : 0;
+        st = mcg::internal::run_staged(e, iteration, 1, word_begin + off, word_count - off);
+    }
+    e->chunk_hook = nullptr;
+    e->d_be_sample = nullptr;
+    e->table_iteration = 0xFFFFFFFFu;
+    if (st != MCG_OK) return st;
+    MCG_CUDA(cudaEventRecord(b->ev1, e->stream));
+    MCG_CUDA(cudaMemcpyAsync(tree_sums, b->d_sums, 4ull * n_inst * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    if (ce_num && g.n_be)
+        MCG_CUDA(cudaMemcpyAsync(ce_num, b->d_ce, g.n_be * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    MCG_CUDA(cudaStreamSynchronize(e->stream));
+    if (kernel_ms) {
+        float ms = 0.f;
+        MCG_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        *kernel_ms = ms;
+    }
     return MCG_OK;
 }
 

@@ -97,24 +97,49 @@ class FlatGraph:
         """p~ = threshold / 2^32: the probability the sampler actually draws."""
         return self.be_threshold.astype(np.float64) / TWO_32
 
+    def edges(self):
+        """Every input slot in gate order: (gate index, input node, position
+        within the gate), int64 arrays of length sum(gate_in_count)."""
+        cnt = self.gate_in_count.astype(np.int64)
+        gid = np.repeat(np.arange(self.n_gates, dtype=np.int64), cnt)
+        within = np.arange(int(cnt.sum()), dtype=np.int64) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+        pos = np.repeat(self.gate_in_begin.astype(np.int64), cnt) + within
+        return gid, self.inputs[pos].astype(np.int64), within
+
     def layers(self) -> np.ndarray:
         """Depth of every gate: 1 + max depth of its gate inputs (basic events are 0),
-        the LayeredTopologicalOrder of mcSCRAM src/preprocessor.cc:130-171."""
+        the LayeredTopologicalOrder of mcSCRAM src/preprocessor.cc:130-171.
+        Computed by relaxation over all gates at once (as many sweeps as
+        there are layers)."""
+        nb, ng = self.n_be, self.n_gates
         depth = np.zeros(self.n_nodes, dtype=np.int64)
-        nb = self.n_be
-        for g in range(self.n_gates):
-            ins = self.gate_inputs(g)
-            depth[nb + g] = 1 + (int(depth[ins].max()) if ins.size else 0)
+        if ng == 0:
+            return depth
+        gid, src, _ = self.edges()
+        cnt = self.gate_in_count.astype(np.int64)
+        has = cnt > 0
+        starts = (np.cumsum(cnt) - cnt)[has]
+        depth[nb:] = 1
+        for _ in range(ng + 1):
+            new = np.ones(ng, dtype=np.int64)
+            if starts.size:
+                new[has] = np.maximum.reduceat(depth[src], starts) + 1
+            if np.array_equal(new, depth[nb:]):
+                break
+            depth[nb:] = new
         return depth
 
     def validate(self) -> None:
         nb = self.n_be
-        for g in range(self.n_gates):
-            if self.gate_neg_count[g] > self.gate_in_count[g]:
-                raise ValueError(f"gate {g}: neg_count > in_count")
-            ins = self.gate_inputs(g)
-            if ins.size and int(ins.max()) >= nb + g:
-                raise ValueError(f"gate {g}: inputs not topologically ordered")
+        bad = np.nonzero(self.gate_neg_count > self.gate_in_count)[0]
+        if bad.size:
+            raise ValueError(f"gate {int(bad[0])}: neg_count > in_count")
+        if np.any(self.gate_in_begin.astype(np.int64) + self.gate_in_count > self.inputs.size):
+            raise ValueError("gate input range outside the input array")
+        gid, src, _ = self.edges()
+        bad = np.nonzero(src >= nb + gid)[0]
+        if bad.size:
+            raise ValueError(f"gate {int(gid[bad[0]])}: inputs not topologically ordered")
         if np.any(self.be_threshold > (1 << 32)):
             raise ValueError("threshold above 2^32")
         if self.tally_nodes.size and int(self.tally_nodes.max()) >= self.n_nodes:
@@ -133,3 +158,45 @@ class FlatGraph:
             "frac_be_fanout_ge2": float((fanout[: self.n_be] >= 2).mean()) if self.n_be else 0.0,
             "n_tally": int(self.tally_nodes.size),
         }
+
+
+def concat(graphs) -> "tuple[FlatGraph, np.ndarray, np.ndarray]":
+    """Disjoint union of several graphs as one graph: the basic events of all
+    graphs first, graph by graph, then their gates, graph by graph (each
+    graph's gates stay in topological order and read only its own nodes).
+    Basic event j of the union gets event index j and PDAG index 2 + j, so
+    every event of the union draws from its own Philox counter stream; the
+    tally list holds the root of every graph.  Returns (union, be_begin,
+    roots): graph k owns basic events [be_begin[k], be_begin[k + 1]) and
+    its top event is node roots[k]."""
+    nbs = np.array([g.n_be for g in graphs], dtype=np.int64)
+    ngs = np.array([g.n_gates for g in graphs], dtype=np.int64)
+    nis = np.array([g.inputs.size for g in graphs], dtype=np.int64)
+    be_begin = np.concatenate([[0], np.cumsum(nbs)])
+    gate_begin = np.concatenate([[0], np.cumsum(ngs)])
+    in_begin = np.concatenate([[0], np.cumsum(nis)])
+    NB = int(be_begin[-1])
+    inputs, begins, roots = [], [], []
+    for k, g in enumerate(graphs):
+        x = g.inputs.astype(np.int64)
+        inputs.append(np.where(x < g.n_be, x + be_begin[k], x - g.n_be + NB + gate_begin[k]))
+        begins.append(g.gate_in_begin.astype(np.int64) + in_begin[k])
+        roots.append(g.root - g.n_be + NB + gate_begin[k])
+    cat = lambda arrs, dt: np.concatenate(arrs).astype(dt) if arrs else np.zeros(0, dtype=dt)
+    roots = np.array(roots, dtype=np.int64)
+    u = FlatGraph(
+        be_pdag_idx=np.arange(NB, dtype=np.int64) + 2,
+        be_event_idx=np.arange(NB, dtype=np.uint32),
+        be_threshold=cat([g.be_threshold for g in graphs], np.uint64),
+        gate_op=cat([g.gate_op for g in graphs], np.uint8),
+        gate_k=cat([g.gate_k for g in graphs], np.uint32),
+        gate_in_begin=cat(begins, np.uint32),
+        gate_in_count=cat([g.gate_in_count for g in graphs], np.uint32),
+        gate_neg_count=cat([g.gate_neg_count for g in graphs], np.uint32),
+        inputs=cat(inputs, np.uint32),
+        tally_nodes=roots.astype(np.uint32),
+        gate_pdag_idx=np.arange(int(gate_begin[-1]), dtype=np.int64) + 2 + NB,
+        root=int(roots[-1]) if roots.size else -1,
+        name=f"union-of-{len(graphs)}",
+    )
+    return u, be_begin, roots

@@ -12,6 +12,11 @@
   the next target, fit the network to it, repeat.
 * ``estimate`` -- the final IS estimate with an effective-sample-size check
   that falls back to the plain sampler when the weights collapse.
+* ``BatchedImportanceSampler`` / ``batched_learned_is`` -- the same for many
+  trees at once: the trees are joined into one graph and sampled in one
+  staged pass per call, one network (with a per-tree input) gives every
+  tree's proposal, and trees leave the batch as they reach the target
+  error (or fall back to plain sampling).
 """
 from __future__ import annotations
 
@@ -23,7 +28,7 @@ from typing import List, Optional
 import numpy as np
 
 from . import _capi
-from .graph import AND, ATLEAST, OR, XOR, FlatGraph, probability_threshold
+from .graph import AND, ATLEAST, OR, XOR, FlatGraph, concat, probability_threshold
 
 N_FEATURES = 16
 N_PARAMS = 16 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -48,6 +53,11 @@ _capi.register_signatures({
     "mcg_is_create": (C.c_int, [C.POINTER(_capi.GraphDesc), C.POINTER(_capi.RunDesc), C.POINTER(_vp)]),
     "mcg_is_destroy": (C.c_int, [_vp]),
     "mcg_is_run": (C.c_int, [_vp, _u64p, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(IsResult), _dp]),
+    "mcg_is_batch_create": (C.c_int, [C.POINTER(_capi.GraphDesc), C.c_uint32, C.POINTER(C.c_uint32),
+                                      C.POINTER(_capi.RunDesc), C.POINTER(_vp)]),
+    "mcg_is_batch_destroy": (C.c_int, [_vp]),
+    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, _u64p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _dp, _dp,
+                                   _dp]),
     "mcg_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_vp)]),
     "mcg_mlp_destroy": (C.c_int, [_vp]),
     "mcg_mlp_set_params": (C.c_int, [_vp, _fp]),
@@ -62,56 +72,208 @@ def _p(a, t):
     return a.ctypes.data_as(C.POINTER(t))
 
 
-def event_features(g: FlatGraph) -> np.ndarray:
-    """16 features per basic event, float32 [n_be, 16]."""
+def approximate_importance(g: FlatGraph):
+    """Node probabilities and per-event conditional marginals under the
+    independence approximation (every gate's inputs taken as independent):
+    one bottom-up pass gives P~ of every node, one reverse-mode pass the
+    sensitivity d log P~_top / d p_i, and
+        P~(x_i = 1 | top) = p_i + p_i (1 - p_i) d log P~_top / d p_i,
+    the approximate conditional marginal that the zero-variance product
+    proposal needs (approximate zero-variance importance sampling).  Exact
+    for trees where no node has two parents; an approximation, and still
+    cheap, for DAGs.  Returns (node_prob [n_nodes], cond [n_be])."""
+    from .graph import NAND, NOR, NOT, NULL
     nb, ng = g.n_be, g.n_gates
-    depth = g.layers()
-    L = max(int(depth.max()), 1)
-    parents = [[] for _ in range(g.n_nodes)]
-    for gi in range(ng):
-        for c in g.gate_inputs(gi):
-            parents[int(c)].append(gi)
+    pr = np.zeros(g.n_nodes)
+    pr[:nb] = g.quantised_probabilities()
+    if ng == 0 or nb == 0:
+        return pr, pr[:nb].copy()
+    depth = g.layers()[nb:]
+    cnt = g.gate_in_count.astype(np.int64)
+    pos_neg = cnt - g.gate_neg_count.astype(np.int64)
+    ops = g.gate_op.astype(np.int64)
+    kk = g.gate_k.astype(np.int64) & 0xFF
+    ib = g.gate_in_begin.astype(np.int64)
+    levels = [np.nonzero(depth == d)[0] for d in range(1, int(depth.max()) + 1)]
+    cache = []
+    for gs in levels:  # bottom-up
+        c = cnt[gs]
+        m = int(c.max())
+        col = np.arange(m)
+        valid = col[None, :] < c[:, None]
+        src = g.inputs[np.where(valid, ib[gs][:, None] + col[None, :], 0)].astype(np.int64)
+        neg = col[None, :] >= pos_neg[gs][:, None]
+        v = np.where(valid, np.where(neg, 1.0 - pr[src], pr[src]), 0.0)
+        op = ops[gs]
+        r = np.zeros(gs.size)
+        d = np.zeros((gs.size, m))  # d gate / d (input value), before the output complement
+        s_and = (op == AND) | (op == NAND)
+        if s_and.any():
+            vv = np.where(valid[s_and], v[s_and], 1.0)
+            r[s_and] = np.prod(vv, axis=1)
+            for j in range(m):  # leave-one-out products
+                d[s_and, j] = np.prod(np.where(col[None, :] == j, 1.0, vv), axis=1)
+        s_or = (op == OR) | (op == NOR)
+        if s_or.any():
+            cv = np.where(valid[s_or], 1.0 - v[s_or], 1.0)
+            with np.errstate(divide="ignore"):
+                r[s_or] = -np.expm1(np.sum(np.log1p(-np.where(valid[s_or], v[s_or], 0.0)), axis=1))
+            for j in range(m):
+                d[s_or, j] = np.prod(np.where(col[None, :] == j, 1.0, cv), axis=1)
+        s_x = op == XOR
+        if s_x.any():
+            vx = v[s_x]
+            acc = np.zeros(vx.shape[0])
+            for j in range(m):
+                acc = acc * (1 - vx[:, j]) + (1 - acc) * vx[:, j]
+            r[s_x] = acc
+            for j in range(m):  # XOR of the others, then d/dv_j = 1 - 2 x_others
+                o = np.zeros(vx.shape[0])
+                for l in range(m):
+                    if l != j:
+                        o = o * (1 - vx[:, l]) + (1 - o) * vx[:, l]
+                d[s_x, j] = 1.0 - 2.0 * o
+        s_k = op == ATLEAST
+        if s_k.any():
+            vk = v[s_k]
+            k = kk[gs][s_k]
+            ck = c[s_k]
+
+            def tail_ge(vals, kth):
+                dist = np.zeros((vals.shape[0], m + 1))
+                dist[:, 0] = 1.0
+                for j in range(vals.shape[1]):
+                    x = vals[:, j][:, None]
+                    dist[:, 1:] = dist[:, 1:] * (1 - x) + dist[:, :-1] * x
+                    dist[:, 0] *= 1 - x[:, 0]
+                t = np.cumsum(dist[:, ::-1], axis=1)[:, ::-1]
+                kth = np.clip(kth, 0, m)
+                return np.where(kth <= m, t[np.arange(vals.shape[0]), kth], 0.0)
+
+            r[s_k] = np.where(k <= ck, tail_ge(vk, k), 0.0)
+            for j in range(m):  # P(count of others >= k - 1) - P(count of others >= k)
+                others = np.where(col[None, :] == j, 0.0, vk)
+                d[s_k, j] = np.where(k <= ck, tail_ge(others, k - 1) - tail_ge(others, k), 0.0)
+        s_l = (op == NOT) | (op == NULL)
+        if s_l.any():
+            last = np.maximum(c[s_l] - 1, 0)
+            r[s_l] = v[s_l][np.arange(last.size), last]
+            d[s_l] = np.where(col[None, :] == last[:, None], 1.0, 0.0)
+        comp = (op == NAND) | (op == NOR) | (op == NOT)
+        r[comp] = 1.0 - r[comp]
+        d = np.where(comp[:, None], -d, d)
+        d = np.where(neg, -d, d)
+        d = np.where(valid, d, 0.0)
+        pr[nb + gs] = r
+        cache.append((gs, src, valid, d))
+    # reverse mode: adj = d log P~_top / d P~_node
+    adj = np.zeros(g.n_nodes)
+    top = pr[g.root]
+    if top <= 0:
+        return pr, pr[:nb].copy()
+    adj[g.root] = 1.0 / top
+    for gs, src, valid, d in reversed(cache):
+        contrib = adj[nb + gs][:, None] * d
+        np.add.at(adj, src[valid], contrib[valid])
+    p = pr[:nb]
+    cond = np.clip(p + p * (1.0 - p) * adj[:nb], 0.0, 1.0)
+    return pr, cond
+
+
+def event_features(g: FlatGraph, instance_scale: Optional[float] = None, importance: bool = False) -> np.ndarray:
+    """16 features per basic event, float32 [n_be, 16]:
+
+    0 log10 p (shifted), 1 fan-out, 2-3 min/max depth of the parents, 4-6
+    fraction of AND/OR/ATLEAST parents, 7 mean parent fan-in, 8 mean k/n of
+    ATLEAST parents, 9 siblings under the first parent, 10 mean log10 p of
+    the sibling events, 11 fraction of sibling gates, 12 parent at the top
+    depth, 13-14 AND/OR share of the first-parent path to the top, 15 a
+    per-instance input: 1 for a single tree, log10 of the instance's
+    probe inflation / 6 when one network serves many trees.  "First parent"
+    is the parent gate of lowest index.  Computed for all events at once.
+    importance=True replaces 11 and 12 with the independence-approximation
+    inputs of approximate_importance: log10 of the first parent's
+    probability / 10 + 1 and log10 P~(x_i = 1 | top) / 4 + 1."""
+    nb, ng = g.n_be, g.n_gates
+    feats = np.zeros((nb, N_FEATURES), dtype=np.float32)
+    feats[:, 15] = 1.0 if instance_scale is None else np.log10(max(instance_scale, 1.0)) / 6.0
     p = np.clip(g.quantised_probabilities(), 1e-12, 1.0)
     logp = np.log10(p)
-    # path from every gate to the top through its first parent
+    feats[:, 0] = (logp + 4.0) / 2.0
+    if ng == 0 or nb == 0:
+        return feats
+    depth = g.layers()
+    L = max(int(depth.max()), 1)
+    gid, src, _ = g.edges()
+    gnode = gid + nb
+    op = g.gate_op.astype(np.int64)
+    fin = g.gate_in_count.astype(np.int64)
+    fanout = np.bincount(src, minlength=g.n_nodes)
+    # first (lowest-index) parent of every node; ng marks "none"
+    first = np.full(g.n_nodes, ng, dtype=np.int64)
+    np.minimum.at(first, src, gid)
+    # AND / OR counts along the first-parent chain from every gate to the top
+    fp_g = first[nb:]
+    has_fp = fp_g < ng
+    fp_safe = np.where(has_fp, fp_g, 0)
+    step_and = np.where(has_fp, (op[fp_safe] == AND).astype(np.float64), 0.0)
+    step_or = np.where(has_fp, (op[fp_safe] == OR).astype(np.float64), 0.0)
+    step_len = has_fp.astype(np.float64)
     up_and = np.zeros(ng)
     up_or = np.zeros(ng)
     up_len = np.zeros(ng)
-    for gi in range(ng - 1, -1, -1):
-        node = nb + gi
-        ps = parents[node]
-        if ps:
-            q = ps[0]
-            up_and[gi] = up_and[q] + (g.gate_op[q] == AND)
-            up_or[gi] = up_or[q] + (g.gate_op[q] == OR)
-            up_len[gi] = up_len[q] + 1
-    feats = np.zeros((nb, N_FEATURES), dtype=np.float32)
-    for e in range(nb):
-        ps = parents[e]
-        feats[e, 0] = (logp[e] + 4.0) / 2.0
-        feats[e, 1] = len(ps) / 4.0
-        if ps:
-            d = [depth[nb + q] for q in ps]
-            ops = [int(g.gate_op[q]) for q in ps]
-            fanin = [int(g.gate_in_count[q]) for q in ps]
-            feats[e, 2] = min(d) / L
-            feats[e, 3] = max(d) / L
-            feats[e, 4] = np.mean([o == AND for o in ops])
-            feats[e, 5] = np.mean([o == OR for o in ops])
-            feats[e, 6] = np.mean([o == ATLEAST for o in ops])
-            feats[e, 7] = np.mean(fanin) / 8.0
-            kn = [int(g.gate_k[q]) / max(int(g.gate_in_count[q]), 1) for q in ps if g.gate_op[q] == ATLEAST]
-            feats[e, 8] = np.mean(kn) if kn else 0.0
-            q0 = ps[0]
-            sib = [int(c) for c in g.gate_inputs(q0) if int(c) != e]
-            feats[e, 9] = (len(sib)) / 8.0
-            sib_be = [logp[c] for c in sib if c < nb]
-            feats[e, 10] = (np.mean(sib_be) + 4.0) / 2.0 if sib_be else 0.0
-            feats[e, 11] = np.mean([c >= nb for c in sib]) if sib else 0.0
-            feats[e, 12] = float(max(d) == L)
-            feats[e, 13] = up_and[q0] / max(up_len[q0] + 1, 1)
-            feats[e, 14] = up_or[q0] / max(up_len[q0] + 1, 1)
-        feats[e, 15] = 1.0
+    for _ in range(ng + 1):
+        na = np.where(has_fp, up_and[fp_safe] + step_and, 0.0)
+        no = np.where(has_fp, up_or[fp_safe] + step_or, 0.0)
+        nl = np.where(has_fp, up_len[fp_safe] + step_len, 0.0)
+        if np.array_equal(na, up_and) and np.array_equal(no, up_or) and np.array_equal(nl, up_len):
+            break
+        up_and, up_or, up_len = na, no, nl
+    # per-event aggregates over parent edges (edges whose input is an event)
+    ev = src < nb
+    e_src, e_gate = src[ev], gid[ev]
+    fo = fanout[:nb].astype(np.float64)
+    has = fo > 0
+    den = np.where(has, fo, 1.0)
+    dmin = np.full(nb, np.iinfo(np.int64).max)
+    dmax = np.zeros(nb, dtype=np.int64)
+    np.minimum.at(dmin, e_src, depth[e_gate + nb])
+    np.maximum.at(dmax, e_src, depth[e_gate + nb])
+    cnt_of = lambda m: np.bincount(e_src, weights=m.astype(np.float64), minlength=nb)
+    feats[:, 1] = fo / 4.0
+    feats[has, 2] = dmin[has] / L
+    feats[has, 3] = dmax[has] / L
+    feats[has, 4] = (cnt_of(op[e_gate] == AND) / den)[has]
+    feats[has, 5] = (cnt_of(op[e_gate] == OR) / den)[has]
+    feats[has, 6] = (cnt_of(op[e_gate] == ATLEAST) / den)[has]
+    feats[has, 7] = (np.bincount(e_src, weights=fin[e_gate].astype(np.float64), minlength=nb) / den / 8.0)[has]
+    is_k = op[e_gate] == ATLEAST
+    kn = (g.gate_k.astype(np.float64)[e_gate] / np.maximum(fin[e_gate], 1))
+    n_k = np.bincount(e_src[is_k], minlength=nb).astype(np.float64)
+    s_k = np.bincount(e_src[is_k], weights=kn[is_k], minlength=nb)
+    feats[:, 8] = np.where(n_k > 0, s_k / np.maximum(n_k, 1.0), 0.0)
+    # siblings under the first parent
+    q0 = first[:nb]
+    q0s = np.where(has, q0, 0)
+    occ = np.bincount(e_src[e_gate == q0s[e_src]], minlength=nb).astype(np.float64)
+    n_sib = np.where(has, fin[q0s] - occ, 0.0)
+    feats[:, 9] = n_sib / 8.0
+    in_be = src < nb
+    g_be_cnt = np.bincount(gid[in_be], minlength=ng).astype(np.float64)
+    g_be_sum = np.bincount(gid[in_be], weights=logp[src[in_be]], minlength=ng)
+    g_gate_cnt = np.bincount(gid[~in_be], minlength=ng).astype(np.float64)
+    sb_cnt = g_be_cnt[q0s] - occ
+    sb_sum = g_be_sum[q0s] - occ * logp
+    feats[:, 10] = np.where(has & (sb_cnt > 0), (sb_sum / np.maximum(sb_cnt, 1.0) + 4.0) / 2.0, 0.0)
+    feats[:, 11] = np.where(has & (n_sib > 0), g_gate_cnt[q0s] / np.maximum(n_sib, 1.0), 0.0)
+    feats[:, 12] = np.where(has, (dmax == L).astype(np.float64), 0.0)
+    feats[:, 13] = np.where(has, up_and[q0s] / np.maximum(up_len[q0s] + 1, 1), 0.0)
+    feats[:, 14] = np.where(has, up_or[q0s] / np.maximum(up_len[q0s] + 1, 1), 0.0)
+    if importance:
+        pr, cond = approximate_importance(g)
+        pp = np.where(has, pr[np.where(has, q0s + nb, 0)], 1.0)
+        feats[:, 11] = np.log10(np.clip(pp, 1e-30, 1.0)) / 10.0 + 1.0
+        feats[:, 12] = np.log10(np.clip(cond, 1e-12, 1.0)) / 4.0 + 1.0
     return feats
 
 
@@ -304,3 +466,316 @@ def estimate(sampler: ImportanceSampler, q: np.ndarray, target_rel_err: float = 
             break
     return {"estimate": est, "std_err": se, "rel_err95": rel95, "samples": int(n), "hits": hits, "ess": ess,
             "batches": b, "gpu_ms": gpu_ms, "fallback": bool(ess < ess_floor)}
+
+
+# --- many trees at once -------------------------------------------------------
+
+def _proposal_thr(nominal: np.ndarray, q: np.ndarray) -> np.ndarray:
+    thr = probability_threshold(np.clip(q, 0.0, 1.0))
+    thr = np.clip(thr, 1, (1 << 32) - 1).astype(np.uint64)
+    fixed = (nominal == 0) | (nominal >= (1 << 32))
+    thr[fixed] = nominal[fixed]
+    return np.ascontiguousarray(thr, dtype=np.uint64)
+
+
+class BatchedImportanceSampler:
+    """Proposal sampling over many trees joined into one graph (mcg_is_batch_*).
+
+    ``run`` returns per-tree FP64 sums over word_count * 64 samples of every
+    tree; tree k's events are ``slice(be_begin[k], be_begin[k + 1])`` of the
+    joined graph."""
+
+    def __init__(self, graphs, device: int = 0, chunk_words: int = 0):
+        self.lib = _capi.load()
+        self.graphs = list(graphs)
+        self.union, self.be_begin, self.roots = concat(self.graphs)
+        self._view = _capi.GraphView(self.union)
+        self._be_begin32 = np.ascontiguousarray(self.be_begin, dtype=np.uint32)
+        run = _capi.RunDesc(mode=_capi.MODE_STAGED, device=device, layered_max_words=chunk_words)
+        self.h = _vp()
+        _capi.check(self.lib.mcg_is_batch_create(C.byref(self._view.desc), len(self.graphs),
+                                                 _p(self._be_begin32, C.c_uint32), C.byref(run), C.byref(self.h)))
+
+    @property
+    def n_trees(self) -> int:
+        return len(self.graphs)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mcg_is_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def proposal_thresholds(self, q: np.ndarray) -> np.ndarray:
+        """Thresholds for proposal probabilities q over all events of the joined
+        graph (events with a constant nominal word keep it)."""
+        return _proposal_thr(self.union.be_threshold, q)
+
+    def run(self, q_thresholds: np.ndarray, iteration: int = 1, word_begin: int = 0, word_count: int = 1 << 14,
+            ce: bool = False, q_defensive: Optional[np.ndarray] = None, words_defensive: int = 0) -> dict:
+        """Per-tree sums of one pass; with q_defensive the first words_defensive
+        words come from it and samples carry the balance-heuristic weight."""
+        q_thresholds = np.ascontiguousarray(q_thresholds, dtype=np.uint64)
+        if q_thresholds.shape != (self.union.n_be,):
+            raise ValueError("one proposal threshold per event of the joined graph")
+        qd = None
+        if q_defensive is not None:
+            qd = np.ascontiguousarray(q_defensive, dtype=np.uint64)
+            if qd.shape != (self.union.n_be,):
+                raise ValueError("one defensive threshold per event of the joined graph")
+        sums = np.zeros((self.n_trees, 4), dtype=np.float64)
+        ce_num = np.zeros(max(self.union.n_be, 1), dtype=np.float64) if ce else None
+        ms = C.c_double()
+        _capi.check(self.lib.mcg_is_batch_run(self.h, _p(q_thresholds, C.c_uint64),
+                                              _p(qd, C.c_uint64) if qd is not None else None, int(words_defensive),
+                                              iteration, word_begin, word_count, _p(sums, C.c_double),
+                                              _p(ce_num, C.c_double) if ce else None, C.byref(ms)))
+        out = {"sum_w": sums[:, 0].copy(), "sum_w2": sums[:, 1].copy(), "hits": sums[:, 2].astype(np.int64),
+               "max_log_w": sums[:, 3].copy(), "samples": int(word_count) * 64, "kernel_ms": float(ms.value)}
+        if ce:
+            out["ce_num"] = ce_num[: self.union.n_be]
+        return out
+
+
+@dataclass
+class BatchedIsResult:
+    estimate: np.ndarray          # per tree
+    rel_err95: np.ndarray         # 1.96 * std_err / estimate
+    samples: np.ndarray
+    hits: np.ndarray
+    ess: np.ndarray
+    converged: np.ndarray         # reached the target error
+    fallback: np.ndarray          # sampled with the nominal probabilities (weights collapsed)
+    scale: np.ndarray             # probe inflation per tree
+    gpu_ms: dict                  # device time per phase (CUDA events)
+    seconds: dict                 # wall time per phase
+    q: np.ndarray = None          # final proposal of every event (trees concatenated)
+    be_begin: np.ndarray = None   # tree k's events: q[be_begin[k]:be_begin[k + 1]]
+    rounds: List[dict] = field(default_factory=list)
+
+
+def _rel95(n, sw, sw2):
+    est = np.where(n > 0, sw / np.maximum(n, 1), 0.0)
+    var = np.maximum(sw2 / np.maximum(n, 1) - est * est, 0.0)
+    se = np.sqrt(var / np.maximum(n - 1, 1))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(est > 0, 1.96 * se / np.where(est > 0, est, 1.0), np.inf)
+    return est, rel
+
+
+def _train_shared(mlp: "ProposalMLP", feats, targets, steps, lr, weights=None, group=None):
+    """Fits the shared network to the rows of every rank: the rows are
+    gathered to all ranks, rank 0's trained parameters are broadcast."""
+    if group is None:
+        import torch.distributed as dist
+        if not (dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1):
+            return mlp.train(feats, targets, weights, steps=steps, lr=lr)
+    from . import parallel
+    if weights is not None:
+        feats = np.concatenate([feats, np.asarray(weights, dtype=np.float32)[:, None]], axis=1)
+    feats, targets = parallel.allgather_rows(feats, targets, group=group)
+    if weights is not None:
+        feats, weights = np.ascontiguousarray(feats[:, :-1]), np.ascontiguousarray(feats[:, -1])
+    loss = mlp.train(feats, targets, weights, steps=steps, lr=lr)
+    mlp.set_params(parallel.broadcast_params(mlp.params(), group=group))
+    return loss
+
+
+def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[ProposalMLP] = None, device: int = 0,
+                       probe_words: int = 1 << 10, min_hits: int = 200, max_probe_rounds: int = 24,
+                       ce_rounds: int = 4, ce_words: int = 1 << 12, smoothing: float = 0.7, train_steps: int = 150,
+                       lr: float = 3e-3, q_max: float = 0.5, est_words: int = 1 << 12, max_est_words: int = 1 << 22,
+                       ess_floor: float = 50.0, collapse_ratio: float = 1e-3, plain_words: int = 1 << 16,
+                       defensive: float = 0.2, chunk_words: int = 0, use_network: bool = True,
+                       importance_features: bool = True, tree_weighting: bool = True, fallback_after: int = 2,
+                       cap_levels=(0.75, 0.9, 0.97, 0.99), confirm_rounds: int = 1,
+                       defensive_proposal: str = "approx", min_words: int = 0, log=None) -> BatchedIsResult:
+    """Learned importance sampling for a batch of rare-event trees.
+
+    1. Probe: q = min(p * s_k, c_k) per tree, s_k x4 per round (x8 without
+       a hit) until the probe sees min_hits top-event failures (the plain
+       sampler fed the inflated thresholds).  The cap c_k starts at q_max and
+       is raised through cap_levels only for a tree whose every event already
+       sits at the cap (a top event that needs many near-certain failures);
+       the tree's proposals stay below c_k from then on.
+    From here on a share `defensive` of every pass's words is drawn from a
+    defensive proposal q_d and every sample carries the balance-heuristic
+    weight p / (defensive * q_d + (1 - defensive) * q) (mcg_is_batch_run):
+    a failure region the learned proposal under-samples is still reached
+    through q_d's share, so the estimate stays unbiased with a bounded
+    variance instead of silently missing that region.  q_d is the
+    approximate zero-variance proposal P~(x_i = 1 | top) of
+    approximate_importance (defensive_proposal="approx"; exact for trees
+    without shared nodes) or the probe's inflation ("probe"), clipped to the
+    tree's cap; the first cross-entropy round samples q_d.
+    2. Cross-entropy rounds over all trees at once: per-event targets are the
+       likelihood-weighted failure frequencies, smoothed with the current
+       proposal; one network, whose 16th input is the tree's log10 s_k / 6,
+       is fitted to the rows of all trees (each tree weighing the same in the
+       loss with tree_weighting) and gives every tree's next q.
+    3. Estimate rounds with doubling words; a tree leaves the batch once
+       1.96 * std_err / estimate <= target_rel_err with ESS >= ess_floor
+       at the end of confirm_rounds consecutive rounds and after at least
+       min_words words (a product-form proposal can leave a failure mode
+       almost unsampled; a sample that has not met it yet shows a small
+       error around a low estimate, so a floor on the sample count guards
+       the error estimate),
+       and the joined graph is rebuilt from the trees left.  A tree whose
+       ESS / hits falls below collapse_ratio after its first estimate round
+       is re-run with its nominal probabilities (plain Monte Carlo, weights 1)
+       and reported as a fallback.
+    Every round draws fresh Philox counters (its own pass number).
+    use_network=False takes the smoothed cross-entropy targets themselves as
+    the next proposal (the method without the network, for comparison);
+    importance_features=False leaves the independence-approximation inputs
+    out of the features (event_features)."""
+    say = log or (lambda *a: None)
+    n = len(graphs)
+    t_all = time.perf_counter()
+    gpu = {"probe": 0.0, "ce": 0.0, "estimate": 0.0}
+    wall = {"features": 0.0, "probe": 0.0, "ce": 0.0, "train": 0.0, "estimate": 0.0, "rebuild": 0.0}
+    rounds = []
+    t0 = time.perf_counter()
+    full = BatchedImportanceSampler(graphs, device=device, chunk_words=chunk_words)
+    wall["rebuild"] += time.perf_counter() - t0
+    bb = full.be_begin
+    p = full.union.quantised_probabilities()
+    sl = [slice(int(bb[k]), int(bb[k + 1])) for k in range(n)]
+    tree_of_event = np.repeat(np.arange(n), np.diff(bb))
+    # 1. probe
+    t0 = time.perf_counter()
+    scale = np.ones(n)
+    cap = np.full(n, float(q_max))
+    ok = np.zeros(n, dtype=bool)
+    p_min = np.array([float(p[sl[k]][p[sl[k]] > 0].min()) if np.any(p[sl[k]] > 0) else 1.0 for k in range(n)])
+    it = 1
+    for r in range(max_probe_rounds):
+        q = np.minimum(p * scale[tree_of_event], cap[tree_of_event])
+        res = full.run(full.proposal_thresholds(q), iteration=it, word_count=probe_words)
+        it += 1
+        gpu["probe"] += res["kernel_ms"]
+        ok |= res["hits"] >= min_hits
+        rounds.append({"phase": "probe", "round": r, "trees_left": int((~ok).sum()), "ms": res["kernel_ms"]})
+        if ok.all():
+            break
+        saturated = ~ok & (scale * p_min >= cap)
+        for k in np.nonzero(saturated)[0]:
+            higher = [c for c in cap_levels if c > cap[k]]
+            if higher:
+                cap[k] = higher[0]
+        grow = ~ok & ~saturated
+        scale = np.where(grow, scale * np.where(res["hits"] == 0, 8.0, 4.0), scale)
+        scale = np.minimum(scale, cap / p_min)
+    wall["probe"] = time.perf_counter() - t0
+    # 2. cross-entropy rounds with the shared network
+    t0 = time.perf_counter()
+    feats = np.concatenate([event_features(g, instance_scale=float(scale[k]), importance=importance_features)
+                            for k, g in enumerate(graphs)])
+    wall["features"] = time.perf_counter() - t0
+    mlp = mlp or (ProposalMLP(device=device) if use_network else None)
+    cap_e = cap[tree_of_event]
+    if defensive_proposal == "approx":
+        q_probe = np.concatenate([np.clip(approximate_importance(g)[1], 1e-7, cap[k]) for k, g in enumerate(graphs)])
+    elif defensive_proposal == "probe":
+        q_probe = np.minimum(p * scale[tree_of_event], cap_e)
+    else:
+        raise ValueError("defensive_proposal must be 'approx' or 'probe'")
+    row_w = (1.0 / np.diff(bb).astype(np.float64))[tree_of_event].astype(np.float32) if tree_weighting else None
+    q = q_probe.copy()
+    thr_probe = full.proposal_thresholds(q_probe)
+    n_def = lambda w: int(round(defensive * w))
+    t0 = time.perf_counter()
+    for r in range(ce_rounds):
+        res = full.run(full.proposal_thresholds(q), iteration=it, word_count=ce_words, ce=True,
+                       q_defensive=thr_probe, words_defensive=n_def(ce_words))
+        it += 1
+        gpu["ce"] += res["kernel_ms"]
+        sw = res["sum_w"][tree_of_event]
+        hit = sw > 0
+        target = np.where(hit, res["ce_num"] / np.where(hit, sw, 1.0), q)
+        target = np.clip(target, 1e-7, cap_e)
+        target = smoothing * target + (1.0 - smoothing) * q
+        t1 = time.perf_counter()
+        if use_network:
+            loss = _train_shared(mlp, feats, target.astype(np.float32), train_steps, lr, weights=row_w)
+            q = np.clip(mlp.forward(feats).astype(np.float64), 1e-7, cap_e)
+        else:
+            loss, q = float("nan"), target
+        wall["train"] += time.perf_counter() - t1
+        est, rel = _rel95(res["samples"], res["sum_w"], res["sum_w2"])
+        rounds.append({"phase": "ce", "round": r, "ms": res["kernel_ms"], "loss": loss,
+                       "median_rel95": float(np.median(rel)), "trees_without_hits": int((res["hits"] == 0).sum())})
+        say(rounds[-1])
+    wall["ce"] = time.perf_counter() - t0
+    # 3. estimate
+    t0 = time.perf_counter()
+    N = np.zeros(n)
+    SW = np.zeros(n)
+    SW2 = np.zeros(n)
+    H = np.zeros(n, dtype=np.int64)
+    converged = np.zeros(n, dtype=bool)
+    fallback = np.zeros(n, dtype=bool)
+    checked = np.zeros(n, dtype=bool)
+    rounds_in = np.zeros(n, dtype=np.int64)
+    streak = np.zeros(n, dtype=np.int64)
+    q_use = q.copy()
+    active = np.arange(n)
+    sampler, members = full, active.copy()
+    words = est_words
+    used = 0
+    while active.size and used < max_est_words:
+        if not np.array_equal(members, active):
+            t1 = time.perf_counter()
+            sampler.close()  # the joined graph of the trees left replaces it (and its device memory)
+            sampler = BatchedImportanceSampler([graphs[k] for k in active], device=device, chunk_words=chunk_words)
+            members = active.copy()
+            wall["rebuild"] += time.perf_counter() - t1
+        qa = np.concatenate([q_use[sl[k]] for k in members])
+        qd = np.concatenate([q_probe[sl[k]] if not fallback[k] else p[sl[k]] for k in members])
+        res = sampler.run(sampler.proposal_thresholds(qa), iteration=it, word_begin=0, word_count=words,
+                          q_defensive=sampler.proposal_thresholds(qd), words_defensive=n_def(words))
+        it += 1
+        gpu["estimate"] += res["kernel_ms"]
+        used += words
+        N[members] += res["samples"]
+        SW[members] += res["sum_w"]
+        SW2[members] += res["sum_w2"]
+        H[members] += res["hits"]
+        est, rel = _rel95(N, SW, SW2)
+        ess = np.where(SW2 > 0, SW * SW / np.where(SW2 > 0, SW2, 1.0), 0.0)
+        ok_now = (rel <= target_rel_err) & (ess >= ess_floor) & (N >= 64.0 * min_words)
+        streak[members] = np.where(ok_now[members], streak[members] + 1, 0)
+        done = streak >= confirm_rounds
+        # weight collapse: few effective samples among many hits after
+        # `fallback_after` rounds -> plain sampling
+        rounds_in[members] += 1
+        first = members[(~checked[members]) & (rounds_in[members] >= fallback_after)]
+        checked[first] = True
+        bad = first[(H[first] > 0) & (ess[first] < collapse_ratio * H[first]) & ~done[first]]
+        for k in bad:
+            fallback[k] = True
+            q_use[sl[k]] = p[sl[k]]
+            N[k] = SW[k] = SW2[k] = 0.0
+            H[k] = 0
+        converged |= done
+        rounds.append({"phase": "estimate", "words": words, "trees": int(members.size), "ms": res["kernel_ms"],
+                       "converged": int(converged.sum()), "fallback": int(fallback.sum())})
+        say(rounds[-1])
+        active = np.nonzero(~converged & ~(fallback & (N >= plain_words * 64)))[0]
+        words = min(words * 2, max(max_est_words - used, est_words))
+    sampler.close()
+    full.close()
+    wall["estimate"] = time.perf_counter() - t0
+    wall["total"] = time.perf_counter() - t_all
+    est, rel = _rel95(N, SW, SW2)
+    ess = np.where(SW2 > 0, SW * SW / np.where(SW2 > 0, SW2, 1.0), 0.0)
+    return BatchedIsResult(estimate=est, rel_err95=rel, samples=N.astype(np.int64), hits=H, ess=ess,
+                           converged=converged, fallback=fallback, scale=scale, gpu_ms=gpu, seconds=wall,
+                           q=q_use, be_begin=bb, rounds=rounds)

@@ -63,3 +63,42 @@ def allreduce_max(values: Sequence[float], group=None, device: Optional[str] = N
     t = torch.tensor(list(values), dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return [float(x) for x in t.cpu()]
+
+
+def allgather_rows(feats: np.ndarray, targets: np.ndarray, group=None, device: Optional[str] = None):
+    """Concatenates every rank's (features [n_r, F], targets [n_r]) rows in rank
+    order, on every rank (for fitting one shared network to all ranks' trees).
+    Ranks may hold different row counts; rows are padded to the largest."""
+    import torch
+    import torch.distributed as dist
+
+    if device is None:
+        device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    world = dist.get_world_size(group)
+    feats = np.ascontiguousarray(feats, dtype=np.float32)
+    targets = np.ascontiguousarray(targets, dtype=np.float32)
+    rows = np.concatenate([feats, targets[:, None]], axis=1)
+    n = torch.tensor([rows.shape[0]], dtype=torch.int64, device=device)
+    counts = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(counts, n, group=group)
+    counts = [int(c.item()) for c in counts]
+    width = rows.shape[1]
+    pad = np.zeros((max(counts), width), dtype=np.float32)
+    pad[: rows.shape[0]] = rows
+    t = torch.from_numpy(pad).to(device)
+    parts = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(parts, t, group=group)
+    out = np.concatenate([parts[r].cpu().numpy()[: counts[r]] for r in range(world)])
+    return np.ascontiguousarray(out[:, :-1]), np.ascontiguousarray(out[:, -1])
+
+
+def broadcast_params(params: np.ndarray, src: int = 0, group=None, device: Optional[str] = None) -> np.ndarray:
+    """Rank src's float32 parameter vector on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    if device is None:
+        device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.from_numpy(np.ascontiguousarray(params, dtype=np.float32)).to(device)
+    dist.broadcast(t, src=src, group=group)
+    return t.cpu().numpy()

@@ -353,41 +353,67 @@ def config3(n_trees: int = 512, seed: int = 3) -> list:
 
 def read_once_probability(g: FlatGraph, p: Optional[np.ndarray] = None) -> np.ndarray:
     """Exact probability of every node of a read-once tree (no node with more
-    than one parent): AND = prod p, OR = 1 - prod (1 - p), XOR of two, NOT,
-    ATLEAST k-of-n by the usual count recursion.  Used to calibrate generated
-    rare-event instances; raises for graphs with shared nodes."""
+    than one parent): AND = prod p, OR = 1 - prod (1 - p) (as -expm1(sum
+    log1p(-p)), which keeps its relative precision for tiny p), XOR as a
+    fold, NOT, ATLEAST k-of-n by the usual count recursion.  Gates of one
+    depth are evaluated together.  Used to calibrate generated rare-event
+    instances; raises for graphs with shared nodes."""
+    from .graph import NAND, NOR, NULL
     fanout = np.bincount(g.inputs, minlength=g.n_nodes)
     if np.any(fanout > 1):
         raise ValueError("read_once_probability needs a tree (a node has several parents)")
+    nb, ng = g.n_be, g.n_gates
     pr = np.zeros(g.n_nodes)
-    pr[: g.n_be] = g.quantised_probabilities() if p is None else p
-    from .graph import NAND, NOR, NULL
-    for gi in range(g.n_gates):
-        ins = g.gate_inputs(gi)
-        off = int(g.gate_in_count[gi] - g.gate_neg_count[gi])
-        v = np.array([pr[c] if i < off else 1.0 - pr[c] for i, c in enumerate(ins)])
-        op = int(g.gate_op[gi])
-        if op in (AND, NAND):
-            r = float(np.prod(v)) if v.size else 1.0
-        elif op in (OR, NOR):
-            r = 1.0 - float(np.prod(1.0 - v)) if v.size else 0.0
-        elif op == XOR:
-            r = 0.0
-            for x in v:
-                r = r * (1 - x) + (1 - r) * x
-        elif op == ATLEAST:
-            k = int(g.gate_k[gi]) & 0xFF
-            dist = np.zeros(v.size + 1)
-            dist[0] = 1.0
-            for x in v:
-                dist[1:] = dist[1:] * (1 - x) + dist[:-1] * x
-                dist[0] *= 1 - x
-            r = float(dist[k:].sum()) if k <= v.size else 0.0
-        else:  # NOT, NULL: the last input
-            r = float(v[-1]) if v.size else 0.0
-        if op in (NAND, NOR, NOT):
-            r = 1.0 - r
-        pr[g.n_be + gi] = r
+    pr[:nb] = g.quantised_probabilities() if p is None else p
+    if ng == 0:
+        return pr
+    depth = g.layers()[nb:]
+    cnt = g.gate_in_count.astype(np.int64)
+    pos_neg = cnt - g.gate_neg_count.astype(np.int64)
+    ops = g.gate_op.astype(np.int64)
+    kk = (g.gate_k.astype(np.int64) & 0xFF)
+    for d in range(1, int(depth.max()) + 1):
+        gs = np.nonzero(depth == d)[0]
+        c = cnt[gs]
+        m = int(c.max()) if gs.size else 0
+        col = np.arange(m)
+        valid = col[None, :] < c[:, None]
+        idx = np.where(valid, g.gate_in_begin.astype(np.int64)[gs][:, None] + col[None, :], 0)
+        v = pr[g.inputs[idx].astype(np.int64)] if g.inputs.size else np.zeros((gs.size, m))
+        v = np.where(col[None, :] >= pos_neg[gs][:, None], 1.0 - v, v)
+        v = np.where(valid, v, 0.0)
+        op = ops[gs]
+        r = np.zeros(gs.size)
+        s_and = (op == AND) | (op == NAND)
+        r[s_and] = np.prod(np.where(valid[s_and], v[s_and], 1.0), axis=1)
+        s_or = (op == OR) | (op == NOR)
+        with np.errstate(divide="ignore"):
+            r[s_or] = -np.expm1(np.sum(np.log1p(-v[s_or]), axis=1))
+        s_x = op == XOR
+        if np.any(s_x):
+            acc = np.zeros(int(s_x.sum()))
+            for j in range(m):
+                x = v[s_x, j]
+                acc = acc * (1 - x) + (1 - acc) * x
+            r[s_x] = acc
+        s_k = op == ATLEAST
+        if np.any(s_k):
+            dist = np.zeros((int(s_k.sum()), m + 1))
+            dist[:, 0] = 1.0
+            for j in range(m):
+                x = v[s_k, j][:, None]
+                dist[:, 1:] = dist[:, 1:] * (1 - x) + dist[:, :-1] * x
+                dist[:, 0] *= 1 - x[:, 0]
+            k = kk[gs][s_k]
+            tail = np.cumsum(dist[:, ::-1], axis=1)[:, ::-1]  # tail[:, j] = P(count >= j)
+            r[s_k] = np.where(k <= c[s_k], tail[np.arange(k.size), np.minimum(k, m)], 0.0)
+        s_l = (op == NOT) | (op == NULL)
+        if np.any(s_l):
+            last = np.maximum(c[s_l] - 1, 0)
+            r[s_l] = np.where(c[s_l] > 0, v[s_l][np.arange(last.size), last] if m else 0.0, 0.0)
+        comp = (op == NAND) | (op == NOR) | (op == NOT)
+        r[comp] = 1.0 - r[comp]
+        pr[nb + gs] = r
     return pr
 
 
@@ -423,27 +449,45 @@ def calibrate_rare(g: FlatGraph, target: float, p_floor: float = 1e-9, p_cap: fl
     return out
 
 
-def config5(n_instances: int = 1024, seed: int = 5) -> list:
-    """Batched rare-event instances: basic events log-uniform in [50, 10,000]
-    (gates = events / 1.6), alternating AND-heavy (60/30/10 AND/OR/ATLEAST) and
-    ATLEAST-heavy (30/30/40) mixes, read-once trees whose base probabilities
-    (log-uniform [1e-6, 1e-3]) are rescaled so that the exact top-event
-    probability is a target drawn log-uniformly from [1e-10, 1e-5]."""
-    rng = np.random.default_rng(seed)
-    out = []
-    while len(out) < n_instances:
-        i = len(out)
+def config5_instance(i: int, seed: int = 5) -> FlatGraph:
+    """Instance i of the batched rare-event set: basic events log-uniform in
+    [50, 10,000] (gates = events / 1.6 for the AND-heavy 60/30/10
+    AND/OR/ATLEAST mix of even i, events / 2 for the ATLEAST-heavy 30/30/40
+    mix of odd i, whose ATLEAST gates take 3-5 inputs), a read-once tree
+    whose base probabilities (log-uniform [1e-6, 1e-3]) are rescaled so that
+    the exact top-event probability is a target drawn log-uniformly from
+    [1e-10, 1e-5].  Draws come from a generator seeded by (seed, i), so
+    every instance can be built on its own; an infeasible draw is redrawn."""
+    rng = np.random.default_rng([seed, i])
+    and_heavy = i % 2 == 0
+    mix = {AND: 0.6, OR: 0.3, ATLEAST: 0.1} if and_heavy else {AND: 0.3, OR: 0.3, ATLEAST: 0.4}
+    for _ in range(100):
         nb = int(round(np.exp(rng.uniform(np.log(50), np.log(10000)))))
-        and_heavy = i % 2 == 0
-        mix = {AND: 0.6, OR: 0.3, ATLEAST: 0.1} if and_heavy else {AND: 0.3, OR: 0.3, ATLEAST: 0.4}
-        # a tree needs events + gates - 1 inputs; ATLEAST gates take 3-5, so that mix gets fewer gates
         ng = max(4, int(round(nb / (1.6 if and_heavy else 2.0))))
         target = float(np.exp(rng.uniform(np.log(1e-10), np.log(1e-5))))
         try:
             g = generate(TreeSpec(n_be=nb, n_gates=ng, mix=mix, p_range=(1e-6, 1e-3),
                                   seed=int(rng.integers(1 << 31)), atleast_n=(3, 5), share_be_frac=0.0,
                                   name=f"config5-{i}-{nb}be"))
-            out.append(calibrate_rare(g, target))
+            return calibrate_rare(g, target)
         except ValueError:
-            continue  # infeasible draw or unreachable target: draw another
-    return out
+            continue
+    raise RuntimeError(f"no feasible draw for instance {i}")
+
+
+def config5(n_instances: int = 1024, seed: int = 5, workers: int = 0, first: int = 0) -> list:
+    """Instances first .. first + n_instances - 1 of the batched rare-event set
+    (config5_instance).  workers > 1 builds them in that many spawned
+    processes."""
+    return config5_instances(range(first, first + n_instances), seed, workers)
+
+
+def config5_instances(ids, seed: int = 5, workers: int = 0) -> list:
+    """The batched rare-event instances with the given indices, in order."""
+    ids = list(ids)
+    if workers and workers > 1 and len(ids) > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(config5_instance, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * workers))))
+    return [config5_instance(i, seed) for i in ids]

@@ -1,0 +1,307 @@
+"""Batched learned importance sampling over many rare-event trees.
+
+CPU: the joined graph evaluates every tree exactly as the tree alone (same
+counters), the vectorised features and exact read-once probabilities agree
+with their direct definitions, the rare-event instance generator meets its
+ranges, and the row gather that feeds the shared network works across two
+gloo ranks.  GPU: per-tree FP64 sums and cross-entropy numerators against
+the CPU, the unbiased proposal against plain tallies, and the whole batched
+pipeline against the exact probabilities."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from mcscram_b200 import graph as G
+from mcscram_b200 import synth
+from mcscram_b200.graph import AND, ATLEAST, OR, XOR, probability_threshold
+
+TWO32 = float(1 << 32)
+
+
+def _small_rare(seed, n_be=60, n_gates=30, p_range=(1e-3, 0.05)):
+    return synth.generate(synth.TreeSpec(n_be=n_be, n_gates=n_gates, mix={AND: 0.5, OR: 0.3, ATLEAST: 0.2},
+                                         p_range=p_range, seed=seed, atleast_n=(3, 4), n_layers=5))
+
+
+def _trees():
+    return [_small_rare(1), synth.small_tree(4, n_be=40, n_gates=24, n_layers=5, p_range=(1e-3, 0.05)),
+            _small_rare(7, n_be=37, n_gates=18)]
+
+
+def test_concat_evaluates_each_tree_as_alone(oracle_mod):
+    trees = _trees()
+    u, bb, roots = G.concat(trees)
+    u.validate()
+    assert u.n_be == sum(t.n_be for t in trees) and u.n_gates == sum(t.n_gates for t in trees)
+    assert list(bb) == [0] + list(np.cumsum([t.n_be for t in trees]))
+    W = 300
+    wu = oracle_mod.eval_words(u, 2, 5, W)
+    g0 = u.n_be
+    for k, t in enumerate(trees):
+        # the same tree with the counters its events have in the union
+        tk = t.with_tallies(t.tally_nodes)
+        tk.be_pdag_idx = u.be_pdag_idx[bb[k]:bb[k + 1]].copy()
+        tk.be_event_idx = u.be_event_idx[bb[k]:bb[k + 1]].copy()
+        wk = oracle_mod.eval_words(tk, 2, 5, W)
+        assert np.array_equal(wk[: t.n_be], wu[bb[k]:bb[k + 1]])
+        assert np.array_equal(wk[t.n_be:], wu[g0:g0 + t.n_gates])
+        assert np.array_equal(wk[t.root], wu[roots[k]])
+        g0 += t.n_gates
+
+
+def _event_features_direct(g):
+    """The features by their definition, one event at a time."""
+    from mcscram_b200.importance import N_FEATURES
+    nb, ng = g.n_be, g.n_gates
+    depth = g.layers()
+    L = max(int(depth.max()), 1)
+    parents = [[] for _ in range(g.n_nodes)]
+    for gi in range(ng):
+        for c in g.gate_inputs(gi):
+            parents[int(c)].append(gi)
+    logp = np.log10(np.clip(g.quantised_probabilities(), 1e-12, 1.0))
+    up = np.zeros((ng, 3))
+    for gi in range(ng - 1, -1, -1):
+        ps = parents[nb + gi]
+        if ps:
+            q = ps[0]
+            up[gi] = up[q] + [g.gate_op[q] == AND, g.gate_op[q] == OR, 1]
+    f = np.zeros((nb, N_FEATURES), dtype=np.float32)
+    for e in range(nb):
+        ps = parents[e]
+        f[e, 0] = (logp[e] + 4.0) / 2.0
+        f[e, 1] = len(ps) / 4.0
+        f[e, 15] = 1.0
+        if not ps:
+            continue
+        d = [depth[nb + q] for q in ps]
+        ops = [int(g.gate_op[q]) for q in ps]
+        f[e, 2], f[e, 3] = min(d) / L, max(d) / L
+        f[e, 4:7] = [np.mean([o == x for o in ops]) for x in (AND, OR, ATLEAST)]
+        f[e, 7] = np.mean([int(g.gate_in_count[q]) for q in ps]) / 8.0
+        kn = [int(g.gate_k[q]) / max(int(g.gate_in_count[q]), 1) for q in ps if g.gate_op[q] == ATLEAST]
+        f[e, 8] = np.mean(kn) if kn else 0.0
+        sib = [int(c) for c in g.gate_inputs(ps[0]) if int(c) != e]
+        f[e, 9] = len(sib) / 8.0
+        sb = [logp[c] for c in sib if c < nb]
+        f[e, 10] = (np.mean(sb) + 4.0) / 2.0 if sb else 0.0
+        f[e, 11] = np.mean([c >= nb for c in sib]) if sib else 0.0
+        f[e, 12] = float(max(d) == L)
+        f[e, 13] = up[ps[0], 0] / max(up[ps[0], 2] + 1, 1)
+        f[e, 14] = up[ps[0], 1] / max(up[ps[0], 2] + 1, 1)
+    return f
+
+
+@pytest.mark.parametrize("make", [synth.config1, lambda: synth.small_tree(3), lambda: synth.config5(1, first=3)[0]])
+def test_event_features_match_definition(make):
+    from mcscram_b200.importance import event_features
+    g = make()
+    np.testing.assert_allclose(event_features(g), _event_features_direct(g), rtol=0, atol=1e-6)
+    f = event_features(g, instance_scale=1e3)
+    assert np.all(f[:, 15] == np.float32(0.5))
+
+
+def test_layers_match_definition():
+    for g in (synth.config1(), synth.small_tree(5, n_be=48, n_gates=24, n_layers=5)):
+        ref = np.zeros(g.n_nodes, dtype=np.int64)
+        for j in range(g.n_gates):
+            ins = g.gate_inputs(j)
+            ref[g.n_be + j] = 1 + (int(ref[ins].max()) if ins.size else 0)
+        assert np.array_equal(g.layers(), ref)
+
+
+@pytest.mark.parametrize("seed", range(5))
+def test_read_once_probability_matches_bdd(oracle_mod, seed):
+    g = synth.generate(synth.TreeSpec(n_be=40, n_gates=20, mix={AND: 0.3, OR: 0.3, ATLEAST: 0.2, XOR: 0.1,
+                                                               synth.NOT: 0.1},
+                                      p_range=(1e-4, 0.5), seed=seed, atleast_n=(3, 5)))
+    pr = synth.read_once_probability(g)
+    assert pr[g.root] == pytest.approx(oracle_mod.bdd_probability(g), rel=1e-12)
+
+
+def test_config5_instances_meet_their_ranges(oracle_mod):
+    gs = synth.config5(6, first=0)
+    for i, g in enumerate(gs):
+        assert 50 <= g.n_be <= 10000
+        t = g.meta["target_p_top"]
+        assert 1e-10 <= t <= 1e-5
+        assert abs(np.log(g.meta["exact_p_top"] / t)) < 0.011
+        ops = np.bincount(g.gate_op, minlength=8) / g.n_gates
+        assert (ops[AND] > 0.5) if i % 2 == 0 else (ops[ATLEAST] > 0.3)
+        assert np.all(np.bincount(g.inputs, minlength=g.n_nodes) <= 1)  # read-once
+        if g.n_be <= 1500:
+            assert g.meta["exact_p_top"] == pytest.approx(oracle_mod.bdd_probability(g), rel=1e-9)
+    # an instance does not depend on the others built with it
+    assert np.array_equal(synth.config5(1, first=4)[0].be_threshold, gs[4].be_threshold)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _gather_main(rank, world, port, queue):
+    import torch.distributed as dist
+    from mcscram_b200 import parallel
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    n = 3 + 4 * rank  # uneven row counts
+    f = np.full((n, 16), rank, dtype=np.float32) + np.arange(n, dtype=np.float32)[:, None]
+    t = np.full(n, 10 + rank, dtype=np.float32)
+    F, T = parallel.allgather_rows(f, t)
+    params = parallel.broadcast_params(np.full(5, rank + 1.0, dtype=np.float32))
+    queue.put((rank, F, T, params))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_gloo_row_gather_and_param_broadcast():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, F, T, params in got:
+        assert F.shape == (3 + 7, 16) and T.shape == (10,)
+        assert np.array_equal(T, [10] * 3 + [11] * 7)
+        assert np.array_equal(F[:3, 0], [0, 1, 2]) and np.array_equal(F[3:, 0], 1 + np.arange(7))
+        assert np.array_equal(params, np.ones(5, dtype=np.float32))
+
+
+# ----------------------------------------------------------------------------- GPU
+
+def _log_ratio(p, thr, bits, s):
+    q = thr.astype(np.float64) / TWO32
+    l1 = np.log1p(-p) - np.log1p(-q)
+    a = np.log(p) - np.log(q) - l1
+    return l1[s].sum() + np.einsum("i,iwb->wb", a[s], bits[s])
+
+
+def _union_weights(oracle_mod, u, bb, roots, qthr, it, W, qdef=None, wdef=0):
+    """Per-tree CPU sums and per-event CE numerators of the joined graph; with
+    qdef the first wdef words come from it and samples get the
+    balance-heuristic weight."""
+    if wdef:
+        words = np.concatenate([oracle_mod.eval_words(u.with_thresholds(qdef), it, 0, wdef),
+                                oracle_mod.eval_words(u.with_thresholds(qthr), it, wdef, W - wdef)], axis=1)
+    else:
+        words = oracle_mod.eval_words(u.with_thresholds(qthr), it, 0, W)
+    p = u.quantised_probabilities()
+    bits = ((words[: u.n_be, :, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(np.float64)
+    sums, ce = [], np.zeros(u.n_be)
+    for k in range(len(roots)):
+        s = slice(int(bb[k]), int(bb[k + 1]))
+        top = ((words[roots[k]][:, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(bool)
+        logw = _log_ratio(p, qthr, bits, s)
+        if wdef:
+            alpha = wdef / W
+            logw = -np.logaddexp(np.log(alpha) - _log_ratio(p, qdef, bits, s), np.log1p(-alpha) - logw)
+        w = np.where(top, np.exp(logw), 0.0)
+        sums.append((w.sum(), (w ** 2).sum(), int(top.sum()), logw[top].max() if top.any() else -np.inf))
+        ce[s] = np.einsum("wb,iwb->i", w, bits[s])
+    return sums, ce
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wdef", [0, 300])
+def test_batched_sums_match_cpu(oracle_mod, gpu, wdef):
+    from mcscram_b200.importance import BatchedImportanceSampler
+    trees = _trees()
+    rng = np.random.default_rng(5)
+    with BatchedImportanceSampler(trees, chunk_words=256) as s:
+        p = s.union.quantised_probabilities()
+        q = probability_threshold(np.minimum(p * rng.uniform(2, 30, p.size), 0.5))
+        qdef = probability_threshold(np.minimum(p * 8.0, 0.5)) if wdef else None
+        W = 700  # three chunks, the last one short
+        r = s.run(q, iteration=4, word_count=W, ce=True, q_defensive=qdef, words_defensive=wdef)
+        sums, ce = _union_weights(oracle_mod, s.union, s.be_begin, s.roots, q, 4, W, qdef, wdef)
+    for k, (sw, sw2, h, mx) in enumerate(sums):
+        assert r["hits"][k] == h
+        assert r["sum_w"][k] == pytest.approx(sw, rel=1e-10)
+        assert r["sum_w2"][k] == pytest.approx(sw2, rel=1e-10)
+        assert r["max_log_w"][k] == pytest.approx(mx, rel=1e-12)
+    np.testing.assert_allclose(r["ce_num"], ce, rtol=1e-10, atol=1e-300)
+    assert r["samples"] == W * 64
+
+
+@pytest.mark.gpu
+def test_batched_nominal_proposal_counts_plain_tallies(oracle_mod, gpu):
+    from mcscram_b200.importance import BatchedImportanceSampler
+    trees = _trees()
+    with BatchedImportanceSampler(trees) as s:
+        r = s.run(s.union.be_threshold, iteration=1, word_count=5000)
+        plain = oracle_mod.tallies(s.union, 1, 1, 0, 5000)  # the union tallies its roots
+    assert np.array_equal(r["hits"], plain.astype(np.int64))
+    np.testing.assert_allclose(r["sum_w"], plain.astype(np.float64), rtol=1e-12)
+
+
+@pytest.mark.gpu
+def test_batched_create_rejects_bad_partitions(capi, gpu):
+    import ctypes as C
+    from mcscram_b200 import _capi
+    trees = _trees()
+    u, bb, roots = G.concat(trees)
+    lib = _capi.load()
+    import mcscram_b200.importance  # registers the signatures  # noqa: F401
+    view = _capi.GraphView(u)
+    h = C.c_void_p()
+    bad = np.ascontiguousarray([0, int(bb[1]) + 3, int(bb[2]), int(bb[3])], dtype=np.uint32)
+    rc = lib.mcg_is_batch_create(C.byref(view.desc), 3, bad.ctypes.data_as(C.POINTER(C.c_uint32)), None, C.byref(h))
+    assert rc == _capi.MCG_ERR_INVALID and b"two trees" in lib.mcg_last_error()
+    swapped = u.with_tallies(roots[[1, 0, 2]])
+    view2 = _capi.GraphView(swapped)
+    good = np.ascontiguousarray(bb, dtype=np.uint32)
+    rc = lib.mcg_is_batch_create(C.byref(view2.desc), 3, good.ctypes.data_as(C.POINTER(C.c_uint32)), None,
+                                 C.byref(h))
+    assert rc == _capi.MCG_ERR_INVALID and b"not a node of tree" in lib.mcg_last_error()
+
+
+def _small_config5(n):
+    """The first n instances of the batched rare-event set with at most 600 events."""
+    out, i = [], 0
+    while len(out) < n:
+        g = synth.config5_instance(i)
+        if g.n_be <= 600:
+            out.append(g)
+        i += 1
+    return out
+
+
+@pytest.mark.gpu
+def test_batched_learned_is_reaches_exact(gpu):
+    from mcscram_b200.importance import BatchedImportanceSampler, batched_learned_is
+    trees = _small_config5(6)
+    exact = np.array([g.meta["exact_p_top"] for g in trees])
+    res = batched_learned_is(trees, target_rel_err=0.05, ce_rounds=6, ce_words=1 << 14, max_est_words=1 << 22)
+    assert res.converged.all() and not res.fallback.any(), [r for r in res.rounds if r["phase"] != "probe"]
+    se = res.estimate * res.rel_err95 / 1.96
+    assert np.all(np.abs(res.estimate - exact) <= 4 * se), (res.estimate, exact, se)
+    assert np.all(res.rel_err95 <= 0.05)
+    # what the network adds: at equal samples, its proposal against the probe's uniform inflation
+    with BatchedImportanceSampler(trees) as s:
+        p = s.union.quantised_probabilities()
+        tree_of = np.repeat(np.arange(len(trees)), np.diff(s.be_begin))
+        q0 = np.minimum(p * res.scale[tree_of], 0.5)
+        W = 1 << 14
+        base = s.run(s.proposal_thresholds(q0), iteration=9000, word_count=W)
+        learned = s.run(s.proposal_thresholds(res.q), iteration=9001, word_count=W)
+
+    def rel(r):
+        n = r["samples"]
+        est = r["sum_w"] / n
+        var = np.maximum(r["sum_w2"] / n - est ** 2, 0)
+        return np.sqrt(var / (n - 1)) / np.where(est > 0, est, np.nan)
+
+    assert np.nanmedian(rel(learned)) < np.nanmedian(rel(base))

@@ -61,11 +61,17 @@ def parse_args():
     ap.add_argument("--is-batch-words", type=int, default=1 << 20)
     ap.add_argument("--plain-words", type=int, default=1 << 23, help="words of the plain-MC rate measurement")
     ap.add_argument("--bis-trees", type=int, default=1024)
-    ap.add_argument("--bis-ce-rounds", type=int, default=4)
-    ap.add_argument("--bis-ce-words", type=int, default=1 << 12, help="words per tree per CE round")
+    ap.add_argument("--bis-ce-rounds", type=int, default=5)
+    ap.add_argument("--bis-ce-words", type=int, default=1 << 13, help="words per tree per CE round")
     ap.add_argument("--bis-est-words", type=int, default=1 << 12, help="words per tree of the first estimate round")
     ap.add_argument("--bis-train-steps", type=int, default=150)
     ap.add_argument("--bis-plain-trees", type=int, default=64, help="trees of the plain-rate measurement")
+    ap.add_argument("--bis-mode-cap", type=float, default=0.5, help="cap of the defensive mode proposals")
+    ap.add_argument("--bis-defensive", default="modes", choices=["modes", "approx", "probe"],
+                    help="defensive proposal of the mixture (ablation)")
+    ap.add_argument("--bis-defensive-share", type=float, default=0.3)
+    ap.add_argument("--bis-no-network", action="store_true", help="CE targets as the proposal (ablation)")
+    ap.add_argument("--bis-no-importance-features", action="store_true", help="ablation")
     ap.add_argument("--bis-workers", type=int, default=0, help="generator processes (0 = host threads, max 32)")
     ap.add_argument("--ua-trees", type=int, default=512)
     ap.add_argument("--ua-draws", type=int, default=16)
@@ -375,7 +381,10 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     t0 = time.perf_counter()
     res = batched_learned_is(trees, target_rel_err=0.05, device=local, ce_rounds=args.bis_ce_rounds,
                              ce_words=args.bis_ce_words, est_words=args.bis_est_words,
-                             train_steps=args.bis_train_steps)
+                             train_steps=args.bis_train_steps, mode_cap=args.bis_mode_cap, workers=workers,
+                             defensive_proposal=args.bis_defensive, defensive=args.bis_defensive_share,
+                             use_network=not args.bis_no_network,
+                             importance_features=not args.bis_no_importance_features)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     clk = clocks.stop()
@@ -387,6 +396,12 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     err = np.abs(res.estimate - exact) / exact
     se = res.estimate * res.rel_err95 / z
     within3 = np.abs(res.estimate - exact) <= 3 * se
+    with np.errstate(divide="ignore", invalid="ignore"):
+        zs = np.where(se > 0, (res.estimate - exact) / se, np.inf)
+    worst = [{"tree": int(mine_idx[k]), "events": trees[k].n_be, "p_exact": float(exact[k]),
+              "est_over_exact": float(res.estimate[k] / exact[k]), "rel_err95": float(res.rel_err95[k]),
+              "z": float(zs[k]), "converged": bool(res.converged[k]), "fallback": bool(res.fallback[k])}
+             for k in np.argsort(-np.abs(np.nan_to_num(zs, nan=np.inf)))[:12] if not within3[k]]
     wall_max, gpu_max = wall, gpu_s
     if world > 1:
         wall_max, gpu_max = parallel.allreduce_max([wall, gpu_s])
@@ -405,13 +420,16 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
                                    "[1e-10, 1e-5]), one shared 16-64-64-1 proposal network, until 5% rel err "
                                    "(95%) per tree or plain fallback",
                        "ce_rounds": args.bis_ce_rounds, "ce_samples_per_tree": args.bis_ce_words * 64,
+                       "defensive": args.bis_defensive, "defensive_share": args.bis_defensive_share,
+                       "network": not args.bis_no_network, "importance_features": not args.bis_no_importance_features,
                        "events": int(nb.sum()), "gates": int(sum(g.n_gates for g in trees))},
             "is": {"wall_s": wall_max, "gpu_s": gpu_max, "gpu_ms_by_phase": res.gpu_ms,
                    "wall_s_by_phase": res.seconds, "trees": int(counts[3]), "converged": int(counts[0]),
                    "fallback": int(counts[1]), "within_3_sigma_of_exact": int(counts[2]),
                    "median_abs_rel_err_vs_exact": float(np.median(err)), "max_abs_rel_err_vs_exact": float(err.max()),
                    "max_rel_err95": float(res.rel_err95.max()), "samples_total": int(res.samples.sum()),
-                   "rounds": len(res.rounds)},
+                   "rounds": len(res.rounds), "converged_outside_3_sigma": int((res.converged & ~within3).sum()),
+                   "outside_3_sigma_rank0": worst},
             "plain": {"event_words_per_s": be_word_s, "measured_on_trees": len(sub), "measured_words": args.plain_words >> 6,
                       "measured_ms": plain_ms, "required_samples_total": float(n_req.sum()), "seconds": plain_s,
                       "note": "plain batched MC time to the same accuracy, extrapolated from the plain staged "

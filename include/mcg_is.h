@@ -67,22 +67,24 @@ mcg_status mcg_is_batch_destroy(mcg_is_batch *b);
 
 /* Samples pass `iteration`, words [word_begin, word_begin + word_count) of
  * every tree with proposal thresholds q_threshold[n_be] (rules as for
- * mcg_is_run).  With a defensive proposal (q_defensive[n_be], words_defensive
- * > 0) the first words_defensive words are drawn from q_defensive and the
- * rest from q_threshold, and every sample is weighted by the balance
- * heuristic of multiple importance sampling,
- *     w = p(x) / (alpha q_defensive(x) + (1 - alpha) q(x)),
- *     alpha = words_defensive / word_count,
- * which stays unbiased and bounds the variance by 1 / alpha times that of
- * the defensive proposal alone (a failure region the proposal misses is
- * still sampled).  q_defensive may be NULL when words_defensive is 0.
+ * mcg_is_run).  With n_defensive > 0 defensive proposals
+ * (q_defensive[n_defensive][n_be], component-major, and their word counts
+ * words_defensive[n_defensive], together at most word_count) the main
+ * proposal draws the first word_count - sum(words_defensive) words and
+ * defensive proposal c the next words_defensive[c], and every sample is
+ * weighted by the balance heuristic of multiple importance sampling,
+ *     w = p(x) / sum_c pi_c q_c(x),   pi_c = words of c / word_count,
+ * which stays unbiased and keeps w <= p / (pi_c q_c) for every component
+ * (a failure region the main proposal misses is still sampled through
+ * the defensive ones).  At most 7 defensive proposals.
  * tree_sums (host, 4 * n_tree doubles) receives per tree {sum w, sum w^2,
  * hits, max log w} over its word_count * 64 samples; ce_num (host, n_be
  * doubles, optional) sum over hits of w * x_i; kernel_ms (optional) the
  * device time of the call (CUDA events). */
-mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_threshold, const uint64_t *q_defensive,
-                            uint64_t words_defensive, uint32_t iteration, uint64_t word_begin, uint64_t word_count,
-                            double *tree_sums, double *ce_num, double *kernel_ms);
+mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_threshold, uint32_t n_defensive,
+                            const uint64_t *q_defensive, const uint64_t *words_defensive, uint32_t iteration,
+                            uint64_t word_begin, uint64_t word_count, double *tree_sums, double *ce_num,
+                            double *kernel_ms);
 
 /* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
  * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32

@@ -11,6 +11,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine_internal.hpp"
@@ -119,27 +120,32 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights(const uint64_t *_
 // Work items are (tree, strip of 256 words), taken from a queue (a counter
 // zeroed before the launch) so that trees of very different size balance.
 // One thread per word: the buffer rows are read coalesced, and because
-// x_i & top is almost always zero under a proposal, the FP64 log-ratio of a
-// sample is only touched where event i fired in a sample where the tree's
-// top event fired.  acc[] (per-thread, local memory) holds the running
-// sum of a_i of sample b, later its weight.
-// With a defensive proposal (a_def != null) every sample is weighted by the
-// balance heuristic of multiple importance sampling,
-//     w = p(x) / (alpha q_def(x) + (1 - alpha) q(x)),
-//     log w = -logaddexp(ln alpha - log(p/q_def), ln(1 - alpha) - log(p/q)),
-// whichever of the two proposals drew it; accd[] holds log(p/q_def).
+// x_i & top is almost always zero under a proposal, the FP64 log-ratios of
+// a sample are only touched where event i fired in a sample where the
+// tree's top event fired.
+// A pass may draw its words from several proposals (components c = 0 ..
+// n_comp - 1, component 0 the main one, c taking a share pi_c of the
+// words).  Every sample is then weighted by the balance heuristic of
+// multiple importance sampling, whichever component drew it:
+//     w = p(x) / sum_c pi_c q_c(x),
+//     log w = -logsumexp_c(ln pi_c - log(p / q_c)(x)),
+// which is unbiased and keeps w <= p / (pi_c q_c) for every c.
+// acc[c][b] (per-thread, local memory) holds log(p / q_c) - C_c of sample
+// b, acc[0][b] later its weight.
+constexpr int kMaxComponents = 8;
+
 struct IsBatchArgs {
     const uint64_t *buf;
     uint64_t W;
     uint32_t n_inst;
     uint32_t strips;               // ceil(W / kWeightThreads)
+    uint32_t n_comp;               // 1 .. kMaxComponents
+    uint32_t n_be;                 // stride of a[] and C[] between components
     const uint32_t *be_begin;      // n_inst + 1
     const uint32_t *root_row;      // n_inst
-    const double *a;               // per event
-    const double *C;               // per tree
-    const double *a_def;           // defensive proposal's terms, or null
-    const double *C_def;
-    double log_alpha, log_1m_alpha;  // share of the samples the defensive proposal draws
+    const double *a;               // [n_comp][n_be]
+    const double *C;               // [n_comp][n_inst]
+    double log_pi[kMaxComponents];
     double *sums;                  // per tree: sum w, sum w^2, hits, max log w
     double *ce;                    // per event, or null
     unsigned long long *queue;
@@ -147,9 +153,9 @@ struct IsBatchArgs {
 
 __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs p) {
     __shared__ unsigned long long s_item;
-    double acc[64], accd[64];
-    const bool mix = p.a_def != nullptr;
+    double acc[kMaxComponents][64];
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nc = p.n_comp;
     const uint64_t items = (uint64_t)p.n_inst * p.strips;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1ull);
@@ -163,8 +169,8 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
         const uint64_t top = valid ? p.buf[(uint64_t)p.root_row[k] * p.W + w] : 0ull;
         if (!__syncthreads_or(top != 0ull)) continue;
         for (uint64_t m = top; m; m &= m - 1) {
-            acc[__ffsll((long long)m) - 1] = 0.0;
-            accd[__ffsll((long long)m) - 1] = 0.0;
+            const int b = __ffsll((long long)m) - 1;
+            for (uint32_t c = 0; c < nc; ++c) acc[c][b] = 0.0;
         }
         const uint32_t b0 = p.be_begin[k], b1 = p.be_begin[k + 1];
         const uint64_t *col = p.buf + w;
@@ -175,42 +181,35 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
             for (int j = 0; j < 4; ++j) x[j] = valid ? col[(uint64_t)(i + j) * p.W] : 0ull;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                uint64_t m = x[j] & top;
-                if (m) {
-                    const double ai = p.a[i + j], di = mix ? p.a_def[i + j] : 0.0;
-                    do {
-                        const int b = __ffsll((long long)m) - 1;
-                        acc[b] += ai;
-                        accd[b] += di;
-                        m &= m - 1;
-                    } while (m);
+                for (uint64_t m = x[j] & top; m; m &= m - 1) {
+                    const int b = __ffsll((long long)m) - 1;
+                    for (uint32_t c = 0; c < nc; ++c) acc[c][b] += p.a[(uint64_t)c * p.n_be + i + j];
                 }
             }
         }
         for (; i < b1; ++i) {
-            uint64_t m = (valid ? col[(uint64_t)i * p.W] : 0ull) & top;
-            if (m) {
-                const double ai = p.a[i], di = mix ? p.a_def[i] : 0.0;
-                do {
-                    const int b = __ffsll((long long)m) - 1;
-                    acc[b] += ai;
-                    accd[b] += di;
-                    m &= m - 1;
-                } while (m);
+            for (uint64_t m = (valid ? col[(uint64_t)i * p.W] : 0ull) & top; m; m &= m - 1) {
+                const int b = __ffsll((long long)m) - 1;
+                for (uint32_t c = 0; c < nc; ++c) acc[c][b] += p.a[(uint64_t)c * p.n_be + i];
             }
         }
-        const double C = p.C[k], Cd = mix ? p.C_def[k] : 0.0;
         double lsum = 0.0, lsum2 = 0.0, lhits = 0.0, lmax = -INFINITY;
         for (uint64_t m = top; m; m &= m - 1) {
             const int b = __ffsll((long long)m) - 1;
-            double lw = C + acc[b];
-            if (mix) {
-                const double u1 = p.log_alpha - (Cd + accd[b]), u2 = p.log_1m_alpha - lw;
-                const double hi = fmax(u1, u2), lo = fmin(u1, u2);
-                lw = -(hi + log1p(exp(lo - hi)));
+            double lw = p.C[k] + acc[0][b];
+            if (nc > 1) {
+                // -logsumexp_c(ln pi_c - log(p/q_c))
+                double u[kMaxComponents], hi = -INFINITY;
+                for (uint32_t c = 0; c < nc; ++c) {
+                    u[c] = p.log_pi[c] - (p.C[(uint64_t)c * p.n_inst + k] + acc[c][b]);
+                    hi = fmax(hi, u[c]);
+                }
+                double s = 0.0;
+                for (uint32_t c = 0; c < nc; ++c) s += exp(u[c] - hi);
+                lw = -(hi + log(s));
             }
             const double wv = exp(lw);
-            acc[b] = wv;
+            acc[0][b] = wv;
             lsum += wv;
             lsum2 += wv * wv;
             lhits += 1.0;
@@ -220,7 +219,7 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
             for (uint32_t e = b0; e < b1; ++e) {
                 uint64_t m = (valid ? col[(uint64_t)e * p.W] : 0ull) & top;
                 double c = 0.0;
-                for (; m; m &= m - 1) c += acc[__ffsll((long long)m) - 1];
+                for (; m; m &= m - 1) c += acc[0][__ffsll((long long)m) - 1];
                 if (__any_sync(0xFFFFFFFFu, c != 0.0)) {
                     c = warp_sum(c);
                     if (lane == 0 && c != 0.0) atomicAdd(&p.ce[e], c);
@@ -406,21 +405,19 @@ mcg_status mcg_is_run(mcg_is *is, const uint64_t *q_thr, uint32_t iteration, uin
 struct mcg_is_batch {
     mcg_engine *engine = nullptr;
     uint32_t n_inst = 0;
+    uint32_t n_comp_cap = 0;             // components the device arrays hold
     std::vector<uint32_t> be_begin;
-    uint4 *d_be_q = nullptr;
-    uint4 *d_be_def = nullptr;
-    double *d_a = nullptr;
-    double *d_C = nullptr;
-    double *d_a_def = nullptr;
-    double *d_C_def = nullptr;
+    uint4 *d_be_q = nullptr;             // [n_comp][n_be] sampler tables
+    double *d_a = nullptr;               // [n_comp][n_be]
+    double *d_C = nullptr;               // [n_comp][n_inst]
     double *d_sums = nullptr;
     double *d_ce = nullptr;
     uint32_t *d_be_begin = nullptr;
     uint32_t *d_root = nullptr;
     unsigned long long *d_queue = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<uint4> beq, beq_def;
-    std::vector<double> a, C, a_def, C_def, init;
+    std::vector<uint4> beq;
+    std::vector<double> a, C, init;
 };
 
 namespace {
@@ -433,11 +430,8 @@ void release_batch(mcg_is_batch *b) {
         cudaStreamSynchronize(b->engine->stream);
     }
     cudaFree(b->d_be_q);
-    cudaFree(b->d_be_def);
     cudaFree(b->d_a);
     cudaFree(b->d_C);
-    cudaFree(b->d_a_def);
-    cudaFree(b->d_C_def);
     cudaFree(b->d_sums);
     cudaFree(b->d_ce);
     cudaFree(b->d_be_begin);
@@ -506,13 +500,7 @@ mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_inst, con
     if (!bad.empty()) return mcg::fail(MCG_ERR_INVALID, bad);
     const uint32_t nb = std::max<uint32_t>(g.n_be, 1);
     MCG_CUDA(cudaSetDevice(b->engine->device));
-    MCG_CUDA(cudaMalloc((void **)&b->d_be_q, nb * sizeof(uint4)));
-    MCG_CUDA(cudaMalloc((void **)&b->d_be_def, nb * sizeof(uint4)));
-    MCG_CUDA(cudaMalloc((void **)&b->d_a_def, nb * sizeof(double)));
-    MCG_CUDA(cudaMalloc((void **)&b->d_C_def, n_inst * sizeof(double)));
-    MCG_CUDA(cudaMalloc((void **)&b->d_a, nb * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_ce, nb * sizeof(double)));
-    MCG_CUDA(cudaMalloc((void **)&b->d_C, n_inst * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_sums, 4ull * n_inst * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_be_begin, (n_inst + 1ull) * sizeof(uint32_t)));
     MCG_CUDA(cudaMalloc((void **)&b->d_root, n_inst * sizeof(uint32_t)));
@@ -521,12 +509,6 @@ mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_inst, con
     MCG_CUDA(cudaMemcpy(b->d_root, g.tally_nodes.data(), n_inst * sizeof(uint32_t), cudaMemcpyHostToDevice));
     MCG_CUDA(cudaEventCreate(&b->ev0));
     MCG_CUDA(cudaEventCreate(&b->ev1));
-    b->beq.resize(nb);
-    b->beq_def.resize(nb);
-    b->a.resize(nb);
-    b->a_def.resize(nb);
-    b->C.resize(n_inst);
-    b->C_def.resize(n_inst);
     b->init.resize(4ull * n_inst);
     for (uint32_t k = 0; k < n_inst; ++k) {
         b->init[4ull * k] = b->init[4ull * k + 1] = b->init[4ull * k + 2] = 0.0;
@@ -544,13 +526,42 @@ mcg_status mcg_is_batch_destroy(mcg_is_batch *b) {
     return MCG_OK;
 }
 
-mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, const uint64_t *q_def, uint64_t words_def,
-                            uint32_t iteration, uint64_t word_begin, uint64_t word_count, double *tree_sums,
-                            double *ce_num, double *kernel_ms) {
+}  // extern "C"
+
+namespace {
+
+// Device arrays for n_comp components, grown on demand.
+mcg_status ensure_components(mcg_is_batch *b, uint32_t n_comp) {
+    if (n_comp <= b->n_comp_cap) return MCG_OK;
+    const uint64_t nb = std::max<uint32_t>(b->engine->graph.n_be, 1);
+    cudaFree(b->d_be_q);
+    cudaFree(b->d_a);
+    cudaFree(b->d_C);
+    b->d_be_q = nullptr;
+    b->d_a = b->d_C = nullptr;
+    b->n_comp_cap = 0;
+    MCG_CUDA(cudaMalloc((void **)&b->d_be_q, n_comp * nb * sizeof(uint4)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_a, n_comp * nb * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_C, (uint64_t)n_comp * b->n_inst * sizeof(double)));
+    b->n_comp_cap = n_comp;
+    return MCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_def, const uint64_t *q_def,
+                            const uint64_t *words_def, uint32_t iteration, uint64_t word_begin, uint64_t word_count,
+                            double *tree_sums, double *ce_num, double *kernel_ms) {
     mcg::clear_error();
     if (!b || !q_thr || !tree_sums) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
-    if (words_def > word_count) return mcg::fail(MCG_ERR_INVALID, "words_defensive exceeds word_count");
-    if (words_def > 0 && !q_def) return mcg::fail(MCG_ERR_INVALID, "words_defensive > 0 needs q_defensive");
+    if (n_def + 1 > (uint32_t)kMaxComponents)
+        return mcg::fail(MCG_ERR_INVALID, "at most " + std::to_string(kMaxComponents - 1) + " defensive proposals");
+    if (n_def && (!q_def || !words_def)) return mcg::fail(MCG_ERR_INVALID, "n_defensive > 0 needs q_defensive and words");
+    uint64_t def_total = 0;
+    for (uint32_t c = 0; c < n_def; ++c) def_total += words_def[c];
+    if (def_total > word_count) return mcg::fail(MCG_ERR_INVALID, "defensive words exceed word_count");
     mcg_engine *e = b->engine;
     const mcg::Graph &g = e->graph;
     if (word_begin + word_count > (1ull << 32) || word_begin + word_count < word_begin)
@@ -558,49 +569,71 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, const uint64
     if ((uint64_t)iteration + 2 >= (1ull << 26))
         return mcg::fail(MCG_ERR_INVALID, "iteration exceeds the 26-bit pass counter field");
     const uint32_t n_inst = b->n_inst;
-    const bool mix = words_def > 0 && words_def < word_count;
-    const uint64_t *q_only = words_def == word_count && words_def ? q_def : q_thr;  // one proposal draws all
-    std::string why;
-    for (uint32_t k = 0; k < n_inst; ++k) {
-        if (!ratio_terms(g, q_only, b->be_begin[k], b->be_begin[k + 1], b->beq.data(), b->a.data(), b->C[k], why))
-            return mcg::fail(MCG_ERR_INVALID, why);
-        if (mix && !ratio_terms(g, q_def, b->be_begin[k], b->be_begin[k + 1], b->beq_def.data(), b->a_def.data(),
-                                b->C_def[k], why))
-            return mcg::fail(MCG_ERR_INVALID, why);
+    const uint64_t nb = g.n_be;
+    // Components that draw words: the main proposal (if it gets any) and
+    // every defensive proposal with words.  A single component needs no mixture.
+    std::vector<const uint64_t *> comp_q;
+    std::vector<uint64_t> comp_words;
+    if (word_count - def_total > 0) {
+        comp_q.push_back(q_thr);
+        comp_words.push_back(word_count - def_total);
     }
-    MCG_CUDA(cudaSetDevice(e->device));
-    if (g.n_be) {
-        MCG_CUDA(cudaMemcpyAsync(b->d_be_q, b->beq.data(), g.n_be * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
-        MCG_CUDA(cudaMemcpyAsync(b->d_a, b->a.data(), g.n_be * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-        MCG_CUDA(cudaMemsetAsync(b->d_ce, 0, g.n_be * sizeof(double), e->stream));
-        if (mix) {
-            MCG_CUDA(cudaMemcpyAsync(b->d_be_def, b->beq_def.data(), g.n_be * sizeof(uint4), cudaMemcpyHostToDevice,
-                                     e->stream));
-            MCG_CUDA(cudaMemcpyAsync(b->d_a_def, b->a_def.data(), g.n_be * sizeof(double), cudaMemcpyHostToDevice,
-                                     e->stream));
+    for (uint32_t c = 0; c < n_def; ++c)
+        if (words_def[c]) {
+            comp_q.push_back(q_def + (uint64_t)c * nb);
+            comp_words.push_back(words_def[c]);
         }
+    if (comp_q.empty()) comp_q.push_back(q_thr), comp_words.push_back(0);
+    const uint32_t nc = (uint32_t)comp_q.size();
+    MCG_CUDA(cudaSetDevice(e->device));
+    mcg_status st = ensure_components(b, nc);
+    if (st != MCG_OK) return st;
+    b->beq.resize(nc * std::max<uint64_t>(nb, 1));
+    b->a.resize(nc * std::max<uint64_t>(nb, 1));
+    b->C.resize((uint64_t)nc * n_inst);
+    // log-ratio terms of every (component, tree), split over the host threads
+    const uint64_t jobs = (uint64_t)nc * n_inst;
+    const unsigned n_thr = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(
+        std::max(1u, std::thread::hardware_concurrency()), std::min<uint64_t>(jobs, nb / 65536 + 1)));
+    std::vector<std::string> why(n_thr);
+    std::vector<char> bad(n_thr, 0);
+    auto work = [&](unsigned t) {
+        for (uint64_t j = t; j < jobs; j += n_thr) {
+            const uint32_t c = (uint32_t)(j / n_inst), k = (uint32_t)(j % n_inst);
+            if (!ratio_terms(g, comp_q[c], b->be_begin[k], b->be_begin[k + 1], b->beq.data() + c * nb,
+                             b->a.data() + c * nb, b->C[(uint64_t)c * n_inst + k], why[t])) {
+                bad[t] = 1;
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < n_thr; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (unsigned t = 0; t < n_thr; ++t)
+        if (bad[t]) return mcg::fail(MCG_ERR_INVALID, why[t]);
+    if (nb) {
+        MCG_CUDA(cudaMemcpyAsync(b->d_be_q, b->beq.data(), nc * nb * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
+        MCG_CUDA(cudaMemcpyAsync(b->d_a, b->a.data(), nc * nb * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        MCG_CUDA(cudaMemsetAsync(b->d_ce, 0, nb * sizeof(double), e->stream));
     }
-    MCG_CUDA(cudaMemcpyAsync(b->d_C, b->C.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-    if (mix)
-        MCG_CUDA(cudaMemcpyAsync(b->d_C_def, b->C_def.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice,
-                                 e->stream));
+    MCG_CUDA(cudaMemcpyAsync(b->d_C, b->C.data(), (uint64_t)nc * n_inst * sizeof(double), cudaMemcpyHostToDevice,
+                             e->stream));
     MCG_CUDA(cudaMemcpyAsync(b->d_sums, b->init.data(), 4ull * n_inst * sizeof(double), cudaMemcpyHostToDevice,
                              e->stream));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
     IsBatchArgs args{};
     args.n_inst = n_inst;
+    args.n_comp = nc;
+    args.n_be = (uint32_t)nb;
     args.be_begin = b->d_be_begin;
     args.root_row = b->d_root;
     args.a = b->d_a;
     args.C = b->d_C;
-    if (mix) {
-        const double alpha = (double)words_def / (double)word_count;
-        args.a_def = b->d_a_def;
-        args.C_def = b->d_C_def;
-        args.log_alpha = std::log(alpha);
-        args.log_1m_alpha = std::log1p(-alpha);
-    }
+    for (uint32_t c = 0; c < nc; ++c)
+        args.log_pi[c] = nc > 1 ? std::log((double)comp_words[c] / (double)word_count) : 0.0;
     args.sums = b->d_sums;
     args.ce = ce_num ? b->d_ce : nullptr;
     args.queue = b->d_queue;
@@ -621,18 +654,14 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, const uint64
         return MCG_OK;
     };
     MCG_CUDA(cudaEventRecord(b->ev0, e->stream));
-    // the defensive proposal draws the first words_def words, the proposal the rest
-    mcg_status st = MCG_OK;
-    if (mix) {
-        e->d_be_sample = b->d_be_def;
-        e->table_iteration = 0xFFFFFFFFu;
-        st = mcg::internal::run_staged(e, iteration, 1, word_begin, words_def);
-    }
-    if (st == MCG_OK && word_count > (mix ? words_def : 0)) {
-        e->d_be_sample = b->d_be_q;
-        e->table_iteration = 0xFFFFFFFFu;
-        const uint64_t off = mix ? words_def : 0;
-        st = mcg::internal::run_staged(e, iteration, 1, word_begin + off, word_count - off);
+    // component c draws the next comp_words[c] words with its own sampler table
+    uint64_t off = 0;
+    for (uint32_t c = 0; c < nc && st == MCG_OK; ++c) {
+        if (!comp_words[c]) continue;
+        e->d_be_sample = b->d_be_q + c * nb;
+        e->table_iteration = 0xFFFFFFFFu;  // the sampler table follows the component
+        st = mcg::internal::run_staged(e, iteration, 1, word_begin + off, comp_words[c]);
+        off += comp_words[c];
     }
     e->chunk_hook = nullptr;
     e->d_be_sample = nullptr;
@@ -640,8 +669,8 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, const uint64
     if (st != MCG_OK) return st;
     MCG_CUDA(cudaEventRecord(b->ev1, e->stream));
     MCG_CUDA(cudaMemcpyAsync(tree_sums, b->d_sums, 4ull * n_inst * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    if (ce_num && g.n_be)
-        MCG_CUDA(cudaMemcpyAsync(ce_num, b->d_ce, g.n_be * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    if (ce_num && nb)
+        MCG_CUDA(cudaMemcpyAsync(ce_num, b->d_ce, nb * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     MCG_CUDA(cudaStreamSynchronize(e->stream));
     if (kernel_ms) {
         float ms = 0.f;

@@ -56,8 +56,8 @@ _capi.register_signatures({
     "mcg_is_batch_create": (C.c_int, [C.POINTER(_capi.GraphDesc), C.c_uint32, C.POINTER(C.c_uint32),
                                       C.POINTER(_capi.RunDesc), C.POINTER(_vp)]),
     "mcg_is_batch_destroy": (C.c_int, [_vp]),
-    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, _u64p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _dp, _dp,
-                                   _dp]),
+    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, C.c_uint32, _u64p, _u64p, C.c_uint32, C.c_uint64, C.c_uint64, _dp,
+                                   _dp, _dp]),
     "mcg_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_vp)]),
     "mcg_mlp_destroy": (C.c_int, [_vp]),
     "mcg_mlp_set_params": (C.c_int, [_vp, _fp]),
@@ -72,7 +72,7 @@ def _p(a, t):
     return a.ctypes.data_as(C.POINTER(t))
 
 
-def approximate_importance(g: FlatGraph):
+def approximate_importance(g: FlatGraph, root=None):
     """Node probabilities and per-event conditional marginals under the
     independence approximation (every gate's inputs taken as independent):
     one bottom-up pass gives P~ of every node, one reverse-mode pass the
@@ -81,13 +81,18 @@ def approximate_importance(g: FlatGraph):
     the approximate conditional marginal that the zero-variance product
     proposal needs (approximate zero-variance importance sampling).  Exact
     for trees where no node has two parents; an approximation, and still
-    cheap, for DAGs.  Returns (node_prob [n_nodes], cond [n_be])."""
+    cheap, for DAGs.  With `root` (a node id) the marginals are conditioned on
+    that node instead of the top event (events outside its cone keep p);
+    with a list of node ids, on each of them (cond then [len(root), n_be]).
+    Returns (node_prob [n_nodes], cond [n_be])."""
     from .graph import NAND, NOR, NOT, NULL
     nb, ng = g.n_be, g.n_gates
     pr = np.zeros(g.n_nodes)
     pr[:nb] = g.quantised_probabilities()
     if ng == 0 or nb == 0:
-        return pr, pr[:nb].copy()
+        roots = [g.root if root is None else int(root)] if np.ndim(root) == 0 else [int(r) for r in root]
+        cond = _conditioned(pr, [], nb, g.n_nodes, roots)
+        return pr, (cond[0] if np.ndim(root) == 0 else cond)
     depth = g.layers()[nb:]
     cnt = g.gate_in_count.astype(np.int64)
     pos_neg = cnt - g.gate_neg_count.astype(np.int64)
@@ -166,18 +171,65 @@ def approximate_importance(g: FlatGraph):
         d = np.where(valid, d, 0.0)
         pr[nb + gs] = r
         cache.append((gs, src, valid, d))
-    # reverse mode: adj = d log P~_top / d P~_node
-    adj = np.zeros(g.n_nodes)
-    top = pr[g.root]
-    if top <= 0:
-        return pr, pr[:nb].copy()
-    adj[g.root] = 1.0 / top
+    roots = [g.root if root is None else int(root)] if np.ndim(root) == 0 else [int(r) for r in root]
+    cond = _conditioned(pr, cache, nb, g.n_nodes, roots)
+    return pr, (cond[0] if np.ndim(root) == 0 else cond)
+
+
+def _conditioned(pr, cache, nb, n_nodes, roots):
+    """Reverse mode for several conditioning nodes at once:
+    adj[:, r] = d log P~_root_r / d P~_node, then the conditional marginals
+    [len(roots), n_be]."""
+    R = len(roots)
+    adj = np.zeros((n_nodes, R))
+    live = np.zeros(R, dtype=bool)
+    for j, r0 in enumerate(roots):
+        if pr[r0] > 1e-300:
+            adj[r0, j] = 1.0 / pr[r0]
+            live[j] = True
     for gs, src, valid, d in reversed(cache):
-        contrib = adj[nb + gs][:, None] * d
+        contrib = adj[nb + gs][:, None, :] * d[:, :, None]
         np.add.at(adj, src[valid], contrib[valid])
     p = pr[:nb]
-    cond = np.clip(p + p * (1.0 - p) * adj[:nb], 0.0, 1.0)
-    return pr, cond
+    cond = np.clip(p[None, :] + (p * (1.0 - p))[None, :] * adj[:nb].T, 0.0, 1.0)
+    for j, r0 in enumerate(roots):
+        if not live[j]:  # nothing to condition on
+            cond[j] = p
+        elif r0 < nb:  # conditioned on a basic event: it fires, the rest keep p
+            cond[j] = p
+            cond[j, r0] = 1.0
+    return cond
+
+
+def mode_proposals(g: FlatGraph, n_comp: int, cap: float) -> np.ndarray:
+    """Defensive proposals for the union-of-modes form of the top event
+    ([n_comp, n_be]).  When the top gate is an OR, component j is the
+    approximate zero-variance proposal conditioned on its child j failing
+    (approximate_importance with that child as root; events outside the
+    child keep p): sampling every child's failure region at a fixed share is
+    the mixture form of importance sampling for a union of rare events.
+    With more children than components the last component is the
+    unconditioned proposal, and with fewer children (or a top gate that is
+    not an OR) components repeat.  Clipped to [1e-7, cap]."""
+    from .graph import OR
+    nb = g.n_be
+    top = g.root - nb
+    kids = []
+    if 0 <= top < g.n_gates and int(g.gate_op[top]) == OR and int(g.gate_neg_count[top]) == 0:
+        kids = [int(c) for c in g.gate_inputs(top)]
+    pr, cond = approximate_importance(g, root=[g.root] + kids)
+    cond = np.clip(cond, 1e-7, cap)
+    whole = cond[0]
+    if not kids:
+        return np.repeat(whole[None, :], n_comp, axis=0)
+    order = sorted(range(len(kids)), key=lambda j: -pr[kids[j]])  # heaviest modes first
+    comps = [cond[1 + j] for j in order[:n_comp]]
+    if len(kids) > n_comp:
+        comps[-1] = whole
+    out = np.empty((n_comp, nb))
+    for j in range(n_comp):
+        out[j] = comps[j % len(comps)]
+    return out
 
 
 def event_features(g: FlatGraph, instance_scale: Optional[float] = None, importance: bool = False) -> np.ndarray:
@@ -519,22 +571,28 @@ class BatchedImportanceSampler:
         return _proposal_thr(self.union.be_threshold, q)
 
     def run(self, q_thresholds: np.ndarray, iteration: int = 1, word_begin: int = 0, word_count: int = 1 << 14,
-            ce: bool = False, q_defensive: Optional[np.ndarray] = None, words_defensive: int = 0) -> dict:
-        """Per-tree sums of one pass; with q_defensive the first words_defensive
-        words come from it and samples carry the balance-heuristic weight."""
+            ce: bool = False, q_defensive: Optional[np.ndarray] = None, words_defensive=0) -> dict:
+        """Per-tree sums of one pass.  q_defensive ([n_be] or [n_comp, n_be]
+        thresholds) with words_defensive (an int or one per component): the
+        main proposal draws the first words, each defensive proposal the next
+        words_defensive[c], and samples carry the balance-heuristic weight."""
         q_thresholds = np.ascontiguousarray(q_thresholds, dtype=np.uint64)
-        if q_thresholds.shape != (self.union.n_be,):
+        nb = self.union.n_be
+        if q_thresholds.shape != (nb,):
             raise ValueError("one proposal threshold per event of the joined graph")
-        qd = None
+        qd, wd, n_def = None, None, 0
         if q_defensive is not None:
-            qd = np.ascontiguousarray(q_defensive, dtype=np.uint64)
-            if qd.shape != (self.union.n_be,):
+            qd = np.ascontiguousarray(np.atleast_2d(q_defensive), dtype=np.uint64)
+            if qd.shape[1] != nb:
                 raise ValueError("one defensive threshold per event of the joined graph")
+            n_def = qd.shape[0]
+            wd = np.ascontiguousarray(np.broadcast_to(np.asarray(words_defensive, dtype=np.uint64), (n_def,)))
         sums = np.zeros((self.n_trees, 4), dtype=np.float64)
-        ce_num = np.zeros(max(self.union.n_be, 1), dtype=np.float64) if ce else None
+        ce_num = np.zeros(max(nb, 1), dtype=np.float64) if ce else None
         ms = C.c_double()
-        _capi.check(self.lib.mcg_is_batch_run(self.h, _p(q_thresholds, C.c_uint64),
-                                              _p(qd, C.c_uint64) if qd is not None else None, int(words_defensive),
+        _capi.check(self.lib.mcg_is_batch_run(self.h, _p(q_thresholds, C.c_uint64), n_def,
+                                              _p(qd, C.c_uint64) if n_def else None,
+                                              _p(wd, C.c_uint64) if n_def else None,
                                               iteration, word_begin, word_count, _p(sums, C.c_double),
                                               _p(ce_num, C.c_double) if ce else None, C.byref(ms)))
         out = {"sum_w": sums[:, 0].copy(), "sum_w2": sums[:, 1].copy(), "hits": sums[:, 2].astype(np.int64),
@@ -559,6 +617,23 @@ class BatchedIsResult:
     q: np.ndarray = None          # final proposal of every event (trees concatenated)
     be_begin: np.ndarray = None   # tree k's events: q[be_begin[k]:be_begin[k + 1]]
     rounds: List[dict] = field(default_factory=list)
+
+
+def _prepare_one(g: FlatGraph, n_modes: int, importance: bool):
+    """Per-tree host inputs of the batched driver: features (the per-tree
+    input 15 filled in later) and the uncapped mode proposals."""
+    return event_features(g, instance_scale=1.0, importance=importance), mode_proposals(g, n_modes, 1.0)
+
+
+def prepare_trees(graphs, n_modes: int = 4, importance: bool = True, workers: int = 0):
+    """_prepare_one for every tree, in `workers` spawned processes when > 1."""
+    if workers and workers > 1 and len(graphs) > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_prepare_one, graphs, [n_modes] * len(graphs), [importance] * len(graphs),
+                               chunksize=max(1, len(graphs) // (4 * workers))))
+    return [_prepare_one(g, n_modes, importance) for g in graphs]
 
 
 def _rel95(n, sw, sw2):
@@ -590,13 +665,14 @@ def _train_shared(mlp: "ProposalMLP", feats, targets, steps, lr, weights=None, g
 
 def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[ProposalMLP] = None, device: int = 0,
                        probe_words: int = 1 << 10, min_hits: int = 200, max_probe_rounds: int = 24,
-                       ce_rounds: int = 4, ce_words: int = 1 << 12, smoothing: float = 0.7, train_steps: int = 150,
+                       ce_rounds: int = 5, ce_words: int = 1 << 13, smoothing: float = 0.7, train_steps: int = 150,
                        lr: float = 3e-3, q_max: float = 0.5, est_words: int = 1 << 12, max_est_words: int = 1 << 22,
                        ess_floor: float = 50.0, collapse_ratio: float = 1e-3, plain_words: int = 1 << 16,
-                       defensive: float = 0.2, chunk_words: int = 0, use_network: bool = True,
+                       defensive: float = 0.3, chunk_words: int = 0, use_network: bool = True,
                        importance_features: bool = True, tree_weighting: bool = True, fallback_after: int = 2,
                        cap_levels=(0.75, 0.9, 0.97, 0.99), confirm_rounds: int = 1,
-                       defensive_proposal: str = "approx", min_words: int = 0, log=None) -> BatchedIsResult:
+                       defensive_proposal: str = "modes", n_modes: int = 4, min_words: int = 0,
+                       mode_cap: float = 0.5, workers: int = 0, prepared=None, log=None) -> BatchedIsResult:
     """Learned importance sampling for a batch of rare-event trees.
 
     1. Probe: q = min(p * s_k, c_k) per tree, s_k x4 per round (x8 without
@@ -610,11 +686,16 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     weight p / (defensive * q_d + (1 - defensive) * q) (mcg_is_batch_run):
     a failure region the learned proposal under-samples is still reached
     through q_d's share, so the estimate stays unbiased with a bounded
-    variance instead of silently missing that region.  q_d is the
-    approximate zero-variance proposal P~(x_i = 1 | top) of
-    approximate_importance (defensive_proposal="approx"; exact for trees
-    without shared nodes) or the probe's inflation ("probe"), clipped to the
-    tree's cap; the first cross-entropy round samples q_d.
+    variance instead of silently missing that region.  q_d is, with
+    defensive_proposal="modes", a mixture of n_modes proposals each
+    conditioned on one child of the top OR gate failing (mode_proposals;
+    a product proposal cannot follow failure modes of very different order
+    at once, a mixture over the top gate's children can), with "approx" the
+    single approximate zero-variance proposal P~(x_i = 1 | top), with
+    "probe" the probe's inflation; all clipped to the tree's cap (the mode
+    proposals to max(cap, mode_cap): a child's failure that needs all of
+    its events is only reached often when they may come close to 1).  The
+    first cross-entropy round samples q_d alone.
     2. Cross-entropy rounds over all trees at once: per-event targets are the
        likelihood-weighted failure frequencies, smoothed with the current
        proposal; one network, whose 16th input is the tree's log10 s_k / 6,
@@ -631,7 +712,9 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
        ESS / hits falls below collapse_ratio after its first estimate round
        is re-run with its nominal probabilities (plain Monte Carlo, weights 1)
        and reported as a fallback.
-    Every round draws fresh Philox counters (its own pass number).
+    Every round draws fresh Philox counters (its own pass number).  The
+    per-tree host inputs (features, mode proposals) are computed by
+    prepare_trees, in `workers` processes, unless given as `prepared`.
     use_network=False takes the smoothed cross-entropy targets themselves as
     the next proposal (the method without the network, for comparison);
     importance_features=False leaves the independence-approximation inputs
@@ -642,6 +725,10 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     gpu = {"probe": 0.0, "ce": 0.0, "estimate": 0.0}
     wall = {"features": 0.0, "probe": 0.0, "ce": 0.0, "train": 0.0, "estimate": 0.0, "rebuild": 0.0}
     rounds = []
+    t0 = time.perf_counter()
+    if prepared is None:
+        prepared = prepare_trees(graphs, n_modes, importance_features, workers)
+    wall["features"] = time.perf_counter() - t0
     t0 = time.perf_counter()
     full = BatchedImportanceSampler(graphs, device=device, chunk_words=chunk_words)
     wall["rebuild"] += time.perf_counter() - t0
@@ -656,12 +743,23 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     ok = np.zeros(n, dtype=bool)
     p_min = np.array([float(p[sl[k]][p[sl[k]] > 0].min()) if np.any(p[sl[k]] > 0) else 1.0 for k in range(n)])
     it = 1
+    probe, probing = full, np.arange(n)  # the joined graph of the trees still probed
     for r in range(max_probe_rounds):
-        q = np.minimum(p * scale[tree_of_event], cap[tree_of_event])
-        res = full.run(full.proposal_thresholds(q), iteration=it, word_count=probe_words)
+        left = np.nonzero(~ok)[0]
+        if left.size <= probing.size // 2:
+            t1 = time.perf_counter()
+            if probe is not full:
+                probe.close()
+            probe, probing = BatchedImportanceSampler([graphs[k] for k in left], device=device,
+                                                      chunk_words=chunk_words), left
+            wall["rebuild"] += time.perf_counter() - t1
+        q = np.concatenate([np.minimum(p[sl[k]] * scale[k], cap[k]) for k in probing])
+        res = probe.run(probe.proposal_thresholds(q), iteration=it, word_count=probe_words)
         it += 1
         gpu["probe"] += res["kernel_ms"]
-        ok |= res["hits"] >= min_hits
+        ok[probing] |= res["hits"] >= min_hits
+        hits = np.zeros(n, dtype=np.int64)
+        hits[probing] = res["hits"]
         rounds.append({"phase": "probe", "round": r, "trees_left": int((~ok).sum()), "ms": res["kernel_ms"]})
         if ok.all():
             break
@@ -671,30 +769,42 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             if higher:
                 cap[k] = higher[0]
         grow = ~ok & ~saturated
-        scale = np.where(grow, scale * np.where(res["hits"] == 0, 8.0, 4.0), scale)
+        scale = np.where(grow, scale * np.where(hits == 0, 8.0, 4.0), scale)
         scale = np.minimum(scale, cap / p_min)
+    if probe is not full:
+        probe.close()
     wall["probe"] = time.perf_counter() - t0
     # 2. cross-entropy rounds with the shared network
-    t0 = time.perf_counter()
-    feats = np.concatenate([event_features(g, instance_scale=float(scale[k]), importance=importance_features)
-                            for k, g in enumerate(graphs)])
-    wall["features"] = time.perf_counter() - t0
+    feats = np.concatenate([f for f, _ in prepared])
+    feats[:, 15] = (np.log10(np.maximum(scale, 1.0)) / 6.0)[tree_of_event]
     mlp = mlp or (ProposalMLP(device=device) if use_network else None)
     cap_e = cap[tree_of_event]
-    if defensive_proposal == "approx":
-        q_probe = np.concatenate([np.clip(approximate_importance(g)[1], 1e-7, cap[k]) for k, g in enumerate(graphs)])
+    if defensive_proposal == "modes":
+        q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
+                        np.maximum(cap_e, mode_cap)[None, :])
+    elif defensive_proposal == "approx":
+        q_def = np.concatenate([np.clip(approximate_importance(g)[1], 1e-7, cap[k])
+                                for k, g in enumerate(graphs)])[None, :]
     elif defensive_proposal == "probe":
-        q_probe = np.minimum(p * scale[tree_of_event], cap_e)
+        q_def = np.minimum(p * scale[tree_of_event], cap_e)[None, :]
     else:
-        raise ValueError("defensive_proposal must be 'approx' or 'probe'")
+        raise ValueError("defensive_proposal must be 'modes', 'approx' or 'probe'")
+    n_comp = q_def.shape[0]
+
+    def def_words(w):  # words per defensive component
+        return max(1, int(round(defensive * w / n_comp))) if defensive > 0 else 0
     row_w = (1.0 / np.diff(bb).astype(np.float64))[tree_of_event].astype(np.float32) if tree_weighting else None
-    q = q_probe.copy()
-    thr_probe = full.proposal_thresholds(q_probe)
-    n_def = lambda w: int(round(defensive * w))
+    thr_def = np.stack([full.proposal_thresholds(qc) for qc in q_def])
+    q = None
     t0 = time.perf_counter()
     for r in range(ce_rounds):
-        res = full.run(full.proposal_thresholds(q), iteration=it, word_count=ce_words, ce=True,
-                       q_defensive=thr_probe, words_defensive=n_def(ce_words))
+        if q is None:  # first round: the defensive mixture alone
+            res = full.run(thr_def[0], iteration=it, word_count=ce_words, ce=True, q_defensive=thr_def,
+                           words_defensive=[ce_words // n_comp + (c < ce_words % n_comp) for c in range(n_comp)])
+            q = q_def.mean(axis=0)
+        else:
+            res = full.run(full.proposal_thresholds(q), iteration=it, word_count=ce_words, ce=True,
+                           q_defensive=thr_def if defensive > 0 else None, words_defensive=def_words(ce_words))
         it += 1
         gpu["ce"] += res["kernel_ms"]
         sw = res["sum_w"][tree_of_event]
@@ -738,9 +848,11 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             members = active.copy()
             wall["rebuild"] += time.perf_counter() - t1
         qa = np.concatenate([q_use[sl[k]] for k in members])
-        qd = np.concatenate([q_probe[sl[k]] if not fallback[k] else p[sl[k]] for k in members])
+        qd = np.concatenate([q_def[:, sl[k]] if not fallback[k] else np.repeat(p[sl[k]][None, :], n_comp, axis=0)
+                             for k in members], axis=1)
         res = sampler.run(sampler.proposal_thresholds(qa), iteration=it, word_begin=0, word_count=words,
-                          q_defensive=sampler.proposal_thresholds(qd), words_defensive=n_def(words))
+                          q_defensive=np.stack([sampler.proposal_thresholds(qc) for qc in qd]) if defensive > 0
+                          else None, words_defensive=def_words(words))
         it += 1
         gpu["estimate"] += res["kernel_ms"]
         used += words

@@ -103,6 +103,44 @@ def test_event_features_match_definition(make):
     assert np.all(f[:, 15] == np.float32(0.5))
 
 
+def _cond_by_definition(g, node):
+    """P(x_i = 1 | node fails) of a read-once tree, one event at a time."""
+    p = g.quantised_probabilities()
+    P = synth.read_once_probability(g, p)[node]
+    out = np.empty(g.n_be)
+    for i in range(g.n_be):
+        pp = p.copy()
+        pp[i] = 1.0
+        out[i] = p[i] * synth.read_once_probability(g, pp)[node] / P
+    return out
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_approximate_importance_is_exact_on_trees(seed):
+    from mcscram_b200.importance import approximate_importance
+    g = synth.generate(synth.TreeSpec(n_be=40, n_gates=20, mix={AND: 0.3, OR: 0.3, ATLEAST: 0.2, XOR: 0.1,
+                                                               synth.NOT: 0.1},
+                                      p_range=(1e-4, 0.5), seed=seed, atleast_n=(3, 5)))
+    pr, cond = approximate_importance(g)
+    np.testing.assert_allclose(pr, synth.read_once_probability(g), rtol=1e-12)
+    np.testing.assert_allclose(cond, _cond_by_definition(g, g.root), rtol=1e-9, atol=1e-14)
+    child = int(g.gate_inputs(g.root - g.n_be)[0])
+    if child >= g.n_be:
+        _, cond_c = approximate_importance(g, root=child)
+        np.testing.assert_allclose(cond_c, _cond_by_definition(g, child), rtol=1e-9, atol=1e-14)
+
+
+def test_mode_proposals_condition_on_top_children():
+    from mcscram_b200.importance import approximate_importance, mode_proposals
+    g = synth.config5_instance(0)
+    kids = [int(c) for c in g.gate_inputs(g.root - g.n_be)]
+    m = mode_proposals(g, 4, 0.5)
+    assert m.shape == (4, g.n_be) and np.all((m >= 1e-7) & (m <= 0.5))
+    pr, _ = approximate_importance(g)
+    heaviest = max(kids, key=lambda c: pr[c])
+    np.testing.assert_allclose(m[0], np.clip(approximate_importance(g, root=heaviest)[1], 1e-7, 0.5))
+
+
 def test_layers_match_definition():
     for g in (synth.config1(), synth.small_tree(5, n_be=48, n_gates=24, n_layers=5)):
         ref = np.zeros(g.n_nodes, dtype=np.int64)
@@ -189,25 +227,29 @@ def _log_ratio(p, thr, bits, s):
     return l1[s].sum() + np.einsum("i,iwb->wb", a[s], bits[s])
 
 
-def _union_weights(oracle_mod, u, bb, roots, qthr, it, W, qdef=None, wdef=0):
-    """Per-tree CPU sums and per-event CE numerators of the joined graph; with
-    qdef the first wdef words come from it and samples get the
-    balance-heuristic weight."""
-    if wdef:
-        words = np.concatenate([oracle_mod.eval_words(u.with_thresholds(qdef), it, 0, wdef),
-                                oracle_mod.eval_words(u.with_thresholds(qthr), it, wdef, W - wdef)], axis=1)
-    else:
-        words = oracle_mod.eval_words(u.with_thresholds(qthr), it, 0, W)
+def _union_weights(oracle_mod, u, bb, roots, comps, it):
+    """Per-tree CPU sums and per-event CE numerators of the joined graph.
+    comps = [(thresholds, words), ...] in drawing order; with more than one
+    component every sample gets the balance-heuristic weight."""
+    W = sum(wc for _, wc in comps)
+    parts, pos = [], 0
+    for thr, wc in comps:
+        if wc:
+            parts.append(oracle_mod.eval_words(u.with_thresholds(thr), it, pos, wc))
+        pos += wc
+    words = np.concatenate(parts, axis=1)
     p = u.quantised_probabilities()
     bits = ((words[: u.n_be, :, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(np.float64)
+    live = [(thr, wc) for thr, wc in comps if wc]
     sums, ce = [], np.zeros(u.n_be)
     for k in range(len(roots)):
         s = slice(int(bb[k]), int(bb[k + 1]))
         top = ((words[roots[k]][:, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(bool)
-        logw = _log_ratio(p, qthr, bits, s)
-        if wdef:
-            alpha = wdef / W
-            logw = -np.logaddexp(np.log(alpha) - _log_ratio(p, qdef, bits, s), np.log1p(-alpha) - logw)
+        lws = [_log_ratio(p, thr, bits, s) for thr, _ in live]
+        if len(live) == 1:
+            logw = lws[0]
+        else:
+            logw = -np.logaddexp.reduce([np.log(wc / W) - lw for (_, wc), lw in zip(live, lws)], axis=0)
         w = np.where(top, np.exp(logw), 0.0)
         sums.append((w.sum(), (w ** 2).sum(), int(top.sum()), logw[top].max() if top.any() else -np.inf))
         ce[s] = np.einsum("wb,iwb->i", w, bits[s])
@@ -215,7 +257,7 @@ def _union_weights(oracle_mod, u, bb, roots, qthr, it, W, qdef=None, wdef=0):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("wdef", [0, 300])
+@pytest.mark.parametrize("wdef", [(), (300,), (120, 0, 250)])
 def test_batched_sums_match_cpu(oracle_mod, gpu, wdef):
     from mcscram_b200.importance import BatchedImportanceSampler
     trees = _trees()
@@ -223,10 +265,12 @@ def test_batched_sums_match_cpu(oracle_mod, gpu, wdef):
     with BatchedImportanceSampler(trees, chunk_words=256) as s:
         p = s.union.quantised_probabilities()
         q = probability_threshold(np.minimum(p * rng.uniform(2, 30, p.size), 0.5))
-        qdef = probability_threshold(np.minimum(p * 8.0, 0.5)) if wdef else None
-        W = 700  # three chunks, the last one short
-        r = s.run(q, iteration=4, word_count=W, ce=True, q_defensive=qdef, words_defensive=wdef)
-        sums, ce = _union_weights(oracle_mod, s.union, s.be_begin, s.roots, q, 4, W, qdef, wdef)
+        qdef = np.stack([probability_threshold(np.minimum(p * f, 0.5)) for f in (8.0, 3.0, 20.0)])[: len(wdef)]
+        W = 700  # chunks of 256 words, the last one short
+        r = s.run(q, iteration=4, word_count=W, ce=True, q_defensive=qdef if wdef else None,
+                  words_defensive=list(wdef))
+        comps = [(q, W - sum(wdef))] + [(qdef[c], wdef[c]) for c in range(len(wdef))]
+        sums, ce = _union_weights(oracle_mod, s.union, s.be_begin, s.roots, comps, 4)
     for k, (sw, sw2, h, mx) in enumerate(sums):
         assert r["hits"][k] == h
         assert r["sum_w"][k] == pytest.approx(sw, rel=1e-10)

@@ -49,7 +49,9 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fused kernel CTAs per SM (0 = engine default)")
     ap.add_argument("--peak-words", type=int, default=1 << 22, help="words per register-only sampler launch")
-    ap.add_argument("--mode", default="staged", choices=["fused", "staged", "layered"])
+    ap.add_argument("--mode", default="staged", choices=["fused", "staged", "layered", "strip"])
+    ap.add_argument("--tree", default="config2", choices=["config1", "config2"],
+                    help="plain workload's tree (config1: the small 200-event tree, for profiling captures)")
     ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")
     ap.add_argument("--sampler-blocks", type=int, default=0, help="staged: sampler blocks per SM (0 = default)")
     ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis"],
@@ -466,7 +468,7 @@ def main() -> int:
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    g = synth.config2()
+    g = synth.config2() if args.tree == "config2" else synth.config1()
     W = args.words
     word_begin, W = parallel.weak_shard(W, rank)  # weak scaling: W words per rank
     # one dedicated stream for the engine and for every torch op and event here
@@ -492,8 +494,8 @@ def main() -> int:
         allreduce_tallies()
     torch.cuda.synchronize()
     eng.reset_tallies()
-    if args.mode == "staged":
-        eng.profile_sampler(True)  # events around every sampler-phase launch
+    if args.mode in ("staged", "strip"):
+        eng.profile_sampler(True)  # events around every sampler-phase (strip: whole-pass) launch
     launches0 = eng.launch_count()
     if world > 1:
         dist.barrier()
@@ -528,8 +530,8 @@ def main() -> int:
     # Roofline of the dominant kernel: basic-event words per launch / its mean
     # launch duration (CUDA events on its own stream), against the
     # register-only sampler measured on this GPU in this run.
-    if args.mode == "staged":
-        kernel = "k_stage_be"
+    if args.mode in ("staged", "strip"):
+        kernel = "k_stage_be" if args.mode == "staged" else "k_strip"
         n_a, ms_a = eng.profile_sampler_read()
         eng.profile_sampler(False)
         kernel_launches = max(n_a, 1)
@@ -557,7 +559,8 @@ def main() -> int:
         if world > 1:
             ts = parallel.allreduce_max([max(ts)])
         e2e_s = statistics.median(ts)
-        h2d = (info["n_ops"] * 16 + g.n_be * 16 + g.n_gates * 20 + g.inputs.size * 4 + g.tally_nodes.size * 4)
+        h2d = ((info["n_ops"] * 16 if args.mode == "fused" else 0) + g.n_be * 16 + g.n_gates * 20 +
+               g.inputs.size * 4 + g.tally_nodes.size * 4)
         e2e = {"value": g.n_gates * samples / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(g.tally_nodes.size * 8), "seconds_per_step": e2e_s}
 
@@ -574,7 +577,8 @@ def main() -> int:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "plain MC pass, 5,000-event / 3,000-gate synthetic tree (seed 11)",
+            "config": {"workload": "plain MC pass, 5,000-event / 3,000-gate synthetic tree (seed 11)"
+                       if args.tree == "config2" else "plain MC pass, 200-event / 100-gate synthetic tree (seed 372)",
                        "samples_per_gpu": W * 64, "words_per_gpu": W, "n_be": g.n_be, "n_gates": g.n_gates,
                        "tallied_nodes": int(g.tally_nodes.size), "parallelism": f"word-range shards x{world}",
                        "l2": "256 MB buffer written between steps", "mode": args.mode},

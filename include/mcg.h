@@ -47,9 +47,13 @@ enum mcg_connective {
 enum mcg_mode {
     MCG_MODE_FUSED = 0,   /* one persistent kernel per launch chunk: sample, gates, tallies fused */
     MCG_MODE_LAYERED = 1, /* reference dataflow: materialised node words, one launch per layer */
-    MCG_MODE_STAGED = 2   /* two-phase pipeline: a pure sampler kernel writes basic-event words to
+    MCG_MODE_STAGED = 2,  /* two-phase pipeline: a pure sampler kernel writes basic-event words to
                              HBM, per-layer gate kernels with fused tallies read them; chunks are
                              double buffered on two streams so the phases overlap */
+    MCG_MODE_STRIP = 3    /* one persistent kernel per pass: each block takes 256-word strips, its
+                             threads sample every event of their word and then evaluate every gate
+                             for it from scratch rows of their own (n_nodes x 32 words per warp);
+                             sampling and gate work of different blocks overlap on every SM */
 };
 
 /* Flattened PDAG handed to the engine.  All arrays are host memory, copied
@@ -84,7 +88,8 @@ typedef struct mcg_run_desc {
     uint32_t block_threads;   /* fused kernel CTA size; 0 = tuned default */
     uint32_t smem_slots;      /* fused kernel shared-memory value slots per thread; 0 = auto,
                                  MCG_SMEM_SLOTS_NONE = keep every value in global scratch */
-    uint32_t ctas_per_sm;     /* fused kernel persistent CTAs per SM; 0 = auto */
+    uint32_t ctas_per_sm;     /* fused kernel persistent CTAs per SM (1..4); strip kernel resident
+                                 blocks per SM (4..6, fewer = more registers per thread); 0 = auto */
     uint64_t chunk_words;     /* words per launch in one mcg_run; 0 = auto */
     uint64_t layered_max_words; /* layered/staged modes: words materialised per chunk; 0 = auto */
     uint32_t sampler_blocks_per_sm; /* staged mode: cap on sampler blocks per SM, to leave room for

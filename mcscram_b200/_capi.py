@@ -27,7 +27,8 @@ MCG_ERR_NO_DEVICE = 6
 MODE_FUSED = 0
 MODE_LAYERED = 1
 MODE_STAGED = 2
-MODES = {"fused": MODE_FUSED, "layered": MODE_LAYERED, "staged": MODE_STAGED}
+MODE_STRIP = 3
+MODES = {"fused": MODE_FUSED, "layered": MODE_LAYERED, "staged": MODE_STAGED, "strip": MODE_STRIP}
 
 _u32p = C.POINTER(C.c_uint32)
 _i32p = C.POINTER(C.c_int32)

@@ -176,7 +176,8 @@ FusedKernel fused_kernel(uint32_t ctas_per_sm) {
     }
 }
 
-mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
+// Host-only compilation of the fused program (launch shape from the options).
+mcg_status compile_fused(mcg_engine *e, const mcg_run_desc &run) {
     cudaDeviceProp prop;
     MCG_CUDA(cudaGetDeviceProperties(&prop, e->device));
     if (run.block_threads != 0 && run.block_threads != kFusedThreads)
@@ -201,7 +202,13 @@ mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
     e->grid = (uint32_t)prop.multiProcessorCount * ctas_per_sm;
     e->scratch_stride = (uint64_t)e->grid * e->nt;
     e->chunk_words = run.chunk_words ? run.chunk_words : kDefaultChunkWords;
+    e->prog_compiled = true;
+    return MCG_OK;
+}
 
+mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
+    mcg_status st = compile_fused(e, run);
+    if (st != MCG_OK) return st;
     MCG_CUDA(cudaFuncSetAttribute(fused_kernel(e->ctas_per_sm), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)std::max<uint32_t>(e->smem_bytes, 1)));
     MCG_CUDA(upload(reinterpret_cast<mcg::Op **>(&e->d_ops), e->prog.ops));
@@ -212,6 +219,7 @@ mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
 }
 
 constexpr uint32_t kStageEventsPerThread = 4;
+constexpr uint32_t kStripBlocksPerSm = 6;
 // Gate-phase blocks are small (128 threads, 2 words each) so that they fit in
 // the registers and threads left next to the capped sampler blocks.
 constexpr int kStageGateThreads = 128;
@@ -246,6 +254,100 @@ mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
     for (cudaEvent_t *ev : {&e->ev_fork, &e->ev_a[0], &e->ev_a[1], &e->ev_b[0], &e->ev_b[1], &e->ev_join_a,
                             &e->ev_join_b})
         MCG_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    return MCG_OK;
+}
+
+// Strip kernel for a residency target: fewer blocks per SM give each thread
+// more registers (6: 40, 5: 48, 4: 64).
+using StripKernel = void (*)(mcg::dev::StripArgs);
+StripKernel strip_kernel(uint32_t blocks_per_sm) {
+    switch (blocks_per_sm) {
+        case 4: return mcg::dev::k_strip<kMulForm, kPackForm, 4>;
+        case 5: return mcg::dev::k_strip<kMulForm, kPackForm, 5>;
+        default: return mcg::dev::k_strip<kMulForm, kPackForm, 6>;
+    }
+}
+
+mcg_status setup_strip(mcg_engine *e, const mcg_run_desc &run) {
+    const mcg::Graph &g = e->graph;
+    cudaDeviceProp prop;
+    MCG_CUDA(cudaGetDeviceProperties(&prop, e->device));
+    const uint32_t target = run.ctas_per_sm ? run.ctas_per_sm : kStripBlocksPerSm;
+    if (target < 4 || target > 6) return mcg::fail(MCG_ERR_INVALID, "strip mode: ctas_per_sm must be 0 or 4..6");
+    e->strip_blocks = target;
+    const uint64_t n_tally = g.tally_nodes.size();
+    // tally counters in shared memory while the target residency still fits
+    const uint64_t tally_bytes = n_tally * sizeof(unsigned long long);
+    const uint64_t per_block = prop.sharedMemPerMultiprocessor / target - 2048;
+    e->strip_smem = tally_bytes <= per_block ? (uint32_t)tally_bytes : 0u;
+    const StripKernel kern = strip_kernel(target);
+    MCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max<uint32_t>(e->strip_smem, 1)));
+    int per_sm = 0;
+    MCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, mcg::dev::kStripThreads, e->strip_smem));
+    if (per_sm < 1) return mcg::fail(MCG_ERR_INVALID, "strip kernel does not fit on an SM");
+    e->strip_grid = (uint32_t)(prop.multiProcessorCount * per_sm);
+    const uint64_t warps = (uint64_t)e->strip_grid * (mcg::dev::kStripThreads / 32);
+    const uint64_t bytes = warps * std::max<uint64_t>(g.n_nodes(), 1) * mcg::dev::kStripLanes * sizeof(uint64_t);
+    MCG_CUDA(cudaMalloc((void **)&e->d_strip_scratch, bytes));
+    MCG_CUDA(cudaMalloc((void **)&e->d_queue, sizeof(unsigned long long)));
+    MCG_CUDA(cudaMalloc((void **)&e->d_event_table,
+                        std::max<uint64_t>(g.n_be, 1) * mcg::dev::kEventTableStride * sizeof(uint2)));
+    return MCG_OK;
+}
+
+// One persistent launch per pass on the engine stream.
+mcg_status run_strip(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t word_begin, uint64_t count) {
+    const mcg::Graph &g = e->graph;
+    mcg::dev::StripArgs a{};
+    a.be = e->d_be;
+    a.table = e->d_event_table;
+    a.n_be = g.n_be;
+    a.n_nodes = g.n_nodes();
+    a.smeta = e->d_smeta;
+    a.inputs = e->d_inputs;
+    a.order = e->d_layer_gates;
+    a.n_gates = g.n_gates;
+    a.gate_tally = e->d_gate_tally;
+    a.tally_list = e->d_gate_tally_list;
+    a.be_tally_nodes = e->d_be_tally_nodes;
+    a.be_tally_idx = e->d_be_tally_idx;
+    a.n_be_tally = e->n_be_tally;
+    a.n_tally = (uint32_t)g.tally_nodes.size();
+    a.tally_in_smem = e->strip_smem ? 1u : 0u;
+    a.ones = e->d_tally;
+    a.scratch = e->d_strip_scratch;
+    a.word_begin = word_begin;
+    a.word_count = count;
+    a.queue = e->d_queue;
+    for (uint32_t it = 0; it < n_it; ++it) {
+        const uint32_t iteration = it_first + it;
+        if (g.n_be > 0 && e->table_iteration != iteration) {
+            const uint64_t n = (uint64_t)g.n_be * mcg::dev::kEventTableStride;
+            mcg::dev::k_event_table<kMulForm><<<(uint32_t)((n + 255) / 256), 256, 0, e->stream>>>(
+                e->d_be, g.n_be, (iteration + 1u) << 6, e->d_event_table);
+            ++e->launches;
+            e->table_iteration = iteration;
+        }
+        MCG_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned long long), e->stream));
+        cudaEvent_t p0 = nullptr, p1 = nullptr;
+        if (e->profile_a) {
+            if (e->prof_used == e->prof_events.size()) {
+                cudaEvent_t x, y;
+                MCG_CUDA(cudaEventCreate(&x));
+                MCG_CUDA(cudaEventCreate(&y));
+                e->prof_events.push_back({x, y});
+            }
+            p0 = e->prof_events[e->prof_used].first;
+            p1 = e->prof_events[e->prof_used].second;
+            ++e->prof_used;
+            MCG_CUDA(cudaEventRecord(p0, e->stream));
+        }
+        strip_kernel(e->strip_blocks)<<<e->strip_grid, mcg::dev::kStripThreads, e->strip_smem, e->stream>>>(a);
+        ++e->launches;
+        if (p1) MCG_CUDA(cudaEventRecord(p1, e->stream));
+        MCG_CUDA(cudaGetLastError());
+    }
     return MCG_OK;
 }
 
@@ -377,6 +479,8 @@ void release(mcg_engine *e) {
     cudaFree(e->d_event_table);
     cudaFree(e->d_stage[0]);
     cudaFree(e->d_stage[1]);
+    cudaFree(e->d_strip_scratch);
+    cudaFree(e->d_queue);
     for (cudaEvent_t ev : {e->ev_fork, e->ev_a[0], e->ev_a[1], e->ev_b[0], e->ev_b[1], e->ev_join_a, e->ev_join_b})
         if (ev) cudaEventDestroy(ev);
     for (auto &pe : e->prof_events) {
@@ -406,7 +510,7 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
     *out = nullptr;
     mcg_run_desc run{};
     if (run_in) run = *run_in;
-    if (run.mode > MCG_MODE_STAGED) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
+    if (run.mode > MCG_MODE_STRIP) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
     auto *e = new (std::nothrow) mcg_engine();
     if (!e) return mcg::fail(MCG_ERR_OOM, "host allocation failed");
     const std::string err = mcg::Graph::from_desc(*graph, e->graph);
@@ -426,6 +530,7 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
     }
     e->device = run.device;
     e->mode = run.mode;
+    e->run_desc = run;
     e->layered_max_words = run.layered_max_words;
     mcg_status st = MCG_OK;
     do {
@@ -450,9 +555,10 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
         }
         st = build_layered_tables(e);
         if (st != MCG_OK) break;
-        st = setup_fused(e, run);
-        if (st != MCG_OK) break;
-        if (e->mode == MCG_MODE_STAGED) st = setup_staged(e, run);
+        // the fused program is compiled here only for the fused mode (on request otherwise)
+        if (e->mode == MCG_MODE_FUSED) st = setup_fused(e, run);
+        else if (e->mode == MCG_MODE_STAGED) st = setup_staged(e, run);
+        else if (e->mode == MCG_MODE_STRIP) st = setup_strip(e, run);
     } while (false);
     if (st != MCG_OK) {
         release(e);
@@ -485,6 +591,9 @@ mcg_status mcg_run(mcg_engine *e, uint32_t iteration_first, uint32_t n_iteration
     MCG_CUDA(cudaSetDevice(e->device));
     if (e->mode == MCG_MODE_STAGED) {
         const mcg_status st = run_staged_impl(e, iteration_first, n_iterations, word_begin, word_count);
+        if (st != MCG_OK) return st;
+    } else if (e->mode == MCG_MODE_STRIP) {
+        const mcg_status st = run_strip(e, iteration_first, n_iterations, word_begin, word_count);
         if (st != MCG_OK) return st;
     } else if (e->mode == MCG_MODE_FUSED) {
         for (uint64_t off = 0; off < word_count; off += e->chunk_words) {
@@ -582,6 +691,13 @@ mcg_status mcg_dump_words(mcg_engine *e, uint32_t iteration, uint64_t word_begin
 mcg_status mcg_program_info_get(mcg_engine *e, mcg_program_info *info) {
     mcg::clear_error();
     if (!e || !info) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    if (!e->prog_compiled) {
+        MCG_CUDA(cudaSetDevice(e->device));
+        mcg_run_desc rd = e->run_desc;
+        rd.ctas_per_sm = 0;  // the other modes' value means something else
+        const mcg_status st = compile_fused(e, rd);
+        if (st != MCG_OK) return st;
+    }
     info->n_ops = e->prog.ops.size();
     info->smem_slots = e->prog.smem_slots;
     info->global_slots = e->prog.global_slots;

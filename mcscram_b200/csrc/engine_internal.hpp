@@ -69,6 +69,15 @@ struct mcg_engine {
     cudaStream_t s_a = nullptr, s_b = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_a[2] = {nullptr, nullptr}, ev_b[2] = {nullptr, nullptr};
     cudaEvent_t ev_join_a = nullptr, ev_join_b = nullptr;
+    // strip
+    uint64_t *d_strip_scratch = nullptr;   // per warp n_nodes x 32 words
+    unsigned long long *d_queue = nullptr; // strip counter
+    uint32_t strip_grid = 0;
+    uint32_t strip_smem = 0;               // tally counters in shared memory (0: global atomics)
+    uint32_t strip_blocks = 6;             // resident blocks per SM the kernel is built for
+
+    mcg_run_desc run_desc{};                  // options the engine was created with
+    bool prog_compiled = false;               // fused program compiled (fused mode, or on request)
     bool profile_a = false;                   // time every sampler-phase launch
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;

@@ -471,6 +471,188 @@ __global__ void __launch_bounds__(NT) k_stage_gates(const uint4 *__restrict__ me
     }
 }
 
+// Strip mode: one persistent kernel per pass.  A block takes strips of 256
+// consecutive words from a queue; warp w owns words [32 w, 32 w + 32) of
+// the strip and a private scratch block of n_nodes rows x 32 words.  Lane l
+// first samples its word of every basic event (one Philox word per event,
+// event table of the pass), then evaluates every gate in layer order for the
+// same word, and adds the popcounts of tallied nodes into the block's
+// shared-memory counters.  A lane only reads the column it wrote, so the
+// only barrier is the strip hand-out: the eight warps of a block walk the
+// events together (the table rows they read stay in L1), while the blocks
+// on an SM drift apart, so the memory-bound gate work of some blocks runs
+// under the multiply-bound sampling of the others.
+constexpr int kStripLanes = 32;
+constexpr int kStripThreads = 256;
+
+struct StripArgs {
+    const uint4 *be;              // {pdag + 1, event + 1, thr lo, thr hi}
+    const uint2 *table;           // event table of the pass
+    uint32_t n_be, n_nodes;
+    const uint4 *smeta;           // per gate: op | k << 8 | nbits << 16, in_begin, in_count, neg_count
+    const uint32_t *inputs;
+    const uint32_t *order;        // gate ids, layer by layer
+    uint32_t n_gates;
+    const uint2 *gate_tally;      // per gate {offset, count} into tally_list
+    const uint32_t *tally_list;
+    const uint32_t *be_tally_nodes, *be_tally_idx;
+    uint32_t n_be_tally;
+    uint32_t n_tally;
+    uint32_t tally_in_smem;
+    unsigned long long *ones;
+    uint64_t *scratch;            // per warp: n_nodes x 32 words
+    uint64_t word_begin, word_count;
+    unsigned long long *queue;
+};
+
+__device__ __forceinline__ void strip_tally(const StripArgs &a, unsigned long long *s_ones, uint32_t idx,
+                                            uint32_t c) {
+    if (a.tally_in_smem) atomicAdd(&s_ones[idx], (unsigned long long)c);
+    else atomicAdd(&a.ones[idx], (unsigned long long)c);
+}
+
+// Bit-sliced count of up to 15 inputs (4 slices); count >= k for k <= 15.
+struct SlicedCount4 {
+    uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    __device__ __forceinline__ void add(uint64_t v) {
+        const uint64_t t = c0 & v;
+        c0 ^= v;
+        const uint64_t t1 = c1 & t;
+        c1 ^= t;
+        const uint64_t t2 = c2 & t1;
+        c2 ^= t1;
+        c3 ^= t2;
+    }
+    __device__ __forceinline__ uint64_t ge(uint32_t k) const {
+        const uint64_t c[4] = {c0, c1, c2, c3};
+        uint64_t gt = 0, eq = kAllOnes;
+#pragma unroll
+        for (int b = 3; b >= 0; --b) {
+            if ((k >> b) & 1u) {
+                eq &= c[b];
+            } else {
+                gt |= eq & c[b];
+                eq &= ~c[b];
+            }
+        }
+        return gt | eq;
+    }
+};
+
+__device__ __forceinline__ uint64_t strip_gate(const StripArgs &a, const uint64_t *col, uint32_t gi) {
+    constexpr uint32_t kMaxIn = 8;
+    const uint4 m = a.smeta[gi];
+    const uint32_t op = m.x & 0xFFu, kk = (m.x >> 8) & 0xFFu, nbits = (m.x >> 16) & 0xFu;
+    const uint32_t n = m.z, off = n - m.w;
+    const uint32_t *in = a.inputs + m.y;
+    if (op == MCG_ATLEAST) {
+        if (n <= kMaxIn) {
+            // counts of at most 8 fit 4 slices; k > 8 can never be reached
+            SlicedCount4 cnt;
+#pragma unroll
+            for (uint32_t i0 = 0; i0 < kMaxIn; i0 += 4) {
+                uint64_t v[4];
+#pragma unroll
+                for (uint32_t j = 0; j < 4; ++j)
+                    if (i0 + j < n) v[j] = col[(uint64_t)in[i0 + j] * kStripLanes];
+#pragma unroll
+                for (uint32_t j = 0; j < 4; ++j)
+                    if (i0 + j < n) cnt.add(i0 + j >= off ? ~v[j] : v[j]);
+            }
+            return kk > 8 ? 0ull : cnt.ge(kk);
+        }
+        SlicedCount cnt;
+        cnt.clear();
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t x = col[(uint64_t)in[i] * kStripLanes];
+            cnt.add(i >= off ? ~x : x, nbits);
+        }
+        return cnt.ge(kk);
+    }
+    uint64_t acc = (op == MCG_AND || op == MCG_NAND) ? kAllOnes : 0ull;
+    if (n <= kMaxIn) {
+#pragma unroll
+        for (uint32_t i0 = 0; i0 < kMaxIn; i0 += 4) {
+            uint64_t v[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j)
+                if (i0 + j < n) v[j] = col[(uint64_t)in[i0 + j] * kStripLanes];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                if (i0 + j < n) {
+                    const uint64_t x = i0 + j >= off ? ~v[j] : v[j];
+                    if (op == MCG_OR || op == MCG_NOR) acc |= x;
+                    else if (op == MCG_AND || op == MCG_NAND) acc &= x;
+                    else if (op == MCG_XOR) acc ^= x;
+                    else acc = x;
+                }
+            }
+        }
+    } else {
+        for (uint32_t i = 0; i < n; ++i) {
+            uint64_t x = col[(uint64_t)in[i] * kStripLanes];
+            if (i >= off) x = ~x;
+            if (op == MCG_OR || op == MCG_NOR) acc |= x;
+            else if (op == MCG_AND || op == MCG_NAND) acc &= x;
+            else if (op == MCG_XOR) acc ^= x;
+            else acc = x;
+        }
+    }
+    return (op == MCG_NAND || op == MCG_NOR || op == MCG_NOT) ? ~acc : acc;
+}
+
+template <int MF, int PF, int MINB>
+__global__ void __launch_bounds__(kStripThreads, MINB) k_strip(StripArgs a) {
+    extern __shared__ unsigned long long s_ones[];
+    __shared__ unsigned long long s_strip;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (a.tally_in_smem)
+        for (uint32_t i = threadIdx.x; i < a.n_tally; i += blockDim.x) s_ones[i] = 0;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    uint64_t *col = a.scratch + gwarp * (uint64_t)a.n_nodes * kStripLanes + lane;
+    const uint64_t n_strips = (a.word_count + kStripThreads - 1) / kStripThreads;
+    for (;;) {
+        __syncthreads();  // s_strip is free again (and the tally counters are zeroed)
+        if (threadIdx.x == 0) s_strip = atomicAdd(a.queue, 1ull);
+        __syncthreads();
+        const unsigned long long strip = s_strip;
+        if (strip >= n_strips) break;
+        const uint64_t wl = strip * kStripThreads + threadIdx.x;
+        const bool valid = wl < a.word_count;
+        const WordCtx ctx = make_word_ctx<MF>((uint32_t)(a.word_begin + wl));
+#pragma unroll 1
+        for (uint32_t e = 0; e < a.n_be; ++e) {
+            const uint4 r = a.be[e];
+            uint64_t v;
+            if (r.w != 0) v = kAllOnes;
+            else if (r.z == 0) v = 0;
+            else v = be_word_tab<MF, PF>(r.y, ctx, a.table + (uint64_t)e * kEventTableStride, r.z);
+            col[(uint64_t)e * kStripLanes] = v;
+        }
+        for (uint32_t j = 0; j < a.n_be_tally; ++j) {
+            const uint64_t v = col[(uint64_t)a.be_tally_nodes[j] * kStripLanes];
+            const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, valid ? (uint32_t)__popcll(v) : 0u);
+            if (lane == 0 && c) strip_tally(a, s_ones, a.be_tally_idx[j], c);
+        }
+#pragma unroll 1
+        for (uint32_t q = 0; q < a.n_gates; ++q) {
+            const uint32_t gi = a.order[q];
+            const uint64_t r = strip_gate(a, col, gi);
+            col[(uint64_t)(a.n_be + gi) * kStripLanes] = r;
+            const uint2 t = a.gate_tally[gi];
+            if (t.y) {
+                const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, valid ? (uint32_t)__popcll(r) : 0u);
+                if (lane == 0 && c)
+                    for (uint32_t j = 0; j < t.y; ++j) strip_tally(a, s_ones, a.tally_list[t.x + j], c);
+            }
+        }
+    }
+    __syncthreads();
+    if (a.tally_in_smem)
+        for (uint32_t i = threadIdx.x; i < a.n_tally; i += blockDim.x)
+            if (s_ones[i]) atomicAdd(&a.ones[i], s_ones[i]);
+}
+
 // Register-only sampler: thread w generates words (e, w) for n_events events
 // (event e: pdag_idx + 1 = e + 3, event_idx + 1 = e + 1, table row e) and
 // xors them together; one store per thread keeps the work alive.  Same

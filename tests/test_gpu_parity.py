@@ -32,7 +32,7 @@ def test_words_match_golden_fixtures(capi, gpu):
             assert np.array_equal(e.dump_words(3, (1 << 32) - 64, 64), npz[str(name) + "words_it3_whigh"])
 
 
-@pytest.mark.parametrize("mode", ["fused", "layered", "staged"])
+@pytest.mark.parametrize("mode", ["fused", "layered", "staged", "strip"])
 def test_small_tree_tallies_golden(capi, oracle_mod, gpu, mode):
     npz = np.load(GOLDEN / "small_trees.npz")
     m = capi.MODES[mode]
@@ -48,7 +48,7 @@ def test_small_tree_tallies_golden(capi, oracle_mod, gpu, mode):
             assert np.array_equal(ones, expect)
 
 
-@pytest.mark.parametrize("mode", ["fused", "layered", "staged"])
+@pytest.mark.parametrize("mode", ["fused", "layered", "staged", "strip"])
 def test_config1_golden_tallies(capi, gpu, mode):
     npz = np.load(GOLDEN / "config1_tallies.npz")
     g = load_graph(npz)
@@ -75,7 +75,7 @@ def test_fused_any_slot_budget(capi, oracle_mod, gpu, slots):
         assert np.array_equal(ones, expect), (slots, it, wb, n)
 
 
-@pytest.mark.parametrize("mode", ["fused", "staged"])
+@pytest.mark.parametrize("mode", ["fused", "staged", "strip"])
 def test_multiple_passes_and_ranges(capi, oracle_mod, gpu, mode):
     g = synth.config1()
     expect = oracle_mod.tallies(g, 2, 3, 500, 3000)
@@ -93,7 +93,7 @@ def test_multiple_passes_and_ranges(capi, oracle_mod, gpu, mode):
         assert total2 == total and np.array_equal(ones2, expect)
 
 
-@pytest.mark.parametrize("mode", ["fused", "staged"])
+@pytest.mark.parametrize("mode", ["fused", "staged", "strip"])
 def test_config2_windows_bit_exact(capi, oracle_mod, gpu, mode):
     g = synth.config2()
     with engine(capi, g, mode=capi.MODES[mode]) as e:
@@ -117,8 +117,11 @@ def test_config2_fused_equals_layered_large(capi, gpu):
     with engine(capi, g, mode=capi.MODE_STAGED, layered_max_words=1 << 17) as st:
         st.run(1, 1, 0, W)
         c, tc = st.tallies()
-    assert ta == tb == tc == W * 64
-    assert np.array_equal(a, b) and np.array_equal(a, c)
+    with engine(capi, g, mode=capi.MODE_STRIP) as sp:
+        sp.run(1, 1, 0, W)
+        d, td = sp.tallies()
+    assert ta == tb == tc == td == W * 64
+    assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
     assert a.sum() > 0
 
 
@@ -135,7 +138,7 @@ def test_edge_cases(capi, oracle_mod, gpu):
         tally_nodes=[5, 6, 7, 8, 9, 10, 11, 12, 0, 12, 2])
     expect = oracle_mod.tallies(g, 1, 1, 0, 4000)
     words = oracle_mod.eval_words(g, 1, 0, 64)
-    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED, capi.MODE_STAGED):
+    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED, capi.MODE_STAGED, capi.MODE_STRIP):
         with engine(capi, g, mode=mode) as e:
             e.run(1, 1, 0, 4000)
             ones, _ = e.tallies()
@@ -152,7 +155,7 @@ def test_atleast_uint8_wrap(capi, oracle_mod, gpu):
                   gate_in_count=[n, n, n], gate_neg_count=[0, 10, 0], inputs=np.arange(n),
                   tally_nodes=[n, n + 1, n + 2])
     expect = oracle_mod.tallies(g, 1, 1, 0, 2000)
-    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED, capi.MODE_STAGED):
+    for mode in (capi.MODE_FUSED, capi.MODE_LAYERED, capi.MODE_STAGED, capi.MODE_STRIP):
         with engine(capi, g, mode=mode) as e:
             e.run(1, 1, 0, 2000)
             assert np.array_equal(e.tallies()[0], expect)

@@ -5,7 +5,8 @@ Workload (one "step" = one pass of the hot path over one batch): the 5,000
 basic-event / 3,000-gate synthetic tree (seed 11, 45% AND, 40% OR, 10%
 ATLEAST, 5% NOT/XOR, 20 layers, 30% of nodes with fan-out >= 2, p
 log-uniform in [1e-5, 1e-2]); 2^30 samples = 2^24 uint64 words per node per
-GPU; every gate tallied.  Each step is a new pass (iteration = step + 1),
+GPU; every gate tallied; strip mode (one persistent kernel per pass) unless
+--mode says otherwise.  Each step is a new pass (iteration = step + 1),
 exactly like the reference's pass loop.  N GPUs shard the sample-word range
 (weak scaling: 2^24 words per GPU) and all-reduce the tallies after each pass.
 
@@ -49,7 +50,7 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fused kernel CTAs per SM (0 = engine default)")
     ap.add_argument("--peak-words", type=int, default=1 << 22, help="words per register-only sampler launch")
-    ap.add_argument("--mode", default="staged", choices=["fused", "staged", "layered", "strip"])
+    ap.add_argument("--mode", default="strip", choices=["fused", "staged", "layered", "strip"])
     ap.add_argument("--tree", default="config2", choices=["config1", "config2"],
                     help="plain workload's tree (config1: the small 200-event tree, for profiling captures)")
     ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")

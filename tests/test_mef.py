@@ -1,0 +1,173 @@
+"""MEF loader: a hand-written model with every construct the loader reads is
+checked against a brute-force evaluation of the XML written here (not via
+the loader), node numbering against the reference's first-encounter rule,
+errors for what it does not read, and -- where the reference project is on
+disk -- its Aralia models against the exact values listed in its benchmark
+table.  The GPU test runs a loaded model through the engine."""
+import csv
+import itertools
+import os
+import xml.etree.ElementTree as ET
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from mcscram_b200 import mef
+
+FIX = Path(__file__).parent / "golden" / "mef" / "features.xml"
+TWO32 = float(1 << 32)
+ARALIA = Path("/root/reference/input/Aralia")
+TABLE = Path("/root/reference/benchmarks/input.csv")
+
+
+def _brute_force(path, top):
+    """P(top) by enumerating the basic events, evaluating the XML directly."""
+    root = ET.parse(path).getroot()
+    gates = {g.get("name"): g[-1] for g in root.iter("define-gate")}
+    params = {p.get("name"): float(p.find("float").get("value")) for p in root.iter("define-parameter")}
+    house = {h.get("name"): h.find("constant").get("value") == "true" for h in root.iter("define-house-event")}
+    prob = {}
+    for b in root.iter("define-basic-event"):
+        e = b[0]
+        v = float(e.get("value")) if e.tag == "float" else params[e.get("name")]
+        prob[b.get("name")] = np.floor(v * TWO32) / TWO32  # the sampler's quantised probability
+
+    def ev(el, x):
+        t = el.tag
+        if t in ("gate", "event") and el.get("name") in gates:
+            return ev(gates[el.get("name")], x)
+        if t in ("basic-event", "event"):
+            return x[el.get("name")]
+        if t == "house-event":
+            return house[el.get("name")]
+        if t == "constant":
+            return el.get("value") == "true"
+        vals = [ev(c, x) for c in el]
+        if t == "and":
+            return all(vals)
+        if t == "or":
+            return any(vals)
+        if t == "not":
+            return not vals[0]
+        if t == "xor":
+            return sum(vals) % 2 == 1
+        if t == "nand":
+            return not all(vals)
+        if t == "nor":
+            return not any(vals)
+        if t == "atleast":
+            return sum(vals) >= int(el.get("min"))
+        raise AssertionError(t)
+
+    names = sorted(prob)
+    total = 0.0
+    for bits in itertools.product([False, True], repeat=len(names)):
+        x = dict(zip(names, bits))
+        w = np.prod([prob[n] if b else 1 - prob[n] for n, b in zip(names, bits)])
+        total += w * ev(gates[top], x)
+    return total
+
+
+def test_features_model_exact(oracle_mod):
+    g = mef.load(FIX, top="top")
+    exact = _brute_force(FIX, "top")
+    assert oracle_mod.bdd_probability(g) == pytest.approx(exact, rel=1e-12)
+
+
+def test_numbering_follows_first_encounter():
+    m = mef.parse(FIX)
+    assert set(m.top_gates()) == {"top", "g_pass"}
+    with pytest.raises(mef.MefError, match="top gates"):
+        m.build()
+    pdag, root, var_index, gate_index = m.build("top")
+    # depth-first over top's arguments: g_and (a, b, g_nor (c)), g_atleast (b, c, e, (f)), g_xor (e, g_nand (a, f)), (d, a)
+    assert var_index == {"a": 2, "b": 3, "c": 4, "e": 5, "f": 6, "d": 7}
+    # then the house events, then the gates in pre-order (top first)
+    assert root == 2 + len(var_index) + 3
+    assert gate_index["g_and"] == root + 1 and gate_index["g_nor"] == root + 2
+    assert pdag.event_order()  # the host layering accepts the PDAG
+
+
+@pytest.mark.parametrize("xml,msg", [
+    ("<opsa-mef><define-gate name='t'><and><basic-event name='x'/></and></define-gate></opsa-mef>",
+     "unknown basic-event"),
+    ("<opsa-mef><define-gate name='t'><or><event name='x'/></or></define-gate>"
+     "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown event"),
+    ("<opsa-mef><define-basic-event name='x'><exponential/></define-basic-event></opsa-mef>",
+     "unsupported expression"),
+    ("<opsa-mef><define-gate name='t'><or/></define-gate><define-gate name='t'><or/></define-gate></opsa-mef>",
+     "defined twice"),
+    ("<opsa-mef><define-gate name='t'><imply/></define-gate></opsa-mef>", "unsupported formula"),
+    ("<opsa-mef><define-basic-event name='x'><float value='1.5'/></define-basic-event></opsa-mef>",
+     "outside"),
+    ("<model/>", "opsa-mef"),
+])
+def test_errors_name_the_problem(xml, msg):
+    with pytest.raises(mef.MefError, match=msg):
+        mef.parse(xml)
+
+
+def _table():
+    rows = list(csv.reader(TABLE.open(encoding="utf-8-sig")))[1:]
+    return [(r[1], float(r[2])) for r in rows if float(r[2]) > 0]
+
+
+# The listed value of das9204 does not belong to the model file: the file's
+# exact probability is 2.1694e-11, and plain sampling of 2^30 of its samples
+# finds no failure where the listed 6.08e-8 would give about 65.
+_LISTED_INCONSISTENT = {"das9204.xml"}
+
+
+@pytest.mark.skipif(not TABLE.exists(), reason="the reference's Aralia models are not on this machine")
+def test_aralia_models_match_reference_values(oracle_mod):
+    checked = 0
+    sampled = []
+    for name, listed in _table():
+        g = mef.load(ARALIA / name)
+        try:
+            exact = oracle_mod.bdd_probability(g, max_nodes=1_000_000)
+        except Exception:
+            sampled.append((name, g, listed))  # BDD too large: checked by sampling below
+            continue
+        if name in _LISTED_INCONSISTENT:
+            assert exact == pytest.approx(2.1694e-11, rel=1e-3)
+            continue
+        assert exact == pytest.approx(listed, rel=5e-5), name  # the table has six significant digits
+        checked += 1
+    assert checked >= 30
+    for name, g, listed in sampled:
+        W = 1 << 15
+        hits = int(oracle_mod.tallies(g, 1, 1, 0, W)[0])
+        n = W * 64
+        sd = np.sqrt(listed * (1 - listed) / n)
+        assert abs(hits / n - listed) <= 4 * sd + 1e-12, (name, hits / n, listed)
+
+
+@pytest.mark.skipif(not TABLE.exists(), reason="the reference's Aralia models are not on this machine")
+def test_das9204_listed_value_is_not_the_files(oracle_mod):
+    g = mef.load(ARALIA / "das9204.xml")
+    hits = int(oracle_mod.tallies(g, 1, 1, 0, 1 << 20)[0])
+    assert hits <= 1  # 6.7e7 samples: ~4 expected at the listed 6.08e-8, ~0.001 at the file's value
+
+
+@pytest.mark.gpu
+def test_loaded_model_runs_bit_exact_on_gpu(capi, oracle_mod, gpu):
+    g = mef.load(FIX, top="top")
+    for mode in (capi.MODE_STRIP, capi.MODE_FUSED):
+        with capi.Engine(g, mode=mode) as e:
+            e.run(2, 1, 5, 20000)
+            ones, total = e.tallies()
+        assert np.array_equal(ones, oracle_mod.tallies(g, 2, 1, 5, 20000))
+        assert total == 20000 * 64
+
+
+@pytest.mark.gpu
+def test_command_line_estimate_within_its_interval(gpu, capsys):
+    import json
+    assert mef.main([str(FIX), "--top", "top", "--samples", str(2 ** 26)]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    exact = _brute_force(FIX, "top")
+    assert out["samples"] == 2 ** 26
+    half = (out["ci95"][1] - out["ci95"][0]) / 2
+    assert abs(out["p_top"] - exact) <= 2.1 * half  # a 4-sigma band around the 95 % half-width

@@ -138,6 +138,30 @@ double mcg_beta_quantile(double a, double b, double q);
 mcg_status mcg_sample_shape(uint64_t num_trials, uint64_t max_words_per_iteration, uint64_t *words_per_iteration,
                             uint64_t *total_iterations, uint64_t *rounded_trials);
 
+/* Monte Carlo importance factors: one pass of word_count words (pass
+ * `iteration`) over the graph, tallying the top event graph->tally_nodes[0]
+ * and, for each requested basic event (flattened ids in [0, n_be); NULL =
+ * every event), the conjunction of the top event and that event.  Fills
+ * out[n_events] with the estimates
+ *     P(top | x=1) = P(top and x) / p,  P(top | x=0) = (P(top) - P(top and x)) / (1 - p),
+ *     mif = P(top | x=1) - P(top | x=0)  (Birnbaum),
+ * and cif, raw, dif, rrw from mif as the exact analysis defines them
+ * (src/importance_analysis.cc:50-56), p being the probability the sampler
+ * draws (threshold / 2^32).  Replaces the Monte Carlo importance analysis
+ * the reference leaves as a stub (src/mc/core/importance_analysis.cc).
+ * run may be NULL (strip mode, device 0).  Conditional estimates of an
+ * event with small p rest on about p * samples draws. */
+typedef struct mcg_importance_factor {
+    uint32_t event;
+    uint64_t samples;
+    double p, p_top, p_joint, p_top_given_1, p_top_given_0;
+    double mif, cif, dif, raw, rrw;
+} mcg_importance_factor;
+
+mcg_status mcg_importance_factors(const mcg_graph_desc *graph, const uint32_t *events, uint32_t n_events,
+                                  const mcg_run_desc *run, uint32_t iteration, uint64_t word_count,
+                                  mcg_importance_factor *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,10 +55,17 @@ def parse_args():
                     help="plain workload's tree (config1: the small 200-event tree, for profiling captures)")
     ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")
     ap.add_argument("--sampler-blocks", type=int, default=0, help="staged: sampler blocks per SM (0 = default)")
-    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis", "converge"],
                     help="plain: the 5,000-event tree (headline); ua: batched uncertainty analysis; "
                          "is: GPU time to 5%% relative error on the 1e-8 tree, learned IS vs plain; "
-                         "bis: the same for 1,024 rare-event trees at once with one shared network")
+                         "bis: the same for 1,024 rare-event trees at once with one shared network; "
+                         "converge: ComputeTallies to a relative error, waiting vs pipelined convergence loop")
+    ap.add_argument("--converge-rel-err", type=float, default=1e-3)
+    ap.add_argument("--converge-words", type=int, default=1 << 14, help="words per pass of the convergence loop")
+    ap.add_argument("--converge-watch", default="top", choices=["top", "gates"],
+                    help="monitored nodes: the top event, or every gate (heavier host statistics per step)")
+    ap.add_argument("--converge-mode", default="fused", choices=["fused", "staged", "strip"],
+                    help="engine mode of the convergence loop (short passes favour the fused kernel)")
     ap.add_argument("--is-rounds", type=int, default=5)
     ap.add_argument("--is-round-words", type=int, default=1 << 20, help="words per CE round (2^26 samples)")
     ap.add_argument("--is-batch-words", type=int, default=1 << 20)
@@ -445,6 +452,48 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
+def run_converge(args, rank: int, world: int, local: int) -> int:
+    """ComputeTallies (the reference's ProbabilityAnalyzer<DirectEval> path) on
+    the 200-event / 100-gate tree to a relative error of the top event:
+    the convergence loop that waits for every pass against the pipelined one
+    that judges pass k while pass k + 1 runs (same tallies and stopping
+    point).  Wall time of the whole call, median of the steps."""
+    if rank != 0:
+        return 0
+    import torch
+    from mcscram_b200 import _capi, host, synth
+
+    torch.cuda.set_device(local)
+    g = synth.config1()
+    p = host.Pdag.from_flat(g)
+    watch = [] if args.converge_watch == "top" else [int(x) for x in g.gate_pdag_idx[:-1]]
+    res = {}
+    for pipelined in (0, 1):
+        kw = {} if args.converge_watch == "top" else dict(num_trials=1 << 26, early_stop=0)  # rare gates never converge
+        s = host.Settings.default(ci_rel_margin_error=args.converge_rel_err, pipelined=pipelined,
+                                  max_words_per_iteration=args.converge_words, **kw)
+        for _ in range(args.warmup):
+            host.compute_tallies(p, s, watch, device=local, mode=_capi.MODES[args.converge_mode])
+        times = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tallies, rep = host.compute_tallies(p, s, watch, device=local, mode=_capi.MODES[args.converge_mode])
+            times.append(time.perf_counter() - t0)
+        res[pipelined] = {"seconds": statistics.median(times), "passes": rep["passes"], "trials": rep["trials"],
+                          "p_top": tallies[0]["mean"], "steps": rep["steps"], "burn_in_steps": rep["burn_in_steps"]}
+    assert res[0]["trials"] == res[1]["trials"] and res[0]["p_top"] == res[1]["p_top"]
+    print(json.dumps({
+        "metric": "ComputeTallies wall time to convergence", "value": res[1]["seconds"], "unit": "s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "data": "synthetic",
+        "dtype": "u64", "vs_baseline": None,
+        "config": {"workload": f"200-event / 100-gate tree (seed 372), monitored: {args.converge_watch}, Bayes policy, relative "
+                               f"error {args.converge_rel_err}, {args.converge_words} words per pass, {args.converge_mode} mode"},
+        "waiting_loop": res[0], "pipelined_loop": res[1],
+        "speedup": res[0]["seconds"] / res[1]["seconds"]}), flush=True)
+    return 0
+
+
 def main() -> int:
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -458,6 +507,8 @@ def main() -> int:
         return run_is(args, rank, world, local)
     if args.workload == "bis":
         return run_bis(args, rank, world, local)
+    if args.workload == "converge":
+        return run_converge(args, rank, world, local)
 
     import numpy as np
     import torch

@@ -149,6 +149,18 @@ mcg_status mcg_set_tallies(mcg_engine *engine, const uint64_t *ones, uint64_t to
 /* Zeroes ones and total_bits. */
 mcg_status mcg_reset_tallies(mcg_engine *engine);
 
+/* Asynchronous snapshot of the tallies: enqueues on the engine's stream,
+ * behind every pass submitted so far, a device-side copy of the counters
+ * into the engine's snapshot slot `slot` (0 or 1) together with the total
+ * bits those passes cover, and returns at once.  mcg_snapshot_read waits for
+ * that copy only -- passes submitted after it keep running -- and returns
+ * it.  Lets a caller decide on pass k while pass k + 1 runs (the pipelined
+ * convergence loop of mcg_run_to_convergence).  No reference counterpart;
+ * the reference waits for its queue before every harvest
+ * (layer_manager.tpp:259). */
+mcg_status mcg_snapshot_tallies(mcg_engine *engine, uint32_t slot);
+mcg_status mcg_snapshot_read(mcg_engine *engine, uint32_t slot, uint64_t *ones, uint64_t *total_bits);
+
 /* Materialised words of every node (n_be + n_gates rows of n_words) for pass
  * `iteration` over words [word_begin, word_begin + n_words), copied to host
  * memory out[node * n_words + w].  Uses the layered kernels; for parity

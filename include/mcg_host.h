@@ -58,6 +58,8 @@ typedef struct mcg_settings {
     double overhead_ratio;       /* default 0.05 (accepted, not needed by the fused kernel) */
     double oracle_p;             /* < 0: unset */
     uint64_t max_words_per_iteration; /* words per pass cap; 0 = 2^24 */
+    uint32_t pipelined;          /* 1 (default): judge pass k while pass k + 1 runs, same results
+                                    as 0 (wait for every pass) at the cost of one discarded pass */
 } mcg_settings;
 
 typedef struct mcg_convergence_report {

@@ -481,6 +481,9 @@ void release(mcg_engine *e) {
     cudaFree(e->d_stage[1]);
     cudaFree(e->d_strip_scratch);
     cudaFree(e->d_queue);
+    for (int i = 0; i < 2; ++i) {
+        if (e->ev_snap[i]) cudaEventDestroy(e->ev_snap[i]);
+    }
     for (cudaEvent_t ev : {e->ev_fork, e->ev_a[0], e->ev_a[1], e->ev_b[0], e->ev_b[1], e->ev_join_a, e->ev_join_b})
         if (ev) cudaEventDestroy(ev);
     for (auto &pe : e->prof_events) {
@@ -548,7 +551,8 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
             e->own_stream = true;
         }
         const size_t nt = std::max<size_t>(e->graph.tally_nodes.size(), 1);
-        if (cudaMalloc((void **)&e->d_tally, nt * sizeof(unsigned long long)) != cudaSuccess ||
+        // the counters and, behind them, two snapshot slots (mcg_snapshot_tallies)
+        if (cudaMalloc((void **)&e->d_tally, 3 * nt * sizeof(unsigned long long)) != cudaSuccess ||
             cudaMemset(e->d_tally, 0, nt * sizeof(unsigned long long)) != cudaSuccess) {
             st = mcg::fail(MCG_ERR_OOM, "tally allocation failed");
             break;
@@ -662,6 +666,36 @@ mcg_status mcg_set_tallies(mcg_engine *e, const uint64_t *ones, uint64_t total_b
     if (!e->graph.tally_nodes.empty())
         MCG_CUDA(cudaMemcpy(e->d_tally, ones, e->graph.tally_nodes.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
     e->total_bits = total_bits;
+    return MCG_OK;
+}
+
+mcg_status mcg_snapshot_tallies(mcg_engine *e, uint32_t slot) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    if (slot > 1) return mcg::fail(MCG_ERR_INVALID, "slot must be 0 or 1");
+    MCG_CUDA(cudaSetDevice(e->device));
+    const size_t n = std::max<size_t>(e->graph.tally_nodes.size(), 1);
+    if (!e->ev_snap[slot]) MCG_CUDA(cudaEventCreateWithFlags(&e->ev_snap[slot], cudaEventDisableTiming));
+    // device-side copy into the slot behind the counters: no host buffer to pin
+    MCG_CUDA(cudaMemcpyAsync(e->d_tally + (1 + slot) * n, e->d_tally, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice,
+                             e->stream));
+    MCG_CUDA(cudaEventRecord(e->ev_snap[slot], e->stream));
+    e->snap_total[slot] = e->total_bits;
+    return MCG_OK;
+}
+
+mcg_status mcg_snapshot_read(mcg_engine *e, uint32_t slot, uint64_t *ones, uint64_t *total_bits) {
+    mcg::clear_error();
+    if (!e || !ones || !total_bits) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    if (slot > 1 || !e->ev_snap[slot]) return mcg::fail(MCG_ERR_STATE, "no snapshot in this slot");
+    MCG_CUDA(cudaSetDevice(e->device));
+    MCG_CUDA(cudaEventSynchronize(e->ev_snap[slot]));
+    // the slot is not written by the passes behind the snapshot: this copy does not wait for them
+    const size_t n = std::max<size_t>(e->graph.tally_nodes.size(), 1);
+    if (!e->graph.tally_nodes.empty())
+        MCG_CUDA(cudaMemcpy(ones, e->d_tally + (1 + slot) * n, e->graph.tally_nodes.size() * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost));
+    *total_bits = e->snap_total[slot];
     return MCG_OK;
 }
 

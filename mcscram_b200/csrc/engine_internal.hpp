@@ -76,6 +76,9 @@ struct mcg_engine {
     uint32_t strip_smem = 0;               // tally counters in shared memory (0: global atomics)
     uint32_t strip_blocks = 6;             // resident blocks per SM the kernel is built for
 
+    cudaEvent_t ev_snap[2] = {nullptr, nullptr};  // tally snapshots (slots behind d_tally)
+    uint64_t snap_total[2] = {0, 0};
+
     mcg_run_desc run_desc{};                  // options the engine was created with
     bool prog_compiled = false;               // fused program compiled (fused mode, or on request)
     bool profile_a = false;                   // time every sampler-phase launch

@@ -72,6 +72,7 @@ mcg::host::settings settings_from(const mcg_settings *s) {
     o.ci_burnin_trials = s->ci_burnin_trials;
     o.overhead_ratio = s->overhead_ratio;
     o.oracle_p = s->oracle_p;
+    o.pipelined = s->pipelined != 0;
     return o;
 }
 
@@ -112,6 +113,7 @@ mcg_status mcg_settings_default(mcg_settings *out) {
     out->overhead_ratio = 0.05;
     out->oracle_p = -1.0;
     out->max_words_per_iteration = 0;
+    out->pipelined = 1;
     return MCG_OK;
 }
 

@@ -146,6 +146,24 @@ TallyNodeMap &layer_manager::collect_tallies(TallyNodeMap &tallies) {
     return tallies;
 }
 
+void layer_manager::snapshot(uint32_t slot) { throw_status(mcg_snapshot_tallies(engine_, slot), "snapshot"); }
+
+TallyNodeMap &layer_manager::collect_snapshot(uint32_t slot, TallyNodeMap &tallies) {
+    std::vector<uint64_t> ones(tally_index_.size());
+    uint64_t total = 0;
+    throw_status(mcg_snapshot_read(engine_, slot, ones.data(), &total), "collect_snapshot");
+    for (size_t i = 0; i < tally_index_.size(); ++i) tallies[tally_index_[i]].tally_stats.update(ones[i], total);
+    return tallies;
+}
+
+void layer_manager::restore_snapshot(uint32_t slot, uint32_t iteration) {
+    std::vector<uint64_t> ones(std::max<size_t>(tally_index_.size(), 1));
+    uint64_t total = 0;
+    throw_status(mcg_snapshot_read(engine_, slot, ones.data(), &total), "restore_snapshot");
+    throw_status(mcg_set_tallies(engine_, ones.data(), total), "restore_snapshot");
+    iteration_ = iteration;
+}
+
 // ------------------------------------------------------------------ controller
 
 convergence_controller::convergence_controller(layer_manager &mgr, const settings &s) : manager_(mgr), settings_(s) {
@@ -223,10 +241,61 @@ bool convergence_controller::burn_in_step(TallyNodeMap &map) {
 
 // convergence_controller.h:371-381
 stats::tally convergence_controller::run_to_convergence(TallyNodeMap &map) {
+    if (settings_.pipelined) return run_to_convergence_pipelined(map);
     while (burn_in_step(map)) {
     }
     while (step(map)) {
     }
+    return current_tally_;
+}
+
+// The decision the synchronous loop takes before each pass: burn-in while
+// the burn-in trials are not reached, then steps until converged (early
+// stop) or the iteration limit.
+convergence_controller::phase convergence_controller::next_pass() {
+    if (!burn_in_complete()) return phase::burn_in;
+    if (all_converged() && settings_.early_stop) return phase::none;
+    if (!fixed_limit_reached_ && iteration_limit_reached()) {
+        fixed_limit_reached_ = true;
+        return phase::none;
+    }
+    return phase::step;
+}
+
+void convergence_controller::after_pass(phase p) {
+    if (p == phase::burn_in) {
+        ++burn_in_steps_;
+        return;
+    }
+    if (!eps_converged_ && eps_bounded()) eps_converged_ = true;
+    if (!log10_converged_ && log_eps_bounded()) log10_converged_ = true;
+    ++steps_;
+}
+
+// The same decisions as run_to_convergence's synchronous loop, taken one
+// pass behind the GPU: while the tallies after pass k are read and judged,
+// pass k + 1 already runs.  When the loop stops after pass k, the passes
+// run ahead are discarded by rolling the counters, their total and the pass
+// number back to the snapshot after pass k, so tallies, statistics and
+// stopping point equal the synchronous loop's; the cost is one pass of GPU
+// time that nobody uses.
+stats::tally convergence_controller::run_to_convergence_pipelined(TallyNodeMap &map) {
+    phase p = next_pass();
+    if (p == phase::none) return current_tally_;
+    uint32_t done = 0;                       // passes judged
+    const uint32_t base = manager_.iteration();
+    manager_.single_pass();                  // pass 1
+    manager_.snapshot(0);
+    for (;;) {
+        manager_.single_pass();              // pass done + 2, ahead of the decision
+        manager_.snapshot((done + 1) & 1u);
+        process_tallies(manager_.collect_snapshot(done & 1u, map));
+        ++done;
+        after_pass(p);
+        p = next_pass();
+        if (p == phase::none) break;
+    }
+    manager_.restore_snapshot((done - 1) & 1u, base + done);
     return current_tally_;
 }
 

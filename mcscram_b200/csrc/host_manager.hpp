@@ -78,6 +78,11 @@ class layer_manager {
     std::size_t node_count() const { return node_count_; }
     const sample_shaper &shaper() const { return shaper_; }
     uint32_t iteration() const { return iteration_; }
+    // Asynchronous harvest: snapshot the counters behind the passes so far,
+    // fold a snapshot into the map, and roll the engine back to a snapshot.
+    void snapshot(uint32_t slot);
+    TallyNodeMap &collect_snapshot(uint32_t slot, TallyNodeMap &tallies);
+    void restore_snapshot(uint32_t slot, uint32_t iteration);
     mcg_engine *engine() const { return engine_; }
     const Graph &graph() const { return graph_; }
     // Position of a basic event in the layer-0 block (the counter's event_idx).
@@ -103,6 +108,7 @@ struct settings {
     stats::policy ci_policy = stats::policy::bayes;
     double overhead_ratio = 0.05;
     double oracle_p = -1.0;
+    bool pipelined = true;  // decide on pass k while pass k + 1 runs (same results)
 };
 
 class convergence_controller {
@@ -113,6 +119,7 @@ class convergence_controller {
     bool step(TallyNodeMap &map);
     bool burn_in_step(TallyNodeMap &map);
     stats::tally run_to_convergence(TallyNodeMap &map);
+    stats::tally run_to_convergence_pipelined(TallyNodeMap &map);
 
     bool all_converged() const { return log10_converged_ && eps_converged_; }
     bool iteration_limit_reached() const;
@@ -132,6 +139,9 @@ class convergence_controller {
     const stats::tally &current_tally() const { return current_tally_; }
 
   private:
+    enum class phase { none, burn_in, step };
+    phase next_pass();  // the phase of the pass the synchronous loop would run next (none: stop)
+    void after_pass(phase p);
     bool eps_bounded() const { return cur_eps_ > 0 && cur_eps_ <= target_eps_; }
     bool log_eps_bounded() const { return cur_eps_log10_ > 0 && cur_eps_log10_ <= settings_.ci_rel_margin_error; }
     layer_manager &manager_;

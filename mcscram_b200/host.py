@@ -39,6 +39,7 @@ class Settings(C.Structure):
         ("num_trials", C.c_uint64), ("early_stop", C.c_uint32), ("policy", C.c_uint32),
         ("ci_confidence", C.c_double), ("ci_rel_margin_error", C.c_double), ("ci_burnin_trials", C.c_double),
         ("overhead_ratio", C.c_double), ("oracle_p", C.c_double), ("max_words_per_iteration", C.c_uint64),
+        ("pipelined", C.c_uint32),
     ]
 
     @classmethod

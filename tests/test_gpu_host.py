@@ -79,3 +79,26 @@ def test_compute_tallies_root_first(oracle_mod, gpu):
     assert [o["index"] for o in out[1:]] == watch
     exact = oracle_mod.bdd_probability(g0)
     assert abs(out[0]["mean"] - exact) <= 3 * out[0]["std_err"] + 1e-12
+
+
+@pytest.mark.parametrize("case", ["bayes", "wald", "fixed"])
+def test_pipelined_loop_equals_waiting_loop(gpu, case):
+    """Judging pass k while pass k + 1 runs gives the waiting loop's tallies,
+    statistics and stopping point."""
+    g0, p = c1_pdag()
+    root = int(g0.gate_pdag_idx[-1])
+    kw = dict(policy=host.POLICY_WALD if case == "wald" else host.POLICY_BAYES, ci_rel_margin_error=0.01,
+              ci_burnin_trials=float(1 << 20))
+    budget = 0
+    if case == "fixed":
+        kw.update(num_trials=3 << 20, early_stop=0, ci_rel_margin_error=1e-6)
+        budget = 3 << 20
+    out = []
+    for pipelined in (0, 1):
+        s = host.Settings.default(pipelined=pipelined, **kw)
+        with host.LayerManager(p, budget, [root], max_words_per_iteration=1 << 14) as m:
+            tallies, rep = m.run_to_convergence(s)
+            out.append((tallies, {k: v for k, v in rep.items() if k != "seconds"}))
+    assert out[0][0] == out[1][0]
+    assert out[0][1] == out[1][1]
+    assert out[1][1]["steps"] + out[1][1]["burn_in_steps"] >= 2

@@ -4,12 +4,17 @@ Reads the subset of the Model Exchange Format that fault-tree models such as
 the Aralia set use: ``define-fault-tree`` / ``model-data`` holding
 ``define-gate`` (formulas ``and``, ``or``, ``not``, ``xor``, ``nand``,
 ``nor``, ``atleast min=k``, or a single event reference, nested formulas
-allowed), ``define-basic-event`` (a ``float`` value or a ``parameter``
-reference), ``define-house-event`` (``constant value="true|false"``) and
-``define-parameter`` (a ``float`` value).  Event references are ``gate``,
+allowed), ``define-basic-event`` and ``define-parameter`` with an
+expression, ``define-house-event`` (``constant value="true|false"``).
+Expressions: ``float``, ``int``, ``parameter``, ``system-mission-time``,
+``exponential`` (1 - exp(-lambda t)), ``GLM`` and ``Weibull`` (the
+formulas of mcSCRAM src/expression/exponential.cc:37-38, 87-91, 108-111),
+``add``, ``sub``, ``mul``, ``div``, ``neg``.  Event references are ``gate``,
 ``basic-event``, ``house-event`` or the untyped ``event``.  Other
-expressions (time-dependent distributions, CCF groups, substitutions) are
-rejected with an error naming the element.
+expressions (random deviates, CCF groups, substitutions) are rejected with
+an error naming the element.  Probabilities are taken at a mission time
+(8760 hours unless given); ``probability_over_time`` evaluates the top
+event on a grid of mission times in one batched GPU pass.
 
 Node numbering follows the reference's PDAG construction from a MEF gate
 (mcSCRAM src/pdag.cc:470-548): basic events get indices 2, 3, ... in the
@@ -23,10 +28,13 @@ differ from the reference's for models the preprocessor rewrites.
 """
 from __future__ import annotations
 
+import math
 import xml.etree.ElementTree as ET
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Dict, List, Optional, Tuple, Union
+
+import numpy as np
 
 from .graph import AND, ATLEAST, NAND, NOR, NOT, NULL, OR, XOR, FlatGraph
 
@@ -37,6 +45,63 @@ _SKIP = ("label", "attributes")
 
 class MefError(ValueError):
     """A model the loader cannot read; the message names the element."""
+
+
+DEFAULT_MISSION_TIME = 8760.0  # hours: SCRAM's default analysis setting
+
+
+@dataclass
+class Expr:
+    """An expression tree: op "value" (args: [float]), "parameter" (args:
+    [name]), "time", or a function of its argument expressions."""
+    op: str
+    args: list
+
+    def value(self, t: float, params: Dict[str, "Expr"], _depth: int = 0) -> float:
+        if _depth > 64:
+            raise MefError("parameters refer to each other in a cycle")
+        op, a = self.op, self.args
+        if op == "value":
+            return a[0]
+        if op == "time":
+            return t
+        if op == "parameter":
+            if a[0] not in params:
+                raise MefError(f"unknown parameter {a[0]!r}")
+            return params[a[0]].value(t, params, _depth + 1)
+        v = [x.value(t, params, _depth + 1) for x in a]
+        if op == "exponential":  # 1 - exp(-lambda t)
+            return 1.0 - math.exp(-v[0] * v[1])
+        if op == "GLM":  # gamma, lambda, mu, t
+            g, lam, mu, tt = v
+            r = lam + mu
+            return (lam - (lam - g * r) * math.exp(-r * tt)) / r
+        if op == "Weibull":  # alpha, beta, t0, t
+            al, be, t0, tt = v
+            return 0.0 if tt <= t0 else 1.0 - math.exp(-(((tt - t0) / al) ** be))
+        if op == "add":
+            return sum(v)
+        if op == "mul":
+            return math.prod(v)
+        if op == "sub":
+            return v[0] - sum(v[1:])
+        if op == "div":
+            out = v[0]
+            for x in v[1:]:
+                out /= x
+            return out
+        if op == "neg":
+            return -v[0]
+        raise MefError(f"unknown expression {op!r}")
+
+    def depends_on_time(self, params: Dict[str, "Expr"], _depth: int = 0) -> bool:
+        if _depth > 64:
+            return False
+        if self.op == "time":
+            return True
+        if self.op == "parameter":
+            return self.args[0] in params and params[self.args[0]].depends_on_time(params, _depth + 1)
+        return self.op not in ("value",) and any(x.depends_on_time(params, _depth + 1) for x in self.args)
 
 
 @dataclass
@@ -52,10 +117,18 @@ class Formula:
 @dataclass
 class MefModel:
     gates: Dict[str, Formula] = field(default_factory=dict)
-    basic_events: Dict[str, float] = field(default_factory=dict)
+    basic_events: Dict[str, Expr] = field(default_factory=dict)
     house_events: Dict[str, bool] = field(default_factory=dict)
-    parameters: Dict[str, float] = field(default_factory=dict)
+    parameters: Dict[str, Expr] = field(default_factory=dict)
     names: List[str] = field(default_factory=list)  # fault-tree names
+    mission_time: float = DEFAULT_MISSION_TIME
+
+    def probability(self, event: str, t: Optional[float] = None) -> float:
+        """Probability of a basic event at mission time t (default: the model's)."""
+        v = self.basic_events[event].value(self.mission_time if t is None else t, self.parameters)
+        if not 0.0 <= v <= 1.0:
+            raise MefError(f"basic event {event!r}: probability {v} outside [0, 1] at t = {t}")
+        return v
 
     def top_gates(self) -> List[str]:
         """Gates that no other gate references, in definition order."""
@@ -110,7 +183,7 @@ class MefModel:
         # 2. gates in pre-order of construction (ConstructGate)
         pdag = Pdag()
         for name, idx in var_index.items():
-            pdag.add_variable(idx, self.basic_events[name])
+            pdag.add_variable(idx, self.probability(name))
         for name, idx in house_index.items():
             pdag.add_variable(idx, 1.0 if self.house_events[name] else 0.0)
         gate_index: Dict[str, int] = {}
@@ -173,17 +246,32 @@ def _local(tag: str) -> str:
     return tag.rsplit("}", 1)[-1]
 
 
-def _parse_expression(el: ET.Element, what: str) -> Tuple[str, Union[float, str]]:
+_ARITY = {"exponential": 2, "GLM": 4, "Weibull": 4, "neg": 1}
+
+
+def _parse_expr(e: ET.Element, what: str) -> Expr:
+    tag = _local(e.tag)
+    if tag in ("float", "int"):
+        return Expr("value", [float(e.get("value"))])
+    if tag == "parameter":
+        return Expr("parameter", [e.get("name")])
+    if tag == "system-mission-time":
+        return Expr("time", [])
+    if tag in ("exponential", "GLM", "Weibull", "add", "sub", "mul", "div", "neg"):
+        args = [_parse_expr(c, what) for c in e if _local(c.tag) not in _SKIP]
+        if tag in _ARITY and len(args) != _ARITY[tag]:
+            raise MefError(f"{what}: <{tag}> takes {_ARITY[tag]} arguments, found {len(args)}")
+        if not args:
+            raise MefError(f"{what}: <{tag}> without arguments")
+        return Expr(tag, args)
+    raise MefError(f"{what}: unsupported expression <{tag}>")
+
+
+def _parse_expression(el: ET.Element, what: str) -> Expr:
     kids = [c for c in el if _local(c.tag) not in _SKIP]
     if len(kids) != 1:
         raise MefError(f"{what}: expected one expression, found {len(kids)}")
-    e = kids[0]
-    tag = _local(e.tag)
-    if tag == "float" or tag == "int":
-        return "value", float(e.get("value"))
-    if tag == "parameter":
-        return "parameter", e.get("name")
-    raise MefError(f"{what}: unsupported expression <{tag}>")
+    return _parse_expr(kids[0], what)
 
 
 def _parse_formula(el: ET.Element, where: str) -> Formula:
@@ -219,8 +307,9 @@ def _parse_arg(el: ET.Element, where: str) -> Tuple[bool, str, object]:
     return False, "formula", _parse_formula(el, where)
 
 
-def parse(source: Union[str, Path]) -> MefModel:
-    """Reads a MEF document (a path, or the XML text itself)."""
+def parse(source: Union[str, Path], mission_time: float = DEFAULT_MISSION_TIME) -> MefModel:
+    """Reads a MEF document (a path, or the XML text itself); probabilities are
+    evaluated at `mission_time` unless asked for at another time."""
     text = Path(source).read_text() if isinstance(source, Path) or (
         isinstance(source, str) and not source.lstrip().startswith("<")) else source
     try:
@@ -229,8 +318,7 @@ def parse(source: Union[str, Path]) -> MefModel:
         raise MefError(f"not well-formed XML: {e}") from None
     if _local(root.tag) != "opsa-mef":
         raise MefError("root element is not <opsa-mef>")
-    m = MefModel()
-    basic_expr: Dict[str, Tuple[str, object]] = {}
+    m = MefModel(mission_time=float(mission_time))
 
     def visit(container: ET.Element):
         for el in container:
@@ -250,29 +338,23 @@ def parse(source: Union[str, Path]) -> MefModel:
                     raise MefError(f"gate {name!r} defined twice")
                 m.gates[name] = _parse_formula(kids[0], f"gate {name!r}")
             elif tag == "define-basic-event":
-                basic_expr[name] = _parse_expression(el, f"basic event {name!r}")
+                m.basic_events[name] = _parse_expression(el, f"basic event {name!r}")
             elif tag == "define-house-event":
                 kids = [c for c in el if _local(c.tag) not in _SKIP]
                 m.house_events[name] = bool(kids) and kids[0].get("value", "").strip().lower() == "true"
             elif tag == "define-parameter":
-                kind, v = _parse_expression(el, f"parameter {name!r}")
-                if kind != "value":
-                    raise MefError(f"parameter {name!r}: only float values are read")
-                m.parameters[name] = float(v)
+                m.parameters[name] = _parse_expression(el, f"parameter {name!r}")
             elif tag in _SKIP:
                 continue
             else:
                 raise MefError(f"unsupported element <{tag}>")
 
     visit(root)
-    for name, (kind, v) in basic_expr.items():
-        if kind == "parameter":
-            if v not in m.parameters:
-                raise MefError(f"basic event {name!r}: unknown parameter {v!r}")
-            v = m.parameters[v]
-        if not 0.0 <= float(v) <= 1.0:
-            raise MefError(f"basic event {name!r}: probability {v} outside [0, 1]")
-        m.basic_events[name] = float(v)
+    for name in m.basic_events:
+        try:
+            m.probability(name)
+        except MefError as e:
+            raise MefError(f"basic event {name!r}: {e}") from None
     # resolve untyped references and constants; check every reference
     consts = {}
 
@@ -302,9 +384,48 @@ def parse(source: Union[str, Path]) -> MefModel:
     return m
 
 
-def load(source: Union[str, Path], top: Optional[str] = None) -> FlatGraph:
-    """MEF document -> flattened graph of its top gate, root tallied."""
-    return parse(source).flat(top)
+def load(source: Union[str, Path], top: Optional[str] = None,
+         mission_time: float = DEFAULT_MISSION_TIME) -> FlatGraph:
+    """MEF document -> flattened graph of its top gate (probabilities at the
+    mission time), root tallied."""
+    return parse(source, mission_time).flat(top)
+
+
+def probability_over_time(model: MefModel, time_step: float, top: Optional[str] = None,
+                          mission_time: Optional[float] = None, words: int = 1 << 16, iteration: int = 1,
+                          device: int = 0):
+    """P(top) at t = 0, dt, 2 dt, ... and at the mission time (when it is not a
+    multiple of dt), as (probability, time) pairs -- the pairs the reference's
+    CalculateProbabilityOverTime returns (mcSCRAM src/mc/core/
+    probability_analysis.cc:280-311, left unimplemented there).  Every time
+    point is one instance of one batched launch over the same tree, with its
+    own thresholds and the same random numbers (the same counters), so for a
+    tree without negations the estimates never decrease in t."""
+    from .graph import probability_threshold
+    from .uncertainty import Batch
+
+    T = model.mission_time if mission_time is None else float(mission_time)
+    if time_step <= 0:
+        return []
+    times = []
+    k = 0
+    while k * time_step < T:
+        times.append(k * time_step)
+        k += 1
+    times.append(T)
+    pdag, root, var_index, _ = model.build(top)
+    g = pdag.flatten([root])
+    g.root = int(g.tally_nodes[0])
+    name_of = {idx: name for name, idx in var_index.items()}
+    thresholds = []
+    for t in times:
+        p = np.array([model.probability(name_of[int(x)], t) if int(x) in name_of else
+                      g.quantised_probabilities()[i] for i, x in enumerate(g.be_pdag_idx)])
+        thresholds.append(probability_threshold(p))
+    with Batch([g], device=device) as b:
+        ones = b.run([0] * len(times), thresholds, iteration=iteration, words_per_instance=words)
+    n = float(words) * 64.0
+    return [(float(o) / n, t) for o, t in zip(ones, times)]
 
 
 def main(argv=None) -> int:

@@ -94,8 +94,10 @@ def test_numbering_follows_first_encounter():
      "unknown basic-event"),
     ("<opsa-mef><define-gate name='t'><or><event name='x'/></or></define-gate>"
      "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown event"),
-    ("<opsa-mef><define-basic-event name='x'><exponential/></define-basic-event></opsa-mef>",
+    ("<opsa-mef><define-basic-event name='x'><lognormal-deviate/></define-basic-event></opsa-mef>",
      "unsupported expression"),
+    ("<opsa-mef><define-basic-event name='x'><exponential><float value='1'/></exponential>"
+     "</define-basic-event></opsa-mef>", "takes 2 arguments"),
     ("<opsa-mef><define-gate name='t'><or/></define-gate><define-gate name='t'><or/></define-gate></opsa-mef>",
      "defined twice"),
     ("<opsa-mef><define-gate name='t'><imply/></define-gate></opsa-mef>", "unsupported formula"),
@@ -171,3 +173,40 @@ def test_command_line_estimate_within_its_interval(gpu, capsys):
     assert out["samples"] == 2 ** 26
     half = (out["ci95"][1] - out["ci95"][0]) / 2
     assert abs(out["p_top"] - exact) <= 2.1 * half  # a 4-sigma band around the 95 % half-width
+
+
+TIMED = Path(__file__).parent / "golden" / "mef" / "timed.xml"
+
+
+def test_time_dependent_expressions():
+    import math
+    m = mef.parse(TIMED)
+    t = 1000.0
+    assert m.probability("pump", t) == pytest.approx(1 - math.exp(-1e-4 * t), rel=1e-15)
+    r = 3e-4 + 1e-2
+    assert m.probability("valve", t) == pytest.approx((3e-4 - (3e-4 - 0.01 * r) * math.exp(-r * t)) / r, rel=1e-15)
+    assert m.probability("sensor2", t) == pytest.approx(1 - math.exp(-4e-4 * t), rel=1e-15)
+    assert m.probability("sensor3", 50.0) == 0.0
+    assert m.probability("sensor3", t) == pytest.approx(1 - math.exp(-((t - 100) / 5000) ** 1.5), rel=1e-15)
+    assert m.probability("demand", t) == 1e-3
+    assert m.probability("pump") == pytest.approx(1 - math.exp(-1e-4 * 8760), rel=1e-15)  # default mission time
+    g = mef.load(TIMED, mission_time=t)
+    assert g.n_be == 6 and g.n_gates == 3
+
+
+@pytest.mark.gpu
+def test_probability_over_time_matches_oracle_per_time_point(oracle_mod, gpu):
+    from mcscram_b200.graph import probability_threshold
+    m = mef.parse(TIMED, mission_time=2000.0)
+    W = 4096
+    out = mef.probability_over_time(m, time_step=450.0, words=W, iteration=3)
+    assert [t for _, t in out] == [0.0, 450.0, 900.0, 1350.0, 1800.0, 2000.0]
+    pdag, root, var_index, _ = m.build()
+    g = pdag.flatten([root])
+    name_of = {idx: name for name, idx in var_index.items()}
+    for p_hat, t in out:
+        thr = probability_threshold(np.array([m.probability(name_of[int(x)], t) for x in g.be_pdag_idx]))
+        ones = oracle_mod.tallies(g.with_thresholds(thr), 3, 1, 0, W)[0]
+        assert p_hat == ones / (W * 64.0), t  # the same counters as a plain pass at that time's thresholds
+    ps = [p for p, _ in out]
+    assert all(b >= a for a, b in zip(ps, ps[1:]))  # same random numbers, rising probabilities: never decreasing

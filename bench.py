@@ -71,13 +71,13 @@ def parse_args():
     ap.add_argument("--is-batch-words", type=int, default=1 << 20)
     ap.add_argument("--plain-words", type=int, default=1 << 23, help="words of the plain-MC rate measurement")
     ap.add_argument("--bis-trees", type=int, default=1024)
-    ap.add_argument("--bis-ce-rounds", type=int, default=5)
+    ap.add_argument("--bis-ce-rounds", type=int, default=0, help="CE rounds (0 = the driver's default)")
     ap.add_argument("--bis-ce-words", type=int, default=1 << 13, help="words per tree per CE round")
     ap.add_argument("--bis-est-words", type=int, default=1 << 12, help="words per tree of the first estimate round")
     ap.add_argument("--bis-train-steps", type=int, default=150)
     ap.add_argument("--bis-plain-trees", type=int, default=64, help="trees of the plain-rate measurement")
     ap.add_argument("--bis-mode-cap", type=float, default=0.5, help="cap of the defensive mode proposals")
-    ap.add_argument("--bis-defensive", default="modes", choices=["modes", "approx", "probe"],
+    ap.add_argument("--bis-defensive", default="auto", choices=["auto", "cutsets", "modes", "approx", "probe"],
                     help="defensive proposal of the mixture (ablation)")
     ap.add_argument("--bis-defensive-share", type=float, default=0.3)
     ap.add_argument("--bis-no-network", action="store_true", help="CE targets as the proposal (ablation)")
@@ -389,7 +389,7 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = batched_learned_is(trees, target_rel_err=0.05, device=local, ce_rounds=args.bis_ce_rounds,
+    res = batched_learned_is(trees, target_rel_err=0.05, device=local, ce_rounds=args.bis_ce_rounds or None,
                              ce_words=args.bis_ce_words, est_words=args.bis_est_words,
                              train_steps=args.bis_train_steps, mode_cap=args.bis_mode_cap, workers=workers,
                              defensive_proposal=args.bis_defensive, defensive=args.bis_defensive_share,
@@ -429,7 +429,8 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
                                    "log-uniform [50, 10000], AND-/ATLEAST-heavy, exact P_top log-uniform "
                                    "[1e-10, 1e-5]), one shared 16-64-64-1 proposal network, until 5% rel err "
                                    "(95%) per tree or plain fallback",
-                       "ce_rounds": args.bis_ce_rounds, "ce_samples_per_tree": args.bis_ce_words * 64,
+                       "ce_rounds": sum(1 for r in res.rounds if r["phase"] == "ce"),
+                       "ce_samples_per_tree": args.bis_ce_words * 64,
                        "defensive": args.bis_defensive, "defensive_share": args.bis_defensive_share,
                        "network": not args.bis_no_network, "importance_features": not args.bis_no_importance_features,
                        "events": int(nb.sum()), "gates": int(sum(g.n_gates for g in trees))},

@@ -390,6 +390,10 @@ mcg_status staged_chunk(mcg_engine *e, uint64_t k, uint32_t iteration, uint64_t 
         ++e->launches;
         if (p1) MCG_CUDA(cudaEventRecord(p1, e->s_a));
     }
+    if (e->sample_hook) {
+        const mcg_status st = e->sample_hook(e->s_a, buf, W, word_begin);
+        if (st != MCG_OK) return st;
+    }
     MCG_CUDA(cudaEventRecord(e->ev_a[set], e->s_a));
     MCG_CUDA(cudaStreamWaitEvent(e->s_b, e->ev_a[set], 0));
     const uint64_t words_per_block = (uint64_t)kStageGateThreads * kStageWordsPerThread;

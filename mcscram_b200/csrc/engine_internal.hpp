@@ -64,6 +64,9 @@ struct mcg_engine {
     const uint4 *d_be_sample = nullptr;  // basic-event table the sampler phase reads (d_be unless overridden)
     // optional work queued on the gate stream after each chunk's gate phase
     std::function<mcg_status(cudaStream_t, const uint64_t *, uint64_t)> chunk_hook;
+    // optional work queued on the sampler stream after a chunk's basic-event
+    // words are written and before its gates read them (buffer, W, word_begin)
+    std::function<mcg_status(cudaStream_t, uint64_t *, uint64_t, uint64_t)> sample_hook;
     uint32_t sampler_smem = 0;          // dynamic smem that caps sampler blocks per SM
     uint64_t stage_words = 0;           // words per chunk the stage buffers hold
     cudaStream_t s_a = nullptr, s_b = nullptr;

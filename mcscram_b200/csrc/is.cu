@@ -134,6 +134,169 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights(const uint64_t *_
 // b, acc[0][b] later its weight.
 constexpr int kMaxComponents = 8;
 
+// ---------------------------------------------------------------------------
+// Cut-set component: importance sampling of a union of rare events over the
+// minimal cut sets of a tree (the "at least one event" mixture of Owen,
+// Maximov & Chertkov).  For a tree of AND / OR / ATLEAST / pass-through
+// gates without shared nodes, S(node) is the sum over its minimal cut sets
+// of the product of their events' probabilities (event: p; AND: product;
+// OR: sum; ATLEAST k: k-th elementary symmetric sum of the children's S).
+// A sample picks a cut set C with probability prod_{i in C} p_i / S(top) by
+// descending from the top (OR: one child with probability S(child)/S(OR);
+// AND: every child; ATLEAST: a k-subset with probability proportional to the
+// product of its members' S), forces C's events to fail and draws the other
+// events at their nominal probabilities.  Its density is
+//     q(x) = p(x) N(x) / S(top),
+// N(x) = the number of minimal cut sets contained in x (event: x_i; AND:
+// product; OR: sum; ATLEAST: k-th elementary symmetric sum of the children's
+// counts), so log(p/q) = log S(top) - log N(x); N(x) >= 1 wherever the top
+// event fires, which bounds the weight of this component by S(top) / pi.
+constexpr int kCutStack = 256;     // descent stack of one sample (node ids)
+constexpr int kCountDepth = 32;    // frames of the N(x) evaluation
+constexpr int kCutMaxK = 8;        // ATLEAST thresholds the count frames hold
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {  // the SplitMix64 finaliser
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Uniform in [0, 1) number `draw` of the stream `base`.
+__device__ __forceinline__ double cut_uniform(uint64_t base, uint32_t draw) {
+    return (double)(mix64(base + (uint64_t)draw * 0x9E3779B97F4A7C15ull) >> 11) * 0x1.0p-53;
+}
+
+struct CutArgs {
+    uint64_t *buf;
+    uint64_t W, word_begin;
+    uint32_t n_inst, n_be;
+    const uint32_t *root_row;      // per tree
+    const uint4 *gate;             // per gate: op | k << 8, in_begin, in_count, table offset
+    const uint32_t *inputs;
+    const double *S;               // per node
+    const double *tab;             // OR: cumulative S(child) / S(OR); ATLEAST: E[j][r] = e_r(S_j..S_n-1)
+    uint64_t seed;
+    unsigned int *error;
+};
+
+// One thread per (tree, word, sample): descends from the tree's top and ORs
+// the sample's bit into the words of the chosen cut set's events.
+__global__ void __launch_bounds__(256) k_cut_force(CutArgs a) {
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)a.n_inst * a.W * 64) return;
+    const uint32_t b = (uint32_t)(item & 63u);
+    const uint64_t wi = item >> 6;
+    const uint64_t w = wi % a.W;
+    const uint32_t k = (uint32_t)(wi / a.W);
+    uint64_t base = mix64(a.seed ^ ((uint64_t)k << 32));
+    base = mix64(base ^ (a.word_begin + w));
+    base = mix64(base ^ (uint64_t)b);
+    uint32_t draw = 0;
+    const unsigned long long bit = 1ull << b;
+    uint32_t stack[kCutStack];
+    int sp = 0;
+    stack[sp++] = a.root_row[k];
+    while (sp) {
+        const uint32_t node = stack[--sp];
+        if (node < a.n_be) {
+            atomicOr(reinterpret_cast<unsigned long long *>(a.buf + (uint64_t)node * a.W + w), bit);
+            continue;
+        }
+        const uint4 g = a.gate[node - a.n_be];
+        const uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu, n = g.z;
+        const uint32_t *in = a.inputs + g.y;
+        const double *tab = a.tab + g.w;
+        if (op == MCG_OR) {
+            const double u = cut_uniform(base, ++draw);
+            uint32_t j = 0;
+            while (j + 1 < n && u >= tab[j]) ++j;
+            if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
+            stack[sp++] = in[j];
+        } else if (op == MCG_ATLEAST) {
+            uint32_t r = kk;
+            for (uint32_t j = 0; j < n && r > 0; ++j) {
+                bool take = n - j == r;
+                if (!take) {  // P(take j | r still to take) = S_j E[j+1][r-1] / E[j][r]
+                    const double e0 = tab[(uint64_t)j * (kk + 1) + r], e1 = tab[(uint64_t)(j + 1) * (kk + 1) + r - 1];
+                    take = cut_uniform(base, ++draw) * e0 < a.S[in[j]] * e1;
+                }
+                if (take) {
+                    if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
+                    stack[sp++] = in[j];
+                    --r;
+                }
+            }
+        } else {  // AND and pass-through gates: every input
+            for (uint32_t j = 0; j < n; ++j) {
+                if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
+                stack[sp++] = in[j];
+            }
+        }
+    }
+}
+
+inline uint64_t mix64_host(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+struct CountFrame {
+    uint32_t node, j;
+    double acc;
+    double dp[kCutMaxK + 1];
+};
+
+__device__ __forceinline__ void count_deliver(CountFrame &f, uint32_t op, uint32_t kk, double v) {
+    if (op == MCG_AND) {
+        f.acc *= v;
+    } else if (op == MCG_ATLEAST) {
+        for (int r = (int)kk; r >= 1; --r) f.dp[r] += f.dp[r - 1] * v;
+    } else {
+        f.acc += v;
+    }
+}
+
+__device__ __forceinline__ void count_init(CountFrame &f, uint32_t node, uint32_t op) {
+    f.node = node;
+    f.j = 0;
+    f.acc = op == MCG_AND ? 1.0 : 0.0;
+    f.dp[0] = 1.0;
+#pragma unroll
+    for (int r = 1; r <= kCutMaxK; ++r) f.dp[r] = 0.0;
+}
+
+// N(x) of sample b of the word whose rows start at col (row stride W), for
+// the tree rooted at the fired gate `root`; only fired children are visited.
+// Returns -1 when the tree is deeper than the frames hold.
+__device__ double cut_count(const uint64_t *col, uint64_t W, uint32_t root, int b, const uint4 *gate,
+                            const uint32_t *inputs, uint32_t n_be) {
+    CountFrame st[kCountDepth];
+    int sp = 1;
+    count_init(st[0], root, gate[root - n_be].x & 0xFFu);
+    for (;;) {
+        CountFrame &f = st[sp - 1];
+        const uint4 g = gate[f.node - n_be];
+        const uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu;
+        if (f.j < g.z) {
+            const uint32_t x = inputs[g.y + f.j++];
+            const bool fired = (col[(uint64_t)x * W] >> b) & 1ull;
+            if (!fired || x < n_be) {
+                count_deliver(f, op, kk, fired ? 1.0 : 0.0);
+                continue;
+            }
+            if (sp == kCountDepth) return -1.0;
+            count_init(st[sp], x, gate[x - n_be].x & 0xFFu);
+            ++sp;
+            continue;
+        }
+        const double v = op == MCG_ATLEAST ? f.dp[kk] : f.acc;
+        if (--sp == 0) return v;
+        const uint32_t pop = gate[st[sp - 1].node - n_be].x;
+        count_deliver(st[sp - 1], pop & 0xFFu, (pop >> 8) & 0xFFu, v);
+    }
+}
+
 struct IsBatchArgs {
     const uint64_t *buf;
     uint64_t W;
@@ -146,6 +309,12 @@ struct IsBatchArgs {
     const double *a;               // [n_comp][n_be]
     const double *C;               // [n_comp][n_inst]
     double log_pi[kMaxComponents];
+    int cut_comp;                  // component drawn by cut sets (its log(p/q) is log S - log N(x)), or -1
+    const double *cut_logS;        // per tree: log S(top)
+    const uint4 *cut_gate;         // per gate (see CutArgs)
+    const uint32_t *inputs;
+    uint32_t n_be_nodes;           // basic events of the joined graph (node ids below are events)
+    unsigned int *error;
     double *sums;                  // per tree: sum w, sum w^2, hits, max log w
     double *ce;                    // per event, or null
     unsigned long long *queue;
@@ -196,12 +365,19 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
         double lsum = 0.0, lsum2 = 0.0, lhits = 0.0, lmax = -INFINITY;
         for (uint64_t m = top; m; m &= m - 1) {
             const int b = __ffsll((long long)m) - 1;
-            double lw = p.C[k] + acc[0][b];
+            double lw_cut = 0.0;
+            if (p.cut_comp >= 0) {
+                const double n_cut = cut_count(col, p.W, p.root_row[k], b, p.cut_gate, p.inputs, p.n_be_nodes);
+                if (!(n_cut >= 1.0)) atomicOr(p.error, 2u);  // too deep, or a failure without a cut set
+                lw_cut = p.cut_logS[k] - log(fmax(n_cut, 1.0));
+            }
+            double lw = p.cut_comp == 0 ? lw_cut : p.C[k] + acc[0][b];
             if (nc > 1) {
                 // -logsumexp_c(ln pi_c - log(p/q_c))
                 double u[kMaxComponents], hi = -INFINITY;
                 for (uint32_t c = 0; c < nc; ++c) {
-                    u[c] = p.log_pi[c] - (p.C[(uint64_t)c * p.n_inst + k] + acc[c][b]);
+                    const double lwc = (int)c == p.cut_comp ? lw_cut : p.C[(uint64_t)c * p.n_inst + k] + acc[c][b];
+                    u[c] = p.log_pi[c] - lwc;
                     hi = fmax(hi, u[c]);
                 }
                 double s = 0.0;
@@ -418,6 +594,11 @@ struct mcg_is_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<uint4> beq;
     std::vector<double> a, C, init;
+    // cut-set component (built on first use)
+    bool cut_ready = false;
+    uint4 *d_cut_gate = nullptr;
+    double *d_cut_S = nullptr, *d_cut_tab = nullptr, *d_cut_logS = nullptr;
+    unsigned int *d_cut_error = nullptr;
 };
 
 namespace {
@@ -437,6 +618,11 @@ void release_batch(mcg_is_batch *b) {
     cudaFree(b->d_be_begin);
     cudaFree(b->d_root);
     cudaFree(b->d_queue);
+    cudaFree(b->d_cut_gate);
+    cudaFree(b->d_cut_S);
+    cudaFree(b->d_cut_tab);
+    cudaFree(b->d_cut_logS);
+    cudaFree(b->d_cut_error);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->engine) mcg_destroy(b->engine);
@@ -530,6 +716,83 @@ mcg_status mcg_is_batch_destroy(mcg_is_batch *b) {
 
 namespace {
 
+// Tables of the cut-set component (see k_cut_force): every gate AND, OR,
+// ATLEAST (k <= 8) or pass-through without complemented inputs, no node read
+// twice (minimal cut sets are then the descents), S(top) > 0 for every tree.
+mcg_status build_cut_tables(mcg_is_batch *b) {
+    const mcg::Graph &g = b->engine->graph;
+    const uint32_t nb = g.n_be, ng = g.n_gates, nn = g.n_nodes();
+    std::vector<uint32_t> fanout(nn, 0);
+    for (uint32_t x : g.inputs) ++fanout[x];
+    for (uint32_t i = 0; i < nn; ++i)
+        if (fanout[i] > 1)
+            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling needs trees: node " + std::to_string(i) +
+                                                  " is read by several gates");
+    std::vector<double> S(nn, 0.0), tab;
+    std::vector<uint4> gate(ng);
+    for (uint32_t i = 0; i < nb; ++i) {
+        const uint64_t t = g.be_threshold[i];
+        S[i] = t >= (1ull << 32) ? 1.0 : (double)t / 4294967296.0;
+    }
+    for (uint32_t j = 0; j < ng; ++j) {
+        const uint32_t op = g.gate_op[j], n = g.gate_in_count[j], k = g.gate_k[j] & 0xFFu;
+        const uint32_t *in = g.inputs.data() + g.gate_in_begin[j];
+        if (g.gate_neg_count[j] || !(op == MCG_AND || op == MCG_OR || op == MCG_ATLEAST || op == MCG_NULL))
+            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling needs AND/OR/ATLEAST gates without complemented "
+                                              "inputs; gate " + std::to_string(j) + " is not one");
+        if (op == MCG_ATLEAST && k > (uint32_t)kCutMaxK)
+            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: ATLEAST threshold above 8");
+        gate[j] = make_uint4(op | (k << 8), g.gate_in_begin[j], n, (uint32_t)tab.size());
+        double v = 0.0;
+        if (op == MCG_AND) {
+            v = 1.0;
+            for (uint32_t c = 0; c < n; ++c) v *= S[in[c]];
+        } else if (op == MCG_OR) {
+            for (uint32_t c = 0; c < n; ++c) v += S[in[c]];
+            double cum = 0.0;
+            for (uint32_t c = 0; c < n; ++c) {
+                cum += S[in[c]];
+                tab.push_back(v > 0 ? cum / v : 1.0);
+            }
+        } else if (op == MCG_ATLEAST) {
+            // E[j][r] = e_r(S_j, ..., S_{n-1}), j = n .. 0
+            std::vector<double> E((size_t)(n + 1) * (k + 1), 0.0);
+            E[(size_t)n * (k + 1)] = 1.0;
+            for (int c = (int)n - 1; c >= 0; --c) {
+                for (uint32_t r = 0; r <= k; ++r) {
+                    double e = E[(size_t)(c + 1) * (k + 1) + r];
+                    if (r > 0) e += S[in[c]] * E[(size_t)(c + 1) * (k + 1) + r - 1];
+                    E[(size_t)c * (k + 1) + r] = e;
+                }
+            }
+            v = E[k];
+            tab.insert(tab.end(), E.begin(), E.end());
+        } else {  // pass-through
+            v = n ? S[in[n - 1]] : 0.0;
+        }
+        S[nb + j] = v;
+    }
+    std::vector<double> logS(b->n_inst);
+    for (uint32_t t = 0; t < b->n_inst; ++t) {
+        const double st = S[g.tally_nodes[t]];
+        if (!(st > 0.0) || !std::isfinite(st))
+            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: tree " + std::to_string(t) + " has no cut set");
+        logS[t] = std::log(st);
+    }
+    if (tab.empty()) tab.push_back(0.0);
+    MCG_CUDA(cudaMalloc((void **)&b->d_cut_gate, std::max<uint32_t>(ng, 1) * sizeof(uint4)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_cut_S, nn * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_cut_tab, tab.size() * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_cut_logS, b->n_inst * sizeof(double)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_cut_error, sizeof(unsigned int)));
+    if (ng) MCG_CUDA(cudaMemcpy(b->d_cut_gate, gate.data(), ng * sizeof(uint4), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_cut_S, S.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_cut_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_cut_logS, logS.data(), b->n_inst * sizeof(double), cudaMemcpyHostToDevice));
+    b->cut_ready = true;
+    return MCG_OK;
+}
+
 // Device arrays for n_comp components, grown on demand.
 mcg_status ensure_components(mcg_is_batch *b, uint32_t n_comp) {
     if (n_comp <= b->n_comp_cap) return MCG_OK;
@@ -552,16 +815,19 @@ mcg_status ensure_components(mcg_is_batch *b, uint32_t n_comp) {
 extern "C" {
 
 mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_def, const uint64_t *q_def,
-                            const uint64_t *words_def, uint32_t iteration, uint64_t word_begin, uint64_t word_count,
-                            double *tree_sums, double *ce_num, double *kernel_ms) {
+                            const uint64_t *words_def, uint64_t words_cutset, uint32_t iteration, uint64_t word_begin,
+                            uint64_t word_count, double *tree_sums, double *ce_num, double *kernel_ms) {
     mcg::clear_error();
     if (!b || !q_thr || !tree_sums) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
     if (n_def + 1 > (uint32_t)kMaxComponents)
         return mcg::fail(MCG_ERR_INVALID, "at most " + std::to_string(kMaxComponents - 1) + " defensive proposals");
     if (n_def && (!q_def || !words_def)) return mcg::fail(MCG_ERR_INVALID, "n_defensive > 0 needs q_defensive and words");
-    uint64_t def_total = 0;
+    uint64_t def_total = words_cutset;
     for (uint32_t c = 0; c < n_def; ++c) def_total += words_def[c];
-    if (def_total > word_count) return mcg::fail(MCG_ERR_INVALID, "defensive words exceed word_count");
+    if (def_total > word_count) return mcg::fail(MCG_ERR_INVALID, "defensive and cut-set words exceed word_count");
+    if (words_cutset && n_def + 2 > (uint32_t)kMaxComponents)
+        return mcg::fail(MCG_ERR_INVALID, "at most " + std::to_string(kMaxComponents - 2) +
+                                              " defensive proposals next to the cut-set component");
     mcg_engine *e = b->engine;
     const mcg::Graph &g = e->graph;
     if (word_begin + word_count > (1ull << 32) || word_begin + word_count < word_begin)
@@ -583,6 +849,17 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
             comp_q.push_back(q_def + (uint64_t)c * nb);
             comp_words.push_back(words_def[c]);
         }
+    int cut_comp = -1;
+    if (words_cutset) {  // nominal thresholds plus a forced cut set per sample
+        if (!b->cut_ready) {
+            MCG_CUDA(cudaSetDevice(e->device));
+            const mcg_status cs = build_cut_tables(b);
+            if (cs != MCG_OK) return cs;
+        }
+        cut_comp = (int)comp_q.size();
+        comp_q.push_back(g.be_threshold.data());
+        comp_words.push_back(words_cutset);
+    }
     if (comp_q.empty()) comp_q.push_back(q_thr), comp_words.push_back(0);
     const uint32_t nc = (uint32_t)comp_q.size();
     MCG_CUDA(cudaSetDevice(e->device));
@@ -637,6 +914,13 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
     args.sums = b->d_sums;
     args.ce = ce_num ? b->d_ce : nullptr;
     args.queue = b->d_queue;
+    args.cut_comp = cut_comp;
+    args.cut_logS = b->d_cut_logS;
+    args.cut_gate = b->d_cut_gate;
+    args.inputs = e->d_inputs;
+    args.n_be_nodes = g.n_be;
+    args.error = b->d_cut_error;
+    if (cut_comp >= 0) MCG_CUDA(cudaMemsetAsync(b->d_cut_error, 0, sizeof(unsigned int), e->stream));
     e->chunk_hook = [=](cudaStream_t s, const uint64_t *buf, uint64_t W) -> mcg_status {
         IsBatchArgs p = args;
         p.buf = buf;
@@ -660,10 +944,35 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
         if (!comp_words[c]) continue;
         e->d_be_sample = b->d_be_q + c * nb;
         e->table_iteration = 0xFFFFFFFFu;  // the sampler table follows the component
+        if ((int)c == cut_comp) {
+            CutArgs ca{};
+            ca.n_inst = n_inst;
+            ca.n_be = g.n_be;
+            ca.root_row = b->d_root;
+            ca.gate = b->d_cut_gate;
+            ca.inputs = e->d_inputs;
+            ca.S = b->d_cut_S;
+            ca.tab = b->d_cut_tab;
+            ca.seed = mix64_host(((uint64_t)iteration << 32) ^ 0x5bd1e995u);
+            ca.error = b->d_cut_error;
+            e->sample_hook = [=](cudaStream_t s, uint64_t *buf, uint64_t W, uint64_t wb) -> mcg_status {
+                CutArgs x = ca;
+                x.buf = buf;
+                x.W = W;
+                x.word_begin = wb;
+                const uint64_t threads = (uint64_t)x.n_inst * W * 64;
+                k_cut_force<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(x);
+                const cudaError_t err = cudaGetLastError();
+                if (err != cudaSuccess) return mcg::fail(MCG_ERR_CUDA, std::string("k_cut_force: ") + cudaGetErrorString(err));
+                return MCG_OK;
+            };
+        }
         st = mcg::internal::run_staged(e, iteration, 1, word_begin + off, comp_words[c]);
+        e->sample_hook = nullptr;
         off += comp_words[c];
     }
     e->chunk_hook = nullptr;
+    e->sample_hook = nullptr;
     e->d_be_sample = nullptr;
     e->table_iteration = 0xFFFFFFFFu;
     if (st != MCG_OK) return st;
@@ -671,7 +980,14 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
     MCG_CUDA(cudaMemcpyAsync(tree_sums, b->d_sums, 4ull * n_inst * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     if (ce_num && nb)
         MCG_CUDA(cudaMemcpyAsync(ce_num, b->d_ce, nb * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    unsigned int cut_error = 0;
+    if (cut_comp >= 0)
+        MCG_CUDA(cudaMemcpyAsync(&cut_error, b->d_cut_error, sizeof(unsigned int), cudaMemcpyDeviceToHost, e->stream));
     MCG_CUDA(cudaStreamSynchronize(e->stream));
+    if (cut_error & 1u) return mcg::fail(MCG_ERR_STATE, "cut-set descent deeper than its stack (256 nodes)");
+    if (cut_error & 2u)
+        return mcg::fail(MCG_ERR_STATE, "cut-set count failed (tree deeper than 32 levels, or a failure without "
+                                        "a cut set)");
     if (kernel_ms) {
         float ms = 0.f;
         MCG_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));

@@ -56,8 +56,8 @@ _capi.register_signatures({
     "mcg_is_batch_create": (C.c_int, [C.POINTER(_capi.GraphDesc), C.c_uint32, C.POINTER(C.c_uint32),
                                       C.POINTER(_capi.RunDesc), C.POINTER(_vp)]),
     "mcg_is_batch_destroy": (C.c_int, [_vp]),
-    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, C.c_uint32, _u64p, _u64p, C.c_uint32, C.c_uint64, C.c_uint64, _dp,
-                                   _dp, _dp]),
+    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, C.c_uint32, _u64p, _u64p, C.c_uint64, C.c_uint32, C.c_uint64,
+                                   C.c_uint64, _dp, _dp, _dp]),
     "mcg_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_vp)]),
     "mcg_mlp_destroy": (C.c_int, [_vp]),
     "mcg_mlp_set_params": (C.c_int, [_vp, _fp]),
@@ -199,6 +199,17 @@ def _conditioned(pr, cache, nb, n_nodes, roots):
             cond[j] = p
             cond[j, r0] = 1.0
     return cond
+
+
+def cut_set_eligible(g: FlatGraph) -> bool:
+    """Whether the cut-set component (mcg_is_batch_run's words_cutset) takes
+    this graph: AND/OR/ATLEAST (k <= 8)/pass-through gates, no complemented
+    inputs, no node read twice."""
+    from .graph import NULL
+    ok_ops = np.isin(g.gate_op, [AND, OR, ATLEAST, NULL])
+    k_ok = np.where(g.gate_op == ATLEAST, (g.gate_k & 0xFF) <= 8, True)
+    return bool(np.all(ok_ops) and np.all(k_ok) and np.all(g.gate_neg_count == 0) and
+                np.all(np.bincount(g.inputs, minlength=g.n_nodes) <= 1))
 
 
 def mode_proposals(g: FlatGraph, n_comp: int, cap: float) -> np.ndarray:
@@ -571,11 +582,13 @@ class BatchedImportanceSampler:
         return _proposal_thr(self.union.be_threshold, q)
 
     def run(self, q_thresholds: np.ndarray, iteration: int = 1, word_begin: int = 0, word_count: int = 1 << 14,
-            ce: bool = False, q_defensive: Optional[np.ndarray] = None, words_defensive=0) -> dict:
+            ce: bool = False, q_defensive: Optional[np.ndarray] = None, words_defensive=0,
+            words_cutset: int = 0) -> dict:
         """Per-tree sums of one pass.  q_defensive ([n_be] or [n_comp, n_be]
         thresholds) with words_defensive (an int or one per component): the
         main proposal draws the first words, each defensive proposal the next
-        words_defensive[c], and samples carry the balance-heuristic weight."""
+        words_defensive[c], the cut-set component the last words_cutset, and
+        samples carry the balance-heuristic weight."""
         q_thresholds = np.ascontiguousarray(q_thresholds, dtype=np.uint64)
         nb = self.union.n_be
         if q_thresholds.shape != (nb,):
@@ -592,7 +605,7 @@ class BatchedImportanceSampler:
         ms = C.c_double()
         _capi.check(self.lib.mcg_is_batch_run(self.h, _p(q_thresholds, C.c_uint64), n_def,
                                               _p(qd, C.c_uint64) if n_def else None,
-                                              _p(wd, C.c_uint64) if n_def else None,
+                                              _p(wd, C.c_uint64) if n_def else None, int(words_cutset),
                                               iteration, word_begin, word_count, _p(sums, C.c_double),
                                               _p(ce_num, C.c_double) if ce else None, C.byref(ms)))
         out = {"sum_w": sums[:, 0].copy(), "sum_w2": sums[:, 1].copy(), "hits": sums[:, 2].astype(np.int64),
@@ -665,13 +678,14 @@ def _train_shared(mlp: "ProposalMLP", feats, targets, steps, lr, weights=None, g
 
 def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[ProposalMLP] = None, device: int = 0,
                        probe_words: int = 1 << 10, min_hits: int = 200, max_probe_rounds: int = 24,
-                       ce_rounds: int = 5, ce_words: int = 1 << 13, smoothing: float = 0.7, train_steps: int = 150,
+                       ce_rounds: Optional[int] = None, ce_words: int = 1 << 13, smoothing: float = 0.7,
+                       train_steps: int = 150,
                        lr: float = 3e-3, q_max: float = 0.5, est_words: int = 1 << 12, max_est_words: int = 1 << 22,
                        ess_floor: float = 50.0, collapse_ratio: float = 1e-3, plain_words: int = 1 << 16,
                        defensive: float = 0.3, chunk_words: int = 0, use_network: bool = True,
                        importance_features: bool = True, tree_weighting: bool = True, fallback_after: int = 2,
                        cap_levels=(0.75, 0.9, 0.97, 0.99), confirm_rounds: int = 1,
-                       defensive_proposal: str = "modes", n_modes: int = 4, min_words: int = 0,
+                       defensive_proposal: str = "auto", n_modes: int = 4, min_words: int = 0,
                        mode_cap: float = 0.5, workers: int = 0, prepared=None, log=None) -> BatchedIsResult:
     """Learned importance sampling for a batch of rare-event trees.
 
@@ -687,7 +701,11 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     a failure region the learned proposal under-samples is still reached
     through q_d's share, so the estimate stays unbiased with a bounded
     variance instead of silently missing that region.  q_d is, with
-    defensive_proposal="modes", a mixture of n_modes proposals each
+    defensive_proposal="cutsets" ("auto" picks it when every tree qualifies),
+    the cut-set component of mcg_is_batch_run
+    (each sample forces a minimal cut set drawn with probability prod p / S:
+    the mixture over all failure modes of the tree, which bounds every
+    weight by S / defensive; trees only), with "modes" a mixture of n_modes proposals each
     conditioned on one child of the top OR gate failing (mode_proposals;
     a product proposal cannot follow failure modes of very different order
     at once, a mixture over the top gate's children can), with "approx" the
@@ -696,7 +714,9 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     proposals to max(cap, mode_cap): a child's failure that needs all of
     its events is only reached often when they may come close to 1).  The
     first cross-entropy round samples q_d alone.
-    2. Cross-entropy rounds over all trees at once: per-event targets are the
+    2. Cross-entropy rounds over all trees at once (ce_rounds: 1 with the
+       cut-set component, whose samples already follow the failure region,
+       5 otherwise): per-event targets are the
        likelihood-weighted failure frequencies, smoothed with the current
        proposal; one network, whose 16th input is the tree's log10 s_k / 6,
        is fitted to the rows of all trees (each tree weighing the same in the
@@ -779,7 +799,18 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     feats[:, 15] = (np.log10(np.maximum(scale, 1.0)) / 6.0)[tree_of_event]
     mlp = mlp or (ProposalMLP(device=device) if use_network else None)
     cap_e = cap[tree_of_event]
-    if defensive_proposal == "modes":
+    if defensive_proposal == "auto":  # cut sets where every tree takes them, modes otherwise
+        defensive_proposal = "cutsets" if all(cut_set_eligible(g) for g in graphs) else "modes"
+    cut = defensive_proposal == "cutsets"
+    if ce_rounds is None:  # cut-set samples give near-ideal targets at once
+        ce_rounds = 1 if cut else 5
+    if cut:
+        bad = [k for k, g in enumerate(graphs) if not cut_set_eligible(g)]
+        if bad:
+            raise ValueError(f"cut-set sampling needs trees of AND/OR/ATLEAST gates without shared nodes or "
+                             f"negations; trees {bad[:5]} are not")
+        q_def = np.zeros((0, full.union.n_be))
+    elif defensive_proposal == "modes":
         q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
                         np.maximum(cap_e, mode_cap)[None, :])
     elif defensive_proposal == "approx":
@@ -788,23 +819,31 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     elif defensive_proposal == "probe":
         q_def = np.minimum(p * scale[tree_of_event], cap_e)[None, :]
     else:
-        raise ValueError("defensive_proposal must be 'modes', 'approx' or 'probe'")
+        raise ValueError("defensive_proposal must be 'cutsets', 'modes', 'approx' or 'probe'")
     n_comp = q_def.shape[0]
 
     def def_words(w):  # words per defensive component
-        return max(1, int(round(defensive * w / n_comp))) if defensive > 0 else 0
+        return max(1, int(round(defensive * w / n_comp))) if defensive > 0 and n_comp else 0
+
+    def cut_words(w):  # words of the cut-set component
+        return max(1, int(round(defensive * w))) if cut and defensive > 0 else 0
     row_w = (1.0 / np.diff(bb).astype(np.float64))[tree_of_event].astype(np.float32) if tree_weighting else None
-    thr_def = np.stack([full.proposal_thresholds(qc) for qc in q_def])
+    thr_def = np.stack([full.proposal_thresholds(qc) for qc in q_def]) if n_comp else None
     q = None
     t0 = time.perf_counter()
     for r in range(ce_rounds):
-        if q is None:  # first round: the defensive mixture alone
+        if q is None and cut:  # first round: cut-set samples alone
+            res = full.run(full.union.be_threshold, iteration=it, word_count=ce_words, ce=True,
+                           words_cutset=ce_words)
+            q = np.minimum(p * scale[tree_of_event], cap_e)
+        elif q is None:  # first round: the defensive mixture alone
             res = full.run(thr_def[0], iteration=it, word_count=ce_words, ce=True, q_defensive=thr_def,
                            words_defensive=[ce_words // n_comp + (c < ce_words % n_comp) for c in range(n_comp)])
             q = q_def.mean(axis=0)
         else:
             res = full.run(full.proposal_thresholds(q), iteration=it, word_count=ce_words, ce=True,
-                           q_defensive=thr_def if defensive > 0 else None, words_defensive=def_words(ce_words))
+                           q_defensive=thr_def if def_words(ce_words) else None, words_defensive=def_words(ce_words),
+                           words_cutset=cut_words(ce_words))
         it += 1
         gpu["ce"] += res["kernel_ms"]
         sw = res["sum_w"][tree_of_event]
@@ -851,8 +890,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         qd = np.concatenate([q_def[:, sl[k]] if not fallback[k] else np.repeat(p[sl[k]][None, :], n_comp, axis=0)
                              for k in members], axis=1)
         res = sampler.run(sampler.proposal_thresholds(qa), iteration=it, word_begin=0, word_count=words,
-                          q_defensive=np.stack([sampler.proposal_thresholds(qc) for qc in qd]) if defensive > 0
-                          else None, words_defensive=def_words(words))
+                          q_defensive=np.stack([sampler.proposal_thresholds(qc) for qc in qd]) if def_words(words)
+                          else None, words_defensive=def_words(words), words_cutset=cut_words(words))
         it += 1
         gpu["estimate"] += res["kernel_ms"]
         used += words

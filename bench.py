@@ -67,6 +67,9 @@ def parse_args():
     ap.add_argument("--converge-mode", default="fused", choices=["fused", "staged", "strip"],
                     help="engine mode of the convergence loop (short passes favour the fused kernel)")
     ap.add_argument("--is-rounds", type=int, default=5)
+    ap.add_argument("--is-pipeline", default="batched", choices=["single", "batched"],
+                    help="single: CE rounds + estimate on the one-tree sampler; batched: the batched pipeline "
+                         "(cut-set defensive component, one CE round) on a batch of this one tree")
     ap.add_argument("--is-round-words", type=int, default=1 << 20, help="words per CE round (2^26 samples)")
     ap.add_argument("--is-batch-words", type=int, default=1 << 20)
     ap.add_argument("--plain-words", type=int, default=1 << 23, help="words of the plain-MC rate measurement")
@@ -307,14 +310,29 @@ def run_is(args, rank: int, world: int, local: int) -> int:
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
-    with ImportanceSampler(g, device=local) as s:
-        q, mlp, hist = cross_entropy(g, rounds=args.is_rounds, words_per_round=args.is_round_words, sampler=s,
-                                     device=local)
-        res = estimate(s, q, target_rel_err=0.05, words_per_batch=args.is_batch_words)
-    torch.cuda.synchronize()
-    is_wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    mlp.close()
+    if args.is_pipeline == "batched":
+        from mcscram_b200.importance import batched_learned_is
+        br = batched_learned_is([g], target_rel_err=0.05, device=local)
+        torch.cuda.synchronize()
+        is_wall = time.perf_counter() - t0
+        clk = clocks.stop()
+        res = {"estimate": float(br.estimate[0]), "rel_err95": float(br.rel_err95[0]), "samples": int(br.samples[0]),
+               "hits": int(br.hits[0]), "ess": float(br.ess[0]), "fallback": bool(br.fallback[0]),
+               "gpu_ms": sum(br.gpu_ms.values())}
+
+        class _H:
+            gpu_ms = 0.0
+            rounds = [r for r in br.rounds if r["phase"] == "ce"]
+        hist = _H()
+    else:
+        with ImportanceSampler(g, device=local) as s:
+            q, mlp, hist = cross_entropy(g, rounds=args.is_rounds, words_per_round=args.is_round_words, sampler=s,
+                                         device=local)
+            res = estimate(s, q, target_rel_err=0.05, words_per_batch=args.is_batch_words)
+        torch.cuda.synchronize()
+        is_wall = time.perf_counter() - t0
+        clk = clocks.stop()
+        mlp.close()
     p_hat = res["estimate"]
     n_req = 1.959963984540054 ** 2 * (1 - p_hat) / (p_hat * 0.05 ** 2) if p_hat > 0 else float("inf")
     plain_s = n_req / plain_rate
@@ -323,7 +341,10 @@ def run_is(args, rank: int, world: int, local: int) -> int:
         "higher_is_better": False, "vs_baseline": None, "dtype": "u64 sampling, fp64 weights, bf16/fp32 MLP",
         "data": "synthetic", "steps": 1, "warmup": args.warmup,
         "config": {"workload": "2,000-event / 1,200-gate rare-event tree (seed 49), learned IS (CE rounds "
-                               f"{args.is_rounds} x {args.is_round_words * 64} samples) vs plain MC"},
+                               f"{args.is_rounds} x {args.is_round_words * 64} samples) vs plain MC"
+                               if args.is_pipeline == "single" else
+                               "2,000-event / 1,200-gate rare-event tree (seed 49), batched learned IS pipeline on "
+                               "this one tree (cut-set defensive component, one CE round) vs plain MC"},
         "is": {"estimate": p_hat, "rel_err95": res["rel_err95"], "samples": res["samples"], "hits": res["hits"],
                "ess": res["ess"], "fallback": res["fallback"], "wall_s": is_wall,
                "gpu_s": (hist.gpu_ms + res["gpu_ms"]) * 1e-3, "ce_rounds": hist.rounds},

@@ -1,20 +1,47 @@
-"""Open-PSA MEF fault trees -> the engine's PDAG.
+"""Open-PSA MEF models -> the engine's PDAG.
 
 Reads the subset of the Model Exchange Format that fault-tree models such as
-the Aralia set use: ``define-fault-tree`` / ``model-data`` holding
-``define-gate`` (formulas ``and``, ``or``, ``not``, ``xor``, ``nand``,
-``nor``, ``atleast min=k``, or a single event reference, nested formulas
-allowed), ``define-basic-event`` and ``define-parameter`` with an
-expression, ``define-house-event`` (``constant value="true|false"``).
-Expressions: ``float``, ``int``, ``parameter``, ``system-mission-time``,
-``exponential`` (1 - exp(-lambda t)), ``GLM`` and ``Weibull`` (the
-formulas of mcSCRAM src/expression/exponential.cc:37-38, 87-91, 108-111),
-``add``, ``sub``, ``mul``, ``div``, ``neg``.  Event references are ``gate``,
-``basic-event``, ``house-event`` or the untyped ``event``.  Other
-expressions (random deviates, CCF groups, substitutions) are rejected with
-an error naming the element.  Probabilities are taken at a mission time
-(8760 hours unless given); ``probability_over_time`` evaluates the top
-event on a grid of mission times in one batched GPU pass.
+the Aralia set and event-tree models use.
+
+Fault trees: ``define-fault-tree`` / ``define-component`` / ``model-data``
+holding ``define-gate`` (formulas ``and``, ``or``, ``not``, ``xor``,
+``nand``, ``nor``, ``atleast min=k``, ``cardinality min max``, ``imply``,
+``iff``, or a single event reference, nested formulas allowed),
+``define-basic-event`` and ``define-parameter`` with an expression,
+``define-house-event`` (``constant value="true|false"``).  Expressions:
+``float``, ``int``, ``bool``, ``pi``, ``parameter``,
+``system-mission-time``, ``exponential`` (1 - exp(-lambda t)), ``GLM`` and
+``Weibull`` (the formulas of mcSCRAM src/expression/exponential.cc:37-38,
+87-91, 108-111), ``add``, ``sub``, ``mul``, ``div``, ``neg``, and the
+boolean ``not``, ``and``, ``or``, ``eq``, ``df``, ``lt``, ``gt``, ``leq``,
+``geq``, ``ite``.  Event references are ``gate``, ``basic-event``,
+``house-event`` or the untyped ``event``.  Other expressions (random
+deviates, CCF groups, substitutions) are rejected with an error naming the
+element.  Probabilities are taken at a mission time (8760 hours unless
+given); ``probability_over_time`` evaluates the top event on a grid of
+mission times in one batched GPU pass.
+
+Event trees (read here, analysed by ``mcscram_b200.eta``):
+``define-initiating-event``, ``define-event-tree`` (functional events,
+sequences, named branches, the initial state with ``fork`` / ``path``
+targets), ``define-rule`` and ``define-alignment`` / ``define-phase``; the
+instructions ``collect-formula``, ``collect-expression``,
+``set-house-event``, ``if`` (with ``test-initiating-event`` and
+``test-functional-event`` conditions), ``block``, ``rule`` and the
+end-state link ``event-tree``.  The checks of the reference's initializer
+are restated (src/initializer.cc:1628-1791): undefined and doubly defined
+elements, cycles of gates, rules, branches and links, the order of
+functional events along fork paths, links only in sequences, and no
+collect-expression mixed with collect-formula on one tree.
+
+Scoping follows the MEF rules of the reference's initializer
+(src/initializer.cc:1400-1466, 736-775): an element defined inside a
+``define-fault-tree`` / ``define-component`` has the container's path as its
+base path and the container's role unless it names its own; a public element
+is known by its name, a private one only by its full path
+(``Tree.Component.name``); a reference is looked up in the referring
+element's own scope first (base path + "." + reference), then among the
+public names (a reference without a dot) or the full paths (with a dot).
 
 Node numbering follows the reference's PDAG construction from a MEF gate
 (mcSCRAM src/pdag.cc:470-548): basic events get indices 2, 3, ... in the
@@ -22,12 +49,15 @@ order a depth-first walk of the top formula first meets them
 (``GatherVariables``), then gates get the next indices in pre-order as they
 are built (``ConstructGate``).  ``not`` of a single event inside a formula
 becomes a complemented argument; other nested formulas become gates of their
-own.  House events become variables with probability 0 or 1 (constant
-words).  SCRAM's preprocessing passes are not applied, so event indices can
-differ from the reference's for models the preprocessor rewrites.
+own.  ``imply``, ``iff`` and ``cardinality`` become the gates the
+reference's ``ConstructComplexGate`` builds (src/pdag.cc:660-716).  House
+events become variables with probability 0 or 1 (constant words).  SCRAM's
+preprocessing passes are not applied, so event indices can differ from the
+reference's for models the preprocessor rewrites.
 """
 from __future__ import annotations
 
+import copy
 import math
 import xml.etree.ElementTree as ET
 from dataclasses import dataclass, field
@@ -39,8 +69,11 @@ import numpy as np
 from .graph import AND, ATLEAST, NAND, NOR, NOT, NULL, OR, XOR, FlatGraph
 
 _CONNECTIVES = {"and": AND, "or": OR, "atleast": ATLEAST, "xor": XOR, "not": NOT, "nand": NAND, "nor": NOR}
+_COMPLEX = ("imply", "iff", "cardinality")
 _REFS = ("gate", "basic-event", "house-event", "event")
 _SKIP = ("label", "attributes")
+_TABLES = ("gate", "basic-event", "house-event", "parameter")
+_EVENTS = ("gate", "basic-event", "house-event")
 
 
 class MefError(ValueError):
@@ -53,11 +86,18 @@ DEFAULT_MISSION_TIME = 8760.0  # hours: SCRAM's default analysis setting
 @dataclass
 class Expr:
     """An expression tree: op "value" (args: [float]), "parameter" (args:
-    [name]), "time", or a function of its argument expressions."""
+    [id]), "time", "test-initiating-event" (args: [name]),
+    "test-functional-event" (args: [name, state]), or a function of its
+    argument expressions."""
     op: str
     args: list
 
-    def value(self, t: float, params: Dict[str, "Expr"], _depth: int = 0) -> float:
+    def value(self, t: float, params: Dict[str, "Expr"], context: Optional[dict] = None,
+              _depth: int = 0) -> float:
+        """Value at mission time t.  `context` ({"initiating_event": name,
+        "functional_events": {name: state}}) answers the test events, as the
+        reference's mef::Context does during an event-tree walk; without one
+        they are false."""
         if _depth > 64:
             raise MefError("parameters refer to each other in a cycle")
         op, a = self.op, self.args
@@ -68,8 +108,15 @@ class Expr:
         if op == "parameter":
             if a[0] not in params:
                 raise MefError(f"unknown parameter {a[0]!r}")
-            return params[a[0]].value(t, params, _depth + 1)
-        v = [x.value(t, params, _depth + 1) for x in a]
+            return params[a[0]].value(t, params, context, _depth + 1)
+        if op == "test-initiating-event":
+            return float(bool(context) and context.get("initiating_event") == a[0])
+        if op == "test-functional-event":
+            return float(bool(context) and context.get("functional_events", {}).get(a[0]) == a[1])
+        if op == "ite":
+            branch = a[1] if a[0].value(t, params, context, _depth + 1) else a[2]
+            return branch.value(t, params, context, _depth + 1)
+        v = [x.value(t, params, context, _depth + 1) for x in a]
         if op == "exponential":  # 1 - exp(-lambda t)
             return 1.0 - math.exp(-v[0] * v[1])
         if op == "GLM":  # gamma, lambda, mu, t
@@ -92,6 +139,14 @@ class Expr:
             return out
         if op == "neg":
             return -v[0]
+        if op == "not":
+            return float(not v[0])
+        if op == "and":
+            return float(all(v))
+        if op == "or":
+            return float(any(v))
+        if op in _COMPARE:
+            return float(_COMPARE[op](v[0], v[1]))
         raise MefError(f"unknown expression {op!r}")
 
     def depends_on_time(self, params: Dict[str, "Expr"], _depth: int = 0) -> bool:
@@ -101,17 +156,61 @@ class Expr:
             return True
         if self.op == "parameter":
             return self.args[0] in params and params[self.args[0]].depends_on_time(params, _depth + 1)
-        return self.op not in ("value",) and any(x.depends_on_time(params, _depth + 1) for x in self.args)
+        if self.op in ("value", "test-initiating-event", "test-functional-event"):
+            return False
+        return any(x.depends_on_time(params, _depth + 1) for x in self.args)
+
+
+_COMPARE = {"eq": lambda x, y: x == y, "df": lambda x, y: x != y, "lt": lambda x, y: x < y,
+            "gt": lambda x, y: x > y, "leq": lambda x, y: x <= y, "geq": lambda x, y: x >= y}
 
 
 @dataclass
 class Formula:
     """A connective over arguments; an argument is (complement, kind, payload)
-    with kind "gate" / "basic-event" / "house-event" (payload: name) or
-    "formula" (payload: a nested Formula)."""
+    with kind "gate" / "basic-event" / "house-event" (payload: the element's
+    id) or "formula" (payload: a nested Formula)."""
     connective: int
     args: List[Tuple[bool, str, object]]
     min_number: int = 0
+
+
+# --- event trees (mcSCRAM src/event_tree.h, src/instruction.h) -------------
+#
+# An instruction is a tuple: ("collect-formula", Formula),
+# ("collect-expression", Expr), ("set-house-event", house id, state),
+# ("if", Expr, then, else or None), ("block", [instructions]),
+# ("rule", name), ("link", event-tree name).
+
+
+@dataclass
+class Branch:
+    """Instructions followed by one target: ("fork", Fork), ("sequence",
+    name) or ("branch", name of a branch of the same event tree)."""
+    instructions: list
+    target: Tuple[str, object]
+
+
+@dataclass
+class Fork:
+    functional_event: str
+    paths: List[Tuple[str, Branch]]  # (state, branch)
+
+
+@dataclass
+class EventTree:
+    name: str
+    functional_events: List[str] = field(default_factory=list)  # definition order = fork order
+    sequences: List[str] = field(default_factory=list)
+    branches: Dict[str, Branch] = field(default_factory=dict)
+    initial_state: Optional[Branch] = None
+
+
+@dataclass
+class Phase:
+    name: str
+    time_fraction: float
+    house_events: List[Tuple[str, bool]]  # set-house-event instructions
 
 
 @dataclass
@@ -122,10 +221,19 @@ class MefModel:
     parameters: Dict[str, Expr] = field(default_factory=dict)
     names: List[str] = field(default_factory=list)  # fault-tree names
     mission_time: float = DEFAULT_MISSION_TIME
+    fault_trees: Dict[str, List[str]] = field(default_factory=dict)  # fault tree -> its gate ids
+    initiating_events: Dict[str, Optional[str]] = field(default_factory=dict)  # -> event tree
+    event_trees: Dict[str, EventTree] = field(default_factory=dict)
+    sequences: Dict[str, list] = field(default_factory=dict)  # sequence -> instructions
+    rules: Dict[str, list] = field(default_factory=dict)
+    alignments: Dict[str, List[Phase]] = field(default_factory=dict)
 
     def probability(self, event: str, t: Optional[float] = None) -> float:
         """Probability of a basic event at mission time t (default: the model's)."""
-        v = self.basic_events[event].value(self.mission_time if t is None else t, self.parameters)
+        e = self.basic_events[event]
+        if e is None:
+            raise MefError(f"basic event {event!r} has no probability expression")
+        v = e.value(self.mission_time if t is None else t, self.parameters)
         if not 0.0 <= v <= 1.0:
             raise MefError(f"basic event {event!r}: probability {v} outside [0, 1] at t = {t}")
         return v
@@ -144,6 +252,35 @@ class MefModel:
         for f in self.gates.values():
             walk(f)
         return [g for g in self.gates if g not in used]
+
+    def fault_tree_tops(self, tree: str) -> List[str]:
+        """Top events of one fault tree: its gates (components included) that
+        no other gate of the same tree references (mcSCRAM
+        src/fault_tree.cc:63-92), in definition order."""
+        own = self.fault_trees[tree]
+        members = set(own)
+        used = set()
+
+        def walk(f: Formula):
+            for _, kind, x in f.args:
+                if kind == "gate" and x in members:
+                    used.add(x)
+                elif kind == "formula":
+                    walk(x)
+
+        for gid in own:
+            walk(self.gates[gid])
+        return [g for g in own if g not in used]
+
+    def with_phase(self, phase: Phase) -> "MefModel":
+        """A copy at the phase's share of the mission time with its house-event
+        states (mcSCRAM src/risk_analysis.cc:68-96)."""
+        m = copy.copy(self)
+        m.mission_time = self.mission_time * phase.time_fraction
+        m.house_events = dict(self.house_events)
+        for name, state in phase.house_events:
+            m.house_events[name] = state
+        return m
 
     def build(self, top: Optional[str] = None):
         """Host PDAG rooted at `top` (the only top gate when None).  Returns
@@ -246,21 +383,37 @@ def _local(tag: str) -> str:
     return tag.rsplit("}", 1)[-1]
 
 
-_ARITY = {"exponential": 2, "GLM": 4, "Weibull": 4, "neg": 1}
+def _kids(el: ET.Element) -> List[ET.Element]:
+    return [c for c in el if _local(c.tag) not in _SKIP]
+
+
+_ARITY = {"exponential": 2, "GLM": 4, "Weibull": 4, "neg": 1, "not": 1, "ite": 3,
+          "eq": 2, "df": 2, "lt": 2, "gt": 2, "leq": 2, "geq": 2}
+_NARY = ("exponential", "GLM", "Weibull", "add", "sub", "mul", "div", "neg", "not", "and", "or", "ite") + tuple(_COMPARE)
 
 
 def _parse_expr(e: ET.Element, what: str) -> Expr:
     tag = _local(e.tag)
     if tag in ("float", "int"):
         return Expr("value", [float(e.get("value"))])
+    if tag == "bool":
+        return Expr("value", [1.0 if e.get("value", "").strip().lower() == "true" else 0.0])
+    if tag == "pi":
+        return Expr("value", [math.pi])
     if tag == "parameter":
         return Expr("parameter", [e.get("name")])
     if tag == "system-mission-time":
         return Expr("time", [])
-    if tag in ("exponential", "GLM", "Weibull", "add", "sub", "mul", "div", "neg"):
-        args = [_parse_expr(c, what) for c in e if _local(c.tag) not in _SKIP]
+    if tag == "test-initiating-event":
+        return Expr(tag, [e.get("name")])
+    if tag == "test-functional-event":
+        return Expr(tag, [e.get("name"), e.get("state")])
+    if tag in _NARY:
+        args = [_parse_expr(c, what) for c in _kids(e)]
         if tag in _ARITY and len(args) != _ARITY[tag]:
             raise MefError(f"{what}: <{tag}> takes {_ARITY[tag]} arguments, found {len(args)}")
+        if tag in ("add", "sub", "mul", "div", "and", "or") and len(args) < 2:
+            raise MefError(f"{what}: <{tag}> takes 2 or more arguments, found {len(args)}")
         if not args:
             raise MefError(f"{what}: <{tag}> without arguments")
         return Expr(tag, args)
@@ -268,25 +421,73 @@ def _parse_expr(e: ET.Element, what: str) -> Expr:
 
 
 def _parse_expression(el: ET.Element, what: str) -> Expr:
-    kids = [c for c in el if _local(c.tag) not in _SKIP]
+    kids = _kids(el)
     if len(kids) != 1:
         raise MefError(f"{what}: expected one expression, found {len(kids)}")
     return _parse_expr(kids[0], what)
 
 
+def _check_arity(tag: str, n: int, where: str, k: Optional[int] = None, kmax: Optional[int] = None):
+    """Argument counts the reference's mef::Formula accepts (src/event.cc:174-225)."""
+    if tag in ("and", "or", "nand", "nor") and n < 2:
+        raise MefError(f"{where}: <{tag}> must have 2 or more arguments")
+    if tag in ("not",) and n != 1:
+        raise MefError(f"{where}: <not> must have exactly one argument")
+    if tag in ("xor", "imply", "iff") and n != 2:
+        raise MefError(f"{where}: <{tag}> must have exactly 2 arguments")
+    if tag == "atleast":
+        if k is None:
+            raise MefError(f"{where}: <atleast> without min")
+        if k < 2:
+            raise MefError(f"{where}: <atleast> min cannot be less than 2")
+        if n <= k:
+            raise MefError(f"{where}: <atleast> must have more arguments than its min number")
+    if tag == "cardinality":
+        if k is None or kmax is None:
+            raise MefError(f"{where}: <cardinality> requires min and max")
+        if k < 0 or k > kmax:
+            raise MefError(f"{where}: <cardinality> min {k} > max {kmax}")
+        if n < 1 or n < kmax:
+            raise MefError(f"{where}: <cardinality> max {kmax} exceeds its {n} arguments")
+
+
+def _threshold_formula(k: int, args: list) -> Tuple[bool, str, object]:
+    """At least k of args, well formed as the reference shapes its two
+    cardinality halves (src/pdag.cc:699-709): true for k = 0, OR for k = 1,
+    AND for k = n, ATLEAST otherwise; a single argument passes through."""
+    if k <= 0:
+        return False, "constant", True
+    if len(args) == 1:
+        return args[0]
+    if k == 1:
+        return False, "formula", Formula(OR, list(args))
+    if k == len(args):
+        return False, "formula", Formula(AND, list(args))
+    return False, "formula", Formula(ATLEAST, list(args), k)
+
+
 def _parse_formula(el: ET.Element, where: str) -> Formula:
     tag = _local(el.tag)
     if tag in _REFS or tag == "constant":
-        # a gate defined as a single event: a pass-through (NULL) gate
+        # a formula of a single event: a pass-through (NULL) gate
         return Formula(NULL, [_parse_arg(el, where)])
-    if tag not in _CONNECTIVES:
+    if tag not in _CONNECTIVES and tag not in _COMPLEX:
         raise MefError(f"{where}: unsupported formula <{tag}>")
-    args = [_parse_arg(c, where) for c in el if _local(c.tag) not in _SKIP]
+    args = [_parse_arg(c, where) for c in _kids(el)]
+    k = int(el.get("min")) if el.get("min") is not None else None
+    kmax = int(el.get("max")) if el.get("max") is not None else None
+    _check_arity(tag, len(args), where, k, kmax)
+    if tag == "imply":  # x -> y  ==  not x or y
+        (c0, k0, x0), second = args
+        return Formula(OR, [(not c0, k0, x0), second])
+    if tag == "iff":  # a NULL gate over the complemented XOR
+        return Formula(NULL, [(True, "formula", Formula(XOR, args))])
+    if tag == "cardinality":  # at least min of args and at least n - max of their complements
+        negated = [(not c, kind, x) for c, kind, x in args]
+        return Formula(AND, [_threshold_formula(k, args), _threshold_formula(len(args) - kmax, negated)])
     f = Formula(_CONNECTIVES[tag], args)
     if tag == "atleast":
-        if el.get("min") is None:
-            raise MefError(f"{where}: <atleast> without min")
-        f.min_number = int(el.get("min"))
+        f.min_number = k
     return f
 
 
@@ -300,88 +501,552 @@ def _parse_arg(el: ET.Element, where: str) -> Tuple[bool, str, object]:
     if tag == "constant":
         return False, "constant", el.get("value", "").strip().lower() == "true"
     if tag == "not":
-        kids = [c for c in el if _local(c.tag) not in _SKIP]
+        kids = _kids(el)
         if len(kids) == 1 and _local(kids[0].tag) in _REFS:
             comp, kind, x = _parse_arg(kids[0], where)
             return (not comp), kind, x
     return False, "formula", _parse_formula(el, where)
 
 
-def parse(source: Union[str, Path], mission_time: float = DEFAULT_MISSION_TIME) -> MefModel:
-    """Reads a MEF document (a path, or the XML text itself); probabilities are
-    evaluated at `mission_time` unless asked for at another time."""
+class _Scope:
+    """Element ids and full paths per element type, and the MEF lookup rule
+    (mcSCRAM src/initializer.cc:1400-1466)."""
+
+    def __init__(self):
+        self.paths: Dict[str, Dict[str, str]] = {k: {} for k in _TABLES}  # full path -> id
+        self.public: Dict[str, set] = {k: set() for k in _TABLES}
+        self.ids: Dict[str, set] = {k: set() for k in _TABLES}
+
+    def register(self, kind: str, name: str, base: str, role: str) -> str:
+        if not name:
+            raise MefError(f"<define-{kind}> without a name")
+        full = f"{base}.{name}" if base else name
+        ident = name if role == "public" else full
+        if full in self.paths[kind] or ident in self.ids[kind]:
+            raise MefError(f"{kind} {ident!r} defined twice")
+        if kind in _EVENTS:  # gates, basic and house events share one namespace
+            for other in _EVENTS:
+                if other != kind and (full in self.paths[other] or ident in self.ids[other]):
+                    raise MefError(f"{kind} {ident!r} clashes with the {other} of that name")
+        self.paths[kind][full] = ident
+        self.ids[kind].add(ident)
+        if role == "public":
+            self.public[kind].add(ident)
+        return ident
+
+    def lookup(self, kinds, ref: str, base: str) -> Optional[Tuple[str, str]]:
+        if base:
+            full = f"{base}.{ref}"
+            for k in kinds:
+                if full in self.paths[k]:
+                    return k, self.paths[k][full]
+        for k in kinds:
+            if "." not in ref:
+                if ref in self.public[k]:
+                    return k, ref
+            elif ref in self.paths[k]:
+                return k, self.paths[k][ref]
+        return None
+
+
+def _role(el: ET.Element, parent: str) -> str:
+    r = (el.get("role") or "").strip()
+    return parent if not r else ("public" if r == "public" else "private")
+
+
+def _parse_instruction(el: ET.Element, where: str):
+    tag = _local(el.tag)
+    kids = _kids(el)
+    if tag == "collect-formula":
+        if len(kids) != 1:
+            raise MefError(f"{where}: <collect-formula> takes one formula")
+        return "collect-formula", _parse_formula(kids[0], where)
+    if tag == "collect-expression":
+        return "collect-expression", _parse_expression(el, where)
+    if tag == "set-house-event":
+        if len(kids) != 1 or _local(kids[0].tag) != "constant":
+            raise MefError(f"{where}: <set-house-event> takes one <constant>")
+        return "set-house-event", el.get("name"), kids[0].get("value", "").strip().lower() == "true"
+    if tag == "if":
+        if len(kids) not in (2, 3):
+            raise MefError(f"{where}: <if> takes a condition, an instruction and an optional else")
+        return ("if", _parse_expr(kids[0], where), _parse_instruction(kids[1], where),
+                _parse_instruction(kids[2], where) if len(kids) == 3 else None)
+    if tag == "block":
+        return "block", [_parse_instruction(c, where) for c in kids]
+    if tag == "rule":
+        return "rule", el.get("name")
+    if tag == "event-tree":
+        return "link", el.get("name")
+    raise MefError(f"{where}: unsupported instruction <{tag}>")
+
+
+def _parse_branch(kids: List[ET.Element], where: str) -> Branch:
+    """Instructions, then the target as the last element (mcSCRAM
+    src/initializer.cc:911-926)."""
+    if not kids:
+        raise MefError(f"{where}: a branch needs a target")
+    *ins, last = kids
+    tag = _local(last.tag)
+    if tag == "fork":
+        paths, states = [], set()
+        for p in last:
+            if _local(p.tag) != "path":
+                continue
+            state = p.get("state")
+            if state in states:
+                raise MefError(f"{where}: path state {state!r} defined twice in a fork")
+            states.add(state)
+            paths.append((state, _parse_branch(_kids(p), where)))
+        if not paths:
+            raise MefError(f"{where}: a fork without paths")
+        target = ("fork", Fork(last.get("functional-event"), paths))
+    elif tag in ("sequence", "branch"):
+        target = (tag, last.get("name"))
+    else:
+        raise MefError(f"{where}: <{tag}> is not a branch target")
+    return Branch([_parse_instruction(c, where) for c in ins], target)
+
+
+def _walk_instructions(ins, fn, rules, seen_rules=None):
+    """Calls fn on every instruction reachable from `ins` (blocks, both arms
+    of an if, rules followed once)."""
+    seen_rules = set() if seen_rules is None else seen_rules
+    for x in ins:
+        fn(x)
+        kind = x[0]
+        if kind == "block":
+            _walk_instructions(x[1], fn, rules, seen_rules)
+        elif kind == "if":
+            arms = [x[2]] + ([x[3]] if x[3] is not None else [])
+            _walk_instructions(arms, fn, rules, seen_rules)
+        elif kind == "rule" and x[1] in rules and x[1] not in seen_rules:
+            seen_rules.add(x[1])
+            _walk_instructions(rules[x[1]], fn, rules, seen_rules)
+
+
+def _find_cycle(edges: Dict[str, List[str]]) -> Optional[str]:
+    state: Dict[str, int] = {}
+    for start in edges:
+        if state.get(start):
+            continue
+        stack = [(start, iter(edges.get(start, ())))]
+        state[start] = 1
+        while stack:
+            node, it = stack[-1]
+            nxt = next(it, None)
+            if nxt is None:
+                state[node] = 2
+                stack.pop()
+                continue
+            s = state.get(nxt, 0)
+            if s == 1:
+                return nxt
+            if s == 0:
+                state[nxt] = 1
+                stack.append((nxt, iter(edges.get(nxt, ()))))
+    return None
+
+
+def _document(source: Union[str, Path]) -> ET.Element:
     text = Path(source).read_text() if isinstance(source, Path) or (
         isinstance(source, str) and not source.lstrip().startswith("<")) else source
     try:
-        root = ET.fromstring(text.lstrip("﻿"))
+        root = ET.fromstring(text.lstrip("\ufeff"))
     except ET.ParseError as e:
         raise MefError(f"not well-formed XML: {e}") from None
     if _local(root.tag) != "opsa-mef":
         raise MefError("root element is not <opsa-mef>")
-    m = MefModel(mission_time=float(mission_time))
+    for el in root.iter():  # names and references without surrounding blanks
+        for a in ("name", "event-tree", "functional-event", "state"):
+            if el.get(a) is not None:
+                el.set(a, el.get(a).strip())
+        if _local(el.tag) == "attributes":
+            names = [a.get("name") for a in el]
+            if len(names) != len(set(names)):
+                raise MefError(f"an element repeats one of its attributes {sorted(names)}")
+    return root
 
-    def visit(container: ET.Element):
+
+def parse(source: Union[str, Path, List[Union[str, Path]]],
+          mission_time: float = DEFAULT_MISSION_TIME) -> MefModel:
+    """Reads a MEF document (a path, or the XML text itself) or several
+    documents forming one model (a list; references may cross them);
+    probabilities are evaluated at `mission_time` unless asked for at another
+    time."""
+    roots = [_document(x) for x in (source if isinstance(source, (list, tuple)) else [source])]
+    m = MefModel(mission_time=float(mission_time))
+    scope = _Scope()
+    gate_base: Dict[str, str] = {}
+    expr_base: List[Tuple[Expr, str]] = []
+    collected: List[Formula] = []  # collect-formula formulas (global scope)
+
+    components = set()
+
+    def visit_data(container: ET.Element, base: str, role: str, tree: Optional[str]):
         for el in container:
             tag = _local(el.tag)
             name = el.get("name")
-            if tag in ("define-fault-tree", "define-component"):
-                if tag == "define-fault-tree":
-                    m.names.append(name)
-                visit(el)
-            elif tag == "model-data":
-                visit(el)
-            elif tag == "define-gate":
-                kids = [c for c in el if _local(c.tag) not in _SKIP]
+            if not base and _role(el, role) != "public":
+                raise MefError(f"{name!r}: private elements need a fault tree or component")
+            if tag == "define-gate":
+                kids = _kids(el)
+                ident = scope.register("gate", name, base, _role(el, role))
                 if len(kids) != 1:
-                    raise MefError(f"gate {name!r}: expected one formula, found {len(kids)}")
-                if name in m.gates:
-                    raise MefError(f"gate {name!r} defined twice")
-                m.gates[name] = _parse_formula(kids[0], f"gate {name!r}")
+                    raise MefError(f"gate {ident!r}: expected one formula, found {len(kids)}")
+                m.gates[ident] = _parse_formula(kids[0], f"gate {ident!r}")
+                gate_base[ident] = base
+                if tree is not None:
+                    m.fault_trees[tree].append(ident)
             elif tag == "define-basic-event":
-                m.basic_events[name] = _parse_expression(el, f"basic event {name!r}")
+                ident = scope.register("basic-event", name, base, _role(el, role))
+                if _kids(el):  # an event without an expression serves qualitative analyses only
+                    m.basic_events[ident] = _parse_expression(el, f"basic event {ident!r}")
+                    expr_base.append((m.basic_events[ident], base))
+                else:
+                    m.basic_events[ident] = None
             elif tag == "define-house-event":
-                kids = [c for c in el if _local(c.tag) not in _SKIP]
-                m.house_events[name] = bool(kids) and kids[0].get("value", "").strip().lower() == "true"
+                ident = scope.register("house-event", name, base, _role(el, role))
+                kids = _kids(el)
+                m.house_events[ident] = bool(kids) and kids[0].get("value", "").strip().lower() == "true"
             elif tag == "define-parameter":
-                m.parameters[name] = _parse_expression(el, f"parameter {name!r}")
+                ident = scope.register("parameter", name, base, _role(el, role))
+                m.parameters[ident] = _parse_expression(el, f"parameter {ident!r}")
+                expr_base.append((m.parameters[ident], base))
+            elif tag == "define-component":
+                if tree is None:
+                    raise MefError("<define-component> outside a fault tree")
+                if f"{base}.{name}" in components:
+                    raise MefError(f"component {base + '.' + name!r} defined twice")
+                components.add(f"{base}.{name}")
+                visit_data(el, f"{base}.{name}", _role(el, role), tree)
             elif tag in _SKIP:
                 continue
             else:
                 raise MefError(f"unsupported element <{tag}>")
 
-    visit(root)
-    for name in m.basic_events:
-        try:
-            m.probability(name)
-        except MefError as e:
-            raise MefError(f"basic event {name!r}: {e}") from None
-    # resolve untyped references and constants; check every reference
-    consts = {}
+    def define_event_tree(el: ET.Element):
+        name = el.get("name")
+        if name in m.event_trees:
+            raise MefError(f"event tree {name!r} defined twice")
+        et = EventTree(name)
+        where = f"event tree {name!r}"
+        for c in el:
+            tag = _local(c.tag)
+            cname = c.get("name")
+            if tag == "define-functional-event":
+                if cname in et.functional_events:
+                    raise MefError(f"{where}: functional event {cname!r} defined twice")
+                et.functional_events.append(cname)
+            elif tag == "define-sequence":
+                if cname in m.sequences:
+                    raise MefError(f"sequence {cname!r} defined twice")
+                m.sequences[cname] = [_parse_instruction(i, f"sequence {cname!r}") for i in _kids(c)]
+                et.sequences.append(cname)
+            elif tag == "define-branch":
+                if cname in et.branches:
+                    raise MefError(f"{where}: branch {cname!r} defined twice")
+                et.branches[cname] = _parse_branch(_kids(c), f"{where}, branch {cname!r}")
+            elif tag == "initial-state":
+                et.initial_state = _parse_branch(_kids(c), f"{where}, initial state")
+            elif tag in _SKIP:
+                continue
+            else:
+                raise MefError(f"{where}: unsupported element <{tag}>")
+        if et.initial_state is None:
+            raise MefError(f"{where}: no initial state")
+        m.event_trees[name] = et
 
-    def resolve(f: Formula, where: str):
+    for el in (x for r in roots for x in r):
+        tag = _local(el.tag)
+        name = el.get("name")
+        if tag == "define-fault-tree":
+            if name in m.fault_trees:
+                raise MefError(f"fault tree {name!r} defined twice")
+            m.names.append(name)
+            m.fault_trees[name] = []
+            visit_data(el, name, "public", name)  # fault trees are public (src/fault_tree.h:128-130)
+        elif tag == "model-data":
+            visit_data(el, "", "public", None)
+        elif tag in ("define-gate", "define-basic-event", "define-house-event", "define-parameter"):
+            visit_data([el], "", "public", None)
+        elif tag == "define-event-tree":
+            define_event_tree(el)
+        elif tag == "define-initiating-event":
+            if name in m.initiating_events:
+                raise MefError(f"initiating event {name!r} defined twice")
+            m.initiating_events[name] = el.get("event-tree") or None
+        elif tag == "define-rule":
+            if name in m.rules:
+                raise MefError(f"rule {name!r} defined twice")
+            m.rules[name] = [_parse_instruction(c, f"rule {name!r}") for c in _kids(el)]
+        elif tag == "define-alignment":
+            if name in m.alignments:
+                raise MefError(f"alignment {name!r} defined twice")
+            phases, total = [], 0.0
+            for ph in el:
+                if _local(ph.tag) != "define-phase":
+                    continue
+                frac = float(ph.get("time-fraction"))
+                if not 0.0 < frac <= 1.0:
+                    raise MefError(f"alignment {name!r}: phase time fraction {frac} outside (0, 1]")
+                if any(p.name == ph.get("name") for p in phases):
+                    raise MefError(f"alignment {name!r}: phase {ph.get('name')!r} defined twice")
+                sets = [_parse_instruction(c, f"phase {ph.get('name')!r}") for c in _kids(ph)]
+                if any(s[0] != "set-house-event" for s in sets):
+                    raise MefError(f"alignment {name!r}: phases hold only set-house-event instructions")
+                phases.append(Phase(ph.get("name"), frac, [(s[1], s[2]) for s in sets]))
+                total += frac
+            if not phases or abs(total - 1.0) > 1e-9:
+                raise MefError(f"alignment {name!r}: phase time fractions sum to {total}, not 1")
+            m.alignments[name] = phases
+        elif tag in _SKIP:
+            continue
+        else:
+            raise MefError(f"unsupported element <{tag}>")
+
+    # resolve parameter references in expressions
+    def resolve_expr(e: Expr, base: str, where: str):
+        if e.op == "parameter":
+            hit = scope.lookup(("parameter",), e.args[0], base)
+            if hit is None:
+                raise MefError(f"{where}: unknown parameter {e.args[0]!r}")
+            e.args = [hit[1]]
+        elif e.op not in ("value", "time", "test-initiating-event", "test-functional-event"):
+            for x in e.args:
+                resolve_expr(x, base, where)
+
+    for e, base in expr_base:
+        resolve_expr(e, base, "expression")
+    for name, e in m.basic_events.items():
+        if e is not None:
+            v = e.value(m.mission_time, m.parameters)
+            if not 0.0 <= v <= 1.0:
+                raise MefError(f"basic event {name!r}: probability {v} outside [0, 1]")
+
+    # resolve event references, untyped references and constants
+    def resolve(f: Formula, base: str, where: str):
         out = []
         for comp, kind, x in f.args:
-            if kind == "event":
-                kind = ("gate" if x in m.gates else "basic-event" if x in m.basic_events
-                        else "house-event" if x in m.house_events else None)
-                if kind is None:
-                    raise MefError(f"{where}: unknown event {x!r}")
             if kind == "constant":
                 key = f"__constant_{'true' if x else 'false'}"
                 m.house_events.setdefault(key, bool(x))
+                scope.public["house-event"].add(key)
                 kind, x = "house-event", key
-                consts[key] = True
-            table = {"gate": m.gates, "basic-event": m.basic_events, "house-event": m.house_events}.get(kind)
-            if table is not None and x not in table:
-                raise MefError(f"{where}: unknown {kind} {x!r}")
-            if kind == "formula":
-                resolve(x, where)
+            elif kind == "formula":
+                resolve(x, base, where)
+            else:
+                kinds = ("gate", "basic-event", "house-event") if kind == "event" else (kind,)
+                hit = scope.lookup(kinds, x, base)
+                if hit is None:
+                    raise MefError(f"{where}: unknown {kind} {x!r}")
+                kind, x = hit
+            if kind != "formula" and any(k == kind and y == x for _, k, y in out):
+                raise MefError(f"{where}: {kind} {x!r} is an argument twice")
             out.append((comp, kind, x))
         f.args = out
 
-    for name, f in m.gates.items():
-        resolve(f, f"gate {name!r}")
+    for gid, f in m.gates.items():
+        resolve(f, gate_base[gid], f"gate {gid!r}")
+
+    def resolve_instructions(ins, where: str):
+        def fn(x):
+            if x[0] == "collect-formula":
+                resolve(x[1], "", where)
+            elif x[0] == "collect-expression":
+                resolve_expr(x[1], "", where)
+            elif x[0] == "if":
+                resolve_expr(x[1], "", where)
+            elif x[0] == "set-house-event":
+                if scope.lookup(("house-event",), x[1], "") is None:
+                    raise MefError(f"{where}: set-house-event of undefined house event {x[1]!r}")
+            elif x[0] == "rule" and x[1] not in m.rules:
+                raise MefError(f"{where}: undefined rule {x[1]!r}")
+            elif x[0] == "link" and x[1] not in m.event_trees:
+                raise MefError(f"{where}: link to undefined event tree {x[1]!r}")
+        _walk_instructions(ins, fn, {})
+
+    for rname, ins in m.rules.items():
+        resolve_instructions(ins, f"rule {rname!r}")
+    for sname, ins in m.sequences.items():
+        resolve_instructions(ins, f"sequence {sname!r}")
+    for aname, phases in m.alignments.items():
+        for ph in phases:
+            for h, _ in ph.house_events:
+                if scope.lookup(("house-event",), h, "") is None:
+                    raise MefError(f"alignment {aname!r}: undefined house event {h!r}")
+    for et in m.event_trees.values():
+        where = f"event tree {et.name!r}"
+        for b in _branches_of(et):
+            resolve_instructions(b.instructions, where)
+            if b.target[0] == "fork" and b.target[1].functional_event not in et.functional_events:
+                raise MefError(f"{where}: undefined functional event {b.target[1].functional_event!r}")
+            if b.target[0] == "sequence" and b.target[1] not in m.sequences:
+                raise MefError(f"{where}: undefined sequence {b.target[1]!r}")
+            if b.target[0] == "branch" and b.target[1] not in et.branches:
+                raise MefError(f"{where}: undefined branch {b.target[1]!r}")
+    for ie, tree in m.initiating_events.items():
+        if tree is not None and tree not in m.event_trees:
+            raise MefError(f"initiating event {ie!r}: undefined event tree {tree!r}")
+
+    _validate(m)
     return m
+
+
+def _branches_of(et: EventTree) -> List[Branch]:
+    """Every branch of an event tree: named branches, the initial state and
+    the paths of their forks."""
+    out, todo = [], list(et.branches.values()) + [et.initial_state]
+    while todo:
+        b = todo.pop()
+        out.append(b)
+        if b.target[0] == "fork":
+            todo.extend(p for _, p in b.target[1].paths)
+    return out
+
+
+def _validate(m: MefModel):
+    """Cycles and the event-tree checks of mcSCRAM src/initializer.cc:1628-1791."""
+    # gates
+    edges: Dict[str, List[str]] = {}
+    for gid, f in m.gates.items():
+        refs: List[str] = []
+
+        def walk(fm: Formula):
+            for _, kind, x in fm.args:
+                if kind == "gate":
+                    refs.append(x)
+                elif kind == "formula":
+                    walk(x)
+
+        walk(f)
+        edges[gid] = refs
+    c = _find_cycle(edges)
+    if c is not None:
+        raise MefError(f"gate {c!r} is part of a cycle")
+    # rules
+    redges = {}
+    for rname, ins in m.rules.items():
+        refs = []
+        _walk_instructions(ins, lambda x: refs.append(x[1]) if x[0] == "rule" else None, {})
+        redges[rname] = refs
+    c = _find_cycle(redges)
+    if c is not None:
+        raise MefError(f"rule {c!r} is part of a cycle")
+    for et in m.event_trees.values():
+        where = f"event tree {et.name!r}"
+        # named branches
+        bedges = {}
+        for bname, b in et.branches.items():
+            refs = []
+            todo = [b]
+            while todo:
+                x = todo.pop()
+                if x.target[0] == "branch":
+                    refs.append(x.target[1])
+                elif x.target[0] == "fork":
+                    todo.extend(p for _, p in x.target[1].paths)
+            bedges[bname] = refs
+        c = _find_cycle(bedges)
+        if c is not None:
+            raise MefError(f"{where}: branch {c!r} is part of a cycle")
+    for et in m.event_trees.values():
+        where = f"event tree {et.name!r}"
+        order = {fe: i for i, fe in enumerate(et.functional_events)}
+        for b in list(et.branches.values()) + [et.initial_state]:
+            _check_fork_order(et, b, order, where)
+            _links_only_in_sequences(m, b, where)
+    # links: event tree -> event trees its sequences link to
+    ledges = {name: sorted(_links_from(m, et)) for name, et in m.event_trees.items()}
+    c = _find_cycle(ledges)
+    if c is not None:
+        raise MefError(f"event-tree link to {c!r} is part of a cycle")
+    for et in m.event_trees.values():
+        for b in list(et.branches.values()) + [et.initial_state]:
+            _check_homogeneous(m, et, b, f"event tree {et.name!r}")
+
+
+def _next_fork(et: EventTree, target) -> Optional[Fork]:
+    seen = set()
+    while target[0] == "branch" and target[1] not in seen:
+        seen.add(target[1])
+        target = et.branches[target[1]].target
+    return target[1] if target[0] == "fork" else None
+
+
+def _check_fork_order(et: EventTree, b: Branch, order: Dict[str, int], where: str):
+    if b.target[0] != "fork":
+        return
+    fork = b.target[1]
+    for _, path in fork.paths:
+        _check_fork_order(et, path, order, where)
+        nxt = _next_fork(et, path.target)
+        if nxt is None:
+            continue
+        a, z = order[fork.functional_event], order[nxt.functional_event]
+        if a == z:
+            raise MefError(f"{where}: functional event {fork.functional_event!r} is duplicated in fork paths")
+        if a > z:
+            raise MefError(f"{where}: functional event {fork.functional_event!r} must appear after "
+                           f"{nxt.functional_event!r} in fork paths")
+
+
+def _links_only_in_sequences(m: MefModel, b: Branch, where: str):
+    todo = [b]
+    while todo:
+        x = todo.pop()
+
+        def fn(ins):
+            if ins[0] == "link":
+                raise MefError(f"{where}: link to {ins[1]!r} can only be used in end-state sequences")
+
+        _walk_instructions(x.instructions, fn, m.rules)
+        if x.target[0] == "fork":
+            todo.extend(p for _, p in x.target[1].paths)
+
+
+def _sequences_reached(et: EventTree) -> List[str]:
+    out = []
+    for b in _branches_of(et):
+        if b.target[0] == "sequence" and b.target[1] not in out:
+            out.append(b.target[1])
+    return out
+
+
+def _links_from(m: MefModel, et: EventTree) -> set:
+    out = set()
+    for s in _sequences_reached(et):
+        _walk_instructions(m.sequences[s], lambda x: out.add(x[1]) if x[0] == "link" else None, m.rules)
+    return out
+
+
+def _check_homogeneous(m: MefModel, et: EventTree, b: Branch, where: str):
+    kind = [None]
+    visited_trees = set()
+
+    def fn(ins):
+        if ins[0] in ("collect-formula", "collect-expression"):
+            if kind[0] is None:
+                kind[0] = ins[0]
+            elif kind[0] != ins[0]:
+                raise MefError(f"{where}: mixed collect-expression and collect-formula")
+        elif ins[0] == "link" and ins[1] not in visited_trees:
+            visited_trees.add(ins[1])
+            walk_branch(m.event_trees[ins[1]], m.event_trees[ins[1]].initial_state, set())
+
+    def walk_branch(tree: EventTree, x: Branch, seen_branches: set):
+        _walk_instructions(x.instructions, fn, m.rules)
+        kind_, tgt = x.target
+        if kind_ == "sequence":
+            _walk_instructions(m.sequences[tgt], fn, m.rules)
+        elif kind_ == "fork":
+            for _, p in tgt.paths:
+                walk_branch(tree, p, seen_branches)
+        elif tgt not in seen_branches:
+            seen_branches.add(tgt)
+            walk_branch(tree, tree.branches[tgt], seen_branches)
+
+    walk_branch(et, b, set())
 
 
 def load(source: Union[str, Path], top: Optional[str] = None,

@@ -491,3 +491,57 @@ def config5_instances(ids, seed: int = 5, workers: int = 0) -> list:
         with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
             return list(ex.map(config5_instance, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * workers))))
     return [config5_instance(i, seed) for i in ids]
+
+
+_MEF_CONNECTIVE = {AND: "and", OR: "or", ATLEAST: "atleast", XOR: "xor", NOT: "not", 5: "nand", 6: "nor"}
+
+
+def event_tree_xml(g: FlatGraph, n_functional: int = 8, initiating_event: str = "IE") -> str:
+    """A MEF model of an event tree over a synthetic fault tree: the gates of
+    `g` as the fault tree "Plant" (basic events e<i> at their quantised
+    probabilities, so the thresholds are the graph's own), the last
+    `n_functional` gates in topological order as the functional events' fault
+    trees, and a complete binary event tree over them -- every path collects
+    each functional event's top (failure) or its negation (success), so the
+    2^n sequences partition the outcomes."""
+    q = g.quantised_probabilities()
+    n_be = g.n_be
+
+    def ref(node: int, neg: bool = False) -> str:
+        r = f'<basic-event name="e{node}"/>' if node < n_be else f'<gate name="g{node - n_be}"/>'
+        return f"<not>{r}</not>" if neg else r
+
+    out = ['<?xml version="1.0"?>', "<opsa-mef>",
+           f'<define-initiating-event name="{initiating_event}" event-tree="Plant-ET"/>',
+           '<define-event-tree name="Plant-ET">']
+    tops = list(range(g.n_gates - n_functional, g.n_gates))
+    out += [f'<define-functional-event name="F{k}"/>' for k in range(n_functional)]
+    out += [f'<define-sequence name="S{s:0{n_functional}b}"/>' for s in range(1 << n_functional)]
+
+    def fork(level: int, bits: int) -> str:
+        if level == n_functional:
+            return f'<sequence name="S{bits:0{n_functional}b}"/>'
+        top = f'<gate name="g{tops[level]}"/>'
+        return (f'<fork functional-event="F{level}">'
+                f'<path state="success"><collect-formula><not>{top}</not></collect-formula>{fork(level + 1, bits << 1)}</path>'
+                f'<path state="failure"><collect-formula>{top}</collect-formula>{fork(level + 1, (bits << 1) | 1)}</path>'
+                "</fork>")
+
+    out += ["<initial-state>", fork(0, 0), "</initial-state>", "</define-event-tree>",
+            '<define-fault-tree name="Plant">']
+    for j in range(g.n_gates):
+        b, c, neg = int(g.gate_in_begin[j]), int(g.gate_in_count[j]), int(g.gate_neg_count[j])
+        args = "".join(ref(int(x), i >= c - neg) for i, x in enumerate(g.inputs[b:b + c]))
+        op = int(g.gate_op[j])
+        if op == 7:  # NULL: a gate defined as its one argument
+            body = args
+        else:
+            name = _MEF_CONNECTIVE[op]
+            attr = f' min="{int(g.gate_k[j])}"' if op == ATLEAST else ""
+            body = f"<{name}{attr}>{args}</{name}>"
+        out.append(f'<define-gate name="g{j}">{body}</define-gate>')
+    out += ["</define-fault-tree>", "<model-data>"]
+    out += [f'<define-basic-event name="e{i}"><float value="{float(q[i])!r}"/></define-basic-event>'
+            for i in range(n_be)]
+    out += ["</model-data>", "</opsa-mef>"]
+    return "\n".join(out)

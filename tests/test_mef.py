@@ -90,17 +90,24 @@ def test_numbering_follows_first_encounter():
 
 
 @pytest.mark.parametrize("xml,msg", [
-    ("<opsa-mef><define-gate name='t'><and><basic-event name='x'/></and></define-gate></opsa-mef>",
-     "unknown basic-event"),
-    ("<opsa-mef><define-gate name='t'><or><event name='x'/></or></define-gate>"
+    ("<opsa-mef><define-gate name='t'><and><basic-event name='x'/><basic-event name='y'/></and></define-gate>"
+     "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown basic-event"),
+    ("<opsa-mef><define-gate name='t'><or><event name='x'/><event name='y'/></or></define-gate>"
      "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown event"),
     ("<opsa-mef><define-basic-event name='x'><lognormal-deviate/></define-basic-event></opsa-mef>",
      "unsupported expression"),
     ("<opsa-mef><define-basic-event name='x'><exponential><float value='1'/></exponential>"
      "</define-basic-event></opsa-mef>", "takes 2 arguments"),
-    ("<opsa-mef><define-gate name='t'><or/></define-gate><define-gate name='t'><or/></define-gate></opsa-mef>",
-     "defined twice"),
-    ("<opsa-mef><define-gate name='t'><imply/></define-gate></opsa-mef>", "unsupported formula"),
+    ("<opsa-mef><define-gate name='t'><house-event name='h'/></define-gate>"
+     "<define-gate name='t'><house-event name='h'/></define-gate></opsa-mef>", "defined twice"),
+    ("<opsa-mef><define-gate name='t'><majority/></define-gate></opsa-mef>", "unsupported formula"),
+    ("<opsa-mef><define-gate name='t'><and><basic-event name='x'/></and></define-gate></opsa-mef>",
+     "2 or more arguments"),
+    ("<opsa-mef><define-gate name='t'><atleast min='2'><house-event name='h'/><house-event name='i'/></atleast>"
+     "</define-gate></opsa-mef>", "more arguments than its min"),
+    ("<opsa-mef><define-gate name='t'><or><gate name='u'/><house-event name='h'/></or></define-gate>"
+     "<define-gate name='u'><or><gate name='t'/><house-event name='h'/></or></define-gate>"
+     "<define-house-event name='h'/></opsa-mef>", "cycle"),
     ("<opsa-mef><define-basic-event name='x'><float value='1.5'/></define-basic-event></opsa-mef>",
      "outside"),
     ("<model/>", "opsa-mef"),

@@ -55,11 +55,13 @@ def parse_args():
                     help="plain workload's tree (config1: the small 200-event tree, for profiling captures)")
     ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")
     ap.add_argument("--sampler-blocks", type=int, default=0, help="staged: sampler blocks per SM (0 = default)")
-    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis", "converge"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis", "converge", "eta"],
                     help="plain: the 5,000-event tree (headline); ua: batched uncertainty analysis; "
                          "is: GPU time to 5%% relative error on the 1e-8 tree, learned IS vs plain; "
                          "bis: the same for 1,024 rare-event trees at once with one shared network; "
-                         "converge: ComputeTallies to a relative error, waiting vs pipelined convergence loop")
+                         "converge: ComputeTallies to a relative error, waiting vs pipelined convergence loop; "
+                         "eta: combined event-tree pass, every sequence of a 2^n-sequence tree tallied")
+    ap.add_argument("--eta-functional", type=int, default=8, help="functional events of the eta workload's tree")
     ap.add_argument("--converge-rel-err", type=float, default=1e-3)
     ap.add_argument("--converge-words", type=int, default=1 << 14, help="words per pass of the convergence loop")
     ap.add_argument("--converge-watch", default="top", choices=["top", "gates"],
@@ -155,7 +157,7 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- CPU baseline
 
-def cpu_rate(g, target_seconds: float, reference: bool = True):
+def cpu_rate(g, target_seconds: float, reference: bool = True, label: str = "the 5,000-event tree"):
     """Gate-evals/s of the CPU reference dataflow on a bounded sample of the
     workload (pass 1, leading words), using every host thread."""
     from oracle import oracle
@@ -176,7 +178,7 @@ def cpu_rate(g, target_seconds: float, reference: bool = True):
             "gate/tally loops restated from src/mc/kernel/gate.h and tally.h" if ref else
             "oracle/liboracle.so: plain-C restatement of the reference dataflow")
     return {"value": rate, "unit": UNIT, "cores": oracle.max_threads(), "kind": kind,
-            "sample": f"{words} words (pass 1, words [0, {words})) of the 5,000-event tree, "
+            "sample": f"{words} words (pass 1, words [0, {words})) of {label}, "
                       f"{g.n_gates} gates tallied, {dt:.2f} s; {what}",
             "seconds": dt, "words": words}
 
@@ -516,6 +518,118 @@ def run_converge(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
+def run_eta(args, rank: int, world: int, local: int) -> int:
+    """The combined event-tree path (the reference's RunCombinedEtaAnalysis):
+    a complete binary event tree over `--eta-functional` functional events
+    whose fault trees are the top gates of the 5,000-event / 3,000-gate tree,
+    written as MEF, loaded, and sampled as one PDAG with the OR root, every
+    sequence gate (2^n) and the fault tree's top tallied.  One step = one
+    pass of 2^30 samples.  `value` = samples/s with every sequence evaluated;
+    `e2e` = eta.run_combined (PDAG from the MEF model, layering, engine, pass,
+    tallies) for the same samples.  The sequences partition the outcomes, so
+    their tallies must add up to the samples exactly."""
+    if rank != 0:
+        return 0
+    import torch
+    from mcscram_b200 import _capi, eta, host, mef, synth
+
+    torch.cuda.set_device(local)
+    g0 = synth.config2()
+    xml = synth.event_tree_xml(g0, args.eta_functional)
+    t0 = time.perf_counter()
+    model = mef.parse(xml)
+    c = eta.combined_pdag(model, "IE")
+    g = c.flat()
+    host_s = time.perf_counter() - t0
+    n_seq = len(c.sequences)
+    W = args.words
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    mode = _capi.MODES[args.mode]
+    eng = _capi.Engine(g, device=local, stream=stream.cuda_stream, mode=mode)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    for i in range(args.warmup):
+        flush.zero_()
+        eng.run(i + 1, 1, 0, W)
+    torch.cuda.synchronize()
+    eng.reset_tallies()
+    if args.mode in ("staged", "strip"):
+        eng.profile_sampler(True)
+    launches0 = eng.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        flush.zero_()
+        eng.run(args.warmup + i + 1, 1, 0, W)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = eng.launch_count() - launches0
+    ms_per_step = t_start.elapsed_time(t_end) / args.steps
+    ones, total = eng.tallies()
+    partition_exact = int(ones[0]) == total and sum(int(x) for x in ones[1:1 + n_seq]) == total
+    samples = W * 64
+    value = samples / (ms_per_step * 1e-3)
+    kernel, roof = None, None
+    if args.mode in ("staged", "strip"):
+        kernel = "k_stage_be" if args.mode == "staged" else "k_strip"
+        n_a, ms_a = eng.profile_sampler_read()
+        eng.profile_sampler(False)
+        avg_launch_s = ms_a * 1e-3 / max(n_a, 1)
+        achieved = g.n_be * W * args.steps / max(n_a, 1) / avg_launch_s
+        peak = _capi.sampler_peak(n_events=256, n_words=args.peak_words, repeats=3, device=local)
+        roof = {"bound": "int-alu", "kernel": kernel, "achieved": achieved / 1e9, "peak": peak / 1e9,
+                "unit": "Gword/s", "frac": achieved / peak, "traffic": None, "launches": n_a,
+                "avg_launch_ms": avg_launch_s * 1e3,
+                "peak_source": "register-only Philox sampler kernel (k_sampler_peak) measured in this run",
+                "work_unit": "basic-event word = 16 Philox4x32-10 calls"}
+    eng.close()
+    e2e = None
+    if args.e2e_steps > 0:
+        s = host.Settings.default(num_trials=samples, early_stop=0, ci_rel_margin_error=1e-9,
+                                  max_words_per_iteration=W)
+        ts = []
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            r = eta.run_combined(model, "IE", s, mode=mode, device=local)
+            ts.append(time.perf_counter() - t1)
+        e2e_s = statistics.median(ts)
+        h2d = g.n_be * 16 + g.n_gates * 20 + g.inputs.size * 4 + g.tally_nodes.size * 4
+        e2e = {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(g.tally_nodes.size * 8), "seconds_per_step": e2e_s,
+               "sequences_reported": len(r.sequences)}
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_rate(g, args.cpu_seconds, reference=True,
+                       label=f"the {n_seq}-sequence event tree's combined PDAG")
+        cpu = dict(cpu, value=cpu["value"] / g.n_gates, unit="samples/s")
+    line = {
+        "metric": "event-tree samples/s", "value": value, "unit": "samples/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"combined event-tree pass: {args.eta_functional} functional events over the top gates "
+                               f"of the 5,000-event / 3,000-gate tree (seed 11), {n_seq} sequences, every sequence "
+                               "tallied, loaded from generated MEF", "samples_per_step": samples,
+                   "n_be": g.n_be, "n_gates": g.n_gates, "tallied_nodes": int(g.tally_nodes.size),
+                   "l2": "256 MB buffer written between steps", "mode": args.mode},
+        "gate_evals_per_s": g.n_gates * value, "sequence_tallies_per_s": n_seq * value,
+        "partition_exact": partition_exact, "host_model_seconds": host_s, "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if roof:
+        line["roofline"] = roof
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main() -> int:
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -531,6 +645,8 @@ def main() -> int:
         return run_bis(args, rank, world, local)
     if args.workload == "converge":
         return run_converge(args, rank, world, local)
+    if args.workload == "eta":
+        return run_eta(args, rank, world, local)
 
     import numpy as np
     import torch

@@ -272,30 +272,47 @@ void convergence_controller::after_pass(phase p) {
     ++steps_;
 }
 
+// True when the synchronous loop would stop after a pass that brings the
+// trial count to `trials` whatever that pass's tallies say: burn-in done and
+// the trial budget reached (next_pass() then returns none).
+bool convergence_controller::stops_after(std::size_t trials) const {
+    const std::size_t max_it = manager_.shaper().TOTAL_ITERATIONS;
+    const std::size_t per = manager_.shaper().SAMPLE_SHAPE.num_bitpacks() * 64;
+    if (!max_it || fixed_limit_reached_ || static_cast<double>(trials) < settings_.ci_burnin_trials) return false;
+    return (trials + per - 1) / per >= max_it;
+}
+
 // The same decisions as run_to_convergence's synchronous loop, taken one
 // pass behind the GPU: while the tallies after pass k are read and judged,
-// pass k + 1 already runs.  When the loop stops after pass k, the passes
-// run ahead are discarded by rolling the counters, their total and the pass
+// pass k + 1 already runs.  When the loop stops after pass k, the pass run
+// ahead is discarded by rolling the counters, their total and the pass
 // number back to the snapshot after pass k, so tallies, statistics and
 // stopping point equal the synchronous loop's; the cost is one pass of GPU
-// time that nobody uses.
+// time that nobody uses -- except where the trial budget already says the
+// pass in flight is the last one, when no pass is run ahead.  Pass k's
+// snapshot sits in slot (k - 1) & 1.
 stats::tally convergence_controller::run_to_convergence_pipelined(TallyNodeMap &map) {
     phase p = next_pass();
     if (p == phase::none) return current_tally_;
-    uint32_t done = 0;                       // passes judged
+    const std::size_t per = manager_.shaper().SAMPLE_SHAPE.num_bitpacks() * 64;
     const uint32_t base = manager_.iteration();
-    manager_.single_pass();                  // pass 1
-    manager_.snapshot(0);
+    uint32_t done = 0, submitted = 0;        // passes judged, passes queued
+    auto submit = [&] {
+        manager_.single_pass();
+        manager_.snapshot(submitted & 1u);
+        ++submitted;
+    };
+    submit();                                // pass 1
     for (;;) {
-        manager_.single_pass();              // pass done + 2, ahead of the decision
-        manager_.snapshot((done + 1) & 1u);
+        if (submitted == done + 1 && !stops_after(current_trials_ + per)) submit();  // ahead of the decision
         process_tallies(manager_.collect_snapshot(done & 1u, map));
         ++done;
         after_pass(p);
         p = next_pass();
         if (p == phase::none) break;
+        if (submitted == done) submit();     // the budget said stop, the loop did not
     }
-    manager_.restore_snapshot((done - 1) & 1u, base + done);
+    if (submitted > done) manager_.restore_snapshot((done - 1) & 1u, base + done);
     return current_tally_;
 }
 

@@ -142,6 +142,7 @@ class convergence_controller {
     enum class phase { none, burn_in, step };
     phase next_pass();  // the phase of the pass the synchronous loop would run next (none: stop)
     void after_pass(phase p);
+    bool stops_after(std::size_t trials) const;
     bool eps_bounded() const { return cur_eps_ > 0 && cur_eps_ <= target_eps_; }
     bool log_eps_bounded() const { return cur_eps_log10_ > 0 && cur_eps_log10_ <= settings_.ci_rel_margin_error; }
     layer_manager &manager_;

@@ -217,3 +217,47 @@ def test_probability_over_time_matches_oracle_per_time_point(oracle_mod, gpu):
         assert p_hat == ones / (W * 64.0), t  # the same counters as a plain pass at that time's thresholds
     ps = [p for p, _ in out]
     assert all(b >= a for a, b in zip(ps, ps[1:]))  # same random numbers, rising probabilities: never decreasing
+
+
+# The reference's initializer test lists for fault-tree inputs
+# (tests/initializer_tests.cc:181-296), minus the correct inputs that use
+# constructs this loader rejects by name (CCF groups, random deviates,
+# periodic tests).
+FTA_IN = Path("/root/reference/tests/input/fta")
+FTA_CORRECT = ["correct_tree_input.xml", "correct_formulas.xml", "constant_in_formulas.xml",
+               "component_definition.xml", "mixed_definitions.xml", "mixed_roles.xml",
+               "model_data_mixed_definitions.xml", "two_trees.xml", "two_top_events.xml",
+               "two_top_through_formula.xml", "orphan_primary_event.xml", "very_long_mcs.xml",
+               "unordered_structure.xml", "non_top_gate.xml", "unused_parameter.xml", "null_gate_with_label.xml",
+               "case_sensitivity.xml", "missing_bool_constant.xml", "correct_tree_input_with_probs.xml",
+               "trailing_spaces.xml", "flavored_types.xml"]
+FTA_UNSUPPORTED = {"mixed_references.xml": "CCF", "ccf_unordered_factors.xml": "CCF",
+                   "missing_ccf_level_number.xml": "CCF", "weibull_lnorm_deviate_2p.xml": "lognormal-deviate",
+                   "weibull_lnorm_deviate_3p.xml": "lognormal-deviate", "correct_expressions.xml": "periodic-test"}
+FTA_INCORRECT = ["invalid_probability.xml", "private_at_model_scope.xml", "doubly_defined_gate.xml",
+                 "doubly_defined_house.xml", "doubly_defined_basic.xml", "doubly_defined_parameter.xml",
+                 "doubly_defined_ccf_group.xml", "doubly_defined_component.xml", "extra_ccf_level_beta_factor.xml",
+                 "missing_gate_definition.xml", "missing_ccf_factor.xml", "missing_ccf_members.xml",
+                 "missing_arg_expression.xml", "undefined_event.xml", "undefined_basic_event.xml",
+                 "undefined_house_event.xml", "undefined_gate.xml", "undefined_parameter.xml",
+                 "reference_missing_fault_tree.xml", "reference_missing_component.xml", "wrong_parameter_unit.xml",
+                 "name_clash_two_trees.xml", "def_clash_basic_gate.xml", "def_clash_house_gate.xml",
+                 "def_clash_gate_primary.xml", "def_clash_basic_house.xml", "def_clash_house_basic.xml",
+                 "atleast_gate.xml", "invalid_min_max_cardinality.xml", "cyclic_tree.xml", "cyclic_formula.xml",
+                 "cyclic_parameter.xml", "cyclic_expression.xml", "invalid_expression.xml",
+                 "invalid_periodic_test_num_args.xml", "repeated_child.xml", "repeated_attribute.xml",
+                 "alpha_ccf_level_error.xml", "beta_ccf_level_error.xml", "mgl_ccf_level_error.xml",
+                 "phi_ccf_wrong_sum.xml", "ccf_negative_factor.xml", "ccf_more_factors_than_needed.xml",
+                 "ccf_wrong_distribution.xml", "repeated_ccf_members.xml", "duplicate_via_not.xml"]
+
+
+@pytest.mark.skipif(not FTA_IN.exists(), reason="the reference's fault-tree inputs are not on this machine")
+def test_reference_fault_tree_inputs_accepted_and_rejected():
+    for name in FTA_CORRECT:
+        mef.parse(FTA_IN / name)
+    for name, what in FTA_UNSUPPORTED.items():
+        with pytest.raises(mef.MefError, match=what):
+            mef.parse(FTA_IN / name)
+    for name in FTA_INCORRECT:
+        with pytest.raises(mef.MefError):
+            mef.parse(FTA_IN / name)

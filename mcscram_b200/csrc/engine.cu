@@ -53,6 +53,85 @@ cudaError_t upload(T **dptr, const std::vector<T> &v) {
 
 namespace {
 
+// Strip mode's gate program: the gates of each layer in groups of up to
+// kStripGroup that the kernel evaluates together (no gate of a group reads
+// another, so all their input loads can be in flight at once).  AND, OR,
+// NAND and NOR gates of at most kStripGroupMaxIn inputs and one-input NOT and
+// NULL gates take the OR form r = outinv ^ OR_i (x_i ^ flip_i) (De Morgan:
+// AND = ~OR(~x), NAND = OR(~x)); flip_i also carries the input's negation.
+// Within a layer they are sorted by fan-in so a group's slots are mostly
+// full.  Every other gate (XOR, ATLEAST, NOT/NULL of other fan-in, wider
+// gates) is a group of one evaluated by strip_gate.  Each group is two
+// uint4 records: its header and the output nodes of its gates.
+mcg_status build_strip_groups(mcg_engine *e, const std::vector<uint32_t> &order,
+                              const std::vector<uint2> &gate_tally) {
+    using mcg::dev::kStripGroup;
+    using mcg::dev::kStripGroupMaxIn;
+    using mcg::dev::kStripNoInput;
+    const mcg::Graph &g = e->graph;
+    if ((uint64_t)g.n_nodes() >= 0x7FFFFFFFull) return mcg::fail(MCG_ERR_INVALID, "strip mode: too many nodes");
+    std::vector<uint4> groups, ginfo;
+    std::vector<uint32_t> gin;
+    auto info = [&](uint32_t gi) { return make_uint4(g.n_be + gi, gate_tally[gi].x, gate_tally[gi].y, gi); };
+    auto or_form = [&](uint32_t gi) {
+        const uint8_t op = g.gate_op[gi];
+        const uint32_t n = g.gate_in_count[gi];
+        if (op == MCG_AND || op == MCG_OR || op == MCG_NAND || op == MCG_NOR) return n <= kStripGroupMaxIn;
+        return (op == MCG_NOT || op == MCG_NULL) && n == 1;
+    };
+    std::vector<uint32_t> eligible;
+    for (size_t l = 0; l + 1 < e->layer_offsets.size(); ++l) {
+        eligible.clear();
+        for (uint32_t q = e->layer_offsets[l]; q < e->layer_offsets[l + 1]; ++q) {
+            const uint32_t gi = order[q];
+            if (or_form(gi)) {
+                eligible.push_back(gi);
+            } else {
+                groups.push_back(make_uint4(1u | (1u << 24), 0u, (uint32_t)ginfo.size(), 0u));
+                groups.push_back(make_uint4(g.n_be + gi, 0u, 0u, 0u));
+                ginfo.push_back(info(gi));
+            }
+        }
+        std::stable_sort(eligible.begin(), eligible.end(),
+                         [&](uint32_t x, uint32_t y) { return g.gate_in_count[x] < g.gate_in_count[y]; });
+        for (size_t b = 0; b < eligible.size(); b += kStripGroup) {
+            const uint32_t cnt = (uint32_t)std::min<size_t>(kStripGroup, eligible.size() - b);
+            uint32_t maxn = 0, outinv = 0;
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const uint32_t gi = eligible[b + j];
+                const uint8_t op = g.gate_op[gi];
+                maxn = std::max(maxn, g.gate_in_count[gi]);
+                if (op == MCG_AND || op == MCG_NOR || op == MCG_NOT) outinv |= 1u << j;
+            }
+            groups.push_back(make_uint4(cnt | (maxn << 8), (uint32_t)gin.size(), (uint32_t)ginfo.size(), outinv));
+            uint32_t outs[kStripGroup] = {0u, 0u, 0u, 0u};
+            for (uint32_t j = 0; j < cnt; ++j) outs[j] = g.n_be + eligible[b + j];
+            groups.push_back(make_uint4(outs[0], outs[1], outs[2], outs[3]));
+            for (uint32_t s = 0; s < maxn; ++s) {
+                for (uint32_t j = 0; j < kStripGroup; ++j) {
+                    uint32_t rec = kStripNoInput;
+                    if (j < cnt) {
+                        const uint32_t gi = eligible[b + j];
+                        const uint32_t n = g.gate_in_count[gi];
+                        if (s < n) {
+                            const bool negated = s >= n - g.gate_neg_count[gi];
+                            const bool and_type = g.gate_op[gi] == MCG_AND || g.gate_op[gi] == MCG_NAND;
+                            rec = (g.inputs[g.gate_in_begin[gi] + s] << 1) | (uint32_t)(negated != and_type);
+                        }
+                    }
+                    gin.push_back(rec);
+                }
+            }
+            for (uint32_t j = 0; j < cnt; ++j) ginfo.push_back(info(eligible[b + j]));
+        }
+    }
+    e->n_strip_groups = (uint32_t)(groups.size() / 2);
+    MCG_CUDA(upload(&e->d_strip_groups, groups));
+    MCG_CUDA(upload(&e->d_strip_gin, gin));
+    MCG_CUDA(upload(&e->d_strip_ginfo, ginfo));
+    return MCG_OK;
+}
+
 mcg_status build_layered_tables(mcg_engine *e) {
     const mcg::Graph &g = e->graph;
     std::vector<uint4> be(g.n_be);
@@ -111,6 +190,10 @@ mcg_status build_layered_tables(mcg_engine *e) {
         gate_tally_list.insert(gate_tally_list.end(), per_gate[i].begin(), per_gate[i].end());
     }
     e->n_be_tally = (uint32_t)be_nodes.size();
+    if (e->mode == MCG_MODE_STRIP) {
+        mcg_status st = build_strip_groups(e, order, gate_tally);
+        if (st != MCG_OK) return st;
+    }
     MCG_CUDA(upload(&e->d_smeta, smeta));
     MCG_CUDA(upload(&e->d_gate_tally, gate_tally));
     MCG_CUDA(upload(&e->d_gate_tally_list, gate_tally_list));
@@ -309,6 +392,10 @@ mcg_status run_strip(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t w
     a.order = e->d_layer_gates;
     a.n_gates = g.n_gates;
     a.gate_tally = e->d_gate_tally;
+    a.groups = e->d_strip_groups;
+    a.n_groups = e->n_strip_groups;
+    a.gin = e->d_strip_gin;
+    a.ginfo = e->d_strip_ginfo;
     a.tally_list = e->d_gate_tally_list;
     a.be_tally_nodes = e->d_be_tally_nodes;
     a.be_tally_idx = e->d_be_tally_idx;
@@ -485,6 +572,9 @@ void release(mcg_engine *e) {
     cudaFree(e->d_stage[1]);
     cudaFree(e->d_strip_scratch);
     cudaFree(e->d_queue);
+    cudaFree(e->d_strip_groups);
+    cudaFree(e->d_strip_gin);
+    cudaFree(e->d_strip_ginfo);
     for (int i = 0; i < 2; ++i) {
         if (e->ev_snap[i]) cudaEventDestroy(e->ev_snap[i]);
     }

@@ -75,6 +75,10 @@ struct mcg_engine {
     // strip
     uint64_t *d_strip_scratch = nullptr;   // per warp n_nodes x 32 words
     unsigned long long *d_queue = nullptr; // strip counter
+    uint4 *d_strip_groups = nullptr;       // strip mode: gate groups, one layer at a time
+    uint32_t *d_strip_gin = nullptr;       // their inputs, slot-major, four records per slot
+    uint4 *d_strip_ginfo = nullptr;        // per grouped gate: output node, tally offset / count, gate id
+    uint32_t n_strip_groups = 0;
     uint32_t strip_grid = 0;
     uint32_t strip_smem = 0;               // tally counters in shared memory (0: global atomics)
     uint32_t strip_blocks = 6;             // resident blocks per SM the kernel is built for

@@ -494,6 +494,11 @@ struct StripArgs {
     const uint32_t *order;        // gate ids, layer by layer
     uint32_t n_gates;
     const uint2 *gate_tally;      // per gate {offset, count} into tally_list
+    const uint4 *groups;          // per group two records: {count | fan-in << 8 | single << 24, gin offset,
+                                  // ginfo offset, outinv} and the output nodes of its gates
+    uint32_t n_groups;
+    const uint32_t *gin;          // group inputs, slot-major, kStripGroup records per slot: node << 1 | flip
+    const uint4 *ginfo;           // per grouped gate: {output node, tally offset, tally count, gate id}
     const uint32_t *tally_list;
     const uint32_t *be_tally_nodes, *be_tally_idx;
     uint32_t n_be_tally;
@@ -509,6 +514,34 @@ __device__ __forceinline__ void strip_tally(const StripArgs &a, unsigned long lo
                                             uint32_t c) {
     if (a.tally_in_smem) atomicAdd(&s_ones[idx], (unsigned long long)c);
     else atomicAdd(&a.ones[idx], (unsigned long long)c);
+}
+
+// Gate groups of the strip kernel: up to kStripGroup gates of one layer
+// evaluated together in the OR form r = outinv ^ OR_i (x_i ^ flip_i); an
+// input record is node << 1 | flip, kStripNoInput an empty slot.
+constexpr uint32_t kStripGroup = 4;
+constexpr uint32_t kStripGroupMaxIn = 8;
+constexpr uint32_t kStripNoInput = 0xFFFFFFFFu;
+static_assert(kStripGroup == 4, "k_strip's group loop packs four gates' tallies into two reductions");
+
+__device__ __forceinline__ uint64_t strip_in(const uint64_t *col, uint32_t rec) {
+    uint64_t x = 0;
+    if (rec != kStripNoInput) {
+        x = col[(uint64_t)(rec >> 1) * kStripLanes];
+        if (rec & 1u) x = ~x;
+    }
+    return x;
+}
+
+// Tally of one gate word column: warp sum of the valid lanes' popcounts,
+// added by lane 0 to every tally slot of the node.
+__device__ __forceinline__ void strip_gate_tally(const StripArgs &a, unsigned long long *s_ones, const uint4 &f,
+                                                 uint64_t r, bool valid, uint32_t lane) {
+    if (f.z) {
+        const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, valid ? (uint32_t)__popcll(r) : 0u);
+        if (lane == 0 && c)
+            for (uint32_t j = 0; j < f.z; ++j) strip_tally(a, s_ones, a.tally_list[f.y + j], c);
+    }
 }
 
 // Bit-sliced count of up to 15 inputs (4 slices); count >= k for k <= 15.
@@ -634,16 +667,48 @@ __global__ void __launch_bounds__(kStripThreads, MINB) k_strip(StripArgs a) {
             const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, valid ? (uint32_t)__popcll(v) : 0u);
             if (lane == 0 && c) strip_tally(a, s_ones, a.be_tally_idx[j], c);
         }
+        // gates, layer by layer, a group at a time: no gate of a group reads
+        // another, so the loads of a whole group are in flight together and
+        // its outputs are stored after them
 #pragma unroll 1
-        for (uint32_t q = 0; q < a.n_gates; ++q) {
-            const uint32_t gi = a.order[q];
-            const uint64_t r = strip_gate(a, col, gi);
-            col[(uint64_t)(a.n_be + gi) * kStripLanes] = r;
-            const uint2 t = a.gate_tally[gi];
-            if (t.y) {
-                const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, valid ? (uint32_t)__popcll(r) : 0u);
-                if (lane == 0 && c)
-                    for (uint32_t j = 0; j < t.y; ++j) strip_tally(a, s_ones, a.tally_list[t.x + j], c);
+        for (uint32_t gq = 0; gq < a.n_groups; ++gq) {
+            const uint4 h = a.groups[2 * gq];
+            if (h.x >> 24) {
+                const uint4 f = a.ginfo[h.z];
+                const uint64_t r = strip_gate(a, col, f.w);
+                col[(uint64_t)f.x * kStripLanes] = r;
+                strip_gate_tally(a, s_ones, f, r, valid, lane);
+                continue;
+            }
+            const uint32_t cnt = h.x & 0xFFu, maxn = (h.x >> 8) & 0xFFFFu;
+            const uint4 *rec = reinterpret_cast<const uint4 *>(a.gin + h.y);
+            uint64_t acc[kStripGroup] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll 2
+            for (uint32_t sl = 0; sl < maxn; ++sl) {
+                const uint4 rr = rec[sl];
+                acc[0] |= strip_in(col, rr.x);
+                acc[1] |= strip_in(col, rr.y);
+                acc[2] |= strip_in(col, rr.z);
+                acc[3] |= strip_in(col, rr.w);
+            }
+            const uint4 out = a.groups[2 * gq + 1];
+            uint32_t pc[kStripGroup];
+#pragma unroll
+            for (uint32_t j = 0; j < kStripGroup; ++j) {
+                const uint64_t r = ((h.w >> j) & 1u) ? ~acc[j] : acc[j];
+                pc[j] = valid && j < cnt ? (uint32_t)__popcll(r) : 0u;
+                const uint32_t node = j == 0 ? out.x : j == 1 ? out.y : j == 2 ? out.z : out.w;
+                if (j < cnt) col[(uint64_t)node * kStripLanes] = r;
+            }
+            // tallies: two gates' warp sums (at most 32 x 64 each) per 32-bit
+            // reduction, then lane j adds gate j's sum to its tally slots
+            const uint32_t s01 = __reduce_add_sync(0xFFFFFFFFu, pc[0] | (pc[1] << 16));
+            const uint32_t s23 = __reduce_add_sync(0xFFFFFFFFu, pc[2] | (pc[3] << 16));
+            if (lane < cnt) {
+                const uint4 f = a.ginfo[h.z + lane];
+                const uint32_t c = ((lane < 2 ? s01 : s23) >> (16 * (lane & 1u))) & 0xFFFFu;
+                if (f.z && c)
+                    for (uint32_t t = 0; t < f.z; ++t) strip_tally(a, s_ones, a.tally_list[f.y + t], c);
             }
         }
     }

@@ -389,9 +389,6 @@ mcg_status run_strip(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_t w
     a.n_nodes = g.n_nodes();
     a.smeta = e->d_smeta;
     a.inputs = e->d_inputs;
-    a.order = e->d_layer_gates;
-    a.n_gates = g.n_gates;
-    a.gate_tally = e->d_gate_tally;
     a.groups = e->d_strip_groups;
     a.n_groups = e->n_strip_groups;
     a.gin = e->d_strip_gin;

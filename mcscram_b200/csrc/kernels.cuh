@@ -491,9 +491,6 @@ struct StripArgs {
     uint32_t n_be, n_nodes;
     const uint4 *smeta;           // per gate: op | k << 8 | nbits << 16, in_begin, in_count, neg_count
     const uint32_t *inputs;
-    const uint32_t *order;        // gate ids, layer by layer
-    uint32_t n_gates;
-    const uint2 *gate_tally;      // per gate {offset, count} into tally_list
     const uint4 *groups;          // per group two records: {count | fan-in << 8 | single << 24, gin offset,
                                   // ginfo offset, outinv} and the output nodes of its gates
     uint32_t n_groups;

@@ -265,6 +265,13 @@ def run_ua(args, rank: int, world: int, local: int) -> int:
     be_words = sum(t.n_be for t in mine) * args.ua_draws * args.ua_words
     gates = sum(t.n_gates for t in mine) * args.ua_draws * args.ua_words * 64
     kms = statistics.mean(ms)
+    # roofline: instance words per second (one launch per step) against the
+    # register-only sampler that shares its Philox calls as the batch does
+    from mcscram_b200 import _capi
+    share = int(info.get("instances_per_item", 1)) or 1
+    kernel = "k_fused_batch_k" if share > 1 else "k_fused_batch"
+    achieved = be_words / (kms * 1e-3)
+    peak = _capi.sampler_peak_shared(share, n_events=256, n_words=args.peak_words, repeats=3, device=local)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": gates / (kms * 1e-3) * world, "unit": UNIT, "n_gpus": world,
@@ -274,6 +281,11 @@ def run_ua(args, rank: int, world: int, local: int) -> int:
                                    f"lognormal draws (EF 3), {args.ua_words * 64} samples per instance",
                        "instances": len(mine) * args.ua_draws, "l2": "inputs > L2 per launch"},
             "sample_words_per_s": be_words / (kms * 1e-3) * world,
+            "roofline": {"bound": "int-alu", "kernel": kernel, "achieved": achieved / 1e9, "peak": peak / 1e9,
+                         "unit": "G instance-words/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"register-only sampler of the batch path ({share} instance(s) per Philox "
+                                        "evaluation, k_sampler_peak_shared) measured in this run",
+                         "work_unit": "instance word = one basic event's 64 draws of one instance"},
             "batch": info, "clocks": clk}), flush=True)
     return 0
 

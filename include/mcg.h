@@ -233,6 +233,12 @@ mcg_status mcg_run_fused_noalloc(const void *d_ops, uint64_t n_ops, uint32_t sme
  * store per thread).  The speed of light of the fused kernel. */
 mcg_status mcg_sampler_peak(int32_t device, uint64_t n_events, uint64_t n_words,
                             uint32_t repeats, double *words_per_second);
+/* The same for the sampler of batches that evaluate several instances of one
+ * tree per Philox call (uncertainty draws): `instances` (1 or 4) words per
+ * Philox evaluation, each against its own threshold, without the per-pass
+ * event table; the rate counts instance words. */
+mcg_status mcg_sampler_peak_shared(int32_t device, uint64_t n_events, uint64_t n_words, uint32_t repeats,
+                                   uint32_t instances, double *instance_words_per_second);
 
 /* Message for the last failure on the calling thread ("" if none). */
 const char *mcg_last_error(void);

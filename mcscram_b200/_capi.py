@@ -111,6 +111,8 @@ _SIGNATURES = {
     "mcg_launch_count": (C.c_int, [C.c_void_p, _u64p]),
     "mcg_time_runs": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
     "mcg_sampler_peak": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
+    "mcg_sampler_peak_shared": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32,
+                                          C.POINTER(C.c_double)]),
     "mcg_profile_sampler": (C.c_int, [C.c_void_p, C.c_int32]),
     "mcg_profile_sampler_read": (C.c_int, [C.c_void_p, _u64p, C.POINTER(C.c_double)]),
     "mcg_last_error": (C.c_char_p, []),
@@ -291,6 +293,16 @@ def sampler_peak(n_events: int = 256, n_words: int = 1 << 21, repeats: int = 5, 
     lib = load()
     r = C.c_double()
     check(lib.mcg_sampler_peak(device, n_events, n_words, repeats, C.byref(r)))
+    return float(r.value)
+
+
+def sampler_peak_shared(instances: int, n_events: int = 256, n_words: int = 1 << 21, repeats: int = 5,
+                        device: int = 0) -> float:
+    """Instance words per second of the register-only sampler of batches that
+    evaluate `instances` (1 or 4) instances per Philox evaluation."""
+    lib = load()
+    r = C.c_double()
+    check(lib.mcg_sampler_peak_shared(device, n_events, n_words, repeats, instances, C.byref(r)))
     return float(r.value)
 
 

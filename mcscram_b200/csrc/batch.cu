@@ -18,6 +18,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMulForm = 1;
 constexpr int kPackForm = 1;
+// Instances of one tree that differ only in thresholds (uncertainty draws)
+// share their Philox calls kShare at a time (k_fused_batch_k) unless a tree
+// has ATLEAST gates.
+constexpr uint32_t kShare = 4;
 
 #define MCG_CUDA(call)                                                                          \
     do {                                                                                        \
@@ -30,7 +34,14 @@ constexpr int kPackForm = 1;
 
 using BatchKernel = void (*)(mcg::dev::BatchArgs);
 
-BatchKernel batch_kernel(uint32_t ctas_per_sm) {
+BatchKernel batch_kernel(uint32_t ctas_per_sm, uint32_t share) {
+    if (share == kShare) {
+        switch (ctas_per_sm) {
+            case 2: return mcg::dev::k_fused_batch_k<kThreads, 2, kMulForm, kPackForm, kShare>;
+            case 3: return mcg::dev::k_fused_batch_k<kThreads, 3, kMulForm, kPackForm, kShare>;
+            default: return mcg::dev::k_fused_batch_k<kThreads, 4, kMulForm, kPackForm, kShare>;
+        }
+    }
     switch (ctas_per_sm) {
         case 2: return mcg::dev::k_fused_batch<kThreads, 2, kMulForm, kPackForm>;
         case 3: return mcg::dev::k_fused_batch<kThreads, 3, kMulForm, kPackForm>;
@@ -56,6 +67,7 @@ struct mcg_batch {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     uint32_t ctas_per_sm = 4;
+    uint32_t share = 1;  // instances per work item (kShare or 1)
     std::vector<mcg::Graph> trees;
     std::vector<uint32_t> tree_op_offset;
     uint32_t smem_slots = 0, max_global = 0, grid = 0, smem_bytes = 0;
@@ -71,6 +83,9 @@ struct mcg_batch {
     uint64_t *d_thr_off = nullptr;
     uint64_t *d_thr = nullptr;
     unsigned long long *d_ones = nullptr;
+    uint32_t *d_group_first = nullptr, *d_group_size = nullptr;
+    uint64_t cap_grp = 0, cap_grp2 = 0;
+    uint32_t n_groups = 0;
     // graph
     cudaGraphExec_t graph = nullptr;
     uint32_t g_instances = 0, g_iteration = 0;
@@ -92,6 +107,8 @@ void release(mcg_batch *b) {
     cudaFree(b->d_thr_off);
     cudaFree(b->d_thr);
     cudaFree(b->d_ones);
+    cudaFree(b->d_group_first);
+    cudaFree(b->d_group_size);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -105,7 +122,12 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
     if (b->ctas_per_sm < 2 || b->ctas_per_sm > 4) return mcg::fail(MCG_ERR_INVALID, "ctas_per_sm must be 2..4");
     const size_t cap = std::min<size_t>(prop.sharedMemPerBlockOptin,
                                         prop.sharedMemPerMultiprocessor / b->ctas_per_sm) - 1024;
-    uint32_t budget = (uint32_t)(cap / (kThreads * sizeof(uint64_t)));
+    b->share = kShare;
+    for (const auto &g : b->trees)
+        for (uint8_t op : g.gate_op)
+            if (op == MCG_ATLEAST) b->share = 1;
+    // a slot holds one word per instance of a work item
+    uint32_t budget = (uint32_t)(cap / (kThreads * sizeof(uint64_t) * b->share));
     if (run.smem_slots == MCG_SMEM_SLOTS_NONE) budget = 0;
     else if (run.smem_slots) budget = std::min(budget, run.smem_slots);
     std::vector<mcg::Op> all;
@@ -120,7 +142,7 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
     }
     if (all.size() >= 0xFFFFFFFFull) return mcg::fail(MCG_ERR_INVALID, "programs too large");
     b->total_ops = all.size();
-    b->smem_bytes = b->smem_slots * kThreads * (uint32_t)sizeof(uint64_t);
+    b->smem_bytes = b->smem_slots * b->share * kThreads * (uint32_t)sizeof(uint64_t);
     b->grid = (uint32_t)prop.multiProcessorCount * b->ctas_per_sm;
     b->scratch_stride = (uint64_t)b->grid * kThreads;
     MCG_CUDA(cudaMalloc((void **)&b->d_ops, all.size() * sizeof(mcg::Op)));
@@ -129,9 +151,10 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
     MCG_CUDA(cudaMemcpy(b->d_tree_off, b->tree_op_offset.data(), b->tree_op_offset.size() * sizeof(uint32_t),
                         cudaMemcpyHostToDevice));
     if (b->max_global)
-        MCG_CUDA(cudaMalloc((void **)&b->d_scratch, (size_t)b->max_global * b->scratch_stride * sizeof(uint64_t)));
+        MCG_CUDA(cudaMalloc((void **)&b->d_scratch,
+                            (size_t)b->max_global * b->share * b->scratch_stride * sizeof(uint64_t)));
     MCG_CUDA(cudaMalloc((void **)&b->d_queue, sizeof(unsigned int)));
-    MCG_CUDA(cudaFuncSetAttribute(batch_kernel(b->ctas_per_sm), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MCG_CUDA(cudaFuncSetAttribute(batch_kernel(b->ctas_per_sm, b->share), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)std::max<uint32_t>(b->smem_bytes, 1)));
     if (run.stream) {
         b->stream = (cudaStream_t)run.stream;
@@ -165,11 +188,14 @@ mcg_status capture(mcg_batch *b, uint32_t n_inst, uint32_t iteration, uint64_t w
     a.scratch_stride = b->scratch_stride;
     a.queue = b->d_queue;
     a.inst_ones = b->d_ones;
+    a.group_first = b->d_group_first;
+    a.group_size = b->d_group_size;
+    a.n_groups = b->n_groups;
     cudaGraph_t g = nullptr;
     MCG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), b->stream);
     cudaMemsetAsync(b->d_ones, 0, (size_t)n_inst * sizeof(unsigned long long), b->stream);
-    batch_kernel(b->ctas_per_sm)<<<b->grid, kThreads, b->smem_bytes, b->stream>>>(a);
+    batch_kernel(b->ctas_per_sm, b->share)<<<b->grid, kThreads, b->smem_bytes, b->stream>>>(a);
     const cudaError_t launch_err = cudaGetLastError();
     const cudaError_t end_err = cudaStreamEndCapture(b->stream, &g);
     if (launch_err != cudaSuccess || end_err != cudaSuccess) {
@@ -247,16 +273,34 @@ mcg_status mcg_batch_run(mcg_batch *b, uint32_t n_inst, const uint32_t *inst_tre
     }
     for (uint64_t k = 0; k < n_thr; ++k)
         if (thresholds[k] > (1ull << 32)) return mcg::fail(MCG_ERR_INVALID, "threshold above 2^32");
+    // groups of up to `share` consecutive instances of one tree
+    std::vector<uint32_t> gfirst, gsize;
+    for (uint32_t i = 0; i < n_inst;) {
+        uint32_t n = 1;
+        while (n < b->share && i + n < n_inst && inst_tree[i + n] == inst_tree[i]) ++n;
+        gfirst.push_back(i);
+        gsize.push_back(n);
+        i += n;
+    }
+    if ((uint64_t)gfirst.size() * slabs >= 0xFFFFFFFFull) return mcg::fail(MCG_ERR_INVALID, "too many work items");
     MCG_CUDA(cudaSetDevice(b->device));
-    const uint32_t *old_tree = b->d_inst_tree;
+    const uint32_t *old_tree = b->d_inst_tree, *old_gf = b->d_group_first, *old_gs = b->d_group_size;
     const uint64_t *old_off = b->d_thr_off, *old_thr = b->d_thr;
     const unsigned long long *old_ones = b->d_ones;
     MCG_CUDA(ensure(&b->d_inst_tree, b->cap_inst, n_inst));
     MCG_CUDA(ensure(&b->d_thr_off, b->cap_inst2, n_inst));
     MCG_CUDA(ensure(&b->d_thr, b->cap_thr, n_thr));
     MCG_CUDA(ensure(&b->d_ones, b->cap_ones, n_inst));
+    MCG_CUDA(ensure(&b->d_group_first, b->cap_grp, gfirst.size()));
+    MCG_CUDA(ensure(&b->d_group_size, b->cap_grp2, gsize.size()));
     const bool moved = old_tree != b->d_inst_tree || old_off != b->d_thr_off || old_thr != b->d_thr ||
-                       old_ones != b->d_ones;
+                       old_ones != b->d_ones || old_gf != b->d_group_first || old_gs != b->d_group_size ||
+                       b->n_groups != (uint32_t)gfirst.size();
+    b->n_groups = (uint32_t)gfirst.size();
+    MCG_CUDA(cudaMemcpyAsync(b->d_group_first, gfirst.data(), gfirst.size() * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, b->stream));
+    MCG_CUDA(cudaMemcpyAsync(b->d_group_size, gsize.data(), gsize.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             b->stream));
     MCG_CUDA(cudaMemcpyAsync(b->d_inst_tree, inst_tree, n_inst * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
     MCG_CUDA(cudaMemcpyAsync(b->d_thr_off, thr_offset, n_inst * sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
     MCG_CUDA(cudaMemcpyAsync(b->d_thr, thresholds, n_thr * sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
@@ -286,6 +330,7 @@ mcg_status mcg_batch_info_get(mcg_batch *b, mcg_batch_info *info) {
     info->total_ops = b->total_ops;
     info->launches = b->launches;
     info->last_kernel_ms = b->last_ms;
+    info->instances_per_item = b->share;
     return MCG_OK;
 }
 

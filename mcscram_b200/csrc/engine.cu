@@ -907,6 +907,40 @@ mcg_status mcg_sampler_peak(int32_t device, uint64_t n_events, uint64_t n_words,
     return MCG_OK;
 }
 
+mcg_status mcg_sampler_peak_shared(int32_t device, uint64_t n_events, uint64_t n_words, uint32_t repeats,
+                                   uint32_t instances, double *instance_words_per_second) {
+    mcg::clear_error();
+    if (!instance_words_per_second || n_events == 0 || n_words == 0 || repeats == 0 || n_events > 0xFFFFFFFFull ||
+        n_words > 0xFFFFFFFFull || (instances != 1 && instances != 4))
+        return mcg::fail(MCG_ERR_INVALID, "bad argument");
+    MCG_CUDA(cudaSetDevice(device));
+    uint64_t *sink = nullptr;
+    MCG_CUDA(cudaMalloc((void **)&sink, n_words * sizeof(uint64_t)));
+    auto launch = [&] {
+        const uint32_t blocks = (uint32_t)((n_words + 255) / 256);
+        if (instances == 4)
+            mcg::dev::k_sampler_peak_shared<kMulForm, kPackForm, 4><<<blocks, 256>>>((uint32_t)n_events, n_words, sink);
+        else
+            mcg::dev::k_sampler_peak_shared<kMulForm, kPackForm, 1><<<blocks, 256>>>((uint32_t)n_events, n_words, sink);
+    };
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    launch();  // warm-up
+    cudaEventRecord(a);
+    for (uint32_t r = 0; r < repeats; ++r) launch();
+    cudaEventRecord(b);
+    cudaError_t err = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (err != cudaSuccess) return mcg::fail(MCG_ERR_CUDA, cudaGetErrorString(err));
+    *instance_words_per_second = (double)n_events * (double)n_words * instances * repeats / (ms * 1e-3);
+    return MCG_OK;
+}
+
 mcg_status mcg_profile_sampler(mcg_engine *e, int32_t enable) {
     mcg::clear_error();
     if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");

@@ -206,6 +206,10 @@ struct BatchArgs {
     uint64_t scratch_stride;
     unsigned int *queue;               // next item; zero before the launch
     unsigned long long *inst_ones;
+    // k_fused_batch_k: groups of up to K consecutive instances of one tree
+    const uint32_t *group_first;
+    const uint32_t *group_size;
+    uint32_t n_groups;
 };
 
 template <int NT, int MINB, int MF, int PF>
@@ -231,6 +235,163 @@ __global__ void __launch_bounds__(NT, MINB) k_fused_batch(BatchArgs a) {
         auto add = [ones](uint32_t, uint32_t c) { atomicAdd(ones, (unsigned long long)c); };
         interpret<NT, MF, PF, true>(a.ops + a.tree_op_offset[a.inst_tree[inst]], ctx, t3, j < a.words_per_instance,
                                     my_slots, my_scratch, a.scratch_stride, a.thr + a.inst_thr_offset[inst], add);
+    }
+}
+
+// Slot planes of the K-wide interpreter: slot s of instance k at [s * K + k].
+template <int K>
+__device__ __forceinline__ uint64_t load_slot_k(uint32_t ref, int k, const uint64_t *my_slots,
+                                                const uint64_t *my_scratch, uint32_t nt, uint64_t stride) {
+    if (ref & kSlotGlobal) return my_scratch[((uint64_t)(ref & kSlotIndexMask) * K + k) * stride];
+    return my_slots[((uint32_t)ref * K + k) * nt];
+}
+
+template <int K>
+__device__ __forceinline__ void store_slot_k(uint32_t ref, int k, uint64_t v, uint64_t *my_slots,
+                                             uint64_t *my_scratch, uint32_t nt, uint64_t stride) {
+    if (ref == kNoSlot) return;
+    if (ref & kSlotGlobal) my_scratch[((uint64_t)(ref & kSlotIndexMask) * K + k) * stride] = v;
+    else my_slots[((uint32_t)ref * K + k) * nt] = v;
+}
+
+// The interpreter over K instances of one tree that differ only in their
+// thresholds (draws of an uncertainty analysis): every op acts on K words, a
+// basic event's 16 Philox calls run once and are compared with the K
+// instances' thresholds (thr[k][op.z]), so word k equals what interpret gives
+// instance k.  Programs with ATLEAST gates are not run here (the batch runs
+// them one instance at a time).  tally(k, count) is called by lane 0 with
+// instance k's warp popcount sum.
+template <int NT, int MF, int PF, int K, class Tally>
+__device__ __forceinline__ void interpret_k(const uint4 *__restrict__ ops, const WordCtx &ctx, uint32_t t3,
+                                            bool valid, uint64_t *my_slots, uint64_t *my_scratch, uint64_t stride,
+                                            const uint64_t *const *thr, Tally &&tally) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint64_t acc[K], last[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = last[k] = 0ull;
+    uint32_t conn = 0;
+    const uint4 *p = ops;
+    uint4 op = __ldg(p);
+    while (true) {
+        const uint4 nxt = __ldg(p + 1);
+        const uint32_t code = op.x & kOpMask;
+        if (code == kOpHalt) break;
+        uint64_t v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = 0ull;
+        if (code == kOpInBe || code == kOpBeDef) {
+            uint32_t t32[K];
+            uint32_t ones = 0, zeros = 0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const uint64_t t = thr[k][op.z];
+                t32[k] = (uint32_t)t;
+                if (t >= (1ull << 32)) {
+                    ones |= 1u << k;
+                    t32[k] = 1u;
+                } else if (t == 0) {
+                    zeros |= 1u << k;
+                    t32[k] = 1u;
+                }
+            }
+            if ((ones | zeros) != (1u << K) - 1u) be_words<MF, PF, K>(op.y, op.w, ctx, t3, t32, v);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if ((ones >> k) & 1u) v[k] = kAllOnes;
+                else if ((zeros >> k) & 1u) v[k] = 0ull;
+            }
+        } else if (code == kOpInSlot) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = load_slot_k<K>(op.y, k, my_slots, my_scratch, NT, stride);
+        } else if (code == kOpInConst || code == kOpConstDef) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = ((uint64_t)op.z << 32) | op.y;
+        }
+        if (code == kOpInBe || code == kOpInSlot || code == kOpInConst) {
+            if (op.x & kNegBit) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) v[k] = ~v[k];
+            }
+            switch (conn) {
+                case MCG_AND: case MCG_NAND:
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[k] &= v[k];
+                    break;
+                case MCG_OR: case MCG_NOR:
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[k] |= v[k];
+                    break;
+                case MCG_XOR:
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[k] ^= v[k];
+                    break;
+                default:  // NOT, NULL: the last input wins
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[k] = v[k];
+                    break;
+            }
+        } else if (code == kOpBeDef || code == kOpConstDef) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                last[k] = v[k];
+                store_slot_k<K>(op.x >> 8, k, last[k], my_slots, my_scratch, NT, stride);
+            }
+        } else if (code == kOpBegin) {
+            conn = (op.x >> 8) & 0xFFu;
+            const uint64_t init = (conn == MCG_AND || conn == MCG_NAND) ? kAllOnes : 0ull;
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = init;
+        } else if (code == kOpEnd) {
+            const bool inv = conn == MCG_NAND || conn == MCG_NOR || conn == MCG_NOT;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                last[k] = inv ? ~acc[k] : acc[k];
+                store_slot_k<K>(op.y, k, last[k], my_slots, my_scratch, NT, stride);
+            }
+        } else if (code == kOpTally) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, valid ? (uint32_t)__popcll(last[k]) : 0u);
+                if (lane == 0) tally((uint32_t)k, c);
+            }
+        }
+        op = nxt;
+        ++p;
+    }
+}
+
+// Batched instances K at a time: a work item is (group, slab), a group up to
+// K consecutive instances of one tree; missing members of a short group
+// repeat its first instance's thresholds and add nothing to any tally.
+template <int NT, int MINB, int MF, int PF, int K>
+__global__ void __launch_bounds__(NT, MINB) k_fused_batch_k(BatchArgs a) {
+    extern __shared__ __align__(16) uint64_t smem[];
+    __shared__ unsigned int s_item;
+    const uint32_t tid = threadIdx.x;
+    const uint64_t gtid = (uint64_t)blockIdx.x * NT + tid;
+    uint64_t *my_slots = smem + tid;
+    uint64_t *my_scratch = a.scratch + gtid;
+    const uint32_t t3 = (a.iteration + 1u) << 6;
+    const unsigned int n_items = a.n_groups * a.slabs_per_instance;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        const unsigned int item = s_item;
+        if (item >= n_items) break;
+        const uint32_t grp = item / a.slabs_per_instance;
+        const uint64_t j = (uint64_t)(item % a.slabs_per_instance) * NT + tid;
+        const uint32_t first = a.group_first[grp], n = a.group_size[grp];
+        const uint64_t *thr[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) thr[k] = a.thr + a.inst_thr_offset[first + ((uint32_t)k < n ? (uint32_t)k : 0u)];
+        const WordCtx ctx = make_word_ctx<MF>((uint32_t)j);
+        unsigned long long *ones = a.inst_ones + first;
+        auto add = [ones, n](uint32_t k, uint32_t c) {
+            if (k < n) atomicAdd(ones + k, (unsigned long long)c);
+        };
+        interpret_k<NT, MF, PF, K>(a.ops + a.tree_op_offset[a.inst_tree[first]], ctx, t3, j < a.words_per_instance,
+                                   my_slots, my_scratch, a.scratch_stride, thr, add);
     }
 }
 
@@ -729,6 +890,28 @@ __global__ void __launch_bounds__(256) k_sampler_peak(uint32_t n_events, uint64_
     for (uint32_t e = 0; e < n_events; ++e) {
         const uint32_t thr = 0x01000000u + (e * 0x9E3779B9u >> 8);  // spread of probabilities
         x ^= be_word_tab<MF, PF>(e + 1u, ctx, table + (uint64_t)e * kEventTableStride, thr);
+    }
+    sink[w] = x;
+}
+
+// Register-only sampler of the shared batch path: thread w generates words
+// (e, w) of K instances per Philox evaluation (be_words, the sampler the
+// batch interpreters call) and xors them together.
+template <int MF, int PF, int K>
+__global__ void __launch_bounds__(256) k_sampler_peak_shared(uint32_t n_events, uint64_t n_words,
+                                                             uint64_t *__restrict__ sink) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_words) return;
+    const WordCtx ctx = make_word_ctx<MF>((uint32_t)w);
+    uint64_t x = 0;
+    for (uint32_t e = 0; e < n_events; ++e) {
+        uint32_t thr[K];
+        uint64_t out[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) thr[k] = 0x01000000u + ((e * 0x9E3779B9u + (uint32_t)k * 0x7F4A7C15u) >> 8);
+        be_words<MF, PF, K>(e + 3u, e + 1u, ctx, 2u << 6, thr, out);
+#pragma unroll
+        for (int k = 0; k < K; ++k) x ^= out[k];
     }
     sink[w] = x;
 }

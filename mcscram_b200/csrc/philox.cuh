@@ -90,9 +90,14 @@ __device__ __forceinline__ uint32_t shift_in_ge(uint32_t acc, uint32_t o, uint32
 //   t3 = (iteration + 1) << 6, thr = threshold in [1, 2^32 - 1]
 //   (thresholds 0 and 2^32 give constant words and are handled by callers).
 // PackForm 0: compare-and-or nibbles; PackForm 1: carry-chain shift-in.
-template <int MulForm, int PackForm>
-__device__ __forceinline__ uint64_t be_word(uint32_t x0, uint32_t x1, const WordCtx &ctx, uint32_t t3,
-                                            uint32_t thr) {
+// be_words gives K such words from one set of Philox outputs: word k
+// compares every output with thr[k] (each in [1, 2^32 - 1]), so out[k] is
+// the word be_word gives for that threshold.  Instances that share a counter
+// stream but not their thresholds (draws of one tree) pay for the 16 Philox
+// calls once.
+template <int MulForm, int PackForm, int K>
+__device__ __forceinline__ void be_words(uint32_t x0, uint32_t x1, const WordCtx &ctx, uint32_t t3,
+                                         const uint32_t (&thr)[K], uint64_t (&out)[K]) {
     // Round 1, shared by the 16 calls.
     uint32_t ha, la;
     mul_hilo<MulForm>(kM0, x0, ha, la);
@@ -110,7 +115,9 @@ __device__ __forceinline__ uint64_t be_word(uint32_t x0, uint32_t x1, const Word
     mul_hilo<MulForm>(kM1, b2, hf, lf);
     const uint32_t c1 = lf;
 
-    uint32_t lo = 0, hi = 0;
+    uint32_t lo[K], hi[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) lo[k] = hi[k] = 0;
 #pragma unroll
     for (int g = 0; g < 16; ++g) {
         // Round 2, per call.
@@ -132,37 +139,52 @@ __device__ __forceinline__ uint64_t be_word(uint32_t x0, uint32_t x1, const Word
         philox_round<7, MulForm>(x0r, x1r, x2r, x3r);
         philox_round<8, MulForm>(x0r, x1r, x2r, x3r);
         philox_round<9, MulForm>(x0r, x1r, x2r, x3r);
-        if constexpr (PackForm == 0) {
-            const uint32_t nib = nibble_lt(x0r, x1r, x2r, x3r, thr);
-            if (g < 8) lo |= nib << (4 * g);
-            else hi |= nib << (4 * (g - 8));
-        } else {
-            // Each generation shifts four ">=" flags in from the right (x3 first),
-            // so generation g ends up at nibble 7 - (g % 8) of its half.
-            if (g < 8) {
-                lo = shift_in_ge(lo, x3r, thr);
-                lo = shift_in_ge(lo, x2r, thr);
-                lo = shift_in_ge(lo, x1r, thr);
-                lo = shift_in_ge(lo, x0r, thr);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if constexpr (PackForm == 0) {
+                const uint32_t nib = nibble_lt(x0r, x1r, x2r, x3r, thr[k]);
+                if (g < 8) lo[k] |= nib << (4 * g);
+                else hi[k] |= nib << (4 * (g - 8));
             } else {
-                hi = shift_in_ge(hi, x3r, thr);
-                hi = shift_in_ge(hi, x2r, thr);
-                hi = shift_in_ge(hi, x1r, thr);
-                hi = shift_in_ge(hi, x0r, thr);
+                // Each generation shifts four ">=" flags in from the right (x3
+                // first), so generation g ends up at nibble 7 - (g % 8) of its half.
+                if (g < 8) {
+                    lo[k] = shift_in_ge(lo[k], x3r, thr[k]);
+                    lo[k] = shift_in_ge(lo[k], x2r, thr[k]);
+                    lo[k] = shift_in_ge(lo[k], x1r, thr[k]);
+                    lo[k] = shift_in_ge(lo[k], x0r, thr[k]);
+                } else {
+                    hi[k] = shift_in_ge(hi[k], x3r, thr[k]);
+                    hi[k] = shift_in_ge(hi[k], x2r, thr[k]);
+                    hi[k] = shift_in_ge(hi[k], x1r, thr[k]);
+                    hi[k] = shift_in_ge(hi[k], x0r, thr[k]);
+                }
             }
         }
     }
-    if constexpr (PackForm == 0) {
-        return ((uint64_t)hi << 32) | (uint64_t)lo;
-    } else {
-        // The shift-in order put generation g at nibble (7 - g) of its half and
-        // stored ">=": reverse nibble order and complement.
-        auto rev_nibbles = [](uint32_t v) -> uint32_t {
-            v = ((v & 0x0F0F0F0Fu) << 4) | ((v >> 4) & 0x0F0F0F0Fu);
-            return __byte_perm(v, 0, 0x0123);
-        };
-        return ((uint64_t)(~rev_nibbles(hi)) << 32) | (uint64_t)(~rev_nibbles(lo));
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if constexpr (PackForm == 0) {
+            out[k] = ((uint64_t)hi[k] << 32) | (uint64_t)lo[k];
+        } else {
+            // The shift-in order put generation g at nibble (7 - g) of its half
+            // and stored ">=": reverse nibble order and complement.
+            auto rev_nibbles = [](uint32_t v) -> uint32_t {
+                v = ((v & 0x0F0F0F0Fu) << 4) | ((v >> 4) & 0x0F0F0F0Fu);
+                return __byte_perm(v, 0, 0x0123);
+            };
+            out[k] = ((uint64_t)(~rev_nibbles(hi[k])) << 32) | (uint64_t)(~rev_nibbles(lo[k]));
+        }
     }
+}
+
+template <int MulForm, int PackForm>
+__device__ __forceinline__ uint64_t be_word(uint32_t x0, uint32_t x1, const WordCtx &ctx, uint32_t t3,
+                                            uint32_t thr) {
+    const uint32_t t[1] = {thr};
+    uint64_t w[1];
+    be_words<MulForm, PackForm, 1>(x0, x1, ctx, t3, t, w);
+    return w[0];
 }
 
 // ---------------------------------------------------------------------------

@@ -28,7 +28,7 @@ _dp = C.POINTER(C.c_double)
 class BatchInfo(C.Structure):
     _fields_ = [("n_trees", C.c_uint32), ("smem_slots", C.c_uint32), ("max_global_slots", C.c_uint32),
                 ("grid_ctas", C.c_uint32), ("total_ops", C.c_uint64), ("launches", C.c_uint64),
-                ("last_kernel_ms", C.c_double)]
+                ("last_kernel_ms", C.c_double), ("instances_per_item", C.c_uint32)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

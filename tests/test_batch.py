@@ -6,7 +6,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from mcscram_b200 import synth
+from mcscram_b200 import mef, synth
 from mcscram_b200.graph import probability_threshold
 from tests.conftest import HAS_GPU
 from tests.program_emulator import emulate
@@ -61,6 +61,59 @@ def test_batch_instances_bit_exact(oracle_mod, gpu):
         assert int(ones[i]) == int(oracle_mod.tallies(g, 1, 1, 0, W)[0]), i
         assert int(ones3[i]) == int(oracle_mod.tallies(g, 2, 1, 0, W)[0]), i
     assert np.array_equal(ones, ones2)
+
+
+# negated event and gate inputs, NAND, NOR, XOR and a nested formula, no ATLEAST
+_NEGATIONS = """<opsa-mef><define-fault-tree name="n">
+<define-gate name="top"><or><gate name="a"/><gate name="b"/><not><basic-event name="e5"/></not></or></define-gate>
+<define-gate name="a"><nand><basic-event name="e1"/><not><basic-event name="e2"/></not><basic-event name="e3"/>
+</nand></define-gate>
+<define-gate name="b"><and><nor><basic-event name="e3"/><basic-event name="e4"/></nor>
+<xor><basic-event name="e1"/><not><gate name="a"/></not></xor><basic-event name="e6"/></and></define-gate>
+</define-fault-tree><model-data>""" + "".join(
+    f'<define-basic-event name="e{i}"><float value="0.{i}"/></define-basic-event>' for i in range(1, 7)) + \
+    "</model-data></opsa-mef>"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slots", [0xFFFFFFFF, 3, 0])
+def test_shared_draws_bit_exact(oracle_mod, gpu, slots):
+    """Trees without ATLEAST gates run up to four instances of one tree per
+    work item, sharing their Philox calls: groups longer than four, groups of
+    one, a tree coming back after another, thresholds 0 and 2^32 inside a
+    group and an instance whose every threshold is constant -- every instance
+    bit-exact against the oracle at its own thresholds."""
+    from mcscram_b200.graph import AND, NOT, OR, XOR
+    from mcscram_b200.uncertainty import Batch
+    rng = np.random.default_rng(23)
+    mix = {AND: 0.4, OR: 0.4, XOR: 0.1, NOT: 0.1}
+    trees = [synth.small_tree(s, n_be=40, n_gates=25, n_layers=5, mix=mix) for s in (3, 4, 5)]
+    trees = [t.with_tallies([t.root]) for t in trees] + [mef.load(_NEGATIONS)]
+    order = [0] * 6 + [1] + [0] * 2 + [2] * 5 + [1] * 4 + [3] * 7
+    inst_tree, thr = [], []
+    for i, t in enumerate(order):
+        th = probability_threshold(rng.uniform(0.02, 0.7, trees[t].n_be))
+        if i % 3 == 1:
+            th[0], th[5] = 0, 1 << 32
+        if i == 7:
+            th = np.where(rng.random(trees[t].n_be) < 0.5, 0, 1 << 32).astype(np.uint64)
+        inst_tree.append(t)
+        thr.append(th)
+    W = 2500
+    with Batch(trees, smem_slots=slots) as b:
+        assert b.info()["instances_per_item"] == 4
+        ones = b.run(inst_tree, thr, iteration=3, words_per_instance=W)
+    for i, (t, th) in enumerate(zip(inst_tree, thr)):
+        assert int(ones[i]) == int(oracle_mod.tallies(trees[t].with_thresholds(th), 3, 1, 0, W)[0]), i
+
+
+@pytest.mark.gpu
+def test_atleast_trees_run_one_instance_per_item(gpu):
+    from mcscram_b200.uncertainty import Batch
+    trees = [synth.small_tree(2, n_be=30, n_gates=18, n_layers=4)]
+    assert any(int(op) == 2 for op in trees[0].gate_op)  # ATLEAST present
+    with Batch([trees[0].with_tallies([trees[0].root])]) as b:
+        assert b.info()["instances_per_item"] == 1
 
 
 @pytest.mark.gpu

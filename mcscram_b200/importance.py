@@ -143,22 +143,31 @@ def approximate_importance(g: FlatGraph, root=None):
             vk = v[s_k]
             k = kk[gs][s_k]
             ck = c[s_k]
+            nk = vk.shape[0]
 
-            def tail_ge(vals, kth):
-                dist = np.zeros((vals.shape[0], m + 1))
-                dist[:, 0] = 1.0
-                for j in range(vals.shape[1]):
+            def count_dists(vals):
+                # F[j][:, t] = P(t of columns 0 .. j-1 fire), j = 0 .. m (padded columns have p = 0)
+                f = np.zeros((m + 1, nk, m + 1))
+                f[0][:, 0] = 1.0
+                for j in range(m):
                     x = vals[:, j][:, None]
-                    dist[:, 1:] = dist[:, 1:] * (1 - x) + dist[:, :-1] * x
-                    dist[:, 0] *= 1 - x[:, 0]
-                t = np.cumsum(dist[:, ::-1], axis=1)[:, ::-1]
-                kth = np.clip(kth, 0, m)
-                return np.where(kth <= m, t[np.arange(vals.shape[0]), kth], 0.0)
+                    f[j + 1] = f[j] * (1.0 - x)
+                    f[j + 1][:, 1:] += f[j][:, :-1] * x
+                return f
 
-            r[s_k] = np.where(k <= ck, tail_ge(vk, k), 0.0)
-            for j in range(m):  # P(count of others >= k - 1) - P(count of others >= k)
-                others = np.where(col[None, :] == j, 0.0, vk)
-                d[s_k, j] = np.where(k <= ck, tail_ge(others, k - 1) - tail_ge(others, k), 0.0)
+            fwd = count_dists(vk)
+            bwd = count_dists(vk[:, ::-1])  # bwd[i]: the last i columns
+            tail = np.cumsum(fwd[m][:, ::-1], axis=1)[:, ::-1]  # P(count >= t)
+            r[s_k] = np.where(k <= ck, tail[np.arange(nk), np.clip(k, 0, m)], 0.0)
+            # d P(count >= k) / d v_j = P(count of the others == k - 1): the
+            # columns before j (fwd[j]) and after it (bwd[m - 1 - j]) combined
+            a = np.arange(m + 1)
+            idx = (k - 1)[None, :, None] - a[None, None, :]
+            ok = (idx >= 0) & (idx <= m)
+            after = bwd[m - 1 - np.arange(m)]
+            picked = np.take_along_axis(after, np.broadcast_to(np.clip(idx, 0, m), after.shape), axis=2)
+            others_eq = np.sum(fwd[:m] * np.where(ok, picked, 0.0), axis=2)  # [m, nk]
+            d[s_k] = np.where((k <= ck)[:, None], others_eq.T, 0.0)
         s_l = (op == NOT) | (op == NULL)
         if s_l.any():
             last = np.maximum(c[s_l] - 1, 0)
@@ -212,7 +221,17 @@ def cut_set_eligible(g: FlatGraph) -> bool:
                 np.all(np.bincount(g.inputs, minlength=g.n_nodes) <= 1))
 
 
-def mode_proposals(g: FlatGraph, n_comp: int, cap: float) -> np.ndarray:
+def _mode_kids(g: FlatGraph) -> List[int]:
+    """Children of the top gate when it is an OR without complemented inputs
+    (the modes of mode_proposals), else none."""
+    from .graph import OR
+    top = g.root - g.n_be
+    if 0 <= top < g.n_gates and int(g.gate_op[top]) == OR and int(g.gate_neg_count[top]) == 0:
+        return [int(c) for c in g.gate_inputs(top)]
+    return []
+
+
+def mode_proposals(g: FlatGraph, n_comp: int, cap: float, approx=None) -> np.ndarray:
     """Defensive proposals for the union-of-modes form of the top event
     ([n_comp, n_be]).  When the top gate is an OR, component j is the
     approximate zero-variance proposal conditioned on its child j failing
@@ -221,14 +240,11 @@ def mode_proposals(g: FlatGraph, n_comp: int, cap: float) -> np.ndarray:
     the mixture form of importance sampling for a union of rare events.
     With more children than components the last component is the
     unconditioned proposal, and with fewer children (or a top gate that is
-    not an OR) components repeat.  Clipped to [1e-7, cap]."""
-    from .graph import OR
+    not an OR) components repeat.  Clipped to [1e-7, cap].  `approx` may pass
+    approximate_importance(g, root=[g.root] + _mode_kids(g)) computed already."""
     nb = g.n_be
-    top = g.root - nb
-    kids = []
-    if 0 <= top < g.n_gates and int(g.gate_op[top]) == OR and int(g.gate_neg_count[top]) == 0:
-        kids = [int(c) for c in g.gate_inputs(top)]
-    pr, cond = approximate_importance(g, root=[g.root] + kids)
+    kids = _mode_kids(g)
+    pr, cond = approx if approx is not None else approximate_importance(g, root=[g.root] + kids)
     cond = np.clip(cond, 1e-7, cap)
     whole = cond[0]
     if not kids:
@@ -243,7 +259,8 @@ def mode_proposals(g: FlatGraph, n_comp: int, cap: float) -> np.ndarray:
     return out
 
 
-def event_features(g: FlatGraph, instance_scale: Optional[float] = None, importance: bool = False) -> np.ndarray:
+def event_features(g: FlatGraph, instance_scale: Optional[float] = None, importance: bool = False,
+                   approx=None) -> np.ndarray:
     """16 features per basic event, float32 [n_be, 16]:
 
     0 log10 p (shifted), 1 fan-out, 2-3 min/max depth of the parents, 4-6
@@ -256,7 +273,8 @@ def event_features(g: FlatGraph, instance_scale: Optional[float] = None, importa
     is the parent gate of lowest index.  Computed for all events at once.
     importance=True replaces 11 and 12 with the independence-approximation
     inputs of approximate_importance: log10 of the first parent's
-    probability / 10 + 1 and log10 P~(x_i = 1 | top) / 4 + 1."""
+    probability / 10 + 1 and log10 P~(x_i = 1 | top) / 4 + 1; `approx` may pass
+    (node probabilities, conditional marginals given the top) computed already."""
     nb, ng = g.n_be, g.n_gates
     feats = np.zeros((nb, N_FEATURES), dtype=np.float32)
     feats[:, 15] = 1.0 if instance_scale is None else np.log10(max(instance_scale, 1.0)) / 6.0
@@ -333,7 +351,7 @@ def event_features(g: FlatGraph, instance_scale: Optional[float] = None, importa
     feats[:, 13] = np.where(has, up_and[q0s] / np.maximum(up_len[q0s] + 1, 1), 0.0)
     feats[:, 14] = np.where(has, up_or[q0s] / np.maximum(up_len[q0s] + 1, 1), 0.0)
     if importance:
-        pr, cond = approximate_importance(g)
+        pr, cond = approx if approx is not None else approximate_importance(g)
         pp = np.where(has, pr[np.where(has, q0s + nb, 0)], 1.0)
         feats[:, 11] = np.log10(np.clip(pp, 1e-30, 1.0)) / 10.0 + 1.0
         feats[:, 12] = np.log10(np.clip(cond, 1e-12, 1.0)) / 4.0 + 1.0
@@ -634,12 +652,21 @@ class BatchedIsResult:
 
 def _prepare_one(g: FlatGraph, n_modes: int, importance: bool):
     """Per-tree host inputs of the batched driver: features (the per-tree
-    input 15 filled in later) and the uncapped mode proposals."""
-    return event_features(g, instance_scale=1.0, importance=importance), mode_proposals(g, n_modes, 1.0)
+    input 15 filled in later) and the uncapped mode proposals, from one
+    independence-approximation pass conditioned on the top and on each mode."""
+    pr, cond = approximate_importance(g, root=[g.root] + _mode_kids(g))
+    return (event_features(g, instance_scale=1.0, importance=importance, approx=(pr, cond[0])),
+            mode_proposals(g, n_modes, 1.0, approx=(pr, cond)))
 
 
-def prepare_trees(graphs, n_modes: int = 4, importance: bool = True, workers: int = 0):
-    """_prepare_one for every tree, in `workers` spawned processes when > 1."""
+def prepare_trees(graphs, n_modes: int = 4, importance: bool = True, workers=0):
+    """_prepare_one for every tree, in `workers` spawned processes when > 1,
+    or on `workers` itself when it is an executor (a process pool kept across
+    calls, whose start-up is then not paid again)."""
+    if hasattr(workers, "map"):
+        n = getattr(workers, "_max_workers", 1) or 1
+        return list(workers.map(_prepare_one, graphs, [n_modes] * len(graphs), [importance] * len(graphs),
+                                chunksize=max(1, len(graphs) // (4 * n))))
     if workers and workers > 1 and len(graphs) > 1:
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
@@ -686,7 +713,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
                        importance_features: bool = True, tree_weighting: bool = True, fallback_after: int = 2,
                        cap_levels=(0.75, 0.9, 0.97, 0.99), confirm_rounds: int = 1,
                        defensive_proposal: str = "auto", n_modes: int = 4, min_words: int = 0,
-                       mode_cap: float = 0.5, workers: int = 0, prepared=None, log=None) -> BatchedIsResult:
+                       mode_cap: float = 0.5, workers=0, prepared=None, log=None) -> BatchedIsResult:
     """Learned importance sampling for a batch of rare-event trees.
 
     1. Probe: q = min(p * s_k, c_k) per tree, s_k x4 per round (x8 without

@@ -482,9 +482,13 @@ def config5(n_instances: int = 1024, seed: int = 5, workers: int = 0, first: int
     return config5_instances(range(first, first + n_instances), seed, workers)
 
 
-def config5_instances(ids, seed: int = 5, workers: int = 0) -> list:
-    """The batched rare-event instances with the given indices, in order."""
+def config5_instances(ids, seed: int = 5, workers=0) -> list:
+    """The batched rare-event instances with the given indices, in order;
+    `workers` > 1 spawned processes, or an executor to run them on."""
     ids = list(ids)
+    if hasattr(workers, "map"):
+        n = getattr(workers, "_max_workers", 1) or 1
+        return list(workers.map(config5_instance, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * n))))
     if workers and workers > 1 and len(ids) > 1:
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor

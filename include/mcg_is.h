@@ -58,7 +58,10 @@ mcg_status mcg_is_run(mcg_is *is, const uint64_t *q_threshold, uint32_t iteratio
  * entries, from 0 to n_be) and its top event is graph->tally_nodes[k]
  * (n_tally == n_tree); create rejects graphs where a gate reads two trees
  * or a tallied node is not in its tree.  Each tree gets its own likelihood
- * ratio (the C and a_i of its events) and its own sums. */
+ * ratio (the C and a_i of its events) and its own sums.  With
+ * run->layered_max_words = 0 a chunk holds at most 2^17 words (the staged
+ * engine's memory budget otherwise), since joined graphs are rebuilt as trees
+ * finish. */
 typedef struct mcg_is_batch mcg_is_batch;
 
 mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_tree, const uint32_t *be_begin,

@@ -455,6 +455,18 @@ struct mcg_is {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
+// Chunk size of the importance-sampling engines when the caller leaves it
+// at 0: the staged engine's budget (two chunk buffers of up to 24 GB each),
+// but at most 2^17 words per chunk.  A small tree would otherwise take
+// 2^20-word chunks of tens of GB that its calls never fill, and these
+// engines are created and destroyed as trees converge; large joined graphs
+// keep their budget-sized chunks (fewer, fuller launches).
+static void default_chunk(const mcg_graph_desc &graph, mcg_run_desc &run) {
+    if (run.layered_max_words) return;
+    const uint64_t nn = std::max<uint64_t>((uint64_t)graph.n_be + graph.n_gates, 1);
+    run.layered_max_words = std::min<uint64_t>(1ull << 17, std::max<uint64_t>(256, (24ull << 30) / (nn * 8)));
+}
+
 extern "C" {
 
 mcg_status mcg_is_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, mcg_is **out) {
@@ -465,6 +477,7 @@ mcg_status mcg_is_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in
     mcg_run_desc run{};
     if (run_in) run = *run_in;
     run.mode = MCG_MODE_STAGED;
+    default_chunk(*graph, run);
     auto is = std::make_unique<mcg_is>();
     mcg_status st = mcg_create(graph, &run, &is->engine);
     if (st != MCG_OK) return st;
@@ -673,6 +686,7 @@ mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_inst, con
     mcg_run_desc run{};
     if (run_in) run = *run_in;
     run.mode = MCG_MODE_STAGED;
+    default_chunk(*graph, run);
     auto b = std::unique_ptr<mcg_is_batch, void (*)(mcg_is_batch *)>(new mcg_is_batch, [](mcg_is_batch *x) {
         release_batch(x);
         delete x;

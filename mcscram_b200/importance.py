@@ -907,7 +907,11 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     words = est_words
     used = 0
     while active.size and used < max_est_words:
-        if not np.array_equal(members, active):
+        # the joined graph is rebuilt once the trees still running hold half
+        # of its events or fewer; until then finished trees ride along and
+        # their sums are left out
+        n_ev = np.diff(bb)
+        if not np.isin(active, members).all() or 2 * n_ev[active].sum() <= n_ev[members].sum():
             t1 = time.perf_counter()
             sampler.close()  # the joined graph of the trees left replaces it (and its device memory)
             sampler = BatchedImportanceSampler([graphs[k] for k in active], device=device, chunk_words=chunk_words)
@@ -922,19 +926,21 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         it += 1
         gpu["estimate"] += res["kernel_ms"]
         used += words
-        N[members] += res["samples"]
-        SW[members] += res["sum_w"]
-        SW2[members] += res["sum_w2"]
-        H[members] += res["hits"]
+        live = np.isin(members, active)
+        run_k = members[live]
+        N[run_k] += res["samples"]
+        SW[run_k] += res["sum_w"][live]
+        SW2[run_k] += res["sum_w2"][live]
+        H[run_k] += res["hits"][live]
         est, rel = _rel95(N, SW, SW2)
         ess = np.where(SW2 > 0, SW * SW / np.where(SW2 > 0, SW2, 1.0), 0.0)
         ok_now = (rel <= target_rel_err) & (ess >= ess_floor) & (N >= 64.0 * min_words)
-        streak[members] = np.where(ok_now[members], streak[members] + 1, 0)
+        streak[run_k] = np.where(ok_now[run_k], streak[run_k] + 1, 0)
         done = streak >= confirm_rounds
         # weight collapse: few effective samples among many hits after
         # `fallback_after` rounds -> plain sampling
-        rounds_in[members] += 1
-        first = members[(~checked[members]) & (rounds_in[members] >= fallback_after)]
+        rounds_in[run_k] += 1
+        first = run_k[(~checked[run_k]) & (rounds_in[run_k] >= fallback_after)]
         checked[first] = True
         bad = first[(H[first] > 0) & (ess[first] < collapse_ratio * H[first]) & ~done[first]]
         for k in bad:
@@ -943,7 +949,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             N[k] = SW[k] = SW2[k] = 0.0
             H[k] = 0
         converged |= done
-        rounds.append({"phase": "estimate", "words": words, "trees": int(members.size), "ms": res["kernel_ms"],
+        rounds.append({"phase": "estimate", "words": words, "trees": int(run_k.size), "ms": res["kernel_ms"],
                        "converged": int(converged.sum()), "fallback": int(fallback.sum())})
         say(rounds[-1])
         active = np.nonzero(~converged & ~(fallback & (N >= plain_words * 64)))[0]

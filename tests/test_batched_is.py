@@ -130,6 +130,54 @@ def test_approximate_importance_is_exact_on_trees(seed):
         np.testing.assert_allclose(cond_c, _cond_by_definition(g, child), rtol=1e-9, atol=1e-14)
 
 
+@pytest.mark.parametrize("n_be,n_gates,seed", [(40, 20, 7), (24, 12, 0), (24, 12, 1)])
+def test_approximate_importance_sensitivities_match_finite_differences(n_be, n_gates, seed):
+    """On DAGs with shared nodes and wide ATLEAST gates the independence pass
+    is an approximation, but its reverse-mode sensitivities must still be
+    the derivatives of its own P~_top: cond_i = p_i + p_i (1 - p_i) d log P~ / d p_i."""
+    from mcscram_b200.importance import approximate_importance
+    g = synth.small_tree(seed, n_be=n_be, n_gates=n_gates, n_layers=4, share_node_frac=0.3, atleast_n=(3, 6),
+                         p_range=(0.05, 0.6))
+    assert int((np.bincount(g.inputs, minlength=g.n_nodes) > 1).sum()) > 0  # a DAG, not a tree
+    assert int(((g.gate_op == ATLEAST) & (g.gate_in_count >= 5)).sum()) > 0
+    pr, cond = approximate_importance(g)
+    p = g.quantised_probabilities()
+    top = pr[g.root]
+    h = 1e-6
+    for i in range(g.n_be):
+        if not 0.0 < p[i] < 1.0:
+            continue
+        up, dn = p.copy(), p.copy()
+        up[i] += h
+        dn[i] -= h
+        pu = approximate_importance(_with_probabilities(g, up))[0][g.root]
+        pd = approximate_importance(_with_probabilities(g, dn))[0][g.root]
+        dlog = (pu - pd) / (2 * h) / top
+        assert cond[i] == pytest.approx(np.clip(p[i] + p[i] * (1 - p[i]) * dlog, 0, 1), rel=1e-5, abs=1e-8), i
+
+
+def _with_probabilities(g, p):
+    """The graph with basic-event probabilities p taken exactly (thresholds
+    p * 2^32 represent them to the precision the check needs)."""
+    out = g.with_thresholds(probability_threshold(p))
+    out.quantised_probabilities = lambda p=p: np.asarray(p, dtype=np.float64)
+    return out
+
+
+def test_prepare_trees_on_an_executor_equals_serial():
+    from concurrent.futures import ThreadPoolExecutor
+
+    from mcscram_b200.importance import prepare_trees
+    trees = [synth.config5_instance(i) for i in range(4)]
+    serial = prepare_trees(trees, 4, True, 0)
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        pooled = prepare_trees(trees, 4, True, ex)
+        made = synth.config5_instances([1, 3], workers=ex)
+    for (f0, m0), (f1, m1) in zip(serial, pooled):
+        assert np.array_equal(f0, f1) and np.array_equal(m0, m1)
+    assert np.array_equal(made[1].be_threshold, trees[3].be_threshold)
+
+
 def test_mode_proposals_condition_on_top_children():
     from mcscram_b200.importance import approximate_importance, mode_proposals
     g = synth.config5_instance(0)

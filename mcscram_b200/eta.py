@@ -28,11 +28,11 @@ import json
 import math
 from dataclasses import dataclass, field
 from pathlib import Path
-from typing import Dict, List, Optional, Sequence, Tuple, Union
+from typing import Dict, List, Optional, Tuple
 
 from . import _capi
 from .graph import AND, NULL, OR, FlatGraph
-from .mef import Expr, Formula, MefError, MefModel, Phase, parse
+from .mef import Expr, Formula, MefError, MefModel, parse
 
 TRUE_HOUSE = "__constant_true"
 

@@ -1,14 +1,11 @@
 """Batched instances and uncertainty analysis.  CPU: the variable-threshold
 program form; GPU: every instance bit-exact against the oracle with its own
 thresholds, and the uncertainty statistics."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
 from mcscram_b200 import mef, synth
 from mcscram_b200.graph import probability_threshold
-from tests.conftest import HAS_GPU
 from tests.program_emulator import emulate
 
 

@@ -11,7 +11,6 @@ import json
 import math
 from pathlib import Path
 
-import numpy as np
 import pytest
 
 from mcscram_b200 import eta, mef

@@ -6,7 +6,6 @@ disk -- its Aralia models against the exact values listed in its benchmark
 table.  The GPU test runs a loaded model through the engine."""
 import csv
 import itertools
-import os
 import xml.etree.ElementTree as ET
 from pathlib import Path
 

@@ -33,7 +33,8 @@ typedef struct mcg_batch_info {
     uint64_t launches;         /* kernel launches so far (graph replays count once each) */
     double last_kernel_ms;     /* duration of the last batched launch (CUDA events) */
     uint32_t instances_per_item; /* instances of one tree evaluated together, sharing their
-                                  * Philox calls (4; 1 when a tree has ATLEAST gates) */
+                                  * Philox calls (4; 1 when a tree has an ATLEAST gate of
+                                  * more than 15 inputs) */
 } mcg_batch_info;
 
 /* Compiles every tree (a flattened graph whose tally_nodes are the nodes to

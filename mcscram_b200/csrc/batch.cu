@@ -20,8 +20,10 @@ constexpr int kMulForm = 1;
 constexpr int kPackForm = 1;
 // Instances of one tree that differ only in thresholds (uncertainty draws)
 // share their Philox calls kShare at a time (k_fused_batch_k) unless a tree
-// has ATLEAST gates.
+// has an ATLEAST gate of more than kShareAtleastMaxIn inputs (the four-wide
+// interpreter counts ATLEAST inputs in four bit slices per instance).
 constexpr uint32_t kShare = 4;
+constexpr uint32_t kShareAtleastMaxIn = 15;
 
 #define MCG_CUDA(call)                                                                          \
     do {                                                                                        \
@@ -34,12 +36,19 @@ constexpr uint32_t kShare = 4;
 
 using BatchKernel = void (*)(mcg::dev::BatchArgs);
 
-BatchKernel batch_kernel(uint32_t ctas_per_sm, uint32_t share) {
+BatchKernel batch_kernel(uint32_t ctas_per_sm, uint32_t share, bool atleast) {
+    if (share == kShare && atleast) {
+        switch (ctas_per_sm) {
+            case 2: return mcg::dev::k_fused_batch_k<kThreads, 2, kMulForm, kPackForm, kShare, true>;
+            case 3: return mcg::dev::k_fused_batch_k<kThreads, 3, kMulForm, kPackForm, kShare, true>;
+            default: return mcg::dev::k_fused_batch_k<kThreads, 4, kMulForm, kPackForm, kShare, true>;
+        }
+    }
     if (share == kShare) {
         switch (ctas_per_sm) {
-            case 2: return mcg::dev::k_fused_batch_k<kThreads, 2, kMulForm, kPackForm, kShare>;
-            case 3: return mcg::dev::k_fused_batch_k<kThreads, 3, kMulForm, kPackForm, kShare>;
-            default: return mcg::dev::k_fused_batch_k<kThreads, 4, kMulForm, kPackForm, kShare>;
+            case 2: return mcg::dev::k_fused_batch_k<kThreads, 2, kMulForm, kPackForm, kShare, false>;
+            case 3: return mcg::dev::k_fused_batch_k<kThreads, 3, kMulForm, kPackForm, kShare, false>;
+            default: return mcg::dev::k_fused_batch_k<kThreads, 4, kMulForm, kPackForm, kShare, false>;
         }
     }
     switch (ctas_per_sm) {
@@ -68,6 +77,7 @@ struct mcg_batch {
     bool own_stream = false;
     uint32_t ctas_per_sm = 4;
     uint32_t share = 1;  // instances per work item (kShare or 1)
+    bool atleast = false; // the shared kernel needs its ATLEAST counters
     std::vector<mcg::Graph> trees;
     std::vector<uint32_t> tree_op_offset;
     uint32_t smem_slots = 0, max_global = 0, grid = 0, smem_bytes = 0;
@@ -124,8 +134,11 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
                                         prop.sharedMemPerMultiprocessor / b->ctas_per_sm) - 1024;
     b->share = kShare;
     for (const auto &g : b->trees)
-        for (uint8_t op : g.gate_op)
-            if (op == MCG_ATLEAST) b->share = 1;
+        for (size_t i = 0; i < g.gate_op.size(); ++i)
+            if (g.gate_op[i] == MCG_ATLEAST) {
+                if (g.gate_in_count[i] <= kShareAtleastMaxIn) b->atleast = true;
+                else b->share = 1;
+            }
     // a slot holds one word per instance of a work item
     uint32_t budget = (uint32_t)(cap / (kThreads * sizeof(uint64_t) * b->share));
     if (run.smem_slots == MCG_SMEM_SLOTS_NONE) budget = 0;
@@ -154,7 +167,7 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
         MCG_CUDA(cudaMalloc((void **)&b->d_scratch,
                             (size_t)b->max_global * b->share * b->scratch_stride * sizeof(uint64_t)));
     MCG_CUDA(cudaMalloc((void **)&b->d_queue, sizeof(unsigned int)));
-    MCG_CUDA(cudaFuncSetAttribute(batch_kernel(b->ctas_per_sm, b->share), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MCG_CUDA(cudaFuncSetAttribute(batch_kernel(b->ctas_per_sm, b->share, b->atleast), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)std::max<uint32_t>(b->smem_bytes, 1)));
     if (run.stream) {
         b->stream = (cudaStream_t)run.stream;
@@ -195,7 +208,7 @@ mcg_status capture(mcg_batch *b, uint32_t n_inst, uint32_t iteration, uint64_t w
     MCG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), b->stream);
     cudaMemsetAsync(b->d_ones, 0, (size_t)n_inst * sizeof(unsigned long long), b->stream);
-    batch_kernel(b->ctas_per_sm, b->share)<<<b->grid, kThreads, b->smem_bytes, b->stream>>>(a);
+    batch_kernel(b->ctas_per_sm, b->share, b->atleast)<<<b->grid, kThreads, b->smem_bytes, b->stream>>>(a);
     const cudaError_t launch_err = cudaGetLastError();
     const cudaError_t end_err = cudaStreamEndCapture(b->stream, &g);
     if (launch_err != cudaSuccess || end_err != cudaSuccess) {

@@ -24,6 +24,34 @@ namespace dev {
 constexpr uint64_t kAllOnes = ~0ull;
 
 // Bit-sliced 8-bit counters (mod 256, like the reference's uint8 count).
+// Bit-sliced count of up to 15 inputs (4 slices); count >= k for k <= 15.
+struct SlicedCount4 {
+    uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    __device__ __forceinline__ void add(uint64_t v) {
+        const uint64_t t = c0 & v;
+        c0 ^= v;
+        const uint64_t t1 = c1 & t;
+        c1 ^= t;
+        const uint64_t t2 = c2 & t1;
+        c2 ^= t1;
+        c3 ^= t2;
+    }
+    __device__ __forceinline__ uint64_t ge(uint32_t k) const {
+        const uint64_t c[4] = {c0, c1, c2, c3};
+        uint64_t gt = 0, eq = kAllOnes;
+#pragma unroll
+        for (int b = 3; b >= 0; --b) {
+            if ((k >> b) & 1u) {
+                eq &= c[b];
+            } else {
+                gt |= eq & c[b];
+                eq &= ~c[b];
+            }
+        }
+        return gt | eq;
+    }
+};
+
 struct SlicedCount {
     uint64_t c[8];
     __device__ __forceinline__ void clear() {
@@ -258,10 +286,11 @@ __device__ __forceinline__ void store_slot_k(uint32_t ref, int k, uint64_t v, ui
 // thresholds (draws of an uncertainty analysis): every op acts on K words, a
 // basic event's 16 Philox calls run once and are compared with the K
 // instances' thresholds (thr[k][op.z]), so word k equals what interpret gives
-// instance k.  Programs with ATLEAST gates are not run here (the batch runs
-// them one instance at a time).  tally(k, count) is called by lane 0 with
-// instance k's warp popcount sum.
-template <int NT, int MF, int PF, int K, class Tally>
+// instance k.  With ATL, ATLEAST gates of at most 15 inputs count in four
+// bit slices per instance; without it the program must have no ATLEAST gate
+// (the batch runs wider ones one instance at a time).  tally(k, count) is
+// called by lane 0 with instance k's warp popcount sum.
+template <int NT, int MF, int PF, int K, bool ATL, class Tally>
 __device__ __forceinline__ void interpret_k(const uint4 *__restrict__ ops, const WordCtx &ctx, uint32_t t3,
                                             bool valid, uint64_t *my_slots, uint64_t *my_scratch, uint64_t stride,
                                             const uint64_t *const *thr, Tally &&tally) {
@@ -269,7 +298,8 @@ __device__ __forceinline__ void interpret_k(const uint4 *__restrict__ ops, const
     uint64_t acc[K], last[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = last[k] = 0ull;
-    uint32_t conn = 0;
+    SlicedCount4 cnt[K];
+    uint32_t conn = 0, kk = 0;
     const uint4 *p = ops;
     uint4 op = __ldg(p);
     while (true) {
@@ -325,6 +355,12 @@ __device__ __forceinline__ void interpret_k(const uint4 *__restrict__ ops, const
 #pragma unroll
                     for (int k = 0; k < K; ++k) acc[k] ^= v[k];
                     break;
+                case MCG_ATLEAST:
+                    if constexpr (ATL) {
+#pragma unroll
+                        for (int k = 0; k < K; ++k) cnt[k].add(v[k]);
+                    }
+                    break;
                 default:  // NOT, NULL: the last input wins
 #pragma unroll
                     for (int k = 0; k < K; ++k) acc[k] = v[k];
@@ -338,14 +374,22 @@ __device__ __forceinline__ void interpret_k(const uint4 *__restrict__ ops, const
             }
         } else if (code == kOpBegin) {
             conn = (op.x >> 8) & 0xFFu;
+            kk = (op.x >> 16) & 0xFFu;
             const uint64_t init = (conn == MCG_AND || conn == MCG_NAND) ? kAllOnes : 0ull;
 #pragma unroll
             for (int k = 0; k < K; ++k) acc[k] = init;
+            if constexpr (ATL) {
+                if (conn == MCG_ATLEAST) {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) cnt[k] = SlicedCount4{};
+                }
+            }
         } else if (code == kOpEnd) {
             const bool inv = conn == MCG_NAND || conn == MCG_NOR || conn == MCG_NOT;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                last[k] = inv ? ~acc[k] : acc[k];
+                if (ATL && conn == MCG_ATLEAST) last[k] = kk > 15 ? 0ull : cnt[k].ge(kk);  // at most 15 inputs
+                else last[k] = inv ? ~acc[k] : acc[k];
                 store_slot_k<K>(op.y, k, last[k], my_slots, my_scratch, NT, stride);
             }
         } else if (code == kOpTally) {
@@ -363,7 +407,7 @@ __device__ __forceinline__ void interpret_k(const uint4 *__restrict__ ops, const
 // Batched instances K at a time: a work item is (group, slab), a group up to
 // K consecutive instances of one tree; missing members of a short group
 // repeat its first instance's thresholds and add nothing to any tally.
-template <int NT, int MINB, int MF, int PF, int K>
+template <int NT, int MINB, int MF, int PF, int K, bool ATL>
 __global__ void __launch_bounds__(NT, MINB) k_fused_batch_k(BatchArgs a) {
     extern __shared__ __align__(16) uint64_t smem[];
     __shared__ unsigned int s_item;
@@ -390,7 +434,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fused_batch_k(BatchArgs a) {
         auto add = [ones, n](uint32_t k, uint32_t c) {
             if (k < n) atomicAdd(ones + k, (unsigned long long)c);
         };
-        interpret_k<NT, MF, PF, K>(a.ops + a.tree_op_offset[a.inst_tree[first]], ctx, t3, j < a.words_per_instance,
+        interpret_k<NT, MF, PF, K, ATL>(a.ops + a.tree_op_offset[a.inst_tree[first]], ctx, t3, j < a.words_per_instance,
                                    my_slots, my_scratch, a.scratch_stride, thr, add);
     }
 }
@@ -702,33 +746,6 @@ __device__ __forceinline__ void strip_gate_tally(const StripArgs &a, unsigned lo
     }
 }
 
-// Bit-sliced count of up to 15 inputs (4 slices); count >= k for k <= 15.
-struct SlicedCount4 {
-    uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
-    __device__ __forceinline__ void add(uint64_t v) {
-        const uint64_t t = c0 & v;
-        c0 ^= v;
-        const uint64_t t1 = c1 & t;
-        c1 ^= t;
-        const uint64_t t2 = c2 & t1;
-        c2 ^= t1;
-        c3 ^= t2;
-    }
-    __device__ __forceinline__ uint64_t ge(uint32_t k) const {
-        const uint64_t c[4] = {c0, c1, c2, c3};
-        uint64_t gt = 0, eq = kAllOnes;
-#pragma unroll
-        for (int b = 3; b >= 0; --b) {
-            if ((k >> b) & 1u) {
-                eq &= c[b];
-            } else {
-                gt |= eq & c[b];
-                eq &= ~c[b];
-            }
-        }
-        return gt | eq;
-    }
-};
 
 __device__ __forceinline__ uint64_t strip_gate(const StripArgs &a, const uint64_t *col, uint32_t gi) {
     constexpr uint32_t kMaxIn = 8;

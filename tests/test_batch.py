@@ -104,13 +104,39 @@ def test_shared_draws_bit_exact(oracle_mod, gpu, slots):
         assert int(ones[i]) == int(oracle_mod.tallies(trees[t].with_thresholds(th), 3, 1, 0, W)[0]), i
 
 
+# an ATLEAST gate of 16 inputs: wider than the shared kernel's four-slice counters
+_WIDE_ATLEAST = ("<opsa-mef><define-fault-tree name='w'><define-gate name='top'><or>"
+                 "<atleast min='3'>" + "".join(f"<basic-event name='x{i}'/>" for i in range(16)) + "</atleast>"
+                 "<basic-event name='y'/></or></define-gate></define-fault-tree><model-data>" +
+                 "".join(f"<define-basic-event name='x{i}'><float value='0.{i % 9 + 1}'/></define-basic-event>"
+                         for i in range(16)) +
+                 "<define-basic-event name='y'><float value='0.01'/></define-basic-event></model-data></opsa-mef>")
+
+
 @pytest.mark.gpu
-def test_atleast_trees_run_one_instance_per_item(gpu):
+def test_atleast_widths_and_instances_per_item(oracle_mod, gpu):
+    """ATLEAST gates of up to 15 inputs run four draws per work item (counted
+    in four bit slices per draw); a wider one sends the batch back to one
+    draw per item.  Both bit-exact against the oracle."""
     from mcscram_b200.uncertainty import Batch
-    trees = [synth.small_tree(2, n_be=30, n_gates=18, n_layers=4)]
-    assert any(int(op) == 2 for op in trees[0].gate_op)  # ATLEAST present
-    with Batch([trees[0].with_tallies([trees[0].root])]) as b:
-        assert b.info()["instances_per_item"] == 1
+    rng = np.random.default_rng(5)
+    narrow = synth.small_tree(2, n_be=30, n_gates=18, n_layers=4)
+    assert any(int(op) == 2 for op in narrow.gate_op)  # ATLEAST present, 3-5 inputs
+    narrow = narrow.with_tallies([narrow.root])
+    wide = mef.load(_WIDE_ATLEAST)
+    for trees, per_item in (([narrow], 4), ([narrow, wide], 1)):
+        inst_tree = [t for t in range(len(trees)) for _ in range(5)]
+        thr = []
+        for i, t in enumerate(inst_tree):
+            th = probability_threshold(rng.uniform(0.05, 0.8, trees[t].n_be))
+            if i == 2:
+                th[0], th[-1] = 0, 1 << 32
+            thr.append(th)
+        with Batch(trees) as b:
+            assert b.info()["instances_per_item"] == per_item
+            ones = b.run(inst_tree, thr, iteration=2, words_per_instance=3000)
+        for i, (t, th) in enumerate(zip(inst_tree, thr)):
+            assert int(ones[i]) == int(oracle_mod.tallies(trees[t].with_thresholds(th), 2, 1, 0, 3000)[0]), (per_item, i)
 
 
 @pytest.mark.gpu

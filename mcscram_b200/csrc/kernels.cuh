@@ -747,7 +747,10 @@ __device__ __forceinline__ void strip_gate_tally(const StripArgs &a, unsigned lo
 }
 
 
-__device__ __forceinline__ uint64_t strip_gate(const StripArgs &a, const uint64_t *col, uint32_t gi) {
+// Not inlined: the one-gate path (ATLEAST counters, wide fan-in loops) then
+// keeps its registers to itself, and k_strip's sampler and gate groups spill
+// 36 bytes instead of 376 at 40 registers.
+static __device__ __noinline__ uint64_t strip_gate(const StripArgs &a, const uint64_t *col, uint32_t gi) {
     constexpr uint32_t kMaxIn = 8;
     const uint4 m = a.smeta[gi];
     const uint32_t op = m.x & 0xFFu, kk = (m.x >> 8) & 0xFFu, nbits = (m.x >> 16) & 0xFu;

@@ -308,7 +308,7 @@ def analyze(model: MefModel, settings=None, mode: int = _capi.MODE_STRIP, device
 
 def main(argv=None) -> int:
     """python -m mcscram_b200.eta MODEL.xml [MORE.xml ...] [--rel-err E] [--trials N]
-    [--mode strip|staged|fused]: event-tree analysis of a MEF model on the GPU;
+    [--mode strip|staged|fused] [--ccf]: event-tree analysis of a MEF model on the GPU;
     prints one JSON line per sequence (probability and 95 % interval) and per
     fault-tree top event."""
     import argparse
@@ -322,9 +322,10 @@ def main(argv=None) -> int:
     ap.add_argument("--mission-time", type=float, default=None)
     ap.add_argument("--mode", default="strip", choices=list(_capi.MODES))
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--ccf", action="store_true", help="expand common-cause groups (CCF analysis)")
     args = ap.parse_args(argv)
     kw = {} if args.mission_time is None else {"mission_time": args.mission_time}
-    m = parse([Path(x) for x in args.model], **kw)
+    m = parse([Path(x) for x in args.model], ccf_analysis=args.ccf, **kw)
     s = host.Settings.default(ci_rel_margin_error=args.rel_err)
     if args.trials:
         s = host.Settings.default(num_trials=int(args.trials), early_stop=0, ci_rel_margin_error=1e-9)

@@ -15,11 +15,14 @@ holding ``define-gate`` (formulas ``and``, ``or``, ``not``, ``xor``,
 87-91, 108-111), ``add``, ``sub``, ``mul``, ``div``, ``neg``, and the
 boolean ``not``, ``and``, ``or``, ``eq``, ``df``, ``lt``, ``gt``, ``leq``,
 ``geq``, ``ite``.  Event references are ``gate``, ``basic-event``,
-``house-event`` or the untyped ``event``.  Other expressions (random
-deviates, CCF groups, substitutions) are rejected with an error naming the
-element.  Probabilities are taken at a mission time (8760 hours unless
-given); ``probability_over_time`` evaluates the top event on a grid of
-mission times in one batched GPU pass.
+``house-event`` or the untyped ``event``.  ``define-CCF-group`` (beta
+factor, MGL, alpha factor and phi factor models) defines its members; with
+``ccf_analysis`` they are expanded into common-cause events
+(``ccf_level_probabilities``).  Other elements and expressions (random
+deviates, periodic tests, substitutions, extern functions) are rejected
+with an error naming the element.  Probabilities are taken at a mission
+time (8760 hours unless given); ``probability_over_time`` evaluates the top
+event on a grid of mission times in one batched GPU pass.
 
 Event trees (read here, analysed by ``mcscram_b200.eta``):
 ``define-initiating-event``, ``define-event-tree`` (functional events,
@@ -214,6 +217,24 @@ class Phase:
 
 
 @dataclass
+class CcfGroup:
+    """A common-cause failure group (mcSCRAM src/ccf_group.h): its members
+    (basic-event ids, defined by the group), their distribution Q and the
+    model's factors by level."""
+    name: str
+    model: str                      # beta-factor, MGL, alpha-factor, phi-factor
+    members: List[str]
+    member_names: List[str]
+    distribution: Expr
+    factors: List[Tuple[int, Expr]]  # (level, factor), levels ascending without gaps
+    base: str = ""
+    role: str = "public"
+
+
+_CCF_MIN_LEVEL = {"beta-factor": None, "MGL": 2, "alpha-factor": 1, "phi-factor": 1}  # beta: the member count
+
+
+@dataclass
 class MefModel:
     gates: Dict[str, Formula] = field(default_factory=dict)
     basic_events: Dict[str, Expr] = field(default_factory=dict)
@@ -227,6 +248,7 @@ class MefModel:
     sequences: Dict[str, list] = field(default_factory=dict)  # sequence -> instructions
     rules: Dict[str, list] = field(default_factory=dict)
     alignments: Dict[str, List[Phase]] = field(default_factory=dict)
+    ccf_groups: Dict[str, CcfGroup] = field(default_factory=dict)
 
     def probability(self, event: str, t: Optional[float] = None) -> float:
         """Probability of a basic event at mission time t (default: the model's)."""
@@ -669,11 +691,13 @@ def _document(source: Union[str, Path]) -> ET.Element:
 
 
 def parse(source: Union[str, Path, List[Union[str, Path]]],
-          mission_time: float = DEFAULT_MISSION_TIME) -> MefModel:
+          mission_time: float = DEFAULT_MISSION_TIME, ccf_analysis: bool = False) -> MefModel:
     """Reads a MEF document (a path, or the XML text itself) or several
     documents forming one model (a list; references may cross them);
     probabilities are evaluated at `mission_time` unless asked for at another
-    time."""
+    time.  With `ccf_analysis` the members of common-cause groups become OR
+    gates over their CCF events (SCRAM's --ccf); without it they are basic
+    events with the group's distribution, as in SCRAM."""
     roots = [_document(x) for x in (source if isinstance(source, (list, tuple)) else [source])]
     m = MefModel(mission_time=float(mission_time))
     scope = _Scope()
@@ -713,6 +737,8 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
                 ident = scope.register("parameter", name, base, _role(el, role))
                 m.parameters[ident] = _parse_expression(el, f"parameter {ident!r}")
                 expr_base.append((m.parameters[ident], base))
+            elif tag == "define-CCF-group":
+                define_ccf(el, base, _role(el, role))
             elif tag == "define-component":
                 if tree is None:
                     raise MefError("<define-component> outside a fault tree")
@@ -724,6 +750,56 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
                 continue
             else:
                 raise MefError(f"unsupported element <{tag}>")
+
+    def define_ccf(el: ET.Element, base: str, role: str):
+        """A CCF group with the checks of mcSCRAM src/ccf_group.cc:51-139."""
+        name, model = el.get("name"), el.get("model")
+        where = f"CCF group {name!r}"
+        if name in m.ccf_groups:
+            raise MefError(f"{where} defined twice")
+        if model not in _CCF_MIN_LEVEL:
+            raise MefError(f"{where}: unknown model {model!r}")
+        members, names, dist, factors = [], [], None, {}
+        prev = 0
+        for c in _kids(el):
+            tag = _local(c.tag)
+            if tag == "members":
+                for b in _kids(c):
+                    nm = b.get("name")
+                    if nm in names:
+                        raise MefError(f"{where}: member {nm!r} listed twice")
+                    names.append(nm)
+                    members.append(scope.register("basic-event", nm, base, role))
+            elif tag == "distribution":
+                dist = _parse_expression(c, where)
+            elif tag in ("factor", "factors"):
+                for f in ([c] if tag == "factor" else _kids(c)):
+                    n = len(members)
+                    min_level = n if model == "beta-factor" else _CCF_MIN_LEVEL[model]
+                    level = int(f.get("level")) if f.get("level") else (prev + 1 if prev else min_level)
+                    if level < min_level:
+                        raise MefError(f"{where}: factor level {level} below the minimum {min_level}")
+                    if level > n:
+                        raise MefError(f"{where}: factor level {level} above the {n} members")
+                    if level in factors:
+                        raise MefError(f"{where}: factor for level {level} defined twice")
+                    factors[level] = _parse_expression(f, where)
+                    prev = level
+            else:
+                raise MefError(f"{where}: unsupported element <{tag}>")
+        if len(members) < 2:
+            raise MefError(f"{where}: a CCF group needs at least 2 members")
+        if dist is None or not factors:
+            raise MefError(f"{where}: distribution and factors are required")
+        min_level = len(members) if model == "beta-factor" else _CCF_MIN_LEVEL[model]
+        if sorted(factors) != list(range(min_level, max(factors) + 1)):
+            raise MefError(f"{where}: missing CCF factors")
+        for mid in members:
+            m.basic_events[mid] = dist
+        expr_base.append((dist, base))
+        for f in factors.values():
+            expr_base.append((f, base))
+        m.ccf_groups[name] = CcfGroup(name, model, members, names, dist, sorted(factors.items()), base, role)
 
     def define_event_tree(el: ET.Element):
         name = el.get("name")
@@ -768,7 +844,8 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
             visit_data(el, name, "public", name)  # fault trees are public (src/fault_tree.h:128-130)
         elif tag == "model-data":
             visit_data(el, "", "public", None)
-        elif tag in ("define-gate", "define-basic-event", "define-house-event", "define-parameter"):
+        elif tag in ("define-gate", "define-basic-event", "define-house-event", "define-parameter",
+                     "define-CCF-group"):
             visit_data([el], "", "public", None)
         elif tag == "define-event-tree":
             define_event_tree(el)
@@ -848,6 +925,8 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
 
     for gid, f in m.gates.items():
         resolve(f, gate_base[gid], f"gate {gid!r}")
+    for grp in m.ccf_groups.values():
+        _check_ccf(m, grp)
 
     def resolve_instructions(ins, where: str):
         def fn(x):
@@ -890,7 +969,93 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
             raise MefError(f"initiating event {ie!r}: undefined event tree {tree!r}")
 
     _validate(m)
+    if ccf_analysis:
+        _expand_ccf(m)
     return m
+
+
+def _check_ccf(m: MefModel, grp: CcfGroup):
+    where = f"CCF group {grp.name!r}"
+    q = grp.distribution.value(m.mission_time, m.parameters)
+    if not 0.0 <= q <= 1.0:
+        raise MefError(f"{where}: distribution {q} is not a probability")
+    vals = [f.value(m.mission_time, m.parameters) for _, f in grp.factors]
+    if any(not 0.0 <= v <= 1.0 for v in vals):
+        raise MefError(f"{where}: factors {vals} are not all probabilities")
+    if grp.model == "phi-factor" and abs(sum(vals) - 1.0) > 1e-4:
+        raise MefError(f"{where}: phi factors sum to {sum(vals)}, not 1")
+
+
+def ccf_level_probabilities(grp: CcfGroup) -> List[Tuple[int, Expr]]:
+    """Probability expression of one CCF event of each level, by model
+    (mcSCRAM src/ccf_group.cc:178-297): beta factor (1 - b) Q and b Q; MGL
+    Q / C(n-1, i) times the factors of levels 2 .. i+1 and (1 - factor of
+    level i+2) below the top level; alpha factor (i+1) / C(n-1, i) * a_(i+1)
+    / sum_l l a_l * Q; phi factor f_l Q."""
+    n = len(grp.members)
+    q = grp.distribution
+    one = Expr("value", [1.0])
+    fs = [f for _, f in grp.factors]
+    levels = [lv for lv, _ in grp.factors]
+    if grp.model == "beta-factor":
+        return [(1, Expr("mul", [Expr("sub", [one, fs[0]]), q])), (levels[0], Expr("mul", [fs[0], q]))]
+    if grp.model == "phi-factor":
+        return [(lv, Expr("mul", [f, q])) for lv, f in grp.factors]
+    top = levels[-1]
+    out = []
+    if grp.model == "MGL":
+        for i in range(top):
+            args = [Expr("value", [1.0 / math.comb(n - 1, i)])] + fs[:i]
+            if i < top - 1:
+                args.append(Expr("sub", [one, fs[i]]))
+            out.append((i + 1, Expr("mul", args + [q])))
+        return out
+    total = Expr("add", [Expr("mul", [Expr("value", [float(lv)]), f]) for lv, f in grp.factors])
+    for i in range(top):
+        out.append((i + 1, Expr("mul", [Expr("value", [float(i + 1)]), Expr("value", [1.0 / math.comb(n - 1, i)]),
+                                        Expr("div", [fs[i], total]), q])))
+    return out
+
+
+def _expand_ccf(m: MefModel):
+    """CCF analysis (mcSCRAM src/ccf_group.cc:141-175): each member becomes
+    an OR gate, under the member's id, over the CCF events of every member
+    combination of every level that contains it; a CCF event \"[a b ...]\"
+    has the probability of its level."""
+    import itertools
+
+    as_gate = set()
+    for grp in m.ccf_groups.values():
+        args = {mid: [] for mid in grp.members}
+        for level, prob in ccf_level_probabilities(grp):
+            for combo in itertools.combinations(range(len(grp.members)), level):
+                nm = "[" + " ".join(grp.member_names[j] for j in combo) + "]"
+                ev = nm if grp.role == "public" or not grp.base else f"{grp.base}.{nm}"
+                if ev in m.basic_events or ev in m.gates:
+                    raise MefError(f"CCF event {ev!r} clashes with an element of that name")
+                m.basic_events[ev] = prob
+                for j in combo:
+                    args[grp.members[j]].append((False, "basic-event", ev))
+        for mid in grp.members:
+            del m.basic_events[mid]
+            m.gates[mid] = Formula(OR, args[mid])
+            as_gate.add(mid)
+
+    def retarget(f: Formula):
+        f.args = [(c, "gate" if k == "basic-event" and x in as_gate else k, x) if k != "formula" else (c, k, x)
+                  for c, k, x in f.args]
+        for _, k, x in f.args:
+            if k == "formula":
+                retarget(x)
+
+    for gid, f in m.gates.items():
+        if gid not in as_gate:
+            retarget(f)
+    for ins in list(m.sequences.values()) + list(m.rules.values()):
+        _walk_instructions(ins, lambda x: retarget(x[1]) if x[0] == "collect-formula" else None, {})
+    for et in m.event_trees.values():
+        for b in _branches_of(et):
+            _walk_instructions(b.instructions, lambda x: retarget(x[1]) if x[0] == "collect-formula" else None, {})
 
 
 def _branches_of(et: EventTree) -> List[Branch]:
@@ -1050,10 +1215,10 @@ def _check_homogeneous(m: MefModel, et: EventTree, b: Branch, where: str):
 
 
 def load(source: Union[str, Path], top: Optional[str] = None,
-         mission_time: float = DEFAULT_MISSION_TIME) -> FlatGraph:
+         mission_time: float = DEFAULT_MISSION_TIME, ccf_analysis: bool = False) -> FlatGraph:
     """MEF document -> flattened graph of its top gate (probabilities at the
     mission time), root tallied."""
-    return parse(source, mission_time).flat(top)
+    return parse(source, mission_time, ccf_analysis).flat(top)
 
 
 def probability_over_time(model: MefModel, time_step: float, top: Optional[str] = None,
@@ -1094,7 +1259,7 @@ def probability_over_time(model: MefModel, time_step: float, top: Optional[str] 
 
 
 def main(argv=None) -> int:
-    """python -m mcscram_b200.mef MODEL.xml [--top GATE] [--samples N] [--mode strip|staged|fused]:
+    """python -m mcscram_b200.mef MODEL.xml [--top GATE] [--samples N] [--mode strip|staged|fused] [--ccf]:
     estimates the top-event probability of a MEF model on the GPU and prints
     it with its 95 % interval as one JSON line."""
     import argparse
@@ -1109,8 +1274,9 @@ def main(argv=None) -> int:
     ap.add_argument("--samples", type=float, default=2 ** 30)
     ap.add_argument("--mode", default="strip", choices=list(_capi.MODES))
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--ccf", action="store_true", help="expand common-cause groups (CCF analysis)")
     args = ap.parse_args(argv)
-    g = load(args.model, args.top)
+    g = load(args.model, args.top, ccf_analysis=args.ccf)
     words = max(1, int(math.ceil(args.samples / 64)))
     with _capi.Engine(g, mode=_capi.MODES[args.mode], device=args.device) as e:
         done, it = 0, 1

@@ -6,6 +6,7 @@ disk -- its Aralia models against the exact values listed in its benchmark
 table.  The GPU test runs a loaded model through the engine."""
 import csv
 import itertools
+import math
 import xml.etree.ElementTree as ET
 from pathlib import Path
 
@@ -220,8 +221,7 @@ def test_probability_over_time_matches_oracle_per_time_point(oracle_mod, gpu):
 
 # The reference's initializer test lists for fault-tree inputs
 # (tests/initializer_tests.cc:181-296), minus the correct inputs that use
-# constructs this loader rejects by name (CCF groups, random deviates,
-# periodic tests).
+# constructs this loader rejects by name (random deviates, periodic tests).
 FTA_IN = Path("/root/reference/tests/input/fta")
 FTA_CORRECT = ["correct_tree_input.xml", "correct_formulas.xml", "constant_in_formulas.xml",
                "component_definition.xml", "mixed_definitions.xml", "mixed_roles.xml",
@@ -229,9 +229,9 @@ FTA_CORRECT = ["correct_tree_input.xml", "correct_formulas.xml", "constant_in_fo
                "two_top_through_formula.xml", "orphan_primary_event.xml", "very_long_mcs.xml",
                "unordered_structure.xml", "non_top_gate.xml", "unused_parameter.xml", "null_gate_with_label.xml",
                "case_sensitivity.xml", "missing_bool_constant.xml", "correct_tree_input_with_probs.xml",
-               "trailing_spaces.xml", "flavored_types.xml"]
-FTA_UNSUPPORTED = {"mixed_references.xml": "CCF", "ccf_unordered_factors.xml": "CCF",
-                   "missing_ccf_level_number.xml": "CCF", "weibull_lnorm_deviate_2p.xml": "lognormal-deviate",
+               "trailing_spaces.xml", "flavored_types.xml", "mixed_references.xml", "ccf_unordered_factors.xml",
+               "missing_ccf_level_number.xml"]
+FTA_UNSUPPORTED = {"weibull_lnorm_deviate_2p.xml": "lognormal-deviate",
                    "weibull_lnorm_deviate_3p.xml": "lognormal-deviate", "correct_expressions.xml": "periodic-test"}
 FTA_INCORRECT = ["invalid_probability.xml", "private_at_model_scope.xml", "doubly_defined_gate.xml",
                  "doubly_defined_house.xml", "doubly_defined_basic.xml", "doubly_defined_parameter.xml",
@@ -254,9 +254,92 @@ FTA_INCORRECT = ["invalid_probability.xml", "private_at_model_scope.xml", "doubl
 def test_reference_fault_tree_inputs_accepted_and_rejected():
     for name in FTA_CORRECT:
         mef.parse(FTA_IN / name)
+        mef.parse(FTA_IN / name, ccf_analysis=True)
     for name, what in FTA_UNSUPPORTED.items():
         with pytest.raises(mef.MefError, match=what):
             mef.parse(FTA_IN / name)
     for name in FTA_INCORRECT:
         with pytest.raises(mef.MefError):
             mef.parse(FTA_IN / name)
+
+
+CCF_FIX = Path(__file__).parent / "golden" / "mef" / "ccf.xml"
+
+
+def _ccf_fixture_exact(ccf: bool) -> float:
+    """P(top) of the CCF fixture by enumeration.  With CCF analysis the
+    independent events are the common-cause events of the published models,
+    written out here: alpha factor (non-staggered testing) Q_k = k /
+    C(n-1, k-1) * a_k / sum_l l a_l * Q, beta factor (1 - b) Q for one valve
+    and b Q for both; a member fails when any event that contains it does."""
+    q = lambda p: math.floor(p * TWO32) / TWO32  # the sampler's quantised probability
+    Qp, a = 0.05, {1: 0.8, 2: 0.15, 3: 0.05}
+    at = sum(k * v for k, v in a.items())
+    Qv, beta = 0.02, 0.1
+    if ccf:
+        events = {}
+        for k in (1, 2, 3):
+            for combo in itertools.combinations((1, 2, 3), k):
+                events[("p",) + combo] = k / math.comb(2, k - 1) * a[k] / at * Qp
+        events[("v", 1)] = events[("v", 2)] = (1 - beta) * Qv
+        events[("v", 1, 2)] = beta * Qv
+    else:
+        events = {("p", 1): Qp, ("p", 2): Qp, ("p", 3): Qp, ("v", 1): Qv, ("v", 2): Qv}
+    events[("power",)] = 0.01
+    names = list(events)
+    total = 0.0
+    for bits in itertools.product([False, True], repeat=len(names)):
+        x = dict(zip(names, bits))
+        w = math.prod(q(events[n]) if b else 1 - q(events[n]) for n, b in zip(names, bits))
+        pump = {i: any(v for n, v in x.items() if n[0] == "p" and i in n[1:]) for i in (1, 2, 3)}
+        valve = {i: any(v for n, v in x.items() if n[0] == "v" and i in n[1:]) for i in (1, 2)}
+        top = ((pump[1] or valve[1]) and (pump[2] or valve[2])) or (pump[3] and x[("power",)])
+        total += w * top
+    return total
+
+
+@pytest.mark.parametrize("ccf", [False, True])
+def test_ccf_fixture_exact(oracle_mod, ccf):
+    g = mef.load(CCF_FIX, ccf_analysis=ccf)
+    assert oracle_mod.bdd_probability(g) == pytest.approx(_ccf_fixture_exact(ccf), rel=1e-9)
+    m = mef.parse(CCF_FIX, ccf_analysis=ccf)
+    assert ("[pump1 pump2 pump3]" in m.basic_events) == ccf and ("pump1" in m.gates) == ccf
+
+
+def test_ccf_errors():
+    grp = ("<opsa-mef><define-fault-tree name='f'><define-gate name='t'><and><basic-event name='a'/>"
+           "<basic-event name='b'/></and></define-gate><define-CCF-group name='g' model='{model}'><members>"
+           "<basic-event name='a'/><basic-event name='b'/></members><distribution><float value='0.1'/>"
+           "</distribution>{factors}</define-CCF-group></define-fault-tree></opsa-mef>")
+    cases = [("MGL", "<factor level='1'><float value='0.1'/></factor>", "below the minimum"),
+             ("alpha-factor", "<factor level='3'><float value='0.1'/></factor>", "above the 2 members"),
+             ("phi-factor", "<factors><factor><float value='0.5'/></factor><factor><float value='0.4'/></factor>"
+                            "</factors>", "sum to"),
+             ("alpha-factor", "<factor level='2'><float value='0.1'/></factor>", "missing CCF factors"),
+             ("gamma", "<factor level='2'><float value='0.1'/></factor>", "unknown model")]
+    for model, factors, msg in cases:
+        with pytest.raises(mef.MefError, match=msg):
+            mef.parse(grp.format(model=model, factors=factors))
+
+
+CORE_IN = Path("/root/reference/tests/input/core")
+
+
+@pytest.mark.skipif(not CORE_IN.exists(), reason="the reference's core inputs are not on this machine")
+@pytest.mark.parametrize("name,expect", [("beta_factor_ccf.xml", 0.04308), ("phi_factor_ccf.xml", 0.04104),
+                                         ("mgl_ccf.xml", 0.01630), ("alpha_factor_ccf.xml", 0.05298)])
+def test_reference_ccf_models(oracle_mod, name, expect):
+    """The exact top-event probabilities the reference's tests expect with CCF
+    analysis on (tests/bench_core_tests.cc:452-527, to their 1e-5)."""
+    g = mef.load(CORE_IN / name, ccf_analysis=True)
+    assert oracle_mod.bdd_probability(g) == pytest.approx(expect, abs=1e-5)
+
+
+@pytest.mark.gpu
+def test_ccf_model_through_the_engine(oracle_mod, gpu):
+    from mcscram_b200 import _capi
+    g = mef.load(CCF_FIX, ccf_analysis=True)
+    with _capi.Engine(g, mode=_capi.MODE_STRIP) as e:
+        e.run(2, 1, 0, 1 << 14)
+        ones, total = e.tallies()
+    assert int(ones[0]) == int(oracle_mod.tallies(g, 2, 1, 0, 1 << 14)[0])

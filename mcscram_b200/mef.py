@@ -12,15 +12,21 @@ holding ``define-gate`` (formulas ``and``, ``or``, ``not``, ``xor``,
 ``float``, ``int``, ``bool``, ``pi``, ``parameter``,
 ``system-mission-time``, ``exponential`` (1 - exp(-lambda t)), ``GLM`` and
 ``Weibull`` (the formulas of mcSCRAM src/expression/exponential.cc:37-38,
-87-91, 108-111), ``add``, ``sub``, ``mul``, ``div``, ``neg``, and the
+87-91, 108-111), ``periodic-test`` (4, 5 and 11 arguments), ``add``,
+``sub``, ``mul``, ``div``, ``neg``, the numeric built-ins (``abs``, ``exp``,
+``log``, ``log10``, ``sqrt``, ``pow``, ``mod``, ``min``, ``max``, ``mean``,
+``ceil``, ``floor`` and the trigonometric and hyperbolic functions), the
 boolean ``not``, ``and``, ``or``, ``eq``, ``df``, ``lt``, ``gt``, ``leq``,
-``geq``, ``ite``.  Event references are ``gate``, ``basic-event``,
+``geq``, ``ite``, ``switch``, and the random deviates (``uniform-``,
+``normal-``, ``lognormal-``, ``gamma-`` and ``beta-deviate``,
+``histogram``), which stand for their means in point values and are drawn
+once per trial by ``sample_expressions`` / ``uncertainty``.  Event references are ``gate``, ``basic-event``,
 ``house-event`` or the untyped ``event``.  ``define-CCF-group`` (beta
 factor, MGL, alpha factor and phi factor models) defines its members; with
 ``ccf_analysis`` they are expanded into common-cause events
-(``ccf_level_probabilities``).  Other elements and expressions (random
-deviates, periodic tests, substitutions, extern functions) are rejected
-with an error naming the element.  Probabilities are taken at a mission
+(``ccf_level_probabilities``).  Other elements and expressions
+(substitutions, extern functions and libraries) are rejected with an error
+naming the element.  Probabilities are taken at a mission
 time (8760 hours unless given); ``probability_over_time`` evaluates the top
 event on a grid of mission times in one batched GPU pass.
 
@@ -119,7 +125,16 @@ class Expr:
         if op == "ite":
             branch = a[1] if a[0].value(t, params, context, _depth + 1) else a[2]
             return branch.value(t, params, context, _depth + 1)
+        if op == "switch":
+            for i in range(0, len(a) - 1, 2):
+                if a[i].value(t, params, context, _depth + 1):
+                    return a[i + 1].value(t, params, context, _depth + 1)
+            return a[-1].value(t, params, context, _depth + 1)
         v = [x.value(t, params, context, _depth + 1) for x in a]
+        if op in _DEVIATES:  # a random deviate stands for its mean (mcSCRAM src/expression/random_deviate.h)
+            return _deviate_mean(op, v)
+        if op == "periodic-test":
+            return periodic_test(*v)
         if op == "exponential":  # 1 - exp(-lambda t)
             return 1.0 - math.exp(-v[0] * v[1])
         if op == "GLM":  # gamma, lambda, mu, t
@@ -142,6 +157,18 @@ class Expr:
             return out
         if op == "neg":
             return -v[0]
+        if op in _UNARY:
+            return float(_UNARY[op](v[0]))
+        if op == "pow":
+            return v[0] ** v[1]
+        if op == "mod":  # integer remainder, truncated like C++'s % on ints
+            return float(int(math.fmod(int(v[0]), int(v[1]))))
+        if op == "min":
+            return min(v)
+        if op == "max":
+            return max(v)
+        if op == "mean":
+            return sum(v) / len(v)
         if op == "not":
             return float(not v[0])
         if op == "and":
@@ -162,6 +189,114 @@ class Expr:
         if self.op in ("value", "test-initiating-event", "test-functional-event"):
             return False
         return any(x.depends_on_time(params, _depth + 1) for x in self.args)
+
+
+_DEVIATES = ("uniform-deviate", "normal-deviate", "lognormal-deviate", "gamma-deviate", "beta-deviate", "histogram")
+
+
+def _deviate_mean(op: str, v: list) -> float:
+    if op == "uniform-deviate":
+        return (v[0] + v[1]) / 2
+    if op == "normal-deviate":
+        return v[0]
+    if op == "lognormal-deviate":  # (mean, error factor, level) or (mu, sigma) of the logarithm
+        return v[0] if len(v) == 3 else math.exp(v[0] + v[1] ** 2 / 2)
+    if op == "gamma-deviate":  # shape k, scale theta
+        return v[0] * v[1]
+    if op == "beta-deviate":
+        return v[0] / (v[0] + v[1])
+    bounds, weights = [v[0]] + v[1::2], v[2::2]  # histogram: lower bound, then (upper, weight) per bin
+    return sum((bounds[i] + bounds[i + 1]) * w for i, w in enumerate(weights)) / (2 * sum(weights))
+
+
+def _p_fail(rate: float, t: float) -> float:
+    return 1.0 - math.exp(-rate * t)
+
+
+def _p_second(p_first: float, p_second: float, first: float, second: float, t: float) -> float:
+    """Probability that the second of two Poisson processes, started when the
+    first (rate `first`) occurs, has occurred by t (rate `second`)."""
+    if first == second:
+        return p_second - (1.0 - p_second) * second * t
+    return (second * p_first - first * p_second) / (second - first)
+
+
+def periodic_test(*v) -> float:
+    """Unavailability of a periodically tested component at time t, the MEF
+    periodic-test (mcSCRAM src/expression/exponential.cc:113-330):
+    (lambda, tau, theta, t) with instant test and repair;
+    (lambda, mu, tau, theta, t) with instant test and repair at rate mu;
+    (lambda, lambda_test, mu, tau, theta, gamma, test_duration,
+    available_at_test, sigma, omega, t) with a test phase of its own.  The
+    first test is at theta, then every tau."""
+    if len(v) == 4:
+        lam, tau, theta, t = v
+        if t <= theta:
+            return _p_fail(lam, t)
+        delta = t - theta
+        after = delta - int(delta / tau) * tau
+        return _p_fail(lam, after if after else tau)
+    if len(v) == 5:
+        lam, mu, tau, theta, t = v
+        if t <= theta:
+            return _p_fail(lam, t)
+
+        def keep(pl, pm, dt):  # state carried through dt: still failed, or failed and not yet repaired
+            return 1.0 - pm + _p_second(pl, pm, lam, mu, dt) - pl
+
+        delta = t - theta
+        n = int(delta / tau)
+        frac = keep(_p_fail(lam, tau), _p_fail(mu, tau), tau)
+        geo = frac ** n
+        prob = _p_fail(lam, theta) * geo + _p_fail(lam, tau) * (geo - 1.0) / (frac - 1.0)
+        after = delta - n * tau
+        pl, pm = _p_fail(lam, after), _p_fail(mu, after)
+        return prob * keep(pl, pm, after) + pl
+    lam, lam_test, mu, tau, theta, gamma, dur, avail_at_test, sigma, omega, t = v
+    if t <= theta:
+        return _p_fail(lam, t)
+    state = {"fail": _p_fail(lam, theta), "repair": 0.0}
+    state["avail"] = 1.0 - state["fail"]
+
+    def repaired_then_failed(pm, pl, dt):
+        return pm * omega + (1.0 - omega) * _p_second(pm, pl, mu, lam, dt)
+
+    def test_phase(pl_test, pm, pl, dt, available=True):
+        transient = state["fail"] + state["avail"] * (gamma + (1.0 - gamma) * pl_test)
+        fail = state["repair"] * repaired_then_failed(pm, pl, dt) + (1.0 - sigma) * transient
+        repair = (1.0 - pm) * state["repair"] + sigma * transient
+        off = 0.0 if available else state["avail"] * (1.0 - gamma) * (1.0 - pl_test)
+        state.update(fail=fail, repair=repair, avail=1.0 - fail - repair - off)
+
+    def run_phase(pl, pm, dt):
+        fail = state["avail"] * pl + state["fail"] + state["repair"] * repaired_then_failed(pm, pl, dt)
+        repair = state["repair"] * (1.0 - pm)
+        state.update(fail=fail, repair=repair, avail=1.0 - fail - repair)
+
+    delta = t - theta
+    n = int(delta / tau)
+    run = tau - dur
+    at_test = (_p_fail(lam_test, dur), _p_fail(mu, dur), _p_fail(lam, dur), dur)
+    between = (_p_fail(lam, run), _p_fail(mu, run), run)
+    for _ in range(n):
+        test_phase(*at_test)
+        run_phase(*between)
+    after = delta - n * tau
+    if after <= dur:
+        test_phase(_p_fail(lam_test, after), _p_fail(mu, after), _p_fail(lam, after), after, bool(avail_at_test))
+    else:
+        test_phase(*at_test)
+        rest = after - dur
+        run_phase(_p_fail(lam, rest), _p_fail(mu, rest), rest)
+    return 1.0 - state["avail"]
+
+
+def _lognormal_scale(ef, level):
+    """sigma of the logarithm from an error factor at a one-sided confidence
+    level: ln(ef) / z(level) (mcSCRAM src/expression/random_deviate.cc:94-101)."""
+    from statistics import NormalDist
+    z = np.vectorize(NormalDist().inv_cdf)(np.asarray(level, dtype=np.float64))
+    return np.log(ef) / z
 
 
 _COMPARE = {"eq": lambda x, y: x == y, "df": lambda x, y: x != y, "lt": lambda x, y: x < y,
@@ -409,9 +544,16 @@ def _kids(el: ET.Element) -> List[ET.Element]:
     return [c for c in el if _local(c.tag) not in _SKIP]
 
 
+_UNARY = {"abs": abs, "acos": math.acos, "asin": math.asin, "atan": math.atan, "cos": math.cos, "sin": math.sin,
+          "tan": math.tan, "cosh": math.cosh, "sinh": math.sinh, "tanh": math.tanh, "exp": math.exp,
+          "log": math.log, "log10": math.log10, "sqrt": math.sqrt, "ceil": math.ceil, "floor": math.floor}
+_UNARY_NP = {"abs": np.abs, "acos": np.arccos, "asin": np.arcsin, "atan": np.arctan, "cos": np.cos, "sin": np.sin,
+             "tan": np.tan, "cosh": np.cosh, "sinh": np.sinh, "tanh": np.tanh, "exp": np.exp, "log": np.log,
+             "log10": np.log10, "sqrt": np.sqrt, "ceil": np.ceil, "floor": np.floor}
 _ARITY = {"exponential": 2, "GLM": 4, "Weibull": 4, "neg": 1, "not": 1, "ite": 3,
-          "eq": 2, "df": 2, "lt": 2, "gt": 2, "leq": 2, "geq": 2}
-_NARY = ("exponential", "GLM", "Weibull", "add", "sub", "mul", "div", "neg", "not", "and", "or", "ite") + tuple(_COMPARE)
+          "eq": 2, "df": 2, "lt": 2, "gt": 2, "leq": 2, "geq": 2, "pow": 2, "mod": 2, **{k: 1 for k in _UNARY}}
+_NARY = ("exponential", "GLM", "Weibull", "add", "sub", "mul", "div", "neg", "not", "and", "or", "ite", "pow", "mod",
+         "min", "max", "mean") + tuple(_COMPARE) + tuple(_UNARY)
 
 
 def _parse_expr(e: ET.Element, what: str) -> Expr:
@@ -430,11 +572,41 @@ def _parse_expr(e: ET.Element, what: str) -> Expr:
         return Expr(tag, [e.get("name")])
     if tag == "test-functional-event":
         return Expr(tag, [e.get("name"), e.get("state")])
+    if tag == "switch":  # cases (condition, value) in order, then the default value
+        kids = _kids(e)
+        if not kids:
+            raise MefError(f"{what}: <switch> needs a default value")
+        args = []
+        for c in kids[:-1]:
+            if _local(c.tag) != "case" or len(_kids(c)) != 2:
+                raise MefError(f"{what}: a <case> holds a condition and a value")
+            args += [_parse_expr(x, what) for x in _kids(c)]
+        return Expr(tag, args + [_parse_expr(kids[-1], what)])
+    if tag == "periodic-test":
+        args = [_parse_expr(c, what) for c in _kids(e)]
+        if len(args) not in (4, 5, 11):
+            raise MefError(f"{what}: <periodic-test> takes 4, 5 or 11 arguments, found {len(args)}")
+        return Expr(tag, args)
+    if tag in _DEVIATES:
+        kids = _kids(e)
+        if tag == "histogram":
+            if len(kids) < 2:
+                raise MefError(f"{what}: <histogram> needs a lower boundary and at least one bin")
+            args = [_parse_expr(kids[0], what)]
+            for b in kids[1:]:
+                if _local(b.tag) != "bin" or len(_kids(b)) != 2:
+                    raise MefError(f"{what}: a histogram <bin> holds an upper boundary and a weight")
+                args += [_parse_expr(x, what) for x in _kids(b)]
+            return Expr(tag, args)
+        need = (3, 2) if tag == "lognormal-deviate" else (2,)
+        if len(kids) not in need:
+            raise MefError(f"{what}: <{tag}> takes {' or '.join(map(str, need))} arguments, found {len(kids)}")
+        return Expr(tag, [_parse_expr(c, what) for c in kids])
     if tag in _NARY:
         args = [_parse_expr(c, what) for c in _kids(e)]
         if tag in _ARITY and len(args) != _ARITY[tag]:
             raise MefError(f"{what}: <{tag}> takes {_ARITY[tag]} arguments, found {len(args)}")
-        if tag in ("add", "sub", "mul", "div", "and", "or") and len(args) < 2:
+        if tag in ("add", "sub", "mul", "div", "and", "or", "min", "max", "mean") and len(args) < 2:
             raise MefError(f"{what}: <{tag}> takes 2 or more arguments, found {len(args)}")
         if not args:
             raise MefError(f"{what}: <{tag}> without arguments")
@@ -895,6 +1067,8 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
 
     for e, base in expr_base:
         resolve_expr(e, base, "expression")
+    for e, _ in expr_base:
+        _check_deviates(e, m)
     for name, e in m.basic_events.items():
         if e is not None:
             v = e.value(m.mission_time, m.parameters)
@@ -972,6 +1146,203 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
     if ccf_analysis:
         _expand_ccf(m)
     return m
+
+
+def _check_deviates(e: Expr, m: MefModel, _depth: int = 0):
+    """Parameter domains of the random deviates (mcSCRAM
+    src/expression/random_deviate.cc), at the arguments' point values."""
+    if _depth > 64 or e.op in ("value", "time", "parameter", "test-initiating-event", "test-functional-event"):
+        return
+    for x in e.args:
+        _check_deviates(x, m, _depth + 1)
+    if e.op in ("log", "log10", "sqrt", "acos", "asin", "div", "mod"):
+        v = [x.value(m.mission_time, m.parameters) for x in e.args]
+        if (e.op in ("log", "log10") and v[0] <= 0) or (e.op == "sqrt" and v[0] < 0) or \
+                (e.op in ("acos", "asin") and not -1 <= v[0] <= 1) or \
+                (e.op == "div" and any(x == 0 for x in v[1:])) or (e.op == "mod" and int(v[1]) == 0):
+            raise MefError(f"<{e.op}>: argument {v} outside its domain")
+        return
+    if e.op == "periodic-test":
+        v = [x.value(m.mission_time, m.parameters) for x in e.args]
+        lam, tau, theta, t = (v[0], v[1], v[2], v[3]) if len(v) == 4 else (v[0], v[2], v[3], v[4]) if len(v) == 5 \
+            else (v[0], v[3], v[4], v[10])
+        bad = lam <= 0 or tau <= 0 or theta < 0 or t < 0
+        if len(v) == 5:
+            bad |= v[1] < 0
+        if len(v) == 11:
+            bad |= v[1] < 0 or v[2] < 0 or v[6] <= 0 or v[6] > tau or not all(0 <= v[i] <= 1 for i in (5, 8, 9))
+        if bad:
+            raise MefError("<periodic-test>: a rate, period, time or probability is out of its domain "
+                           "(or the test lasts longer than the period)")
+        return
+    if e.op not in _DEVIATES:
+        return
+    v = [x.value(m.mission_time, m.parameters) for x in e.args]
+    op = e.op
+    bad = None
+    if op == "uniform-deviate" and v[0] >= v[1]:
+        bad = "min is not below max"
+    elif op == "normal-deviate" and v[1] <= 0:
+        bad = "standard deviation is not positive"
+    elif op == "lognormal-deviate" and len(v) == 3 and not (0 < v[2] < 1 and v[1] > 1 and v[0] > 0):
+        bad = "needs a positive mean, an error factor above 1 and a level in (0, 1)"
+    elif op == "lognormal-deviate" and len(v) == 2 and v[1] <= 0:
+        bad = "standard deviation is not positive"
+    elif op in ("gamma-deviate", "beta-deviate") and (v[0] <= 0 or v[1] <= 0):
+        bad = "shape and scale parameters must be positive"
+    elif op == "histogram":
+        bounds, weights = [v[0]] + v[1::2], v[2::2]
+        if any(w < 0 for w in weights) or any(b1 <= b0 for b0, b1 in zip(bounds, bounds[1:])):
+            bad = "weights must not be negative and boundaries must increase"
+    if bad:
+        raise MefError(f"<{op}>: {bad}")
+
+
+def sample_expressions(model: MefModel, exprs: Dict[str, Expr], n: int, rng: np.random.Generator,
+                       t: Optional[float] = None) -> Dict[str, np.ndarray]:
+    """n joint samples of several expressions, as one uncertainty trial each
+    (UncertaintyAnalyzer::SampleExpressions, mcSCRAM
+    src/uncertainty_analysis.cc:108-120): every random deviate is drawn once
+    per trial however many expressions reach it (through parameters or
+    otherwise) and the rest is evaluated on those draws.  Draws come from
+    numpy's generator, not the reference's mt19937, so the numbers differ and
+    the distributions agree."""
+    t = model.mission_time if t is None else float(t)
+    cache: Dict[int, np.ndarray] = {}
+
+    def s(e: Expr, depth: int = 0) -> np.ndarray:
+        if depth > 64:
+            raise MefError("parameters refer to each other in a cycle")
+        key = id(e)
+        if key in cache:
+            return cache[key]
+        op, a = e.op, e.args
+        if op == "value":
+            r = np.full(n, float(a[0]))
+        elif op == "time":
+            r = np.full(n, t)
+        elif op == "parameter":
+            r = s(model.parameters[a[0]], depth + 1)
+        elif op in ("test-initiating-event", "test-functional-event"):
+            r = np.zeros(n)
+        elif op == "ite":
+            r = np.where(s(a[0], depth + 1) != 0, s(a[1], depth + 1), s(a[2], depth + 1))
+        elif op == "switch":
+            r = s(a[-1], depth + 1)
+            for i in range(len(a) - 3, -1, -2):  # the first true case wins
+                r = np.where(s(a[i], depth + 1) != 0, s(a[i + 1], depth + 1), r)
+        else:
+            v = [s(x, depth + 1) for x in a]
+            if op == "uniform-deviate":
+                r = rng.uniform(v[0], v[1])
+            elif op == "normal-deviate":
+                r = rng.normal(v[0], v[1])
+            elif op == "lognormal-deviate":
+                if len(v) == 3:
+                    sigma = _lognormal_scale(v[1], v[2])
+                    r = np.exp(rng.normal(np.log(v[0]) - sigma ** 2 / 2, sigma))
+                else:
+                    r = np.exp(rng.normal(v[0], v[1]))
+            elif op == "gamma-deviate":
+                r = rng.gamma(v[0], v[1])
+            elif op == "beta-deviate":
+                r = rng.beta(v[0], v[1])
+            elif op == "histogram":  # piecewise constant: a bin by weight, then uniform within it
+                bounds = np.stack([v[0]] + v[1::2], axis=1)
+                weights = np.stack(v[2::2], axis=1)
+                cum = np.cumsum(weights, axis=1)
+                k = np.minimum((cum < rng.random(n)[:, None] * cum[:, -1:]).sum(axis=1), weights.shape[1] - 1)
+                lo = np.take_along_axis(bounds, k[:, None], axis=1)[:, 0]
+                hi = np.take_along_axis(bounds, k[:, None] + 1, axis=1)[:, 0]
+                r = rng.uniform(lo, hi)
+            elif op == "periodic-test":
+                r = np.array([periodic_test(*(float(x[i]) for x in v)) for i in range(n)])
+            elif op == "exponential":
+                r = -np.expm1(-v[0] * v[1])
+            elif op == "GLM":
+                g, lam, mu, tt = v
+                rr = lam + mu
+                r = (lam - (lam - g * rr) * np.exp(-rr * tt)) / rr
+            elif op == "Weibull":
+                al, be, t0, tt = v
+                r = np.where(tt <= t0, 0.0, -np.expm1(-(np.maximum(tt - t0, 0.0) / al) ** be))
+            elif op == "add":
+                r = np.sum(v, axis=0)
+            elif op == "mul":
+                r = np.prod(v, axis=0)
+            elif op == "sub":
+                r = v[0] - np.sum(v[1:], axis=0)
+            elif op == "div":
+                r = v[0]
+                for x in v[1:]:
+                    r = r / x
+            elif op == "neg":
+                r = -v[0]
+            elif op in _UNARY_NP:
+                r = _UNARY_NP[op](v[0]).astype(np.float64)
+            elif op == "pow":
+                r = np.power(v[0], v[1])
+            elif op == "mod":
+                r = np.fmod(np.trunc(v[0]), np.trunc(v[1]))
+            elif op == "min":
+                r = np.min(v, axis=0)
+            elif op == "max":
+                r = np.max(v, axis=0)
+            elif op == "mean":
+                r = np.mean(v, axis=0)
+            elif op == "not":
+                r = (v[0] == 0).astype(np.float64)
+            elif op == "and":
+                r = np.all(np.stack(v) != 0, axis=0).astype(np.float64)
+            elif op == "or":
+                r = np.any(np.stack(v) != 0, axis=0).astype(np.float64)
+            elif op in _COMPARE:
+                r = _COMPARE[op](v[0], v[1]).astype(np.float64)
+            else:
+                raise MefError(f"unknown expression {op!r}")
+        cache[key] = r
+        return r
+
+    return {name: s(e) for name, e in exprs.items()}
+
+
+def uncertainty(model: MefModel, trials: int = 1000, words: int = 1 << 14, seed: int = 0,
+                top: Optional[str] = None, device: int = 0, iteration: int = 1):
+    """Uncertainty analysis of a MEF model on the GPU (UncertaintyAnalyzer,
+    mcSCRAM src/uncertainty_analysis.h:154-168, .cc:122-158): each trial draws
+    the model's random deviates once, evaluates the basic-event probabilities
+    and estimates P(top) from `words` * 64 samples; all trials are instances
+    of one tree in one batched launch (they share their counters, so four at a
+    time share their Philox calls).  Returns the per-trial estimates, the
+    point estimate's inputs and the reference's statistics (mean, sigma,
+    error factor exp(1.96 sigma), 95 % interval of the mean, quantiles)."""
+    from .graph import probability_threshold
+    from .uncertainty import Batch
+
+    pdag, root, var_index, _ = model.build(top)
+    g = pdag.flatten([root])
+    g.root = int(g.tally_nodes[0])
+    name_of = {idx: name for name, idx in var_index.items()}
+    rng = np.random.default_rng(seed)
+    draws = sample_expressions(model, {n: model.basic_events[n] for n in var_index}, trials, rng)
+    qp = g.quantised_probabilities()
+    p = np.empty((trials, g.n_be))
+    for i, x in enumerate(g.be_pdag_idx):
+        name = name_of.get(int(x))
+        p[:, i] = qp[i] if name is None else draws[name]  # house events keep their constant word
+    p = np.clip(p, 0.0, 1.0)
+    thr = [probability_threshold(row) for row in p]
+    with Batch([g], device=device) as b:
+        ones = b.run([0] * trials, thr, iteration=iteration, words_per_instance=words)
+        ms = b.info()["last_kernel_ms"]
+    v = np.asarray(ones, dtype=np.float64) / (words * 64.0)
+    mean = float(v.mean())
+    sd = float(v.std(ddof=1)) if trials > 1 else 0.0
+    half = 1.96 * sd / math.sqrt(trials)
+    stats = {"mean": mean, "sigma": sd, "error_factor": math.exp(1.96 * sd), "ci95": [mean - half, mean + half],
+             "p05": float(np.quantile(v, 0.05)), "p50": float(np.quantile(v, 0.50)),
+             "p95": float(np.quantile(v, 0.95)), "min": float(v.min()), "max": float(v.max())}
+    return {"p_top": v, "stats": stats, "thresholds": thr, "graph": g, "kernel_ms": ms}
 
 
 def _check_ccf(m: MefModel, grp: CcfGroup):

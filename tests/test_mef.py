@@ -94,7 +94,7 @@ def test_numbering_follows_first_encounter():
      "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown basic-event"),
     ("<opsa-mef><define-gate name='t'><or><event name='x'/><event name='y'/></or></define-gate>"
      "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown event"),
-    ("<opsa-mef><define-basic-event name='x'><lognormal-deviate/></define-basic-event></opsa-mef>",
+    ("<opsa-mef><define-basic-event name='x'><extern-function name='f'/></define-basic-event></opsa-mef>",
      "unsupported expression"),
     ("<opsa-mef><define-basic-event name='x'><exponential><float value='1'/></exponential>"
      "</define-basic-event></opsa-mef>", "takes 2 arguments"),
@@ -220,8 +220,7 @@ def test_probability_over_time_matches_oracle_per_time_point(oracle_mod, gpu):
 
 
 # The reference's initializer test lists for fault-tree inputs
-# (tests/initializer_tests.cc:181-296), minus the correct inputs that use
-# constructs this loader rejects by name (random deviates, periodic tests).
+# (tests/initializer_tests.cc:181-296).
 FTA_IN = Path("/root/reference/tests/input/fta")
 FTA_CORRECT = ["correct_tree_input.xml", "correct_formulas.xml", "constant_in_formulas.xml",
                "component_definition.xml", "mixed_definitions.xml", "mixed_roles.xml",
@@ -230,9 +229,9 @@ FTA_CORRECT = ["correct_tree_input.xml", "correct_formulas.xml", "constant_in_fo
                "unordered_structure.xml", "non_top_gate.xml", "unused_parameter.xml", "null_gate_with_label.xml",
                "case_sensitivity.xml", "missing_bool_constant.xml", "correct_tree_input_with_probs.xml",
                "trailing_spaces.xml", "flavored_types.xml", "mixed_references.xml", "ccf_unordered_factors.xml",
-               "missing_ccf_level_number.xml"]
-FTA_UNSUPPORTED = {"weibull_lnorm_deviate_2p.xml": "lognormal-deviate",
-                   "weibull_lnorm_deviate_3p.xml": "lognormal-deviate", "correct_expressions.xml": "periodic-test"}
+               "missing_ccf_level_number.xml", "weibull_lnorm_deviate_2p.xml", "weibull_lnorm_deviate_3p.xml",
+               "correct_expressions.xml"]
+FTA_UNSUPPORTED = {}
 FTA_INCORRECT = ["invalid_probability.xml", "private_at_model_scope.xml", "doubly_defined_gate.xml",
                  "doubly_defined_house.xml", "doubly_defined_basic.xml", "doubly_defined_parameter.xml",
                  "doubly_defined_ccf_group.xml", "doubly_defined_component.xml", "extra_ccf_level_beta_factor.xml",
@@ -343,3 +342,173 @@ def test_ccf_model_through_the_engine(oracle_mod, gpu):
         e.run(2, 1, 0, 1 << 14)
         ones, total = e.tallies()
     assert int(ones[0]) == int(oracle_mod.tallies(g, 2, 1, 0, 1 << 14)[0])
+
+
+DEV_FIX = Path(__file__).parent / "golden" / "mef" / "deviates.xml"
+
+
+def test_deviate_point_values_and_moments():
+    """Point values are the distributions' means (as the reference's value()),
+    and 200,000 draws have the distributions' means and variances; a deviate
+    reached through two parameters is drawn once per trial."""
+    m = mef.parse(DEV_FIX, mission_time=1000.0)
+    z95 = 1.6448536269514722
+    s_log = math.log(3) / z95
+    theory = {  # (mean, variance) of each parameter's distribution
+        "lambda": (2e-4, (2e-4) ** 2 * (math.exp(s_log ** 2) - 1)),
+        "log2": (math.exp(-2.5 + 0.08), (math.exp(0.16) - 1) * math.exp(-5 + 0.16)),
+        "gamma": (0.1, 2 * 0.05 ** 2),
+        "beta": (0.1, 2 * 18 / (20 ** 2 * 21)),
+        "normal": (0.1, 0.01 ** 2),
+        "uniform": (0.002, 0.002 ** 2 / 12),
+        "histogram": ((0.0005 * 3 + 0.0025 * 1) / 4, None),
+    }
+    for name, (mu, _) in theory.items():
+        assert m.parameters[name].value(1000.0, m.parameters) == pytest.approx(mu, rel=1e-12), name
+    n = 200_000
+    d = mef.sample_expressions(m, {k: m.parameters[k] for k in list(theory) + ["lambda-alias"]}, n,
+                               np.random.default_rng(3))
+    for name, (mu, var) in theory.items():
+        x = d[name]
+        sd = math.sqrt(var) if var is not None else x.std()
+        assert abs(x.mean() - mu) <= 5 * sd / math.sqrt(n), name
+        if var is not None:
+            assert x.var() == pytest.approx(var, rel=0.05), name
+    assert np.array_equal(d["lambda"], d["lambda-alias"])
+    h = d["histogram"]
+    assert np.all((h >= 0) & (h <= 0.004)) and abs(np.mean(h < 0.001) - 0.75) < 0.01
+    b = mef.sample_expressions(m, {"a": m.basic_events["e-log3"], "b": m.basic_events["e-log3-again"]}, 10,
+                               np.random.default_rng(1))
+    np.testing.assert_allclose(-np.log1p(-b["a"]) / 1000.0, -np.log1p(-b["b"]) / 2000.0, rtol=1e-9)
+
+
+@pytest.mark.parametrize("body,msg", [
+    ("<uniform-deviate><float value='2'/><float value='1'/></uniform-deviate>", "min is not below max"),
+    ("<normal-deviate><float value='0.1'/><float value='0'/></normal-deviate>", "not positive"),
+    ("<lognormal-deviate><float value='0.1'/><float value='0.5'/><float value='0.95'/></lognormal-deviate>",
+     "error factor"),
+    ("<gamma-deviate><float value='0'/><float value='1'/></gamma-deviate>", "must be positive"),
+    ("<histogram><float value='0'/><bin><float value='0'/><float value='1'/></bin></histogram>", "increase"),
+    ("<beta-deviate><float value='1'/></beta-deviate>", "takes 2 arguments"),
+])
+def test_deviate_domain_errors(body, msg):
+    with pytest.raises(mef.MefError, match=msg):
+        mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")
+
+
+SMALL_TREE = Path("/root/reference/input/SmallTree/SmallTree.xml")
+
+
+@pytest.mark.skipif(not SMALL_TREE.exists(), reason="the reference's SmallTree model is not on this machine")
+def test_reference_small_tree_uncertainty(oracle_mod):
+    """The reference's uncertainty test on its SmallTree model
+    (tests/bench_small_tree_tests.cc:22-40): point value 0.02678 (1e-5), and
+    over 10,000 trials of its lognormal deviates a mean of 0.0253 (1e-3) and a
+    sigma of 0.022 (2e-3), here from exact per-trial probabilities."""
+    m = mef.parse(SMALL_TREE)
+    g = m.flat()
+    assert oracle_mod.bdd_probability(g) == pytest.approx(0.02678, abs=1e-5)
+    _, _, var_index, _ = m.build()
+    d = mef.sample_expressions(m, {n: m.basic_events[n] for n in var_index}, 10_000, np.random.default_rng(11))
+    p = {n: d[n] for n in var_index}
+    top = 1 - (1 - p["e1"] * p["e2"]) * (1 - p["e3"] * p["e4"])  # the model's two cut sets, exactly
+    assert top.mean() == pytest.approx(0.0253, abs=1e-3)
+    assert top.std(ddof=1) == pytest.approx(0.022, abs=2e-3)
+
+
+@pytest.mark.gpu
+def test_mef_uncertainty_on_the_gpu(oracle_mod, gpu):
+    """Trials of the deviate fixture run as one batch: every trial's count
+    bit-exact against the oracle at its sampled thresholds, and the mean of
+    the estimates within 5 sigma of the mean of the exact trial values."""
+    m = mef.parse(DEV_FIX, mission_time=1000.0)
+    trials, words = 400, 1 << 12
+    r = mef.uncertainty(m, trials=trials, words=words, seed=7, iteration=2)
+    g = r["graph"]
+    exact = np.array([oracle_mod.bdd_probability(g.with_thresholds(t)) for t in r["thresholds"]])
+    for k in (0, 1, 2, 3, 4, 199, 399):
+        want = int(oracle_mod.tallies(g.with_thresholds(r["thresholds"][k]), 2, 1, 0, words)[0])
+        assert int(round(r["p_top"][k] * words * 64)) == want, k
+    se = math.sqrt(np.sum(exact * (1 - exact)) / (words * 64)) / trials
+    assert abs(r["stats"]["mean"] - exact.mean()) <= 5 * se + 1e-12
+    assert r["stats"]["sigma"] == pytest.approx(exact.std(ddof=1), rel=0.1)
+
+
+# (arguments, value) of the reference's periodic-test cases
+# (tests/expression_tests.cc:216-324), to their 1e-5
+_PERIODIC = [
+    ((0.1, 1, 2, 5), 1 - math.exp(-0.1)),
+    ((7e-4, 4e-4, 4020, 4740, 8760), 0.817508),
+    ((7e-4, 4e-4, 2010, 4740, 8760), 0.736611),
+    ((7e-4, 4e-4, 120, 4740, 8760), 0.645377),
+    ((7e-4, 7e-4, 120, 4740, 8760), 0.511579),   # mu == lambda
+    ((7e-4, 0.0, 120, 4740, 8760), 0.997828),    # no repair
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.01, 20, 1, 0.9, 0.01, 8760), 0.668316),
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.01, 20, 0, 0.9, 0.01, 8760), 0.668316),
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.01, 20, 0, 0.9, 0.01, 4750), 1.0),
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.01, 20, 0, 0.9, 0.01, 4870), 0.996715),
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.01, 20, 0, 0.9, 0.01, 8710), 0.997478),
+    ((7e-4, 7e-4, 7e-4, 120, 4740, 0.01, 20, 1, 0.9, 0.01, 8760), 0.543401),
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.01, 120, 1, 0.9, 0.01, 8760), 0.6469),
+    ((7e-4, 6e-4, 4e-4, 4020, 4740, 0.0, 0, 1, 1.0, 0.0, 8760), 0.817508),
+    ((7e-4, 6e-4, 4e-4, 120, 4740, 0.0, 0, 1, 1.0, 0.0, 8760), 0.645377),
+]
+
+
+@pytest.mark.parametrize("args,want", _PERIODIC)
+def test_periodic_test_values(args, want):
+    assert mef.periodic_test(*args) == pytest.approx(want, abs=1e-5)
+
+
+def test_periodic_test_in_a_model():
+    """The 5-argument form read from MEF, its point value and its draws when
+    its failure rate is a deviate; a huge repair rate gives the 4-argument
+    form."""
+    xml = ("<opsa-mef><define-basic-event name='pump'><periodic-test><parameter name='lam'/>"
+           "<float value='4e-4'/><float value='4020'/><float value='4740'/><system-mission-time/></periodic-test>"
+           "</define-basic-event><define-parameter name='lam'>{}</define-parameter></opsa-mef>")
+    m = mef.parse(xml.format("<float value='7e-4'/>"), mission_time=8760.0)
+    assert m.probability("pump") == pytest.approx(0.817508, abs=1e-5)
+    m = mef.parse(xml.format("<uniform-deviate><float value='6e-4'/><float value='8e-4'/></uniform-deviate>"),
+                  mission_time=8760.0)
+    d = mef.sample_expressions(m, {"pump": m.basic_events["pump"], "lam": m.parameters["lam"]}, 50,
+                               np.random.default_rng(2))
+    for lam, val in zip(d["lam"], d["pump"]):
+        assert val == pytest.approx(mef.periodic_test(lam, 4e-4, 4020, 4740, 8760), rel=1e-12)
+    assert mef.periodic_test(7e-4, 1e300, 120, 4740, 8760) == pytest.approx(
+        mef.periodic_test(7e-4, 120, 4740, 8760), abs=1e-5)
+    with pytest.raises(mef.MefError, match="takes 4, 5 or 11"):
+        mef.parse("<opsa-mef><define-parameter name='p'><periodic-test><float value='1'/>"
+                  "<float value='1'/></periodic-test></define-parameter></opsa-mef>")
+
+
+@pytest.mark.parametrize("body,want", [
+    ("<abs><float value='-0.25'/></abs>", 0.25),
+    ("<sqrt><float value='0.09'/></sqrt>", 0.3),
+    ("<log10><float value='1e-3'/></log10>", -3.0),
+    ("<exp><log><float value='0.2'/></log></exp>", 0.2),
+    ("<pow><float value='0.5'/><int value='3'/></pow>", 0.125),
+    ("<mod><int value='-7'/><int value='3'/></mod>", -1.0),  # truncated, as C++ % on ints
+    ("<mean><float value='0.1'/><float value='0.3'/><float value='0.5'/></mean>", 0.3),
+    ("<max><float value='0.1'/><float value='0.3'/></max>", 0.3),
+    ("<floor><float value='2.7'/></floor>", 2.0),
+    ("<atan><tan><float value='0.4'/></tan></atan>", 0.4),
+    ("<switch><case><bool value='false'/><float value='0.1'/></case><case><bool value='true'/><float value='0.2'/>"
+     "</case><case><bool value='true'/><float value='0.3'/></case><float value='0.4'/></switch>", 0.2),
+    ("<switch><case><bool value='false'/><float value='0.1'/></case><float value='0.4'/></switch>", 0.4),
+])
+def test_numeric_expressions(body, want):
+    """The MEF's numeric built-ins and switch, as point values and as the
+    vectorised form the uncertainty draws use."""
+    m = mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")
+    assert m.parameters["p"].value(m.mission_time, m.parameters) == pytest.approx(want, rel=1e-12, abs=1e-15)
+    d = mef.sample_expressions(m, {"p": m.parameters["p"]}, 3, np.random.default_rng(0))
+    np.testing.assert_allclose(d["p"], want, rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("body", ["<log><float value='0'/></log>", "<sqrt><float value='-1'/></sqrt>",
+                                  "<acos><float value='2'/></acos>", "<mod><int value='3'/><int value='0'/></mod>",
+                                  "<div><float value='1'/><float value='0'/></div>"])
+def test_numeric_domain_errors(body):
+    with pytest.raises(mef.MefError, match="outside its domain"):
+        mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")

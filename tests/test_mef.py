@@ -420,7 +420,8 @@ def test_reference_small_tree_uncertainty(oracle_mod):
 def test_mef_uncertainty_on_the_gpu(oracle_mod, gpu):
     """Trials of the deviate fixture run as one batch: every trial's count
     bit-exact against the oracle at its sampled thresholds, and the mean of
-    the estimates within 5 sigma of the mean of the exact trial values."""
+    the estimates within 5 sigma (of one trial, the errors being correlated)
+    of the mean of the exact trial values."""
     m = mef.parse(DEV_FIX, mission_time=1000.0)
     trials, words = 400, 1 << 12
     r = mef.uncertainty(m, trials=trials, words=words, seed=7, iteration=2)
@@ -429,7 +430,9 @@ def test_mef_uncertainty_on_the_gpu(oracle_mod, gpu):
     for k in (0, 1, 2, 3, 4, 199, 399):
         want = int(oracle_mod.tallies(g.with_thresholds(r["thresholds"][k]), 2, 1, 0, words)[0])
         assert int(round(r["p_top"][k] * words * 64)) == want, k
-    se = math.sqrt(np.sum(exact * (1 - exact)) / (words * 64)) / trials
+    # the trials share their counters (as a fresh manager per trial would), so
+    # their sampling errors are correlated: bound the mean by one trial's error
+    se = float(np.mean(np.sqrt(exact * (1 - exact) / (words * 64))))
     assert abs(r["stats"]["mean"] - exact.mean()) <= 5 * se + 1e-12
     assert r["stats"]["sigma"] == pytest.approx(exact.std(ddof=1), rel=0.1)
 

@@ -323,9 +323,10 @@ def main(argv=None) -> int:
     ap.add_argument("--mode", default="strip", choices=list(_capi.MODES))
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--ccf", action="store_true", help="expand common-cause groups (CCF analysis)")
+    ap.add_argument("--allow-extern", action="store_true", help="load the model's extern libraries (runs their code)")
     args = ap.parse_args(argv)
     kw = {} if args.mission_time is None else {"mission_time": args.mission_time}
-    m = parse([Path(x) for x in args.model], ccf_analysis=args.ccf, **kw)
+    m = parse([Path(x) for x in args.model], ccf_analysis=args.ccf, allow_extern=args.allow_extern, **kw)
     s = host.Settings.default(ci_rel_margin_error=args.rel_err)
     if args.trials:
         s = host.Settings.default(num_trials=int(args.trials), early_stop=0, ci_rel_margin_error=1e-9)

@@ -24,9 +24,13 @@ once per trial by ``sample_expressions`` / ``uncertainty``.  Event references ar
 ``house-event`` or the untyped ``event``.  ``define-CCF-group`` (beta
 factor, MGL, alpha factor and phi factor models) defines its members; with
 ``ccf_analysis`` they are expanded into common-cause events
-(``ccf_level_probabilities``).  Other elements and expressions
-(substitutions, extern functions and libraries) are rejected with an error
-naming the element.  Probabilities are taken at a mission
+(``ccf_level_probabilities``).  ``define-substitution``: declarative
+substitutions constrain the analysed top as the reference's PDAG does
+(``MefModel.build``); non-declarative ones are checked and kept, and serve
+no Monte Carlo graph.  ``define-extern-library`` / ``define-extern-function``
+and the ``extern-function`` expression call into a shared library, loaded
+only when ``allow_extern`` asks for it.  Other elements and expressions are
+rejected with an error naming the element.  Probabilities are taken at a mission
 time (8760 hours unless given); ``probability_over_time`` evaluates the top
 event on a grid of mission times in one batched GPU pass.
 
@@ -130,6 +134,10 @@ class Expr:
                 if a[i].value(t, params, context, _depth + 1):
                     return a[i + 1].value(t, params, context, _depth + 1)
             return a[-1].value(t, params, context, _depth + 1)
+        if op == "extern-function":  # args: the function, then its argument expressions
+            if not isinstance(a[0], ExternFunction):
+                raise MefError(f"extern function {a[0]!r} is not resolved")
+            return a[0](*(x.value(t, params, context, _depth + 1) for x in a[1:]))
         v = [x.value(t, params, context, _depth + 1) for x in a]
         if op in _DEVIATES:  # a random deviate stands for its mean (mcSCRAM src/expression/random_deviate.h)
             return _deviate_mean(op, v)
@@ -188,7 +196,43 @@ class Expr:
             return self.args[0] in params and params[self.args[0]].depends_on_time(params, _depth + 1)
         if self.op in ("value", "test-initiating-event", "test-functional-event"):
             return False
-        return any(x.depends_on_time(params, _depth + 1) for x in self.args)
+        return any(x.depends_on_time(params, _depth + 1) for x in _expr_args(self))
+
+
+def _expr_args(e: Expr) -> list:
+    """The argument expressions (an extern function's first arg is the function)."""
+    return e.args[1:] if e.op == "extern-function" else e.args
+
+
+class ExternFunction:
+    """A function of an extern library (mcSCRAM src/expression/extern.h:84-198):
+    `int` or `double` return and up to 5 `int`/`double` parameters; arguments
+    are evaluated as doubles and converted to the parameter types as C++
+    converts them (toward zero for int), the result returned as a double."""
+    MAX_PARAMS = 5
+
+    def __init__(self, name: str, symbol: str, library, types: List[str]):
+        import ctypes
+        self.name, self.types = name, types
+        try:
+            fn = getattr(library, symbol)
+        except AttributeError:
+            raise MefError(f"extern function {name!r}: symbol {symbol!r} is not in the library") from None
+        ct = {"int": ctypes.c_int, "double": ctypes.c_double}
+        fn.restype = ct[types[0]]
+        fn.argtypes = [ct[x] for x in types[1:]]
+        self._fn = fn
+
+    @property
+    def arity(self) -> int:
+        return len(self.types) - 1
+
+    def __call__(self, *args) -> float:
+        conv = [int(x) if ty == "int" else float(x) for x, ty in zip(args, self.types[1:])]
+        return float(self._fn(*conv))
+
+    def __repr__(self):
+        return f"ExternFunction({self.name!r})"
 
 
 _DEVIATES = ("uniform-deviate", "normal-deviate", "lognormal-deviate", "gamma-deviate", "beta-deviate", "histogram")
@@ -370,6 +414,26 @@ _CCF_MIN_LEVEL = {"beta-factor": None, "MGL": 2, "alpha-factor": 1, "phi-factor"
 
 
 @dataclass
+class Substitution:
+    """A substitution (mcSCRAM src/substitution.h): a hypothesis over basic
+    events, the source events it replaces (none: declarative) and a target,
+    either an argument (False, "basic-event" or -- members under CCF analysis
+    -- "gate", id) or a constant."""
+    name: str
+    hypothesis: Formula
+    source: List[str]
+    target: Union[Tuple[bool, str, str], bool]
+    type: Optional[str] = None
+
+    @property
+    def declarative(self) -> bool:
+        return not self.source
+
+
+_SUBSTITUTION_TYPES = ("delete-terms", "recovery-rule", "exchange-event")
+
+
+@dataclass
 class MefModel:
     gates: Dict[str, Formula] = field(default_factory=dict)
     basic_events: Dict[str, Expr] = field(default_factory=dict)
@@ -384,6 +448,9 @@ class MefModel:
     rules: Dict[str, list] = field(default_factory=dict)
     alignments: Dict[str, List[Phase]] = field(default_factory=dict)
     ccf_groups: Dict[str, CcfGroup] = field(default_factory=dict)
+    substitutions: Dict[str, Substitution] = field(default_factory=dict)
+    extern_libraries: Dict[str, object] = field(default_factory=dict)  # name -> loaded ctypes library
+    extern_functions: Dict[str, "ExternFunction"] = field(default_factory=dict)
 
     def probability(self, event: str, t: Optional[float] = None) -> float:
         """Probability of a basic event at mission time t (default: the model's)."""
@@ -441,7 +508,16 @@ class MefModel:
 
     def build(self, top: Optional[str] = None):
         """Host PDAG rooted at `top` (the only top gate when None).  Returns
-        (host.Pdag, root index, {basic-event name: index}, {gate name: index})."""
+        (host.Pdag, root index, {basic-event name: index}, {gate name: index}).
+
+        Declarative substitutions constrain the analysed root as the
+        reference's Pdag(mef::Gate, ccf, model) does (src/pdag.cc:470-494,
+        721-734): the root becomes AND(S1, ..., Sn, top) with Si = OR(NOT
+        hypothesis, target), or NULL(NOT hypothesis) for a false target; the
+        returned root is then that AND and gate_index[top] the top's own gate.
+        Non-declarative substitutions serve cut-set approximations only: their
+        events are gathered, as the reference gathers them, but the graph
+        does not change."""
         from .host import Pdag
 
         if top is None:
@@ -468,8 +544,26 @@ class MefModel:
                 elif kind == "formula":
                     gather(x)
 
+        def gather_arg(kind: str, x: str):
+            gather(Formula(NULL, [(False, kind, x)]))
+
         seen_gates.add(top)
         gather(self.gates[top])
+        outside = set()  # events only non-declarative substitutions name: never in the graph
+        for s in self.substitutions.values():  # GatherVariables(mef::Substitution)
+            before = set(var_index)
+            gather(s.hypothesis)
+            for x in s.source:
+                gather_arg("basic-event", x)
+            if not isinstance(s.target, bool):
+                gather_arg(s.target[1], s.target[2])
+            if not s.declarative:
+                outside.update(set(var_index) - before)
+        for s in self.substitutions.values():
+            if s.declarative:
+                outside.difference_update(x for _, _, x in s.hypothesis.args)
+                if not isinstance(s.target, bool):
+                    outside.discard(s.target[2])
         nxt = 2 + len(var_index)
         for f_name in self._house_events_in(top):
             house_index[f_name] = nxt
@@ -477,7 +571,8 @@ class MefModel:
         # 2. gates in pre-order of construction (ConstructGate)
         pdag = Pdag()
         for name, idx in var_index.items():
-            pdag.add_variable(idx, self.probability(name))
+            unused = name in outside and self.basic_events[name] is None
+            pdag.add_variable(idx, 0.0 if unused else self.probability(name))
         for name, idx in house_index.items():
             pdag.add_variable(idx, 1.0 if self.house_events[name] else 0.0)
         gate_index: Dict[str, int] = {}
@@ -505,6 +600,26 @@ class MefModel:
 
         root = construct(self.gates[top])
         gate_index[top] = root
+        application = counter[0]  # made whether or not a substitution applies
+        counter[0] += 1
+        applied = []
+        for s in self.substitutions.values():
+            if not s.declarative:
+                continue
+            idx = counter[0]
+            counter[0] += 1
+            hyp = construct(s.hypothesis)
+            if isinstance(s.target, bool):  # a delete term
+                pending.append((idx, Formula(NULL, [-hyp])))
+            else:
+                _, kind, x = s.target
+                if kind == "gate" and x not in gate_index:
+                    gate_index[x] = construct(self.gates[x])
+                pending.append((idx, Formula(OR, [-hyp, var_index[x] if kind == "basic-event" else gate_index[x]])))
+            applied.append(idx)
+        if applied:
+            pending.append((application, Formula(AND, applied + [root])))
+            root = application
         for idx, f in pending:
             pdag.add_gate(idx, f.connective, f.args, f.min_number)
         pdag.set_root(root)
@@ -602,6 +717,8 @@ def _parse_expr(e: ET.Element, what: str) -> Expr:
         if len(kids) not in need:
             raise MefError(f"{what}: <{tag}> takes {' or '.join(map(str, need))} arguments, found {len(kids)}")
         return Expr(tag, [_parse_expr(c, what) for c in kids])
+    if tag == "extern-function":  # the function is resolved by name once the model is read
+        return Expr(tag, [e.get("name")] + [_parse_expr(c, what) for c in _kids(e)])
     if tag in _NARY:
         args = [_parse_expr(c, what) for c in _kids(e)]
         if tag in _ARITY and len(args) != _ARITY[tag]:
@@ -862,15 +979,48 @@ def _document(source: Union[str, Path]) -> ET.Element:
     return root
 
 
+def _directory(source: Union[str, Path]) -> Path:
+    """The directory relative library paths of a document start from."""
+    if isinstance(source, Path) or not source.lstrip().startswith("<"):
+        return Path(source).resolve().parent
+    return Path.cwd()
+
+
+def _load_library(el: ET.Element, directory: Path):
+    """An extern library (mcSCRAM src/expression/extern.cc:29-65): the path
+    is relative to the defining document unless `system` asks for the
+    loader's own search (a bare name); `decorate` adds the platform's lib
+    prefix and .so suffix."""
+    import ctypes
+    name, path = el.get("name"), el.get("path") or ""
+    fname = Path(path).name
+    if not path or fname in (".", "..") or path[-1] in ":/\\":
+        raise MefError(f"extern library {name!r}: invalid library path format {path!r}")
+    system = (el.get("system") or "false").strip().lower() == "true"
+    if (el.get("decorate") or "false").strip().lower() == "true":
+        path = str(Path(path).with_name(f"lib{fname}.so"))
+    if not system or "/" in path:
+        path = str(directory / path)
+    try:
+        return ctypes.CDLL(path)
+    except OSError as e:
+        raise MefError(f"extern library {name!r}: {e}") from None
+
+
 def parse(source: Union[str, Path, List[Union[str, Path]]],
-          mission_time: float = DEFAULT_MISSION_TIME, ccf_analysis: bool = False) -> MefModel:
+          mission_time: float = DEFAULT_MISSION_TIME, ccf_analysis: bool = False,
+          allow_extern: bool = False) -> MefModel:
     """Reads a MEF document (a path, or the XML text itself) or several
     documents forming one model (a list; references may cross them);
     probabilities are evaluated at `mission_time` unless asked for at another
     time.  With `ccf_analysis` the members of common-cause groups become OR
     gates over their CCF events (SCRAM's --ccf); without it they are basic
-    events with the group's distribution, as in SCRAM."""
-    roots = [_document(x) for x in (source if isinstance(source, (list, tuple)) else [source])]
+    events with the group's distribution, as in SCRAM.  Extern libraries
+    are loaded only with `allow_extern` (SCRAM's --allow-extern): loading one
+    runs its code."""
+    sources = source if isinstance(source, (list, tuple)) else [source]
+    roots = [_document(x) for x in sources]
+    dirs = [_directory(x) for x in sources]
     m = MefModel(mission_time=float(mission_time))
     scope = _Scope()
     gate_base: Dict[str, str] = {}
@@ -1005,7 +1155,37 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
             raise MefError(f"{where}: no initial state")
         m.event_trees[name] = et
 
-    for el in (x for r in roots for x in r):
+    def define_substitution(el: ET.Element):
+        """<define-substitution> as read by mcSCRAM src/initializer.cc:619-669;
+        references are resolved, and the checks made, once every file is read."""
+        name = el.get("name")
+        if not name:
+            raise MefError("<define-substitution> without a name")
+        where = f"substitution {name!r}"
+        if name in m.substitutions:
+            raise MefError(f"{where} defined twice")
+        parts = {_local(c.tag): c for c in _kids(el)}
+        hyp, tgt = parts.get("hypothesis"), parts.get("target")
+        if hyp is None or len(_kids(hyp)) != 1 or tgt is None or len(_kids(tgt)) != 1:
+            raise MefError(f"{where}: needs one hypothesis formula and one target")
+        source = []
+        for b in _kids(parts["source"]) if "source" in parts else []:
+            if _local(b.tag) != "basic-event":
+                raise MefError(f"{where}: the source holds basic events only")
+            source.append(b.get("name"))
+        t = _kids(tgt)[0]
+        if _local(t.tag) == "basic-event":
+            target = (False, "basic-event", t.get("name"))
+        elif _local(t.tag) == "constant":
+            target = t.get("value", "").strip().lower() == "true"
+        else:
+            raise MefError(f"{where}: the target is a basic event or a constant")
+        stype = el.get("type")
+        if stype is not None and stype not in _SUBSTITUTION_TYPES:
+            raise MefError(f"{where}: unknown type {stype!r}")
+        m.substitutions[name] = Substitution(name, _parse_formula(_kids(hyp)[0], where), source, target, stype)
+
+    for el, doc_dir in ((x, d) for r, d in zip(roots, dirs) for x in r):
         tag = _local(el.tag)
         name = el.get("name")
         if tag == "define-fault-tree":
@@ -1021,6 +1201,16 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
             visit_data([el], "", "public", None)
         elif tag == "define-event-tree":
             define_event_tree(el)
+        elif tag == "define-substitution":
+            define_substitution(el)
+        elif tag == "define-extern-library":  # initializer.cc:481-488
+            if not allow_extern:
+                raise MefError(f"extern library {name!r}: loading external libraries is disallowed")
+            if name in m.extern_libraries:
+                raise MefError(f"extern library {name!r} defined twice")
+            m.extern_libraries[name] = _load_library(el, doc_dir)
+        elif tag == "define-extern-function":
+            continue  # once every library is loaded
         elif tag == "define-initiating-event":
             if name in m.initiating_events:
                 raise MefError(f"initiating event {name!r} defined twice")
@@ -1054,13 +1244,41 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
         else:
             raise MefError(f"unsupported element <{tag}>")
 
-    # resolve parameter references in expressions
+    # extern functions, from every document (initializer.cc:1578-1626)
+    for el in (x for r in roots for x in r if _local(x.tag) == "define-extern-function"):
+        name = el.get("name")
+        where = f"extern function {name!r}"
+        if name in m.extern_functions:
+            raise MefError(f"{where} defined twice")
+        if el.get("library") not in m.extern_libraries:
+            raise MefError(f"{where}: undefined extern library {el.get('library')!r}")
+        types = [_local(c.tag) for c in _kids(el)]
+        if not types or any(t not in ("int", "double") for t in types):
+            raise MefError(f"{where}: needs a return type and parameter types, each <int/> or <double/>")
+        if len(types) - 1 > ExternFunction.MAX_PARAMS:
+            raise MefError(f"{where}: the number of function parameters {len(types) - 1} exceeds the "
+                           f"{ExternFunction.MAX_PARAMS} allowed")
+        m.extern_functions[name] = ExternFunction(name, el.get("symbol") or "", m.extern_libraries[el.get("library")],
+                                                  types)
+
+    # resolve parameter references and extern functions in expressions
     def resolve_expr(e: Expr, base: str, where: str):
         if e.op == "parameter":
             hit = scope.lookup(("parameter",), e.args[0], base)
             if hit is None:
                 raise MefError(f"{where}: unknown parameter {e.args[0]!r}")
             e.args = [hit[1]]
+        elif e.op == "extern-function":
+            if not isinstance(e.args[0], ExternFunction):
+                fn = m.extern_functions.get(e.args[0])
+                if fn is None:
+                    raise MefError(f"{where}: undefined extern function {e.args[0]!r}")
+                if len(e.args) - 1 != fn.arity:
+                    raise MefError(f"{where}: extern function {fn.name!r} takes {fn.arity} arguments, "
+                                   f"found {len(e.args) - 1}")
+                e.args[0] = fn
+            for x in e.args[1:]:
+                resolve_expr(x, base, where)
         elif e.op not in ("value", "time", "test-initiating-event", "test-functional-event"):
             for x in e.args:
                 resolve_expr(x, base, where)
@@ -1101,6 +1319,25 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
         resolve(f, gate_base[gid], f"gate {gid!r}")
     for grp in m.ccf_groups.values():
         _check_ccf(m, grp)
+    for s in m.substitutions.values():
+        where = f"substitution {s.name!r}"
+        resolve(s.hypothesis, "", where)
+        seen = set()
+        for i, x in enumerate(s.source):
+            hit = scope.lookup(("basic-event",), x, "")
+            if hit is None:
+                raise MefError(f"{where}: unknown basic event {x!r}")
+            if hit[1] in seen:
+                raise MefError(f"{where}: source event {hit[1]!r} listed twice")
+            seen.add(hit[1])
+            s.source[i] = hit[1]
+        if not isinstance(s.target, bool):
+            hit = scope.lookup(("basic-event",), s.target[2], "")
+            if hit is None:
+                raise MefError(f"{where}: unknown basic event {s.target[2]!r}")
+            s.target = (False, "basic-event", hit[1])
+        _check_substitution(s)
+    _check_substitution_conflicts(m)
 
     def resolve_instructions(ins, where: str):
         def fn(x):
@@ -1153,7 +1390,7 @@ def _check_deviates(e: Expr, m: MefModel, _depth: int = 0):
     src/expression/random_deviate.cc), at the arguments' point values."""
     if _depth > 64 or e.op in ("value", "time", "parameter", "test-initiating-event", "test-functional-event"):
         return
-    for x in e.args:
+    for x in _expr_args(e):
         _check_deviates(x, m, _depth + 1)
     if e.op in ("log", "log10", "sqrt", "acos", "asin", "div", "mod"):
         v = [x.value(m.mission_time, m.parameters) for x in e.args]
@@ -1231,6 +1468,9 @@ def sample_expressions(model: MefModel, exprs: Dict[str, Expr], n: int, rng: np.
             r = s(a[-1], depth + 1)
             for i in range(len(a) - 3, -1, -2):  # the first true case wins
                 r = np.where(s(a[i], depth + 1) != 0, s(a[i + 1], depth + 1), r)
+        elif op == "extern-function":  # one call per trial
+            v = [np.broadcast_to(s(x, depth + 1), (n,)) for x in a[1:]]
+            r = np.array([a[0](*(x[i] for x in v)) for i in range(n)], dtype=np.float64)
         else:
             v = [s(x, depth + 1) for x in a]
             if op == "uniform-deviate":
@@ -1323,8 +1563,10 @@ def uncertainty(model: MefModel, trials: int = 1000, words: int = 1 << 14, seed:
     g = pdag.flatten([root])
     g.root = int(g.tally_nodes[0])
     name_of = {idx: name for name, idx in var_index.items()}
+    in_graph = set(map(int, g.be_pdag_idx))
     rng = np.random.default_rng(seed)
-    draws = sample_expressions(model, {n: model.basic_events[n] for n in var_index}, trials, rng)
+    draws = sample_expressions(model, {n: model.basic_events[n] for n, i in var_index.items() if i in in_graph},
+                               trials, rng)
     qp = g.quantised_probabilities()
     p = np.empty((trials, g.n_be))
     for i, x in enumerate(g.be_pdag_idx):
@@ -1355,6 +1597,81 @@ def _check_ccf(m: MefModel, grp: CcfGroup):
         raise MefError(f"{where}: factors {vals} are not all probabilities")
     if grp.model == "phi-factor" and abs(sum(vals) - 1.0) > 1e-4:
         raise MefError(f"{where}: phi factors sum to {sum(vals)}, not 1")
+
+
+def substitution_type(s: Substitution) -> Optional[str]:
+    """The type a substitution's form implies (mcSCRAM
+    src/substitution.cc:92-133): delete-terms for a false target over two
+    mutually exclusive events (AND of two, or at least 2 of n), recovery-rule
+    for a declarative AND or a source equal to the hypothesis' events,
+    exchange-event for one source event of an AND/NULL hypothesis."""
+    hyp = s.hypothesis
+    events = [x for _, _, x in hyp.args]
+    if not s.source:
+        if isinstance(s.target, bool):
+            exclusive = (hyp.connective == ATLEAST and hyp.min_number == 2) or (
+                hyp.connective == AND and len(hyp.args) == 2)
+            return "delete-terms" if exclusive else None
+        return "recovery-rule" if hyp.connective == AND else None
+    if isinstance(s.target, bool) or hyp.connective not in (AND, NULL):
+        return None
+    if len(s.source) == len(events):
+        return "recovery-rule" if all(x in events for x in s.source) else None
+    if len(s.source) == 1 and s.source[0] in events:
+        return "exchange-event"
+    return None
+
+
+def _check_substitution(s: Substitution):
+    """Substitution::Validate and the declared-type check (mcSCRAM
+    src/substitution.cc:38-90, src/initializer.cc:655-668)."""
+    where = f"substitution {s.name!r}"
+    hyp = s.hypothesis
+    if any(kind != "basic-event" for _, kind, _ in hyp.args):
+        raise MefError(f"{where}: the hypothesis must be built over basic events only")
+    if any(comp for comp, _, _ in hyp.args):
+        raise MefError(f"{where}: the hypothesis must be coherent")
+    if s.declarative:
+        if hyp.connective not in (NULL, AND, ATLEAST, OR):
+            raise MefError(f"{where}: the hypothesis must be coherent")
+        if s.target is True:
+            raise MefError(f"{where}: the substitution has no effect")
+    else:
+        if hyp.connective not in (NULL, AND, OR):
+            raise MefError(f"{where}: a non-declarative hypothesis allows AND/OR/NULL connectives only")
+        if s.target is False:
+            raise MefError(f"{where}: the source set is irrelevant")
+    if s.type is not None and substitution_type(s) != s.type:
+        raise MefError(f"{where}: the declared type {s.type!r} does not match the deduced one")
+
+
+def _check_substitution_conflicts(m: MefModel):
+    """EnsureNoSubstitutionConflicts and EnsureNoCcfSubstitutions (mcSCRAM
+    src/initializer.cc:1805-1866) over the non-declarative substitutions.
+    Non-declarative substitutions are kept for a Monte Carlo analysis, whose
+    approximation is not `none` (src/settings.cc:30-45), as the reference
+    keeps them; they do not change its graph."""
+    subs = [s for s in m.substitutions.values() if not s.declarative]
+    ccf_members = {x for grp in m.ccf_groups.values() for x in grp.members}
+    for origin in subs:
+        where = f"substitution {origin.name!r}"
+        target = None if isinstance(origin.target, bool) else origin.target[2]
+        for other in subs:
+            if target is not None and target in other.source:
+                raise MefError(f"{where}: the target event should not appear in any substitution source")
+            if other is origin:
+                continue
+            events = {x for _, _, x in other.hypothesis.args}
+            if target is not None and target in events:
+                raise MefError(f"{where}: the target event should not appear in another substitution hypothesis")
+            if any(x in events for x in origin.source):
+                raise MefError(f"{where}: a source event should not appear in another substitution hypothesis")
+    for s in subs:
+        events = [x for _, _, x in s.hypothesis.args] + list(s.source)
+        if not isinstance(s.target, bool):
+            events.append(s.target[2])
+        if any(x in ccf_members for x in events):
+            raise MefError(f"substitution {s.name!r}: non-declarative substitution events cannot be in a CCF group")
 
 
 def ccf_level_probabilities(grp: CcfGroup) -> List[Tuple[int, Expr]]:
@@ -1427,6 +1744,10 @@ def _expand_ccf(m: MefModel):
     for et in m.event_trees.values():
         for b in _branches_of(et):
             _walk_instructions(b.instructions, lambda x: retarget(x[1]) if x[0] == "collect-formula" else None, {})
+    for s in m.substitutions.values():  # declarative ones: non-declarative events are never CCF members
+        retarget(s.hypothesis)
+        if not isinstance(s.target, bool) and s.target[2] in as_gate:
+            s.target = (False, "gate", s.target[2])
 
 
 def _branches_of(et: EventTree) -> List[Branch]:
@@ -1586,10 +1907,11 @@ def _check_homogeneous(m: MefModel, et: EventTree, b: Branch, where: str):
 
 
 def load(source: Union[str, Path], top: Optional[str] = None,
-         mission_time: float = DEFAULT_MISSION_TIME, ccf_analysis: bool = False) -> FlatGraph:
+         mission_time: float = DEFAULT_MISSION_TIME, ccf_analysis: bool = False,
+         allow_extern: bool = False) -> FlatGraph:
     """MEF document -> flattened graph of its top gate (probabilities at the
     mission time), root tallied."""
-    return parse(source, mission_time, ccf_analysis).flat(top)
+    return parse(source, mission_time, ccf_analysis, allow_extern).flat(top)
 
 
 def probability_over_time(model: MefModel, time_step: float, top: Optional[str] = None,
@@ -1646,8 +1968,9 @@ def main(argv=None) -> int:
     ap.add_argument("--mode", default="strip", choices=list(_capi.MODES))
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--ccf", action="store_true", help="expand common-cause groups (CCF analysis)")
+    ap.add_argument("--allow-extern", action="store_true", help="load the model's extern libraries (runs their code)")
     args = ap.parse_args(argv)
-    g = load(args.model, args.top, ccf_analysis=args.ccf)
+    g = load(args.model, args.top, ccf_analysis=args.ccf, allow_extern=args.allow_extern)
     words = max(1, int(math.ceil(args.samples / 64)))
     with _capi.Engine(g, mode=_capi.MODES[args.mode], device=args.device) as e:
         done, it = 0, 1

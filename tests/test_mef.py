@@ -95,7 +95,7 @@ def test_numbering_follows_first_encounter():
     ("<opsa-mef><define-gate name='t'><or><event name='x'/><event name='y'/></or></define-gate>"
      "<define-basic-event name='y'><float value='0.1'/></define-basic-event></opsa-mef>", "unknown event"),
     ("<opsa-mef><define-basic-event name='x'><extern-function name='f'/></define-basic-event></opsa-mef>",
-     "unsupported expression"),
+     "undefined extern function"),
     ("<opsa-mef><define-basic-event name='x'><exponential><float value='1'/></exponential>"
      "</define-basic-event></opsa-mef>", "takes 2 arguments"),
     ("<opsa-mef><define-gate name='t'><house-event name='h'/></define-gate>"
@@ -515,3 +515,191 @@ def test_numeric_expressions(body, want):
 def test_numeric_domain_errors(body):
     with pytest.raises(mef.MefError, match="outside its domain"):
         mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")
+
+
+SUB_FIX = Path(__file__).parent / "golden" / "mef" / "substitution.xml"
+
+
+def _substitution_fixture_exact() -> float:
+    """P(top AND the declarative substitutions' implications) of the
+    substitution fixture by enumeration, from its formulas written out here:
+    top = atleast 2 of the pumps or the heat exchanger; no two of pump a,
+    pump b and maintenance; pumps b and c imply the operator's failure; the
+    heat exchanger implies the backup's; pump a or the heat exchanger imply
+    the alarm's.  The non-declarative exchange event changes nothing."""
+    q = lambda p: math.floor(p * TWO32) / TWO32  # the sampler's quantised probability
+    p = {"a": 0.3, "b": 0.25, "c": 0.2, "hx": 0.05, "maint": 0.1, "op": 0.4, "backup": 0.6, "alarm": 0.9}
+    names = list(p)
+    total = 0.0
+    for bits in itertools.product([False, True], repeat=len(names)):
+        x = dict(zip(names, bits))
+        w = math.prod(q(p[n]) if b else 1 - q(p[n]) for n, b in zip(names, bits))
+        top = (x["a"] + x["b"] + x["c"] >= 2) or x["hx"]
+        ok = (x["a"] + x["b"] + x["maint"] < 2) and (not (x["b"] and x["c"]) or x["op"]) and \
+            (not x["hx"] or x["backup"]) and (not (x["a"] or x["hx"]) or x["alarm"])
+        total += w * (top and ok)
+    return total
+
+
+def test_substitution_fixture_exact(oracle_mod):
+    m = mef.parse(SUB_FIX)
+    assert [mef.substitution_type(s) for s in m.substitutions.values()] == [
+        "delete-terms", "recovery-rule", None, None, "exchange-event"]
+    pdag, root, var_index, gate_index = m.build("top")
+    assert gate_index["top"] != root  # the analysed root is AND(implications..., top)
+    # the top's events first, then the substitutions' in definition order (GatherVariables)
+    assert list(var_index)[:9] == ["pump_a", "pump_b", "pump_c", "heat_exchanger", "maintenance",
+                                   "operator_fails", "backup_fails", "alarm_fails", "valve_x"]
+    g = mef.load(SUB_FIX)
+    assert g.n_be == 8  # the non-declarative substitution's events are not in the graph
+    assert oracle_mod.bdd_probability(g) == pytest.approx(_substitution_fixture_exact(), rel=1e-9)
+
+
+def test_substitution_errors():
+    model = ("<opsa-mef><define-substitution name='s'{attr}><hypothesis>{hyp}</hypothesis>{src}<target>{tgt}"
+             "</target></define-substitution><model-data>" +
+             "".join(f"<define-basic-event name='{n}'><float value='0.1'/></define-basic-event>" for n in "abcd") +
+             "</model-data></opsa-mef>")
+    ab = "<and><basic-event name='a'/><basic-event name='b'/></and>"
+    d = "<basic-event name='d'/>"
+    cases = [("", "<xor><basic-event name='a'/><basic-event name='b'/></xor>", "", d, "must be coherent"),
+             ("", ab, "", "<constant value='true'/>", "no effect"),
+             ("", ab, "<source><basic-event name='c'/></source>", "<constant value='false'/>", "irrelevant"),
+             ("", "<atleast min='2'><basic-event name='a'/><basic-event name='b'/><basic-event name='c'/></atleast>",
+              "<source><basic-event name='c'/></source>", d, "AND/OR/NULL"),
+             (" type='exchange-event'", ab, "", d, "does not match"),
+             ("", "<and><basic-event name='a'/><gate name='b'/></and>", "", d, "unknown gate"),
+             ("", ab, "<source><basic-event name='c'/><basic-event name='c'/></source>", d, "listed twice")]
+    for attr, hyp, src, tgt, msg in cases:
+        with pytest.raises(mef.MefError, match=msg):
+            mef.parse(model.format(attr=attr, hyp=hyp, src=src, tgt=tgt))
+
+
+TWO_TRAIN = Path("/root/reference/input/TwoTrain")
+
+
+@pytest.mark.skipif(not TWO_TRAIN.exists(), reason="the reference's TwoTrain model is not on this machine")
+def test_reference_two_train_substitutions(oracle_mod):
+    """The exact probabilities the reference's tests expect of its two-train
+    model, plain and with declarative substitutions (tests/bench_two_train_tests.cc:
+    24-72); its non-declarative substitutions leave the Monte Carlo graph as
+    the plain model's."""
+    assert oracle_mod.bdd_probability(mef.load(TWO_TRAIN / "two_train.xml")) == pytest.approx(0.7225, rel=1e-9)
+    assert oracle_mod.bdd_probability(mef.load(TWO_TRAIN / "substitutions.xml")) == pytest.approx(0.329175, rel=1e-9)
+    assert oracle_mod.bdd_probability(mef.load(TWO_TRAIN / "nondeclarative_substitutions.xml")) == \
+        pytest.approx(0.7225, rel=1e-9)
+
+
+MODEL_IN = Path("/root/reference/tests/input/model")
+MODEL_CORRECT = ["extern_library.xml", "extern_function.xml", "extern_expression.xml", "valid_alignment.xml",
+                 "valid_sum_alignment.xml", "private_phases.xml", "substitution.xml",
+                 "substitution_optional_source.xml", "substitution_types.xml",
+                 "substitution_declarative_target_is_another_source.xml", "substitution_target_is_hypothesis.xml",
+                 "substitution_declarative_ccf.xml"]
+MODEL_INCORRECT = [
+    "duplicate_extern_libraries.xml", "duplicate_extern_functions.xml", "undefined_extern_library.xml",
+    "invalid_num_param_extern_function.xml", "undefined_extern_function.xml",
+    "invalid_num_args_extern_expression.xml", "extern_library_invalid_path_format.xml", "duplicate_phases.xml",
+    "invalid_phase_fraction.xml", "zero_phase_fraction.xml", "negative_phase_fraction.xml",
+    "undefined_target_set_house_event.xml", "duplicate_alignment.xml", "excess_alignment.xml",
+    "incomplete_alignment.xml", "duplicate_substitution.xml", "substitution_undefined_hypothesis_event.xml",
+    "substitution_undefined_source_event.xml", "substitution_undefined_target_event.xml",
+    "substitution_duplicate_source_event.xml", "substitution_duplicate_hypothesis_event.xml",
+    "substitution_nested_formula.xml", "substitution_non_basic_event_formula.xml", "substitution_type_mismatch.xml",
+    "substitution_no_effect.xml", "substitution_nondeclarative_complex.xml", "substitution_source_equal_target.xml",
+    "substitution_target_is_another_source.xml", "substitution_target_is_another_hypothesis.xml",
+    "substitution_source_is_another_hypothesis.xml", "substitution_source_false_target.xml",
+    "substitution_declarative_noncoherent.xml", "substitution_nondeclarative_ccf_hypothesis.xml",
+    "substitution_nondeclarative_ccf_source.xml", "substitution_nondeclarative_ccf_target.xml",
+    "empty_extern_function.xml", "empty_alignment.xml", "extern_library_ioerror.xml",
+    "undefined_symbol_extern_function.xml"]
+
+# a stand-in for the reference's test library: the symbols its model inputs name
+_DUMMY_EXTERN = "int foo(void) { return 42; }\ndouble bar(void) { return 42; }\ndouble identity(double x) { return x; }\n"
+
+
+def _shared_library(source: str, out: Path):
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler for the extern-function library")
+    out.parent.mkdir(parents=True, exist_ok=True)
+    src = out.with_suffix(".c")
+    src.write_text(source)
+    subprocess.run(["gcc", "-shared", "-fPIC", "-O1", "-o", str(out), str(src)], check=True)
+
+
+@pytest.mark.skipif(not MODEL_IN.exists(), reason="the reference's model inputs are not on this machine")
+def test_reference_model_inputs_accepted_and_rejected(tmp_path):
+    """The reference's initializer lists of correct and incorrect model
+    inputs (tests/initializer_tests.cc:332-414), read with extern libraries
+    allowed; the inputs are copied beside a library of the symbols they name,
+    at the relative path they load it from."""
+    _shared_library(_DUMMY_EXTERN, tmp_path / "build" / "lib" / "scram" / "libscram_dummy_extern.so")
+    d = tmp_path / "tests" / "input" / "model"
+    d.mkdir(parents=True)
+    for f in MODEL_IN.glob("*.xml"):
+        (d / f.name).write_text(f.read_text())
+    for name in MODEL_CORRECT:
+        mef.parse(d / name, allow_extern=True)
+    m = mef.parse(d / "extern_expression.xml", allow_extern=True)
+    assert {k: e.value(0.0, m.parameters) for k, e in m.parameters.items()} == {
+        "param1": 1.0, "param2": 42.0, "param": 42.0}
+    for name in MODEL_INCORRECT:
+        with pytest.raises(mef.MefError):
+            mef.parse(d / name, allow_extern=True)
+    with pytest.raises(mef.MefError, match="disallowed"):  # DefaultExternDisable
+        mef.parse(d / "extern_library.xml")
+    g = mef.load(d / "extern_full_check.xml", allow_extern=True)
+    assert float(g.quantised_probabilities()[0]) == pytest.approx(0.1, abs=1e-9)
+
+
+_SCALE_EXTERN = "double scale(double p, int n) { return p / n; }\nint twice(int x) { return 2 * x; }\n"
+
+
+def test_extern_functions_in_a_model(oracle_mod, tmp_path):
+    """Extern functions with int and double parameters: arguments convert as
+    C++ converts them (2.9 -> 2, 3.7 -> 3), values feed basic events, and
+    the uncertainty draws call them once per trial."""
+    _shared_library(_SCALE_EXTERN, tmp_path / "lib" / "libscale.so")
+    xml = tmp_path / "m.xml"
+    xml.write_text(
+        "<opsa-mef><define-extern-library name='l' path='lib/scale' decorate='true'/>"
+        "<define-extern-function name='scale' symbol='scale' library='l'><double/><double/><int/>"
+        "</define-extern-function><define-extern-function name='twice' symbol='twice' library='l'><int/><int/>"
+        "</define-extern-function><define-fault-tree name='f'><define-gate name='top'><or>"
+        "<basic-event name='e1'/><basic-event name='e2'/></or></define-gate>"
+        "<define-basic-event name='e1'><extern-function name='scale'><float value='0.9'/><float value='3.7'/>"
+        "</extern-function></define-basic-event>"
+        "<define-basic-event name='e2'><div><float value='1'/><extern-function name='twice'>"
+        "<float value='2.9'/></extern-function></div></define-basic-event>"
+        "<define-basic-event name='e3'><extern-function name='scale'><uniform-deviate><float value='0.2'/>"
+        "<float value='0.4'/></uniform-deviate><int value='2'/></extern-function></define-basic-event>"
+        "</define-fault-tree></opsa-mef>")
+    m = mef.parse(xml, allow_extern=True)
+    assert m.probability("e1") == pytest.approx(0.3, rel=1e-15)
+    assert m.probability("e2") == pytest.approx(0.25, rel=1e-15)
+    assert m.probability("e3") == pytest.approx(0.15, rel=1e-15)  # the deviate's mean
+    g = mef.load(xml, allow_extern=True)
+    q = lambda p: math.floor(p * TWO32) / TWO32
+    assert oracle_mod.bdd_probability(g) == pytest.approx(1 - (1 - q(0.3)) * (1 - q(0.25)), rel=1e-9)
+    d = mef.sample_expressions(m, {"e3": m.basic_events["e3"]}, 2000, np.random.default_rng(3))["e3"]
+    assert d.min() >= 0.1 and d.max() <= 0.2 and abs(d.mean() - 0.15) < 0.005
+    with pytest.raises(mef.MefError, match="disallowed"):
+        mef.parse(xml)
+    for path, msg in [("", "invalid library path"), ("lib/", "invalid library path"), ("lib:", "invalid library path"),
+                      ("..", "invalid library path"), ("lib/none", "cannot open")]:
+        with pytest.raises(mef.MefError, match=msg):
+            mef.parse(f"<opsa-mef><define-extern-library name='l' path='{path}'/></opsa-mef>", allow_extern=True)
+
+
+@pytest.mark.gpu
+def test_substitution_model_through_the_engine(oracle_mod, gpu):
+    from mcscram_b200 import _capi
+    g = mef.load(SUB_FIX)
+    with _capi.Engine(g, mode=_capi.MODE_STRIP) as e:
+        e.run(2, 1, 0, 1 << 14)
+        ones, total = e.tallies()
+    assert int(ones[0]) == int(oracle_mod.tallies(g, 2, 1, 0, 1 << 14)[0])
+    p = int(ones[0]) / total
+    assert abs(p - _substitution_fixture_exact()) <= 5 * math.sqrt(p * (1 - p) / total)

@@ -6,7 +6,8 @@ the Aralia set and event-tree models use.
 Fault trees: ``define-fault-tree`` / ``define-component`` / ``model-data``
 holding ``define-gate`` (formulas ``and``, ``or``, ``not``, ``xor``,
 ``nand``, ``nor``, ``atleast min=k``, ``cardinality min max``, ``imply``,
-``iff``, or a single event reference, nested formulas allowed),
+``iff``, or a single event reference; the arguments are events, their
+negations or constants, as the reference's schema has them),
 ``define-basic-event`` and ``define-parameter`` with an expression,
 ``define-house-event`` (``constant value="true|false"``).  Expressions:
 ``float``, ``int``, ``bool``, ``pi``, ``parameter``,
@@ -61,8 +62,7 @@ Node numbering follows the reference's PDAG construction from a MEF gate
 order a depth-first walk of the top formula first meets them
 (``GatherVariables``), then gates get the next indices in pre-order as they
 are built (``ConstructGate``).  ``not`` of a single event inside a formula
-becomes a complemented argument; other nested formulas become gates of their
-own.  ``imply``, ``iff`` and ``cardinality`` become the gates the
+becomes a complemented argument.  ``imply``, ``iff`` and ``cardinality`` become the gates the
 reference's ``ConstructComplexGate`` builds (src/pdag.cc:660-716).  House
 events become variables with probability 0 or 1 (constant words).  SCRAM's
 preprocessing passes are not applied, so event indices can differ from the
@@ -784,6 +784,8 @@ def _parse_formula(el: ET.Element, where: str) -> Formula:
         return Formula(NULL, [_parse_arg(el, where)])
     if tag not in _CONNECTIVES and tag not in _COMPLEX:
         raise MefError(f"{where}: unsupported formula <{tag}>")
+    if tag == "not" and not (len(_kids(el)) == 1 and _local(_kids(el)[0].tag) in _REFS):
+        raise MefError(f"{where}: <not> takes one event")
     args = [_parse_arg(c, where) for c in _kids(el)]
     k = int(el.get("min")) if el.get("min") is not None else None
     kmax = int(el.get("max")) if el.get("max") is not None else None
@@ -816,7 +818,8 @@ def _parse_arg(el: ET.Element, where: str) -> Tuple[bool, str, object]:
         if len(kids) == 1 and _local(kids[0].tag) in _REFS:
             comp, kind, x = _parse_arg(kids[0], where)
             return (not comp), kind, x
-    return False, "formula", _parse_formula(el, where)
+    # share/input.rng:664-672: an argument is an event, the negation of one or a constant
+    raise MefError(f"{where}: nested formula <{tag}>: an argument is an event, its negation or a constant")
 
 
 class _Scope:
@@ -959,20 +962,56 @@ def _find_cycle(edges: Dict[str, List[str]]) -> Optional[str]:
     return None
 
 
-def _document(source: Union[str, Path]) -> ET.Element:
-    text = Path(source).read_text() if isinstance(source, Path) or (
-        isinstance(source, str) and not source.lstrip().startswith("<")) else source
+_XINCLUDE = "{http://www.w3.org/2001/XInclude}include"
+_INT_MAX = (1 << 31) - 1
+
+
+def _document(source: Union[str, Path], _including: Tuple[Path, ...] = ()) -> ET.Element:
+    """One MEF document, its XIncludes resolved, with the checks the
+    reference's RELAX NG schema makes on what this reader keeps
+    (share/input.rng): no element or attribute of a foreign namespace, no
+    blank label or attribute value, ints within 32 bits."""
+    is_file = isinstance(source, Path) or not source.lstrip().startswith("<")
+    if is_file and Path(source).resolve() in _including:
+        raise MefError(f"XInclude cycle through {str(source)!r}")
+    text = Path(source).read_text() if is_file else source
     try:
         root = ET.fromstring(text.lstrip("\ufeff"))
     except ET.ParseError as e:
         raise MefError(f"not well-formed XML: {e}") from None
     if _local(root.tag) != "opsa-mef":
         raise MefError("root element is not <opsa-mef>")
-    for el in root.iter():  # names and references without surrounding blanks
-        for a in ("name", "event-tree", "functional-event", "state"):
+    chain = _including + ((Path(source).resolve(),) if is_file else ())
+    for parent in list(root.iter()):  # XInclude of another document's top-level elements
+        for i, child in reversed(list(enumerate(parent))):
+            if child.tag != _XINCLUDE:
+                continue
+            href, xp = child.get("href"), (child.get("xpointer") or "").replace(" ", "")
+            if not href or xp != "xpointer(/opsa-mef/*)":
+                raise MefError(f"XInclude of {href!r}: only xpointer(/opsa-mef/*) of a file is read")
+            target = _directory(source) / href
+            if not target.is_file():
+                raise MefError(f"XInclude of {href!r}: no such file")
+            parent[i:i + 1] = list(_document(target, chain))
+    for el in root.iter():
+        if "}" in el.tag or any("}" in a for a in el.keys()):
+            raise MefError(f"<{el.tag}>: elements and attributes of other namespaces are not MEF")
+        for a in ("name", "event-tree", "functional-event", "state"):  # names without surrounding blanks
             if el.get(a) is not None:
                 el.set(a, el.get(a).strip())
-        if _local(el.tag) == "attributes":
+        tag = el.tag
+        if tag == "label" and not (el.text or "").strip():
+            raise MefError("a <label> without text")
+        if tag == "attribute" and not (el.get("value") or "").strip():
+            raise MefError(f"attribute {el.get('name')!r} without a value")
+        if tag == "int" and el.get("value") is not None:  # a valueless <int/> is an extern parameter type
+            try:
+                v = int((el.get("value") or "").strip())
+            except ValueError:
+                raise MefError(f"<int value={el.get('value')!r}> is not an integer") from None
+            if abs(v) > _INT_MAX:
+                raise MefError(f"<int value={el.get('value')!r}> overflows a 32-bit int")
+        if tag == "attributes":
             names = [a.get("name") for a in el]
             if len(names) != len(set(names)):
                 raise MefError(f"an element repeats one of its attributes {sorted(names)}")
@@ -1019,6 +1058,9 @@ def parse(source: Union[str, Path, List[Union[str, Path]]],
     are loaded only with `allow_extern` (SCRAM's --allow-extern): loading one
     runs its code."""
     sources = source if isinstance(source, (list, tuple)) else [source]
+    files = [Path(x).resolve() for x in sources if isinstance(x, Path) or not x.lstrip().startswith("<")]
+    if len(files) != len(set(files)):
+        raise MefError("the same file is given twice")
     roots = [_document(x) for x in sources]
     dirs = [_directory(x) for x in sources]
     m = MefModel(mission_time=float(mission_time))

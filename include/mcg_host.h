@@ -149,7 +149,10 @@ mcg_status mcg_sample_shape(uint64_t num_trials, uint64_t max_words_per_iteratio
  *     mif = P(top | x=1) - P(top | x=0)  (Birnbaum),
  * and cif, raw, dif, rrw from mif as the exact analysis defines them
  * (src/importance_analysis.cc:50-56), p being the probability the sampler
- * draws (threshold / 2^32).  Replaces the Monte Carlo importance analysis
+ * draws (threshold / 2^32); as there, cif, raw, dif and rrw stay 0 when
+ * P(top) = 0, and rrw stays 0 when P(top) = p * mif.  A conditional that no
+ * sample can estimate (p = 0 or p = 1) and the mif from it are NaN.
+ * Replaces the Monte Carlo importance analysis
  * the reference leaves as a stub (src/mc/core/importance_analysis.cc).
  * run may be NULL (strip mode, device 0).  Conditional estimates of an
  * event with small p rest on about p * samples draws. */
@@ -163,6 +166,13 @@ typedef struct mcg_importance_factor {
 mcg_status mcg_importance_factors(const mcg_graph_desc *graph, const uint32_t *events, uint32_t n_events,
                                   const mcg_run_desc *run, uint32_t iteration, uint64_t word_count,
                                   mcg_importance_factor *out);
+
+/* The factors of one event from its probability p and the top event's
+ * P(top), P(top | x=1) and P(top | x=0) (exact, or estimated elsewhere), by
+ * the same relations as mcg_importance_factors; p_joint = p * P(top | x=1),
+ * samples = 0.  Host only: it needs no device. */
+mcg_status mcg_importance_from_conditionals(double p, double p_top, double p_top_given_1, double p_top_given_0,
+                                            mcg_importance_factor *out);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,36 @@
 #include "mcg.h"
 #include "mcg_host.h"
 
+// mif from the conditionals, then the exact analysis's relations and its
+// zeros where they are undefined (src/importance_analysis.cc:50-56)
+static void factors_from_conditionals(double p, double p_top, double given_1, double given_0,
+                                      mcg_importance_factor &f) {
+    f.p = p;
+    f.p_top = p_top;
+    f.p_top_given_1 = given_1;
+    f.p_top_given_0 = given_0;
+    f.mif = given_1 - given_0;
+    f.cif = f.raw = f.dif = f.rrw = 0.0;
+    if (p_top != 0) {
+        f.cif = p * f.mif / p_top;
+        f.raw = 1.0 + (1.0 - p) * f.mif / p_top;
+        f.dif = p * f.raw;
+        if (p_top != p * f.mif) f.rrw = p_top / (p_top - p * f.mif);
+    }
+}
+
+extern "C" mcg_status mcg_importance_from_conditionals(double p, double p_top, double p_top_given_1,
+                                                       double p_top_given_0, mcg_importance_factor *out) {
+    mcg::clear_error();
+    if (!out) return mcg::fail(MCG_ERR_INVALID, "out must not be NULL");
+    if (!(p >= 0.0 && p <= 1.0) || !(p_top >= 0.0 && p_top <= 1.0))
+        return mcg::fail(MCG_ERR_INVALID, "p and p_top must be probabilities");
+    std::memset(out, 0, sizeof(*out));
+    out->p_joint = p * p_top_given_1;
+    factors_from_conditionals(p, p_top, p_top_given_1, p_top_given_0, *out);
+    return MCG_OK;
+}
+
 extern "C" mcg_status mcg_importance_factors(const mcg_graph_desc *graph, const uint32_t *events, uint32_t n_events,
                                              const mcg_run_desc *run_in, uint32_t iteration, uint64_t word_count,
                                              mcg_importance_factor *out) {
@@ -93,22 +123,9 @@ extern "C" mcg_status mcg_importance_factors(const mcg_graph_desc *graph, const 
         const uint64_t thr = g.be_threshold[ev[j]];
         const double p = thr >= (1ull << 32) ? 1.0 : (double)thr / 4294967296.0;  // the probability sampled
         const double joint = (double)ones[1 + j] / n;
-        f.p = p;
         f.samples = total;
-        f.p_top = p_top;
         f.p_joint = joint;
-        f.p_top_given_1 = p > 0 ? joint / p : nan;
-        f.p_top_given_0 = p < 1 ? (p_top - joint) / (1.0 - p) : nan;
-        f.mif = f.p_top_given_1 - f.p_top_given_0;
-        // the exact analysis's relations (src/importance_analysis.cc:50-56)
-        if (p_top > 0) {
-            f.cif = p * f.mif / p_top;
-            f.raw = 1.0 + (1.0 - p) * f.mif / p_top;
-            f.dif = p * f.raw;
-            f.rrw = p_top != p * f.mif ? p_top / (p_top - p * f.mif) : std::numeric_limits<double>::infinity();
-        } else {
-            f.cif = f.raw = f.dif = f.rrw = nan;
-        }
+        factors_from_conditionals(p, p_top, p > 0 ? joint / p : nan, p < 1 ? (p_top - joint) / (1.0 - p) : nan, f);
     }
     return MCG_OK;
 }

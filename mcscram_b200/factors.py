@@ -31,7 +31,17 @@ _capi.register_signatures({
     "mcg_importance_factors": (C.c_int, [C.POINTER(_capi.GraphDesc), C.POINTER(C.c_uint32), C.c_uint32,
                                          C.POINTER(_capi.RunDesc), C.c_uint32, C.c_uint64,
                                          C.POINTER(ImportanceFactor)]),
+    "mcg_importance_from_conditionals": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double,
+                                                   C.POINTER(ImportanceFactor)]),
 })
+
+
+def factors_from_conditionals(p: float, p_top: float, p_top_given_1: float, p_top_given_0: float) -> dict:
+    """The factors of one event from exact (or externally estimated)
+    conditionals, by the relations mcg_importance_factors applies; host only."""
+    out = ImportanceFactor()
+    _capi.check(_capi.load().mcg_importance_from_conditionals(p, p_top, p_top_given_1, p_top_given_0, C.byref(out)))
+    return out.as_dict()
 
 
 def importance_factors(g: FlatGraph, events: Optional[Sequence[int]] = None, words: int = 1 << 20,

@@ -1993,6 +1993,64 @@ def probability_over_time(model: MefModel, time_step: float, top: Optional[str] 
     return [(float(o) / n, t) for o, t in zip(ones, times)]
 
 
+_SIL_PFD_BOUNDS = (1e-5, 1e-4, 1e-3, 1e-2, 1e-1, 1.0)  # SIL 4 .. 1, then beyond; lower bound 0
+_SIL_PFH_BOUNDS = (1e-9, 1e-8, 1e-7, 1e-6, 1e-5, 1.0)
+
+
+def _average_y(points) -> float:
+    """Trapezoid integral of y over x divided by the x range (points are
+    (y, x) in ascending x)."""
+    area = sum((y1 + y0) * (x1 - x0) for (y0, x0), (y1, x1) in zip(points, points[1:])) / 2
+    return area / (points[-1][1] - points[0][1])
+
+
+def _partition_y(points, bounds) -> List[Tuple[float, float]]:
+    """Share of the x range over which the piecewise-linear y lies in each
+    bucket (lower, upper], the first bucket's lower bound being 0."""
+    share = [0.0] * len(bounds)
+    for (p0, t0), (p1, t1) in zip(points, points[1:]):
+        k = (p1 - p0) / (t1 - t0)
+        if k < 0:
+            k, p0, p1 = -k, p1, p0
+        b0 = 0.0
+        for i, b1 in enumerate(bounds):
+            if p0 <= b0 and b1 <= p1:  # the bucket lies inside the segment's y range
+                share[i] += (b1 - b0) / k
+            elif b0 <= p0 and p1 <= b1:  # the segment lies inside the bucket (k = 0 included)
+                share[i] += t1 - t0
+            elif p0 <= b0 <= p1:
+                share[i] += (p1 - b0) / k
+            elif p0 <= b1 <= p1:
+                share[i] += (b1 - p0) / k
+            b0 = b1
+    span = points[-1][1] - points[0][1]
+    return [(b, s / span) for b, s in zip(bounds, share)]
+
+
+def safety_integrity_levels(curve) -> dict:
+    """SIL metrics of a probability-over-time curve of (P(top), t) pairs, as
+    the reference's ComputeSil makes them (mcSCRAM
+    src/probability_analysis.cc:58-155): the average probability of failure
+    on demand (PFD, the curve's time average), the average failure frequency
+    per hour (PFH, the time average of P(t) / t, 0 at t = 0), and the share
+    of the mission time spent in each SIL band, as (upper bound, fraction)
+    pairs for the PFD bands 1e-5 .. 1 and the PFH bands 1e-9 .. 1.  A curve of
+    one point puts its whole weight in the PFD band holding it."""
+    curve = [(float(p), float(t)) for p, t in curve]
+    if not curve:
+        raise MefError("an empty probability curve")
+    if len(curve) == 1:
+        pfd = curve[0][0]
+        band = next(i for i, b in enumerate(_SIL_PFD_BOUNDS) if pfd <= b)
+        return {"pfd_avg": pfd, "pfh_avg": 0.0,
+                "pfd_fractions": [(b, 1.0 if i == band else 0.0) for i, b in enumerate(_SIL_PFD_BOUNDS)],
+                "pfh_fractions": [(b, 0.0) for b in _SIL_PFH_BOUNDS]}
+    pfh = [(p / t if t else 0.0, t) for p, t in curve]
+    return {"pfd_avg": _average_y(curve), "pfh_avg": _average_y(pfh),
+            "pfd_fractions": _partition_y(curve, _SIL_PFD_BOUNDS),
+            "pfh_fractions": _partition_y(pfh, _SIL_PFH_BOUNDS)}
+
+
 def main(argv=None) -> int:
     """python -m mcscram_b200.mef MODEL.xml [--top GATE] [--samples N] [--mode strip|staged|fused] [--ccf]:
     estimates the top-event probability of a MEF model on the GPU and prints

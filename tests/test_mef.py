@@ -835,3 +835,69 @@ def test_reference_bscu_uncertainty(oracle_mod):
     assert top.mean() == pytest.approx(0.117, abs=5e-3)
     assert top.std(ddof=1) == pytest.approx(0.183, abs=5e-3)
 
+
+
+def _exact_curve(oracle_mod, m, step, mission_time):
+    """(P(top), t) at the reference's time grid, each point exact (BDD)."""
+    times, k = [], 0
+    while k * step < mission_time:
+        times.append(k * step)
+        k += 1
+    times.append(mission_time)
+    _, _, var_index, _ = m.build()
+    g = m.flat()
+    name_of = {i: n for n, i in var_index.items()}
+    return [(oracle_mod.bdd_probability(g, np.array([m.probability(name_of[int(x)], t) for x in g.be_pdag_idx])), t)
+            for t in times]
+
+
+SINGLE_EXP = Path("/root/reference/tests/input/core/single_exponential.xml")
+
+
+@pytest.mark.skipif(not SINGLE_EXP.exists(), reason="the reference's test models are not on this machine")
+def test_reference_probability_curve_and_sil(oracle_mod):
+    """tests/risk_analysis_tests.cc:355-408: the curve of a single exponential
+    event (rate 1e-5) at steps of 24 h up to 120 h, and its SIL metrics over
+    the default 8760 h (PFD 0.04255, PFH 9.77e-6 and the band fractions),
+    all to the reference's 1e-3."""
+    m = mef.parse(SINGLE_EXP)
+    curve = _exact_curve(oracle_mod, m, 24.0, 120.0)
+    assert [t for _, t in curve] == [0, 24, 48, 72, 96, 120]
+    for (p, _), want in zip(curve, [0, 2.399e-4, 4.7989e-4, 7.197e-4, 9.595e-4, 1.199e-3]):
+        assert p == pytest.approx(want, rel=1e-3, abs=1e-12)
+    sil = mef.safety_integrity_levels(_exact_curve(oracle_mod, m, 24.0, 8760.0))
+    assert sil["pfd_avg"] == pytest.approx(0.04255, rel=1e-3)
+    assert sil["pfh_avg"] == pytest.approx(9.77e-6, rel=1e-3)
+    for (_, got), want in zip(sil["pfd_fractions"], [1.142e-4, 1.0275e-3, 1.02796e-2, 0.1033, 0.88527, 0]):
+        assert got == pytest.approx(want, rel=1e-3, abs=1e-12)
+    for (_, got), want in zip(sil["pfh_fractions"], [2.74e-7, 2.466e-6, 2.466e-5, 2.466e-4, 0.999726, 0]):
+        assert got == pytest.approx(want, rel=1e-3, abs=1e-12)
+
+
+def test_sil_of_simple_curves():
+    """Hand-checkable curves: a constant curve puts all the time in its band;
+    a straight line from 0 to 2e-5 spends half its time below 1e-5; one point
+    counts whole."""
+    flat = mef.safety_integrity_levels([(0.05, 0.0), (0.05, 100.0)])
+    assert flat["pfd_avg"] == pytest.approx(0.05)
+    assert [f for _, f in flat["pfd_fractions"]] == [0, 0, 0, 0, 1.0, 0]
+    line = mef.safety_integrity_levels([(0.0, 0.0), (2e-5, 10.0)])
+    assert line["pfd_avg"] == pytest.approx(1e-5)
+    assert [f for _, f in line["pfd_fractions"]][:2] == [pytest.approx(0.5), pytest.approx(0.5)]
+    one = mef.safety_integrity_levels([(3e-3, 10.0)])
+    assert one["pfd_avg"] == 3e-3 and [f for _, f in one["pfd_fractions"]] == [0, 0, 0, 1.0, 0, 0]
+
+
+@pytest.mark.gpu
+def test_sil_from_the_gpu_curve(oracle_mod, gpu):
+    """SIL metrics of the batched GPU curve of the timed fixture against those
+    of the exact curve: averages within 1 % (2^20 samples a point, p from 1e-3
+    to 0.3), band fractions within 0.02 of the mission time."""
+    m = mef.parse(TIMED, mission_time=2000.0)
+    got = mef.safety_integrity_levels(mef.probability_over_time(m, time_step=50.0, words=1 << 14, iteration=5))
+    want = mef.safety_integrity_levels(_exact_curve(oracle_mod, m, 50.0, 2000.0))
+    assert got["pfd_avg"] == pytest.approx(want["pfd_avg"], rel=1e-2)
+    assert got["pfh_avg"] == pytest.approx(want["pfh_avg"], rel=1e-2)
+    for key in ("pfd_fractions", "pfh_fractions"):
+        for (b, f), (_, w) in zip(got[key], want[key]):
+            assert abs(f - w) <= 0.02, (key, b)

@@ -100,6 +100,7 @@ _SIGNATURES = {
     "mcg_destroy": (C.c_int, [C.c_void_p]),
     "mcg_run": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64]),
     "mcg_synchronize": (C.c_int, [C.c_void_p]),
+    "mcg_trim_memory": (C.c_int, [C.c_int]),
     "mcg_read_tallies": (C.c_int, [C.c_void_p, _u64p, _u64p]),
     "mcg_tally_device_ptr": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "mcg_set_tallies": (C.c_int, [C.c_void_p, _u64p, C.c_uint64]),

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -49,7 +50,80 @@ cudaError_t upload(T **dptr, const std::vector<T> &v) {
     return cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
+// The engines' large work buffers (strip and fused scratch, staged chunk
+// buffers: gigabytes for a large tree) come from one stream-ordered pool per
+// device that keeps what is freed.  Destroying an engine then neither
+// synchronises the device nor unmaps the pages, and the next engine on the
+// device takes the memory back without a driver allocation; mcg_trim_memory
+// hands it back to the driver.
+std::mutex g_pool_mutex;
+std::vector<cudaMemPool_t> g_pools;
+
+cudaError_t work_pool(int device, cudaMemPool_t *out) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (g_pools.size() <= (size_t)device) g_pools.resize((size_t)device + 1, nullptr);
+    if (!g_pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t err = cudaMemPoolCreate(&pool, &props);
+        if (err != cudaSuccess) return err;
+        uint64_t keep = ~0ull;  // never release on synchronisation
+        err = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (err != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return err;
+        }
+        g_pools[device] = pool;
+    }
+    *out = g_pools[device];
+    return cudaSuccess;
+}
+
+// Ordered on the engine's stream; on a failed allocation the pool's unused
+// memory goes back to the driver and the allocation is tried once more.
+cudaError_t work_alloc(mcg_engine *e, void **ptr, size_t bytes) {
+    *ptr = nullptr;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t err = work_pool(e->device, &pool);
+    if (err != cudaSuccess) return err;
+    err = cudaMallocFromPoolAsync(ptr, bytes, pool, e->stream);
+    if (err == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        cudaStreamSynchronize(e->stream);
+        cudaMemPoolTrimTo(pool, 0);
+        err = cudaMallocFromPoolAsync(ptr, bytes, pool, e->stream);
+    }
+    return err;
+}
+
+void work_free(mcg_engine *e, void *ptr) {
+    if (ptr) cudaFreeAsync(ptr, e->stream);
+}
+
 }  // namespace
+
+extern "C" mcg_status mcg_trim_memory(int device) {
+    mcg::clear_error();
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        if (device >= 0 && (size_t)device < g_pools.size()) pool = g_pools[device];
+    }
+    if (!pool) return MCG_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
+        cudaSetDevice(prev);
+        return mcg::fail(MCG_ERR_CUDA, std::string("mcg_trim_memory: ") + cudaGetErrorString(cudaGetLastError()));
+    }
+    cudaSetDevice(prev);
+    return MCG_OK;
+}
 
 namespace {
 
@@ -297,7 +371,8 @@ mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
                                   (int)std::max<uint32_t>(e->smem_bytes, 1)));
     MCG_CUDA(upload(reinterpret_cast<mcg::Op **>(&e->d_ops), e->prog.ops));
     if (e->prog.global_slots && e->mode == MCG_MODE_FUSED) {
-        MCG_CUDA(cudaMalloc((void **)&e->d_scratch, (size_t)e->prog.global_slots * e->scratch_stride * sizeof(uint64_t)));
+        MCG_CUDA(work_alloc(e, (void **)&e->d_scratch,
+                            (size_t)e->prog.global_slots * e->scratch_stride * sizeof(uint64_t)));
     }
     return MCG_OK;
 }
@@ -316,7 +391,7 @@ mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
     words = std::max<uint64_t>(256, std::min<uint64_t>(words, 1ull << 20));
     words = (words + 255) / 256 * 256;
     e->stage_words = words;
-    for (int i = 0; i < 2; ++i) MCG_CUDA(cudaMalloc((void **)&e->d_stage[i], nn * words * sizeof(uint64_t)));
+    for (int i = 0; i < 2; ++i) MCG_CUDA(work_alloc(e, (void **)&e->d_stage[i], nn * words * sizeof(uint64_t)));
     MCG_CUDA(cudaMalloc((void **)&e->d_event_table,
                         std::max<uint64_t>(e->graph.n_be, 1) * mcg::dev::kEventTableStride * sizeof(uint2)));
     // Cap the resident sampler blocks per SM through their shared-memory
@@ -373,7 +448,7 @@ mcg_status setup_strip(mcg_engine *e, const mcg_run_desc &run) {
     e->strip_grid = (uint32_t)(prop.multiProcessorCount * per_sm);
     const uint64_t warps = (uint64_t)e->strip_grid * (mcg::dev::kStripThreads / 32);
     const uint64_t bytes = warps * std::max<uint64_t>(g.n_nodes(), 1) * mcg::dev::kStripLanes * sizeof(uint64_t);
-    MCG_CUDA(cudaMalloc((void **)&e->d_strip_scratch, bytes));
+    MCG_CUDA(work_alloc(e, (void **)&e->d_strip_scratch, bytes));
     MCG_CUDA(cudaMalloc((void **)&e->d_queue, sizeof(unsigned long long)));
     MCG_CUDA(cudaMalloc((void **)&e->d_event_table,
                         std::max<uint64_t>(g.n_be, 1) * mcg::dev::kEventTableStride * sizeof(uint2)));
@@ -551,8 +626,16 @@ mcg_status launch_fused(mcg_engine *e, uint32_t it_first, uint32_t n_it, uint64_
 }
 
 void release(mcg_engine *e) {
+    // the side streams' work ends before their buffers go back to the pool
+    if (e->s_a) cudaStreamSynchronize(e->s_a);
+    if (e->s_b) cudaStreamSynchronize(e->s_b);
+    if (e->stream) {
+        work_free(e, e->d_scratch);
+        work_free(e, e->d_stage[0]);
+        work_free(e, e->d_stage[1]);
+        work_free(e, e->d_strip_scratch);
+    }
     cudaFree(e->d_ops);
-    cudaFree(e->d_scratch);
     cudaFree(e->d_tally);
     cudaFree(e->d_be);
     cudaFree(e->d_meta);
@@ -566,9 +649,6 @@ void release(mcg_engine *e) {
     cudaFree(e->d_be_tally_nodes);
     cudaFree(e->d_be_tally_idx);
     cudaFree(e->d_event_table);
-    cudaFree(e->d_stage[0]);
-    cudaFree(e->d_stage[1]);
-    cudaFree(e->d_strip_scratch);
     cudaFree(e->d_queue);
     cudaFree(e->d_strip_groups);
     cudaFree(e->d_strip_gin);
@@ -655,6 +735,9 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
         if (e->mode == MCG_MODE_FUSED) st = setup_fused(e, run);
         else if (e->mode == MCG_MODE_STAGED) st = setup_staged(e, run);
         else if (e->mode == MCG_MODE_STRIP) st = setup_strip(e, run);
+        // the pool's buffers are ordered on e->stream: complete them for every stream
+        if (st == MCG_OK && cudaStreamSynchronize(e->stream) != cudaSuccess)
+            st = mcg::fail(MCG_ERR_CUDA, "stream synchronisation after set-up failed");
     } while (false);
     if (st != MCG_OK) {
         release(e);

@@ -175,3 +175,22 @@ def test_config1_top_within_3sigma_of_bdd(capi, oracle_mod, gpu):
 def test_sampler_peak_runs(capi, gpu):
     rate = capi.sampler_peak(n_events=64, n_words=1 << 18, repeats=2)
     assert rate > 1e9
+
+
+def test_engines_reuse_the_work_pool(capi, oracle_mod, gpu):
+    """Engines created one after another (every mode, and the strip engine
+    again after the pool is trimmed) take their work buffers from the
+    per-device pool a destroyed engine returned them to: every one still
+    gives the oracle's tallies."""
+    g = synth.config1()
+    words = 1 << 12
+    want = oracle_mod.tallies(g, 2, 1, 0, words)
+    for mode in ("strip", "fused", "staged", "strip", "fused"):
+        with engine(capi, g, mode=capi.MODES[mode]) as e:
+            e.run(2, 1, 0, words)
+            ones, total = e.tallies()
+        assert np.array_equal(ones, want) and total == words * 64, mode
+    capi.check(capi.load().mcg_trim_memory(0))
+    with engine(capi, g, mode=capi.MODE_STRIP) as e:
+        e.run(2, 1, 0, words)
+        assert np.array_equal(e.tallies()[0], want)

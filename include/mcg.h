@@ -117,14 +117,15 @@ typedef struct mcg_program_info {
 mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run, mcg_engine **out);
 
 /* Frees every device allocation of the engine.  The large work buffers
- * (strip and fused scratch, staged chunk buffers) return to a per-device
- * pool that keeps them for the next engine on the device, without a device
- * synchronisation; mcg_trim_memory gives them back to the driver.
+ * (strip and fused scratch, staged chunk buffers) are kept for the next
+ * engine on the device, which takes the smallest kept one that fits instead
+ * of allocating (at most 2 buffers, 32 GB per device; an allocation that
+ * fails frees them first); mcg_trim_memory frees them.
  * Replaces layer_manager::~layer_manager (src/mc/queue/layer_manager.tpp:282-301). */
 mcg_status mcg_destroy(mcg_engine *engine);
 
-/* Waits for the device, then returns the work-buffer pool's unused memory
- * on `device` to the driver (nothing to do when no engine ran there). */
+/* Frees the work buffers kept on `device` (none when no engine was
+ * destroyed there).  No engine may be mid-destruction on that device. */
 mcg_status mcg_trim_memory(int device);
 
 /* Enqueues n_iterations passes, numbered iteration_first, iteration_first+1, ...

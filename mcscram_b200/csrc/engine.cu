@@ -51,76 +51,95 @@ cudaError_t upload(T **dptr, const std::vector<T> &v) {
 }
 
 // The engines' large work buffers (strip and fused scratch, staged chunk
-// buffers: gigabytes for a large tree) come from one stream-ordered pool per
-// device that keeps what is freed.  Destroying an engine then neither
-// synchronises the device nor unmaps the pages, and the next engine on the
-// device takes the memory back without a driver allocation; mcg_trim_memory
-// hands it back to the driver.
-std::mutex g_pool_mutex;
-std::vector<cudaMemPool_t> g_pools;
+// buffers: gigabytes for a large tree) are kept per device when an engine is
+// destroyed (it has synchronised its streams by then), and the next engine
+// takes the smallest kept buffer that fits instead of allocating.  What does
+// not fit comes from cudaMalloc; at most kKeptBuffers buffers and
+// kKeptBytes bytes are kept per device, and a failed allocation first
+// frees the kept ones.  mcg_trim_memory frees them all.
+constexpr size_t kKeptBuffers = 2;
+constexpr size_t kKeptBytes = 32ull << 30;
 
-cudaError_t work_pool(int device, cudaMemPool_t *out) {
-    std::lock_guard<std::mutex> lock(g_pool_mutex);
-    if (g_pools.size() <= (size_t)device) g_pools.resize((size_t)device + 1, nullptr);
-    if (!g_pools[device]) {
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.handleTypes = cudaMemHandleTypeNone;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = device;
-        cudaMemPool_t pool = nullptr;
-        cudaError_t err = cudaMemPoolCreate(&pool, &props);
-        if (err != cudaSuccess) return err;
-        uint64_t keep = ~0ull;  // never release on synchronisation
-        err = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        if (err != cudaSuccess) {
-            cudaMemPoolDestroy(pool);
-            return err;
-        }
-        g_pools[device] = pool;
-    }
-    *out = g_pools[device];
-    return cudaSuccess;
+struct KeptBuffer {
+    void *ptr;
+    size_t bytes;
+};
+std::mutex g_kept_mutex;
+std::vector<std::vector<KeptBuffer>> g_kept;  // per device
+
+std::vector<KeptBuffer> &kept_on(int device) {
+    if (g_kept.size() <= (size_t)device) g_kept.resize((size_t)device + 1);
+    return g_kept[device];
 }
 
-// Ordered on the engine's stream; on a failed allocation the pool's unused
-// memory goes back to the driver and the allocation is tried once more.
+void free_kept(int device) {
+    std::vector<KeptBuffer> drop;
+    {
+        std::lock_guard<std::mutex> lock(g_kept_mutex);
+        drop.swap(kept_on(device));
+    }
+    for (const KeptBuffer &b : drop) cudaFree(b.ptr);
+}
+
 cudaError_t work_alloc(mcg_engine *e, void **ptr, size_t bytes) {
     *ptr = nullptr;
-    cudaMemPool_t pool = nullptr;
-    cudaError_t err = work_pool(e->device, &pool);
-    if (err != cudaSuccess) return err;
-    err = cudaMallocFromPoolAsync(ptr, bytes, pool, e->stream);
+    {
+        std::lock_guard<std::mutex> lock(g_kept_mutex);
+        std::vector<KeptBuffer> &kept = kept_on(e->device);
+        size_t best = kept.size();
+        for (size_t i = 0; i < kept.size(); ++i)
+            if (kept[i].bytes >= bytes && (best == kept.size() || kept[i].bytes < kept[best].bytes)) best = i;
+        if (best < kept.size()) {
+            *ptr = kept[best].ptr;
+            e->work_bytes[*ptr] = kept[best].bytes;
+            kept.erase(kept.begin() + (std::ptrdiff_t)best);
+            return cudaSuccess;
+        }
+    }
+    cudaError_t err = cudaMalloc(ptr, bytes);
     if (err == cudaErrorMemoryAllocation) {
         cudaGetLastError();
-        cudaStreamSynchronize(e->stream);
-        cudaMemPoolTrimTo(pool, 0);
-        err = cudaMallocFromPoolAsync(ptr, bytes, pool, e->stream);
+        free_kept(e->device);
+        err = cudaMalloc(ptr, bytes);
     }
+    if (err == cudaSuccess) e->work_bytes[*ptr] = bytes;
     return err;
 }
 
 void work_free(mcg_engine *e, void *ptr) {
-    if (ptr) cudaFreeAsync(ptr, e->stream);
+    if (!ptr) return;
+    const size_t bytes = e->work_bytes[ptr];
+    std::vector<KeptBuffer> drop;
+    {
+        std::lock_guard<std::mutex> lock(g_kept_mutex);
+        std::vector<KeptBuffer> &kept = kept_on(e->device);
+        kept.push_back({ptr, bytes});
+        size_t total = 0;
+        for (const KeptBuffer &b : kept) total += b.bytes;
+        while (!kept.empty() && (kept.size() > kKeptBuffers || total > kKeptBytes)) {
+            auto smallest = std::min_element(kept.begin(), kept.end(),
+                                             [](const KeptBuffer &a, const KeptBuffer &b) { return a.bytes < b.bytes; });
+            total -= smallest->bytes;
+            drop.push_back(*smallest);
+            kept.erase(smallest);
+        }
+    }
+    for (const KeptBuffer &b : drop) cudaFree(b.ptr);
 }
 
 }  // namespace
 
 extern "C" mcg_status mcg_trim_memory(int device) {
     mcg::clear_error();
-    cudaMemPool_t pool = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_pool_mutex);
-        if (device >= 0 && (size_t)device < g_pools.size()) pool = g_pools[device];
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) {
+        cudaGetLastError();
+        return mcg::fail(MCG_ERR_INVALID, "mcg_trim_memory: device ordinal out of range");
     }
-    if (!pool) return MCG_OK;
     int prev = 0;
     cudaGetDevice(&prev);
-    if (cudaSetDevice(device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
-        cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
-        cudaSetDevice(prev);
-        return mcg::fail(MCG_ERR_CUDA, std::string("mcg_trim_memory: ") + cudaGetErrorString(cudaGetLastError()));
-    }
+    cudaSetDevice(device);
+    free_kept(device);
     cudaSetDevice(prev);
     return MCG_OK;
 }
@@ -629,12 +648,11 @@ void release(mcg_engine *e) {
     // the side streams' work ends before their buffers go back to the pool
     if (e->s_a) cudaStreamSynchronize(e->s_a);
     if (e->s_b) cudaStreamSynchronize(e->s_b);
-    if (e->stream) {
-        work_free(e, e->d_scratch);
-        work_free(e, e->d_stage[0]);
-        work_free(e, e->d_stage[1]);
-        work_free(e, e->d_strip_scratch);
-    }
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    work_free(e, e->d_scratch);
+    work_free(e, e->d_stage[0]);
+    work_free(e, e->d_stage[1]);
+    work_free(e, e->d_strip_scratch);
     cudaFree(e->d_ops);
     cudaFree(e->d_tally);
     cudaFree(e->d_be);
@@ -735,9 +753,6 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
         if (e->mode == MCG_MODE_FUSED) st = setup_fused(e, run);
         else if (e->mode == MCG_MODE_STAGED) st = setup_staged(e, run);
         else if (e->mode == MCG_MODE_STRIP) st = setup_strip(e, run);
-        // the pool's buffers are ordered on e->stream: complete them for every stream
-        if (st == MCG_OK && cudaStreamSynchronize(e->stream) != cudaSuccess)
-            st = mcg::fail(MCG_ERR_CUDA, "stream synchronisation after set-up failed");
     } while (false);
     if (st != MCG_OK) {
         release(e);

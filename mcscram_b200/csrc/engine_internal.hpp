@@ -4,6 +4,7 @@
 
 #include <functional>
 #include <utility>
+#include <unordered_map>
 #include <vector>
 
 #include "graph.hpp"
@@ -21,6 +22,7 @@ struct mcg_engine {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    std::unordered_map<void *, size_t> work_bytes;  // sizes of the kept-buffer cache's allocations
     uint32_t mode = MCG_MODE_FUSED;
     mcg::Graph graph;
     mcg::Program prog;

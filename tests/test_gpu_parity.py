@@ -177,11 +177,10 @@ def test_sampler_peak_runs(capi, gpu):
     assert rate > 1e9
 
 
-def test_engines_reuse_the_work_pool(capi, oracle_mod, gpu):
+def test_engines_reuse_kept_work_buffers(capi, oracle_mod, gpu):
     """Engines created one after another (every mode, and the strip engine
-    again after the pool is trimmed) take their work buffers from the
-    per-device pool a destroyed engine returned them to: every one still
-    gives the oracle's tallies."""
+    again after mcg_trim_memory) take the work buffers a destroyed engine
+    left behind: every one still gives the oracle's tallies."""
     g = synth.config1()
     words = 1 << 12
     want = oracle_mod.tallies(g, 2, 1, 0, words)

@@ -901,3 +901,24 @@ def test_sil_from_the_gpu_curve(oracle_mod, gpu):
     for key in ("pfd_fractions", "pfh_fractions"):
         for (b, f), (_, w) in zip(got[key], want[key]):
             assert abs(f - w) <= 0.02, (key, b)
+
+
+CORE_EXACT = {  # tests/bench_core_tests.cc: the exact branch of each model's p_total expectation
+    "abc": 0.496, "ab_bc": 0.074, "ab_or_not_ac": 0.29, "atleast": 0.098, "a_or_not_a": 1.0, "a_or_not_b": 0.82,
+    "a_and_not_a": 0.0, "a_and_not_b": 0.08, "a_or_not_ab": 0.28, "multiple_parent_negative_gate": 0.9,
+    "nand_or_equality": 1.0, "not_and_or_equality": 1.0, "unity": 1.0, "null": 0.0, "xor": 0.404, "iff": 0.404,
+    "imply": 0.986, "cardinality": 0.49, "subtle_unity": 1.0, "subtle_null": 0.0, "zero_prob": 0.0, "one_prob": 1.0,
+    "beta_factor_ccf": 0.04308, "phi_factor_ccf": 0.04104, "mgl_ccf": 0.01630, "alpha_factor_ccf": 0.05298,
+}
+
+
+@pytest.mark.skipif(not CORE_IN.exists(), reason="the reference's core inputs are not on this machine")
+@pytest.mark.parametrize("name", list(CORE_EXACT))
+def test_reference_core_models(oracle_mod, name):
+    """Negations, constants, house events, the complex connectives and the
+    CCF models of the reference's core tests: exact probability of the
+    loaded graph (the sampler's quantised probabilities) against its
+    expectation (CCF ones to its 1e-5)."""
+    g = mef.parse(CORE_IN / f"{name}.xml", ccf_analysis="ccf" in name).flat()
+    tol = 1e-5 if "ccf" in name else 1e-8
+    assert oracle_mod.bdd_probability(g) == pytest.approx(CORE_EXACT[name], abs=tol)

@@ -922,3 +922,19 @@ def test_reference_core_models(oracle_mod, name):
     g = mef.parse(CORE_IN / f"{name}.xml", ccf_analysis="ccf" in name).flat()
     tol = 1e-5 if "ccf" in name else 1e-8
     assert oracle_mod.bdd_probability(g) == pytest.approx(CORE_EXACT[name], abs=tol)
+
+
+@pytest.mark.parametrize("body,want", [
+    # tests/expression_tests.cc:152-215, 419-448, 517-546 at the arguments' means
+    ("<exponential><float value='10'/><float value='5'/></exponential>", 1 - math.exp(-50)),
+    ("<GLM><float value='0.1'/><float value='10'/><float value='100'/><float value='5'/></GLM>",
+     (10 - (10 - 0.10 * 110) * math.exp(-110 * 5)) / 110),
+    ("<Weibull><float value='0.1'/><float value='10'/><float value='10'/><float value='500'/></Weibull>", 1.0),
+    ("<lognormal-deviate><float value='10'/><float value='5'/></lognormal-deviate>", 5.9105e9),
+    ("<histogram><float value='0'/><bin><float value='1'/><float value='2'/></bin>"
+     "<bin><float value='3'/><float value='4'/></bin></histogram>", 1.5),
+])
+def test_reference_expression_values(body, want):
+    m = mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")
+    got = m.parameters["p"].value(m.mission_time, m.parameters)
+    assert got == pytest.approx(want, rel=1e-12) if want != 5.9105e9 else abs(got - want) <= 1e6

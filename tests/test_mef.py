@@ -3,7 +3,10 @@ checked against a brute-force evaluation of the XML written here (not via
 the loader), node numbering against the reference's first-encounter rule,
 errors for what it does not read, and -- where the reference project is on
 disk -- its Aralia models against the exact values listed in its benchmark
-table.  The GPU test runs a loaded model through the engine."""
+table, and its own test expectations: initializer input lists, core and
+benchmark models, substitutions, extern functions, expressions, the
+probability curve and SIL metrics.  The GPU tests run loaded models through
+the engine.
 import csv
 import itertools
 import math

@@ -6,7 +6,7 @@ disk -- its Aralia models against the exact values listed in its benchmark
 table, and its own test expectations: initializer input lists, core and
 benchmark models, substitutions, extern functions, expressions, the
 probability curve and SIL metrics.  The GPU tests run loaded models through
-the engine.
+the engine."""
 import csv
 import itertools
 import math

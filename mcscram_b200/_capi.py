@@ -289,6 +289,12 @@ class Engine:
         return float(ms.value)
 
 
+def trim_memory(device: int = 0) -> None:
+    """Frees the work buffers destroyed engines left on `device` for the next
+    engine (mcg_trim_memory)."""
+    check(load().mcg_trim_memory(device))
+
+
 def sampler_peak(n_events: int = 256, n_words: int = 1 << 21, repeats: int = 5, device: int = 0) -> float:
     """Basic-event words per second of the register-only sampler kernel."""
     lib = load()

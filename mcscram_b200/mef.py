@@ -2052,9 +2052,11 @@ def safety_integrity_levels(curve) -> dict:
 
 
 def main(argv=None) -> int:
-    """python -m mcscram_b200.mef MODEL.xml [--top GATE] [--samples N] [--mode strip|staged|fused] [--ccf]:
-    estimates the top-event probability of a MEF model on the GPU and prints
-    it with its 95 % interval as one JSON line."""
+    """python -m mcscram_b200.mef MODEL.xml [--top GATE] [--samples N] [--mode strip|staged|fused] [--ccf]
+    [--allow-extern] [--time-step DT [--sil]]: estimates the top-event probability of a MEF model on the GPU
+    and prints it with its 95 % interval as one JSON line; with --time-step also the probability at t = 0,
+    DT, ... and the mission time (one batched launch, --samples per time point up to 2^30), and with --sil
+    the SIL metrics of that curve."""
     import argparse
     import json
     import math
@@ -2069,8 +2071,13 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--ccf", action="store_true", help="expand common-cause groups (CCF analysis)")
     ap.add_argument("--allow-extern", action="store_true", help="load the model's extern libraries (runs their code)")
+    ap.add_argument("--time-step", type=float, default=0.0, help="hours between points of the probability curve")
+    ap.add_argument("--sil", action="store_true", help="SIL metrics of the probability curve (needs --time-step)")
     args = ap.parse_args(argv)
-    g = load(args.model, args.top, ccf_analysis=args.ccf, allow_extern=args.allow_extern)
+    if args.sil and args.time_step <= 0:
+        ap.error("--sil needs --time-step")
+    m = parse(args.model, ccf_analysis=args.ccf, allow_extern=args.allow_extern)
+    g = m.flat(args.top)
     words = max(1, int(math.ceil(args.samples / 64)))
     with _capi.Engine(g, mode=_capi.MODES[args.mode], device=args.device) as e:
         done, it = 0, 1
@@ -2084,6 +2091,11 @@ def main(argv=None) -> int:
     half = 1.959963984540054 * math.sqrt(max(p * (1 - p), 0.0) / total)
     out = {"model": args.model, "top": g.name, "basic_events": g.n_be, "gates": g.n_gates, "samples": int(total),
            "p_top": p, "ci95": [max(p - half, 0.0), min(p + half, 1.0)]}
+    if args.time_step > 0:
+        curve = probability_over_time(m, args.time_step, args.top, words=min(words, 1 << 24), device=args.device)
+        out["p_time"] = [[pt, t] for pt, t in curve]
+        if args.sil:
+            out["sil"] = safety_integrity_levels(curve)
     print(json.dumps(out))
     return 0
 

@@ -941,3 +941,15 @@ def test_reference_expression_values(body, want):
     m = mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")
     got = m.parameters["p"].value(m.mission_time, m.parameters)
     assert got == pytest.approx(want, rel=1e-12) if want != 5.9105e9 else abs(got - want) <= 1e6
+
+
+@pytest.mark.gpu
+def test_command_line_curve_and_sil(oracle_mod, gpu, capsys):
+    import json
+    assert mef.main([str(TIMED), "--samples", str(2 ** 20), "--time-step", "1000", "--sil"]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert [t for _, t in out["p_time"]] == [1000.0 * k for k in range(9)] + [8760.0]
+    ps = [p for p, _ in out["p_time"]]
+    assert all(b >= a for a, b in zip(ps, ps[1:]))
+    want = mef.safety_integrity_levels(_exact_curve(oracle_mod, mef.parse(TIMED), 1000.0, 8760.0))
+    assert out["sil"]["pfd_avg"] == pytest.approx(want["pfd_avg"], rel=2e-2)

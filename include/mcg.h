@@ -230,7 +230,9 @@ mcg_status mcg_profile_sampler_read(mcg_engine *engine, uint64_t *launches, doub
  * another device context of the same process on the same GPU) race and give
  * wrong counts; serialise them.  The first call on a device resolves the
  * array's address and sets the kernel's shared-memory limit, so make that
- * first call before any stream capture on that device. */
+ * first call before any stream capture on that device.  That set-up is kept
+ * for the life of the process: after cudaDeviceReset on a device, do not call
+ * this entry point again in the same process. */
 #define MCG_NOALLOC_SCRATCH_BYTES (32ull << 20)
 mcg_status mcg_run_fused_noalloc(const void *d_ops, uint64_t n_ops, uint32_t smem_slots, uint32_t global_slots,
                                  uint64_t *d_ones, uint32_t n_tally, uint32_t iteration_first, uint32_t n_iterations,

@@ -12,6 +12,7 @@
 #include "kernels.cuh"
 #include "mcg_batch.h"
 #include "program.hpp"
+#include "smem_limit.hpp"
 
 namespace {
 
@@ -167,8 +168,8 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
         MCG_CUDA(cudaMalloc((void **)&b->d_scratch,
                             (size_t)b->max_global * b->share * b->scratch_stride * sizeof(uint64_t)));
     MCG_CUDA(cudaMalloc((void **)&b->d_queue, sizeof(unsigned int)));
-    MCG_CUDA(cudaFuncSetAttribute(batch_kernel(b->ctas_per_sm, b->share, b->atleast), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max<uint32_t>(b->smem_bytes, 1)));
+    const mcg_status lim = mcg::set_smem_limit(batch_kernel(b->ctas_per_sm, b->share, b->atleast), b->smem_bytes);
+    if (lim != MCG_OK) return lim;
     if (run.stream) {
         b->stream = (cudaStream_t)run.stream;
     } else {

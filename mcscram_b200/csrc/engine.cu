@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "mcg.h"
 #include "program.hpp"
+#include "smem_limit.hpp"
 
 namespace {
 
@@ -386,8 +387,8 @@ mcg_status compile_fused(mcg_engine *e, const mcg_run_desc &run) {
 mcg_status setup_fused(mcg_engine *e, const mcg_run_desc &run) {
     mcg_status st = compile_fused(e, run);
     if (st != MCG_OK) return st;
-    MCG_CUDA(cudaFuncSetAttribute(fused_kernel(e->ctas_per_sm), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max<uint32_t>(e->smem_bytes, 1)));
+    st = mcg::set_smem_limit(fused_kernel(e->ctas_per_sm), e->smem_bytes);
+    if (st != MCG_OK) return st;
     MCG_CUDA(upload(reinterpret_cast<mcg::Op **>(&e->d_ops), e->prog.ops));
     if (e->prog.global_slots && e->mode == MCG_MODE_FUSED) {
         MCG_CUDA(work_alloc(e, (void **)&e->d_scratch,
@@ -420,8 +421,9 @@ mcg_status setup_staged(mcg_engine *e, const mcg_run_desc &run) {
     const uint32_t blocks = run.sampler_blocks_per_sm ? run.sampler_blocks_per_sm : 8u;
     if (blocks < 1 || blocks > 8) return mcg::fail(MCG_ERR_INVALID, "sampler_blocks_per_sm must be 1..8");
     e->sampler_smem = blocks >= 8 ? 0u : (uint32_t)(prop.sharedMemPerMultiprocessor / blocks - 2048);
-    MCG_CUDA(cudaFuncSetAttribute(mcg::dev::k_stage_be<kMulForm, kPackForm, kStageEventsPerThread>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<uint32_t>(e->sampler_smem, 1)));
+    const mcg_status lim = mcg::set_smem_limit(mcg::dev::k_stage_be<kMulForm, kPackForm, kStageEventsPerThread>,
+                                               e->sampler_smem);
+    if (lim != MCG_OK) return lim;
     // The gate phase of chunk k runs while chunk k+1 is sampled: giving its
     // stream the higher priority lets its (memory-bound) blocks be scheduled
     // in between the sampler's blocks instead of after all of them.
@@ -459,8 +461,8 @@ mcg_status setup_strip(mcg_engine *e, const mcg_run_desc &run) {
     const uint64_t per_block = prop.sharedMemPerMultiprocessor / target - 2048;
     e->strip_smem = tally_bytes <= per_block ? (uint32_t)tally_bytes : 0u;
     const StripKernel kern = strip_kernel(target);
-    MCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max<uint32_t>(e->strip_smem, 1)));
+    const mcg_status lim = mcg::set_smem_limit(kern, e->strip_smem);
+    if (lim != MCG_OK) return lim;
     int per_sm = 0;
     MCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, mcg::dev::kStripThreads, e->strip_smem));
     if (per_sm < 1) return mcg::fail(MCG_ERR_INVALID, "strip kernel does not fit on an SM");

@@ -17,6 +17,7 @@
 #include "engine_internal.hpp"
 #include "error.hpp"
 #include "mcg_is.h"
+#include "smem_limit.hpp"
 
 namespace {
 
@@ -491,7 +492,11 @@ mcg_status mcg_is_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in
         mcg_destroy(e);
         return mcg::fail(MCG_ERR_INVALID, "too many basic events for the weights kernel's shared memory");
     }
-    MCG_CUDA(cudaFuncSetAttribute(k_is_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)is->weight_smem));
+    st = mcg::set_smem_limit(k_is_weights, is->weight_smem);
+    if (st != MCG_OK) {
+        mcg_destroy(e);
+        return st;
+    }
     MCG_CUDA(cudaMalloc((void **)&is->d_be_q, std::max<uint32_t>(nb, 1) * sizeof(uint4)));
     MCG_CUDA(cudaMalloc((void **)&is->d_a, std::max<uint32_t>(nb, 1) * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&is->d_ce, std::max<uint32_t>(nb, 1) * sizeof(double)));

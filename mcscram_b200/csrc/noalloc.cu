@@ -18,6 +18,7 @@
 #include "error.hpp"
 #include "kernels.cuh"
 #include "mcg.h"
+#include "smem_limit.hpp"
 
 // Global-scratch slots of the fused kernel, one array per device that loads
 // the library, held until the process exits.  Every call shares it; no call
@@ -44,6 +45,9 @@ DeviceSetup g_setup[kMaxDevices];
 // Once per device, with that device current: resolve the array's device
 // address (the host-side symbol is only a stand-in), read the SM count and
 // raise the kernel's dynamic shared-memory limit.  Nothing is allocated.
+// The result is kept for the life of the process: a caller that resets the
+// device (cudaDeviceReset) drops the module that holds the array, and this
+// entry point must not be called again in that process.
 mcg_status setup_device(int dev, DeviceSetup *&out) {
     if (dev < 0 || dev >= kMaxDevices) return mcg::fail(MCG_ERR_INVALID, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -57,10 +61,11 @@ mcg_status setup_device(int dev, DeviceSetup *&out) {
             (err = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess ||
             (err = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
             return mcg::fail(MCG_ERR_CUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(err));
+        // what one of the two CTAs per SM may use; the kernel's limit itself
+        // is the device maximum, as engines with this kernel set it too
         const size_t cap = std::min<size_t>((size_t)optin, (size_t)per_sm / kCtasPerSm) - 1024;
-        err = cudaFuncSetAttribute(mcg::dev::k_fused<kThreads, kCtasPerSm, 1, 1>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
-        if (err != cudaSuccess) return mcg::fail(MCG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
+        const mcg_status lim = mcg::set_smem_limit(mcg::dev::k_fused<kThreads, kCtasPerSm, 1, 1>, cap);
+        if (lim != MCG_OK) return lim;
         s.scratch = static_cast<uint64_t *>(p);
         s.sms = sms;
         s.smem_cap = cap;

@@ -1956,6 +1956,16 @@ def load(source: Union[str, Path], top: Optional[str] = None,
     return parse(source, mission_time, ccf_analysis, allow_extern).flat(top)
 
 
+# Most time points of one probability curve: each point is one instance of a
+# batched launch with its own threshold table held on the host and the device.
+MAX_TIME_POINTS = 1 << 16
+
+
+def time_points(mission_time: float, time_step: float) -> int:
+    """Points t = 0, dt, 2 dt, ... below the mission time, plus the mission time."""
+    return int(math.ceil(mission_time / time_step)) + 1 if time_step > 0 else 0
+
+
 def probability_over_time(model: MefModel, time_step: float, top: Optional[str] = None,
                           mission_time: Optional[float] = None, words: int = 1 << 16, iteration: int = 1,
                           device: int = 0):
@@ -1972,6 +1982,8 @@ def probability_over_time(model: MefModel, time_step: float, top: Optional[str] 
     T = model.mission_time if mission_time is None else float(mission_time)
     if time_step <= 0:
         return []
+    if time_points(T, time_step) > MAX_TIME_POINTS:
+        raise ValueError(f"time step {time_step} gives more than {MAX_TIME_POINTS} points up to {T}")
     times = []
     k = 0
     while k * time_step < T:
@@ -2077,6 +2089,9 @@ def main(argv=None) -> int:
     if args.sil and args.time_step <= 0:
         ap.error("--sil needs --time-step")
     m = parse(args.model, ccf_analysis=args.ccf, allow_extern=args.allow_extern)
+    if time_points(m.mission_time, args.time_step) > MAX_TIME_POINTS:
+        ap.error(f"--time-step {args.time_step} gives more than {MAX_TIME_POINTS} points up to the mission time "
+                 f"{m.mission_time}")
     g = m.flat(args.top)
     words = max(1, int(math.ceil(args.samples / 64)))
     with _capi.Engine(g, mode=_capi.MODES[args.mode], device=args.device) as e:

@@ -14,9 +14,10 @@ from pathlib import Path
 import pytest
 
 from mcscram_b200 import eta, mef
+from tests.conftest import reference_path
 
 PLANT = Path(__file__).parent / "golden" / "eta" / "plant.xml"
-REF = Path("/root/reference")
+REF = reference_path()
 ETA_IN = REF / "tests" / "input" / "eta"
 EVENT_TREES = REF / "input" / "EventTrees"
 TWO32 = float(1 << 32)

@@ -11,8 +11,9 @@ import numpy as np
 import pytest
 
 from mcscram_b200 import mef
+from tests.conftest import reference_path
 
-REF = Path("/root/reference")
+REF = reference_path()
 needs_ref = pytest.mark.skipif(not REF.exists(), reason="the reference's test models are not on this machine")
 
 

@@ -193,3 +193,22 @@ def test_engines_reuse_kept_work_buffers(capi, oracle_mod, gpu):
     with engine(capi, g, mode=capi.MODE_STRIP) as e:
         e.run(2, 1, 0, words)
         assert np.array_equal(e.tallies()[0], want)
+
+
+@pytest.mark.parametrize("mode", ["fused", "staged", "strip"])
+def test_engine_created_later_with_a_smaller_program(capi, oracle_mod, gpu, mode):
+    """A kernel's shared-memory limit is shared by every engine that launches
+    it: an engine created after another one, with a program that needs less
+    shared memory, must leave the first engine's launches working."""
+    big = synth.config1()
+    small = synth.small_tree(5, n_be=12, n_gates=6)
+    small = small.with_tallies([small.root])
+    words = 1 << 12
+    m = capi.MODES[mode]
+    kw = dict(sampler_blocks_per_sm=2) if mode == "staged" else {}
+    with engine(capi, big, mode=m, **kw) as a:
+        with engine(capi, small, mode=m) as b:
+            b.run(1, 1, 0, words)
+            assert np.array_equal(b.tallies()[0], oracle_mod.tallies(small, 1, 1, 0, words))
+        a.run(1, 1, 0, words)
+        assert np.array_equal(a.tallies()[0], oracle_mod.tallies(big, 1, 1, 0, words))

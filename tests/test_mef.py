@@ -17,11 +17,12 @@ import numpy as np
 import pytest
 
 from mcscram_b200 import mef
+from tests.conftest import reference_path
 
 FIX = Path(__file__).parent / "golden" / "mef" / "features.xml"
 TWO32 = float(1 << 32)
-ARALIA = Path("/root/reference/input/Aralia")
-TABLE = Path("/root/reference/benchmarks/input.csv")
+ARALIA = reference_path("input", "Aralia")
+TABLE = reference_path("benchmarks", "input.csv")
 
 
 def _brute_force(path, top):
@@ -224,7 +225,7 @@ def test_probability_over_time_matches_oracle_per_time_point(oracle_mod, gpu):
 
 # The reference's initializer test lists for fault-tree inputs
 # (tests/initializer_tests.cc:181-296).
-FTA_IN = Path("/root/reference/tests/input/fta")
+FTA_IN = reference_path("tests", "input", "fta")
 FTA_CORRECT = ["correct_tree_input.xml", "correct_formulas.xml", "constant_in_formulas.xml",
                "component_definition.xml", "mixed_definitions.xml", "mixed_roles.xml",
                "model_data_mixed_definitions.xml", "two_trees.xml", "two_top_events.xml",
@@ -324,7 +325,7 @@ def test_ccf_errors():
             mef.parse(grp.format(model=model, factors=factors))
 
 
-CORE_IN = Path("/root/reference/tests/input/core")
+CORE_IN = reference_path("tests", "input", "core")
 
 
 @pytest.mark.skipif(not CORE_IN.exists(), reason="the reference's core inputs are not on this machine")
@@ -399,7 +400,7 @@ def test_deviate_domain_errors(body, msg):
         mef.parse(f"<opsa-mef><define-parameter name='p'>{body}</define-parameter></opsa-mef>")
 
 
-SMALL_TREE = Path("/root/reference/input/SmallTree/SmallTree.xml")
+SMALL_TREE = reference_path("input", "SmallTree", "SmallTree.xml")
 
 
 @pytest.mark.skipif(not SMALL_TREE.exists(), reason="the reference's SmallTree model is not on this machine")
@@ -578,7 +579,7 @@ def test_substitution_errors():
             mef.parse(model.format(attr=attr, hyp=hyp, src=src, tgt=tgt))
 
 
-TWO_TRAIN = Path("/root/reference/input/TwoTrain")
+TWO_TRAIN = reference_path("input", "TwoTrain")
 
 
 @pytest.mark.skipif(not TWO_TRAIN.exists(), reason="the reference's TwoTrain model is not on this machine")
@@ -593,7 +594,7 @@ def test_reference_two_train_substitutions(oracle_mod):
         pytest.approx(0.7225, rel=1e-9)
 
 
-MODEL_IN = Path("/root/reference/tests/input/model")
+MODEL_IN = reference_path("tests", "input", "model")
 MODEL_CORRECT = ["extern_library.xml", "extern_function.xml", "extern_expression.xml", "valid_alignment.xml",
                  "valid_sum_alignment.xml", "private_phases.xml", "substitution.xml",
                  "substitution_optional_source.xml", "substitution_types.xml",
@@ -708,7 +709,7 @@ def test_substitution_model_through_the_engine(oracle_mod, gpu):
     assert abs(p - _substitution_fixture_exact()) <= 5 * math.sqrt(p * (1 - p) / total)
 
 
-INPUT_DIR = Path("/root/reference/tests/input")
+INPUT_DIR = reference_path("tests", "input")
 
 
 @pytest.mark.skipif(not INPUT_DIR.exists(), reason="the reference's test inputs are not on this machine")
@@ -760,7 +761,7 @@ def test_formula_arguments_follow_the_schema():
     mef.parse("<opsa-mef><define-parameter name='p'><int value='-2147483647'/></define-parameter></opsa-mef>")
 
 
-REF_INPUT = Path("/root/reference/input")
+REF_INPUT = reference_path("input")
 
 # (files, the reference's exact-probability expectation, its tolerance): the
 # non-rare-event branches of tests/bench_*_tests.cc
@@ -854,7 +855,7 @@ def _exact_curve(oracle_mod, m, step, mission_time):
             for t in times]
 
 
-SINGLE_EXP = Path("/root/reference/tests/input/core/single_exponential.xml")
+SINGLE_EXP = reference_path("tests", "input", "core", "single_exponential.xml")
 
 
 @pytest.mark.skipif(not SINGLE_EXP.exists(), reason="the reference's test models are not on this machine")
@@ -953,3 +954,15 @@ def test_command_line_curve_and_sil(oracle_mod, gpu, capsys):
     assert all(b >= a for a, b in zip(ps, ps[1:]))
     want = mef.safety_integrity_levels(_exact_curve(oracle_mod, mef.parse(TIMED), 1000.0, 8760.0))
     assert out["sil"]["pfd_avg"] == pytest.approx(want["pfd_avg"], rel=2e-2)
+
+
+def test_command_line_refuses_a_curve_with_too_many_points(capsys):
+    """A time step that would make more than MAX_TIME_POINTS curve points is
+    refused before any point is built (8760 h / 1e-3 h = 8.76e6 points)."""
+    assert mef.time_points(8760.0, 1000.0) == 10
+    with pytest.raises(SystemExit) as exc:
+        mef.main([str(TIMED), "--time-step", "1e-3"])
+    assert exc.value.code == 2
+    assert "points" in capsys.readouterr().err
+    with pytest.raises(ValueError):
+        mef.probability_over_time(mef.parse(TIMED), time_step=1e-3)

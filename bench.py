@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--words", type=int, default=WORDS_PER_GPU, help="sample words per GPU per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-is", action="store_true",
+                    help="plain workload: leave out the learned-IS time to accuracy on the 1e-8 tree")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fused kernel CTAs per SM (0 = engine default)")
     ap.add_argument("--peak-words", type=int, default=1 << 22, help="words per register-only sampler launch")
@@ -290,14 +292,13 @@ def run_ua(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
-def run_is(args, rank: int, world: int, local: int) -> int:
+def measure_is(args, local: int) -> dict:
     """GPU time to a 5% relative error (95% confidence) on the 2,000-event tree
     whose exact top-event probability is ~1e-8: the learned-IS pipeline
     (cross-entropy rounds with on-GPU MLP training, then IS batches until the
     target) measured end to end, against the plain sampler's time derived
-    from its rate measured on the same tree."""
-    if rank != 0:
-        return 0
+    from its rate measured on the same tree.  Returns the fields of the
+    `is` workload's line."""
     import numpy as np
     import torch
     from mcscram_b200 import _capi, synth
@@ -350,7 +351,9 @@ def run_is(args, rank: int, world: int, local: int) -> int:
     p_hat = res["estimate"]
     n_req = 1.959963984540054 ** 2 * (1 - p_hat) / (p_hat * 0.05 ** 2) if p_hat > 0 else float("inf")
     plain_s = n_req / plain_rate
-    print(json.dumps({
+    exact = float(synth.read_once_probability(g)[g.root])
+    se = p_hat * res["rel_err95"] / 1.959963984540054
+    return {
         "metric": "GPU time to 5% rel err at P_top~1e-8", "value": is_wall, "unit": "s", "n_gpus": 1,
         "higher_is_better": False, "vs_baseline": None, "dtype": "u64 sampling, fp64 weights, bf16/fp32 MLP",
         "data": "synthetic", "steps": 1, "warmup": args.warmup,
@@ -361,11 +364,20 @@ def run_is(args, rank: int, world: int, local: int) -> int:
                                "this one tree (cut-set defensive component, one CE round) vs plain MC"},
         "is": {"estimate": p_hat, "rel_err95": res["rel_err95"], "samples": res["samples"], "hits": res["hits"],
                "ess": res["ess"], "fallback": res["fallback"], "wall_s": is_wall,
-               "gpu_s": (hist.gpu_ms + res["gpu_ms"]) * 1e-3, "ce_rounds": hist.rounds},
+               "gpu_s": (hist.gpu_ms + res["gpu_ms"]) * 1e-3, "ce_rounds": hist.rounds,
+               "exact_p_top": exact, "z_vs_exact": (p_hat - exact) / se if se > 0 else None},
         "plain": {"samples_per_s": plain_rate, "required_samples": n_req, "seconds": plain_s,
                   "measured_words": args.plain_words, "measured_ms": plain_ms,
                   "note": "time derived from the rate measured on this tree"},
-        "speedup": plain_s / is_wall, "clocks": clk}), flush=True)
+        "speedup": plain_s / is_wall, "clocks": clk}
+
+
+def run_is(args, rank: int, world: int, local: int) -> int:
+    """The `is` workload: one line with the learned-IS time to 5% on the
+    2,000-event rare-event tree against plain MC (measure_is)."""
+    if rank != 0:
+        return 0
+    print(json.dumps(measure_is(args, local)), flush=True)
     return 0
 
 
@@ -661,9 +673,16 @@ def run_eta(args, rank: int, world: int, local: int) -> int:
 
 def main() -> int:
     args = parse_args()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # N ranks, one per GPU, on this node (the same launch as torchrun's)
+        from mcscram_b200 import parallel
+        return parallel.launch_local_ranks(args.gpus, str(Path(__file__).resolve()), sys.argv[1:],
+                                           need_gpus=args.impl != "reference")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus not in (1, world):
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload == "ua":
@@ -699,12 +718,18 @@ def main() -> int:
     info = eng.program_info()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
+    # the one exchange of the multi-GPU path: after every pass, the sum over
+    # ranks of the engine's uint64 tallies, device to device over NCCL
+    local_ones = global_ones = None
+    if world > 1:
+        local_ones = parallel.device_counters(eng.tally_device_ptr(), eng.n_tally)
+        global_ones = torch.zeros_like(local_ones)
+
     def allreduce_tallies():
-        # the one exchange of the multi-GPU path: sum of uint64 tallies over ranks (NCCL)
         if world == 1:
             return
-        ones, total = eng.tallies()
-        parallel.allreduce_tallies(ones)
+        global_ones.copy_(local_ones)
+        parallel.allreduce_counters_(global_ones)
 
     # warm-up passes (iterations 1..W); then the timed passes continue the numbering
     for i in range(args.warmup):
@@ -739,6 +764,13 @@ def main() -> int:
     launches = eng.launch_count() - launches0
     elapsed_ms = t_start.elapsed_time(t_end)
     run_ms = sum(a.elapsed_time(b) for a, b in ev_run)
+    allreduced = None
+    if world > 1:
+        # the reduced counters equal the sum of every rank's own counters
+        own = torch.tensor(eng.tallies()[0].astype(np.int64), device="cuda")
+        parallel.allreduce_counters_(own)
+        allreduced = bool(torch.equal(own, global_ones))
+        local_ones = None
     if world > 1:
         elapsed_ms, run_ms = parallel.allreduce_max([elapsed_ms, run_ms])
     ms_per_step = elapsed_ms / args.steps
@@ -809,6 +841,9 @@ def main() -> int:
                          "peak_source": "register-only Philox sampler kernel (k_sampler_peak) measured in this run",
                          "work_unit": "basic-event word = 16 Philox4x32-10 calls"},
             "pipeline": {"be_words_per_s": be_words_per_s, "frac_of_peak": be_words_per_s / world / peak},
+            "tally_allreduce": None if world == 1 else {"backend": "nccl", "device_to_device": True,
+                                                        "bytes_per_step": int(g.tally_nodes.size) * 8,
+                                                        "sum_checked": allreduced},
             "clocks": clk,
             "program": info,
         }
@@ -819,8 +854,19 @@ def main() -> int:
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
-        print(json.dumps(line), flush=True)
     eng.close()
+    if rank == 0 and world == 1 and not args.no_is:
+        # the metric's second half: learned-IS time to 5 % at P_top ~ 1e-8,
+        # after the timed region (its own clocks inside)
+        torch.cuda.set_stream(torch.cuda.default_stream())
+        m = measure_is(args, local)
+        line["is"] = {"workload": m["config"]["workload"], "metric": m["metric"], "wall_s": m["value"],
+                      "unit": "s", **{k: v for k, v in m["is"].items() if k != "ce_rounds"},
+                      "plain_samples_per_s": m["plain"]["samples_per_s"],
+                      "plain_seconds_derived": m["plain"]["seconds"], "speedup_vs_plain": m["speedup"],
+                      "clocks": m["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0

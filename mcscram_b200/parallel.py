@@ -37,6 +37,54 @@ def shard_items(n_items: int, world: int, rank: int) -> List[int]:
     return list(range(rank, n_items, world))
 
 
+def launch_local_ranks(n: int, script: str, argv: Sequence[str], need_gpus: bool = True,
+                       timeout_s: Optional[float] = None) -> int:
+    """Runs `script argv` as n ranks on this node under torch.distributed.run
+    (one process per GPU; RANK, LOCAL_RANK, WORLD_SIZE and MASTER_* set for
+    each, rendezvous on 127.0.0.1) and returns the launcher's exit code.
+    Refuses to start when `need_gpus` and fewer than n GPUs are visible."""
+    import socket
+    import subprocess
+    import sys
+
+    if n < 1:
+        raise ValueError("at least one rank")
+    if need_gpus:
+        import torch
+        have = torch.cuda.device_count() if torch.cuda.is_available() else 0
+        if have < n:
+            raise RuntimeError(f"{n} ranks need {n} GPUs; {have} visible")
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", script, *argv]
+    return subprocess.run(cmd, timeout=timeout_s).returncode
+
+
+def device_counters(ptr: int, n: int):
+    """n uint64 counters in device memory at `ptr` (an engine's tallies,
+    mcg_tally_device_ptr) as an int64 CUDA tensor over the same memory, no
+    copy.  The memory stays the engine's: drop the tensor before the engine."""
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (int(n),), "typestr": "<i8", "data": (int(ptr), False),
+                                    "version": 3, "strides": None}
+
+    return torch.as_tensor(_View(), device="cuda")
+
+
+def allreduce_counters_(counters, group=None):
+    """In-place sum over ranks of an int64 tensor of counters, on its own
+    device (CUDA tensors over NCCL, CPU tensors over gloo); the uint64 sums
+    wrap the same way in two's complement, and tallies stay below 2^63."""
+    import torch.distributed as dist
+
+    dist.all_reduce(counters, op=dist.ReduceOp.SUM, group=group)
+    return counters
+
+
 def allreduce_tallies(ones: np.ndarray, group=None, device: Optional[str] = None) -> np.ndarray:
     """Sum of every rank's uint64 counters (tallies stay below 2^63)."""
     import torch

@@ -51,8 +51,10 @@ def _rank_main(rank, world, port, words, queue):
     local = oracle.tallies(g, 1, 1, b, c, threads=1)
     total = parallel.allreduce_tallies(local)
     slowest = parallel.allreduce_max([float(rank)])
+    import torch
+    in_place = parallel.allreduce_counters_(torch.from_numpy(local.astype(np.int64)))
     if rank == 0:
-        queue.put((total, slowest))
+        queue.put((total, slowest, in_place.numpy().astype(np.uint64)))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -66,10 +68,40 @@ def test_gloo_two_ranks_allreduce_equals_single_rank(oracle_mod):
     procs = [ctx.Process(target=_rank_main, args=(r, 2, port, words, q)) for r in range(2)]
     for p in procs:
         p.start()
-    total, slowest = q.get(timeout=120)
+    total, slowest, in_place = q.get(timeout=120)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
     expect = oracle_mod.tallies(synth.config1(), 1, 1, 0, words)
     assert np.array_equal(total, expect)
+    assert np.array_equal(in_place, expect)
     assert slowest == [1.0]
+
+
+def test_bench_gpus_two_launches_two_ranks(oracle_mod):
+    """`bench.py --gpus 2` without a launcher around it starts two ranks on
+    this node (here the CPU reference arm: rank 0 measures and prints one
+    line, rank 1 exits without work)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    env = dict(os.environ)
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+                        "--warmup", "0", "--cpu-seconds", "0.2"], capture_output=True, text=True, env=env,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference"
+    assert lines[0]["value"] > 0
+
+
+def test_launcher_refuses_more_ranks_than_gpus():
+    from mcscram_b200 import parallel
+    import torch
+    have = torch.cuda.device_count() if torch.cuda.is_available() else 0
+    with pytest.raises(RuntimeError, match="GPUs"):
+        parallel.launch_local_ranks(have + 1, "bench.py", [])

@@ -45,15 +45,17 @@ enum mcg_connective {
 
 /* Evaluation strategies for mcg_run. */
 enum mcg_mode {
-    MCG_MODE_FUSED = 0,   /* one persistent kernel per launch chunk: sample, gates, tallies fused */
+    MCG_MODE_AUTO = 0,    /* the launch shape mcg_tune picks for the tree's shape and the device
+                             (include/mcg_tune.h): strip, staged or fused, with its CTAs per SM */
     MCG_MODE_LAYERED = 1, /* reference dataflow: materialised node words, one launch per layer */
     MCG_MODE_STAGED = 2,  /* two-phase pipeline: a pure sampler kernel writes basic-event words to
                              HBM, per-layer gate kernels with fused tallies read them; chunks are
                              double buffered on two streams so the phases overlap */
-    MCG_MODE_STRIP = 3    /* one persistent kernel per pass: each block takes 256-word strips, its
+    MCG_MODE_STRIP = 3,   /* one persistent kernel per pass: each block takes 256-word strips, its
                              threads sample every event of their word and then evaluate every gate
                              for it from scratch rows of their own (n_nodes x 32 words per warp);
                              sampling and gate work of different blocks overlap on every SM */
+    MCG_MODE_FUSED = 4    /* one persistent kernel per launch chunk: sample, gates, tallies fused */
 };
 
 /* Flattened PDAG handed to the engine.  All arrays are host memory, copied
@@ -94,6 +96,8 @@ typedef struct mcg_run_desc {
     uint64_t layered_max_words; /* layered/staged modes: words materialised per chunk; 0 = auto */
     uint32_t sampler_blocks_per_sm; /* staged mode: cap on sampler blocks per SM, to leave room for
                                        gate-phase blocks; 0 or 8 = no cap (measured best) */
+    uint64_t tune_pass_words; /* MCG_MODE_AUTO: expected words per mcg_run call, the pass length the
+                                 launch shape is tuned for; 0 = 2^24 */
 } mcg_run_desc;
 
 typedef struct mcg_engine mcg_engine;

@@ -24,11 +24,14 @@ MCG_ERR_TIMEOUT = 4
 MCG_ERR_STATE = 5
 MCG_ERR_NO_DEVICE = 6
 
-MODE_FUSED = 0
+MODE_AUTO = 0
 MODE_LAYERED = 1
 MODE_STAGED = 2
 MODE_STRIP = 3
-MODES = {"fused": MODE_FUSED, "layered": MODE_LAYERED, "staged": MODE_STAGED, "strip": MODE_STRIP}
+MODE_FUSED = 4
+MODES = {"auto": MODE_AUTO, "fused": MODE_FUSED, "layered": MODE_LAYERED, "staged": MODE_STAGED,
+         "strip": MODE_STRIP}
+MODE_NAMES = {v: k for k, v in MODES.items()}
 
 _u32p = C.POINTER(C.c_uint32)
 _i32p = C.POINTER(C.c_int32)
@@ -67,6 +70,7 @@ class RunDesc(C.Structure):
         ("chunk_words", C.c_uint64),
         ("layered_max_words", C.c_uint64),
         ("sampler_blocks_per_sm", C.c_uint32),
+        ("tune_pass_words", C.c_uint64),
     ]
 
 
@@ -85,6 +89,28 @@ class ProgramInfo(C.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class TuneChoice(C.Structure):
+    _fields_ = [
+        ("mode", C.c_uint32),
+        ("ctas_per_sm", C.c_uint32),
+        ("layered_max_words", C.c_uint64),
+        ("words_per_second", C.c_double),
+        ("probe_words", C.c_uint64),
+        ("key", C.c_uint64),
+        ("from_cache", C.c_uint32),
+        ("candidates", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["mode_name"] = MODE_NAMES.get(self.mode, str(self.mode))
+        return d
+
+
+# double probe(void *user, const mcg_graph_desc *graph, const mcg_run_desc *candidate, uint64_t probe_words)
+TUNE_PROBE = C.CFUNCTYPE(C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64)
 
 
 class McgError(RuntimeError):
@@ -116,6 +142,11 @@ _SIGNATURES = {
                                           C.POINTER(C.c_double)]),
     "mcg_profile_sampler": (C.c_int, [C.c_void_p, C.c_int32]),
     "mcg_profile_sampler_read": (C.c_int, [C.c_void_p, _u64p, C.POINTER(C.c_double)]),
+    "mcg_tune": (C.c_int, [C.POINTER(GraphDesc), C.POINTER(RunDesc), C.c_uint64, C.c_void_p, C.c_void_p,
+                           C.POINTER(TuneChoice)]),
+    "mcg_tune_set_cache_file": (C.c_int, [C.c_char_p]),
+    "mcg_tune_forget": (C.c_int, []),
+    "mcg_engine_launch_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "mcg_last_error": (C.c_char_p, []),
     "mcg_version": (C.c_char_p, []),
 }
@@ -203,13 +234,14 @@ class Engine:
 
     def __init__(self, g: FlatGraph, mode: int = MODE_FUSED, device: int = 0, stream: Optional[int] = None,
                  smem_slots: int = 0, ctas_per_sm: int = 0, chunk_words: int = 0, layered_max_words: int = 0,
-                 sampler_blocks_per_sm: int = 0):
+                 sampler_blocks_per_sm: int = 0, tune_pass_words: int = 0):
         self.lib = load()
         self.graph = g
         self._view = GraphView(g)
         run = RunDesc(mode=mode, device=device, stream=C.c_void_p(stream) if stream else None, block_threads=0,
                       smem_slots=smem_slots, ctas_per_sm=ctas_per_sm, chunk_words=chunk_words,
-                      layered_max_words=layered_max_words, sampler_blocks_per_sm=sampler_blocks_per_sm)
+                      layered_max_words=layered_max_words, sampler_blocks_per_sm=sampler_blocks_per_sm,
+                      tune_pass_words=tune_pass_words)
         h = C.c_void_p()
         check(self.lib.mcg_create(C.byref(self._view.desc), C.byref(run), C.byref(h)))
         self.handle = h
@@ -283,10 +315,46 @@ class Engine:
         check(self.lib.mcg_profile_sampler_read(self.handle, C.byref(n), C.byref(ms)))
         return int(n.value), float(ms.value)
 
+    def launch_shape(self):
+        """(mode, CTAs per SM) the engine runs with (the tuner's choice under MODE_AUTO)."""
+        mode, ctas = C.c_uint32(), C.c_uint32()
+        check(self.lib.mcg_engine_launch_shape(self.handle, C.byref(mode), C.byref(ctas)))
+        return int(mode.value), int(ctas.value)
+
     def time_runs(self, iteration_first: int, word_begin: int, word_count: int, repeats: int) -> float:
         ms = C.c_double()
         check(self.lib.mcg_time_runs(self.handle, iteration_first, word_begin, word_count, repeats, C.byref(ms)))
         return float(ms.value)
+
+
+def tune(g: FlatGraph, pass_words: int = 0, device: int = 0, probe=None) -> dict:
+    """The launch shape mcg_tune picks for g's shape on `device` (cached per
+    shape and device).  `probe`, when given, is called as
+    probe(mode, ctas_per_sm, probe_words) -> basic-event words per second
+    instead of timing passes on the GPU."""
+    lib = load()
+    view = GraphView(g)
+    run = RunDesc(mode=MODE_AUTO, device=device)
+    out = TuneChoice()
+    cb = None
+    if probe is not None:
+        def _probe(user, graph, cand, words):
+            c = C.cast(cand, C.POINTER(RunDesc)).contents
+            return float(probe(int(c.mode), int(c.ctas_per_sm), int(words)))
+        cb = TUNE_PROBE(_probe)
+    check(lib.mcg_tune(C.byref(view.desc), C.byref(run), pass_words, C.cast(cb, C.c_void_p) if cb else None, None,
+                       C.byref(out)))
+    return out.as_dict()
+
+
+def tune_set_cache_file(path: str) -> None:
+    """Cache file of the tuner for later calls ("" = memory only)."""
+    check(load().mcg_tune_set_cache_file(str(path).encode()))
+
+
+def tune_forget() -> None:
+    """Drops the tuner's in-memory entries (its file stays)."""
+    check(load().mcg_tune_forget())
 
 
 def trim_memory(device: int = 0) -> None:

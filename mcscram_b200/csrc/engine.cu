@@ -21,6 +21,7 @@
 #include "graph.hpp"
 #include "kernels.cuh"
 #include "mcg.h"
+#include "mcg_tune.h"
 #include "program.hpp"
 #include "smem_limit.hpp"
 
@@ -705,7 +706,7 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
     *out = nullptr;
     mcg_run_desc run{};
     if (run_in) run = *run_in;
-    if (run.mode > MCG_MODE_STRIP) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
+    if (run.mode > MCG_MODE_FUSED) return mcg::fail(MCG_ERR_INVALID, "unknown mode");
     auto *e = new (std::nothrow) mcg_engine();
     if (!e) return mcg::fail(MCG_ERR_OOM, "host allocation failed");
     const std::string err = mcg::Graph::from_desc(*graph, e->graph);
@@ -722,6 +723,22 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
     if (run.device < 0 || run.device >= n_dev) {
         delete e;
         return mcg::fail(MCG_ERR_INVALID, "device ordinal out of range");
+    }
+    if (run.mode == MCG_MODE_AUTO) {
+        // the launch shape tuned (or cached) for this tree shape on this device
+        mcg_tune_choice ch{};
+        const mcg_status ts = mcg_tune(graph, &run, run.tune_pass_words, nullptr, nullptr, &ch);
+        if (ts != MCG_OK) {
+            delete e;
+            return ts;
+        }
+        run.mode = ch.mode;
+        run.ctas_per_sm = ch.ctas_per_sm;
+        run.layered_max_words = ch.layered_max_words;
+        run.smem_slots = 0;
+        run.chunk_words = 0;
+        run.sampler_blocks_per_sm = 0;
+        mcg::clear_error();
     }
     e->device = run.device;
     e->mode = run.mode;
@@ -762,6 +779,15 @@ mcg_status mcg_create(const mcg_graph_desc *graph, const mcg_run_desc *run_in, m
         return st;
     }
     *out = e;
+    return MCG_OK;
+}
+
+mcg_status mcg_engine_launch_shape(mcg_engine *e, uint32_t *mode, uint32_t *ctas_per_sm) {
+    mcg::clear_error();
+    if (!e) return mcg::fail(MCG_ERR_INVALID, "engine is NULL");
+    if (mode) *mode = e->mode;
+    if (ctas_per_sm)
+        *ctas_per_sm = e->mode == MCG_MODE_STRIP ? e->strip_blocks : e->mode == MCG_MODE_FUSED ? e->ctas_per_sm : 0u;
     return MCG_OK;
 }
 

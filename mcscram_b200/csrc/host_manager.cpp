@@ -76,7 +76,9 @@ layer_manager::layer_manager(const Pdag &pdag, std::size_t num_trials, const Tal
     d.n_inputs = graph_.inputs.size();
     d.n_tally = (uint32_t)graph_.tally_nodes.size();
     d.tally_nodes = graph_.tally_nodes.data();
-    throw_status(mcg_create(&d, &run, &engine_), "layer_manager");
+    mcg_run_desc r = run;
+    if (r.mode == MCG_MODE_AUTO && !r.tune_pass_words) r.tune_pass_words = shaper_.SAMPLE_SHAPE.num_bitpacks();
+    throw_status(mcg_create(&d, &r, &engine_), "layer_manager");
 }
 
 layer_manager::~layer_manager() {

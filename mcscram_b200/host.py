@@ -195,7 +195,7 @@ class LayerManager:
     """Mirror of layer_manager(pdag, num_trials, to_tally, overhead_ratio)."""
 
     def __init__(self, pdag: Pdag, num_trials: int, to_tally: Iterable[int], overhead_ratio: float = 0.05,
-                 mode: int = _capi.MODE_FUSED, device: int = 0, max_words_per_iteration: int = 0, **run_kw):
+                 mode: int = _capi.MODE_AUTO, device: int = 0, max_words_per_iteration: int = 0, **run_kw):
         self.pdag = pdag
         self.order = list(dict.fromkeys(int(x) for x in to_tally))
         run = _capi.RunDesc(mode=mode, device=device, **run_kw)
@@ -261,7 +261,7 @@ class LayerManager:
 
 
 def compute_tallies(pdag: Pdag, settings: Optional[Settings] = None, watch: Sequence[int] = (), device: int = 0,
-                    mode: int = _capi.MODE_FUSED):
+                    mode: int = _capi.MODE_AUTO):
     """Root tally first, then the watched nodes; plus the convergence report."""
     s = settings or Settings.default()
     w = _arr(list(watch), C.c_int32)

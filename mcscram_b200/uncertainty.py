@@ -68,7 +68,7 @@ class Batch:
         self.trees = list(trees)
         self._views = [_capi.GraphView(t) for t in self.trees]
         descs = (_capi.GraphDesc * len(self.trees))(*[v.desc for v in self._views])
-        run = _capi.RunDesc(mode=0, device=device, stream=C.c_void_p(stream) if stream else None,
+        run = _capi.RunDesc(mode=_capi.MODE_FUSED, device=device, stream=C.c_void_p(stream) if stream else None,
                             ctas_per_sm=ctas_per_sm, smem_slots=smem_slots)
         self.h = _vp()
         _capi.check(self.lib.mcg_batch_create(descs, len(self.trees), C.byref(run), C.byref(self.h)))

@@ -81,21 +81,27 @@ mcg_status mcg_is_batch_destroy(mcg_is_batch *b);
  * (a failure region the main proposal misses is still sampled through
  * the defensive ones).  At most 7 defensive proposals.
  * words_cutset > 0 adds, after them, a cut-set component for trees of
- * AND/OR/ATLEAST gates (threshold <= 8) without shared nodes or negations:
- * each of its samples draws a minimal cut set C of its tree with
- * probability prod_{i in C} p_i / S (S the sum of that product over all
- * minimal cut sets), forces C's events and draws the others at their nominal
- * probabilities; its density p(x) N(x) / S (N(x): minimal cut sets inside x)
- * enters the same mixture, bounding every weight by S / pi_cutset -- the
- * mixture form of importance sampling for a union of rare events.
+ * AND/OR/ATLEAST gates (threshold <= 8) without negations and without gates
+ * read by several gates: each of its samples draws a minimal cut set C of
+ * its tree with probability prod_{i in C} p_i / S (S the sum of that product
+ * over all minimal cut sets), forces C's events and draws the others at
+ * their nominal probabilities; its density p(x) N(x) / S (N(x): minimal cut
+ * sets inside x) enters the same mixture, bounding every weight by
+ * S / pi_cutset -- the mixture form of importance sampling for a union of
+ * rare events.  Basic events read by several gates (shared events) are
+ * drawn first, from q_cutset's thresholds (NULL: their nominal ones), and
+ * the cut set is then drawn on the tree conditioned on them; the density
+ * becomes r(z) p(x_private) N(x) / S_z (z: the shared events, r their
+ * proposal, S_z the sum over the conditioned tree's cut sets).  q_cutset's
+ * entries for other events are ignored.
  * tree_sums (host, 4 * n_tree doubles) receives per tree {sum w, sum w^2,
  * hits, max log w} over its word_count * 64 samples; ce_num (host, n_be
  * doubles, optional) sum over hits of w * x_i; kernel_ms (optional) the
  * device time of the call (CUDA events). */
 mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_threshold, uint32_t n_defensive,
                             const uint64_t *q_defensive, const uint64_t *words_defensive, uint64_t words_cutset,
-                            uint32_t iteration, uint64_t word_begin, uint64_t word_count, double *tree_sums,
-                            double *ce_num, double *kernel_ms);
+                            const uint64_t *q_cutset, uint32_t iteration, uint64_t word_begin, uint64_t word_count,
+                            double *tree_sums, double *ce_num, double *kernel_ms);
 
 /* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
  * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32

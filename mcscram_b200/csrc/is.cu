@@ -137,24 +137,44 @@ constexpr int kMaxComponents = 8;
 
 // ---------------------------------------------------------------------------
 // Cut-set component: importance sampling of a union of rare events over the
-// minimal cut sets of a tree (the "at least one event" mixture of Owen,
-// Maximov & Chertkov).  For a tree of AND / OR / ATLEAST / pass-through
-// gates without shared nodes, S(node) is the sum over its minimal cut sets
-// of the product of their events' probabilities (event: p; AND: product;
-// OR: sum; ATLEAST k: k-th elementary symmetric sum of the children's S).
-// A sample picks a cut set C with probability prod_{i in C} p_i / S(top) by
-// descending from the top (OR: one child with probability S(child)/S(OR);
-// AND: every child; ATLEAST: a k-subset with probability proportional to the
-// product of its members' S), forces C's events to fail and draws the other
-// events at their nominal probabilities.  Its density is
+// cut sets of a tree (the "at least one event" mixture of Owen, Maximov &
+// Chertkov).  For a tree of AND / OR / ATLEAST / pass-through gates without
+// shared nodes, S(node) is the sum over its minimal cut sets of the product
+// of their events' probabilities (event: p; AND: product; OR: sum; ATLEAST
+// k: k-th elementary symmetric sum of the children's S).  A sample picks a
+// cut set C with probability prod_{i in C} p_i / S(top) by descending from
+// the top (OR: one child with probability S(child)/S(OR); AND: every child;
+// ATLEAST: a k-subset with probability proportional to the product of its
+// members' S), forces C's events to fail and draws the other events at their
+// nominal probabilities.  Its density is
 //     q(x) = p(x) N(x) / S(top),
 // N(x) = the number of minimal cut sets contained in x (event: x_i; AND:
 // product; OR: sum; ATLEAST: k-th elementary symmetric sum of the children's
 // counts), so log(p/q) = log S(top) - log N(x); N(x) >= 1 wherever the top
 // event fires, which bounds the weight of this component by S(top) / pi.
+//
+// Basic events read by several gates (gates still read by one gate each)
+// are drawn first, z_i = 1 with a proposal probability r_i, and the tree is
+// then one of private events with the shared ones as constants: S_z(node)
+// uses z_i for a shared event's leaves (a leaf with z_i = 1 holds the empty
+// cut set), and the descent and forcing above run on that conditioned tree
+// (no forcing when S_z(top) = 0: z leaves no cut set).  The density is
+//     q(x) = r(z) p(x_private) N(x) / S_z(top),
+// with N(x) the same count (a shared leaf counts x_i), so
+//     log(p/q) = log(p(z) / r(z)) + log S_z(top) - log N(x).
+// S_z differs from S_0 (all z_i = 0) only above the shared leaves with
+// z_i = 1, so S_z is evaluated by a descent that enters only those gates and
+// takes S_0 for every other one.  In the forcing kernel a gate is entered
+// when its range of shared-leaf occurrences (the leaves in depth-first
+// order) holds one of the sample's z_i = 1 occurrences; in the weights
+// kernel when its companion gate fired (an OR over the shared leaves below
+// the gate, evaluated with the other gates).
 constexpr int kCutStack = 256;     // descent stack of one sample (node ids)
-constexpr int kCountDepth = 32;    // frames of the N(x) evaluation
+constexpr int kCountDepth = 32;    // frames of the N(x) and S_z evaluations
 constexpr int kCutMaxK = 8;        // ATLEAST thresholds the count frames hold
+constexpr int kCutMaxN = 32;       // ATLEAST fan-in above shared leaves (suffix sums in registers)
+constexpr int kZOcc = 32;          // z_i = 1 occurrences a sample keeps for pruning (more: no pruning)
+constexpr uint32_t kNoNode = 0xFFFFFFFFu;
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {  // the SplitMix64 finaliser
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -174,73 +194,19 @@ struct CutArgs {
     const uint32_t *root_row;      // per tree
     const uint4 *gate;             // per gate: op | k << 8, in_begin, in_count, table offset
     const uint32_t *inputs;
-    const double *S;               // per node
-    const double *tab;             // OR: cumulative S(child) / S(OR); ATLEAST: E[j][r] = e_r(S_j..S_n-1)
+    const double *S;               // per node: S_0
+    const double *tab;             // OR: cumulative S_0(child) / S_0(OR); ATLEAST: E[j][r] = e_r(S_j..S_n-1)
+    const unsigned char *shared;   // per basic event: read by several gates
+    const uint2 *gate_occ;         // per gate: [lo, hi) of the shared-leaf occurrences below it
+    const uint32_t *z_begin;       // per tree: its shared events are z_event[z_begin[k] .. z_begin[k + 1])
+    const uint32_t *z_event;
+    const uint64_t *z_thr;         // per shared event: z_i = 1 with probability z_thr / 2^32
+    const uint32_t *z_index;       // per basic event: its entry in z_event (shared events only)
+    const uint32_t *z_occ_begin;   // per shared event: its occurrences z_occ[z_occ_begin[j] .. z_occ_begin[j + 1])
+    const uint32_t *z_occ;
     uint64_t seed;
     unsigned int *error;
 };
-
-// One thread per (tree, word, sample): descends from the tree's top and ORs
-// the sample's bit into the words of the chosen cut set's events.
-__global__ void __launch_bounds__(256) k_cut_force(CutArgs a) {
-    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (item >= (uint64_t)a.n_inst * a.W * 64) return;
-    const uint32_t b = (uint32_t)(item & 63u);
-    const uint64_t wi = item >> 6;
-    const uint64_t w = wi % a.W;
-    const uint32_t k = (uint32_t)(wi / a.W);
-    uint64_t base = mix64(a.seed ^ ((uint64_t)k << 32));
-    base = mix64(base ^ (a.word_begin + w));
-    base = mix64(base ^ (uint64_t)b);
-    uint32_t draw = 0;
-    const unsigned long long bit = 1ull << b;
-    uint32_t stack[kCutStack];
-    int sp = 0;
-    stack[sp++] = a.root_row[k];
-    while (sp) {
-        const uint32_t node = stack[--sp];
-        if (node < a.n_be) {
-            atomicOr(reinterpret_cast<unsigned long long *>(a.buf + (uint64_t)node * a.W + w), bit);
-            continue;
-        }
-        const uint4 g = a.gate[node - a.n_be];
-        const uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu, n = g.z;
-        const uint32_t *in = a.inputs + g.y;
-        const double *tab = a.tab + g.w;
-        if (op == MCG_OR) {
-            const double u = cut_uniform(base, ++draw);
-            uint32_t j = 0;
-            while (j + 1 < n && u >= tab[j]) ++j;
-            if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
-            stack[sp++] = in[j];
-        } else if (op == MCG_ATLEAST) {
-            uint32_t r = kk;
-            for (uint32_t j = 0; j < n && r > 0; ++j) {
-                bool take = n - j == r;
-                if (!take) {  // P(take j | r still to take) = S_j E[j+1][r-1] / E[j][r]
-                    const double e0 = tab[(uint64_t)j * (kk + 1) + r], e1 = tab[(uint64_t)(j + 1) * (kk + 1) + r - 1];
-                    take = cut_uniform(base, ++draw) * e0 < a.S[in[j]] * e1;
-                }
-                if (take) {
-                    if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
-                    stack[sp++] = in[j];
-                    --r;
-                }
-            }
-        } else {  // AND and pass-through gates: every input
-            for (uint32_t j = 0; j < n; ++j) {
-                if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
-                stack[sp++] = in[j];
-            }
-        }
-    }
-}
-
-inline uint64_t mix64_host(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
 
 struct CountFrame {
     uint32_t node, j;
@@ -267,11 +233,13 @@ __device__ __forceinline__ void count_init(CountFrame &f, uint32_t node, uint32_
     for (int r = 1; r <= kCutMaxK; ++r) f.dp[r] = 0.0;
 }
 
-// N(x) of sample b of the word whose rows start at col (row stride W), for
-// the tree rooted at the fired gate `root`; only fired children are visited.
-// Returns -1 when the tree is deeper than the frames hold.
-__device__ double cut_count(const uint64_t *col, uint64_t W, uint32_t root, int b, const uint4 *gate,
-                            const uint32_t *inputs, uint32_t n_be) {
+// The AND / OR / ATLEAST recursion (product, sum, k-th elementary symmetric
+// sum) from gate `root`: a basic event x gives leaf(x), a gate x is entered
+// when enter(x) holds and gives other(x) otherwise.  Returns -1 when the
+// tree is deeper than the frames hold.
+template <class Leaf, class Enter, class Other>
+__device__ double tree_eval(uint32_t root, const uint4 *gate, const uint32_t *inputs, uint32_t n_be, Leaf leaf,
+                            Enter enter, Other other) {
     CountFrame st[kCountDepth];
     int sp = 1;
     count_init(st[0], root, gate[root - n_be].x & 0xFFu);
@@ -281,9 +249,12 @@ __device__ double cut_count(const uint64_t *col, uint64_t W, uint32_t root, int 
         const uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu;
         if (f.j < g.z) {
             const uint32_t x = inputs[g.y + f.j++];
-            const bool fired = (col[(uint64_t)x * W] >> b) & 1ull;
-            if (!fired || x < n_be) {
-                count_deliver(f, op, kk, fired ? 1.0 : 0.0);
+            if (x < n_be) {
+                count_deliver(f, op, kk, leaf(x));
+                continue;
+            }
+            if (!enter(x)) {
+                count_deliver(f, op, kk, other(x));
                 continue;
             }
             if (sp == kCountDepth) return -1.0;
@@ -298,6 +269,154 @@ __device__ double cut_count(const uint64_t *col, uint64_t W, uint32_t root, int 
     }
 }
 
+// One thread per (tree, word, sample): draws the tree's shared events, then
+// descends from the tree's top on the conditioned tree and ORs the sample's
+// bit into the words of the chosen cut set's private events.
+__global__ void __launch_bounds__(256) k_cut_force(CutArgs a) {
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)a.n_inst * a.W * 64) return;
+    const uint32_t b = (uint32_t)(item & 63u);
+    const uint64_t wi = item >> 6;
+    const uint64_t w = wi % a.W;
+    const uint32_t k = (uint32_t)(wi / a.W);
+    uint64_t base = mix64(a.seed ^ ((uint64_t)k << 32));
+    base = mix64(base ^ (a.word_begin + w));
+    base = mix64(base ^ (uint64_t)b);
+    uint32_t draw = 0;
+    const unsigned long long bit = 1ull << b;
+    const uint32_t n_be = a.n_be;
+    // z: every shared event of the tree from its own draw of the stream zbase
+    const uint32_t z0 = a.z_begin[k], z1 = a.z_begin[k + 1];
+    const uint64_t zbase = mix64(base ^ 0x2545F4914F6CDD1Dull);
+    auto z_of = [&](uint32_t j) -> bool {  // entry j of z_event
+        return (mix64(zbase + (uint64_t)(j - z0 + 1) * 0x9E3779B97F4A7C15ull) >> 32) < a.z_thr[j];
+    };
+    uint32_t occ[kZOcc];
+    int n_occ = 0;
+    bool prune = true;
+    for (uint32_t j = z0; j < z1; ++j) {
+        if (!z_of(j)) continue;
+        atomicOr(reinterpret_cast<unsigned long long *>(a.buf + (uint64_t)a.z_event[j] * a.W + w), bit);
+        for (uint32_t o = a.z_occ_begin[j]; prune && o < a.z_occ_begin[j + 1]; ++o) {
+            if (n_occ == kZOcc) {
+                prune = false;
+                break;
+            }
+            const uint32_t v = a.z_occ[o];
+            int q = n_occ++;
+            while (q > 0 && occ[q - 1] > v) {
+                occ[q] = occ[q - 1];
+                --q;
+            }
+            occ[q] = v;
+        }
+    }
+    // a gate whose subtree holds a z_i = 1 leaf (every gate with shared leaves
+    // below when the sample has too many to keep)
+    auto affected = [&](uint32_t node) -> bool {
+        const uint2 r = a.gate_occ[node - n_be];
+        if (r.x >= r.y) return false;
+        if (!prune) return true;
+        for (int q = 0; q < n_occ; ++q)
+            if (occ[q] >= r.x) return occ[q] < r.y;
+        return false;
+    };
+    auto leaf = [&](uint32_t x) -> double { return a.shared[x] ? (z_of(a.z_index[x]) ? 1.0 : 0.0) : a.S[x]; };
+    auto s0 = [&](uint32_t x) -> double { return a.S[x]; };
+    auto sz = [&](uint32_t x) -> double {  // S_z of any node
+        if (x < n_be) return leaf(x);
+        if (!affected(x)) return a.S[x];
+        const double v = tree_eval(x, a.gate, a.inputs, n_be, leaf, affected, s0);
+        if (v < 0.0) atomicOr(a.error, 4u);
+        return v;
+    };
+    uint32_t stack[kCutStack];
+    int sp = 0;
+    const uint32_t root = a.root_row[k];
+    if (!(sz(root) > 0.0)) return;  // z leaves no cut set: nominal private events
+    stack[sp++] = root;
+    while (sp) {
+        const uint32_t node = stack[--sp];
+        if (node < n_be) {
+            if (!a.shared[node])
+                atomicOr(reinterpret_cast<unsigned long long *>(a.buf + (uint64_t)node * a.W + w), bit);
+            continue;
+        }
+        const uint4 g = a.gate[node - n_be];
+        const uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu, n = g.z;
+        const uint32_t *in = a.inputs + g.y;
+        const double *tab = a.tab + g.w;
+        const bool cond = affected(node);
+        if (op == MCG_OR) {
+            const double u = cut_uniform(base, ++draw);
+            uint32_t j = 0;
+            if (!cond) {
+                while (j + 1 < n && u >= tab[j]) ++j;
+            } else {  // shares of S_z: the children's sum, then the first child whose cumulative share passes u
+                double tot = 0.0;
+                for (uint32_t c = 0; c < n; ++c) tot += sz(in[c]);
+                double cum = 0.0;
+                for (; j + 1 < n; ++j) {
+                    cum += sz(in[j]);
+                    if (u * tot < cum) break;
+                }
+            }
+            if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
+            stack[sp++] = in[j];
+        } else if (op == MCG_ATLEAST) {
+            double v[kCutMaxN], E[(kCutMaxN + 1) * (kCutMaxK + 1)];
+            const double *Et = tab;
+            if (cond) {  // E[j][r] = e_r(S_z of children j .. n - 1)
+                if (n > (uint32_t)kCutMaxN) { atomicOr(a.error, 4u); return; }
+                for (uint32_t c = 0; c < n; ++c) v[c] = sz(in[c]);
+                for (uint32_t r = 0; r <= kk; ++r) E[(uint64_t)n * (kk + 1) + r] = r == 0 ? 1.0 : 0.0;
+                for (int c = (int)n - 1; c >= 0; --c)
+                    for (uint32_t r = 0; r <= kk; ++r) {
+                        double e = E[(uint64_t)(c + 1) * (kk + 1) + r];
+                        if (r > 0) e += v[c] * E[(uint64_t)(c + 1) * (kk + 1) + r - 1];
+                        E[(uint64_t)c * (kk + 1) + r] = e;
+                    }
+                Et = E;
+            }
+            uint32_t r = kk;
+            for (uint32_t j = 0; j < n && r > 0; ++j) {
+                bool take = n - j == r;
+                if (!take) {  // P(take j | r still to take) = S_j E[j+1][r-1] / E[j][r]
+                    const double e0 = Et[(uint64_t)j * (kk + 1) + r], e1 = Et[(uint64_t)(j + 1) * (kk + 1) + r - 1];
+                    take = cut_uniform(base, ++draw) * e0 < (cond ? v[j] : a.S[in[j]]) * e1;
+                }
+                if (take) {
+                    if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
+                    stack[sp++] = in[j];
+                    --r;
+                }
+            }
+        } else {  // AND and pass-through gates: every input
+            for (uint32_t j = 0; j < n; ++j) {
+                if (sp == kCutStack) { atomicOr(a.error, 1u); return; }
+                stack[sp++] = in[j];
+            }
+        }
+    }
+}
+
+inline uint64_t mix64_host(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// N(x) of sample b of the word whose rows start at col (row stride W), for
+// the tree rooted at the fired gate `root`; only fired children are visited.
+// Returns -1 when the tree is deeper than the frames hold.
+__device__ double cut_count(const uint64_t *col, uint64_t W, uint32_t root, int b, const uint4 *gate,
+                            const uint32_t *inputs, uint32_t n_be) {
+    auto fired = [&](uint32_t x) -> bool { return (col[(uint64_t)x * W] >> b) & 1ull; };
+    return tree_eval(
+        root, gate, inputs, n_be, [&](uint32_t x) { return fired(x) ? 1.0 : 0.0; }, fired,
+        [&](uint32_t) { return 0.0; });
+}
+
 struct IsBatchArgs {
     const uint64_t *buf;
     uint64_t W;
@@ -310,9 +429,13 @@ struct IsBatchArgs {
     const double *a;               // [n_comp][n_be]
     const double *C;               // [n_comp][n_inst]
     double log_pi[kMaxComponents];
-    int cut_comp;                  // component drawn by cut sets (its log(p/q) is log S - log N(x)), or -1
-    const double *cut_logS;        // per tree: log S(top)
+    int cut_comp;                  // component drawn by cut sets, or -1: its log(p/q) is
+                                   // C + acc (the shared events' log(p(z) / r(z))) + log S_z - log N(x)
+    const double *cut_logS;        // per tree: log S_0(top)
     const uint4 *cut_gate;         // per gate (see CutArgs)
+    const double *cut_S;           // per node: S_0
+    const unsigned char *shared;   // per basic event: read by several gates
+    const uint32_t *companion;     // per gate: node of the OR over the shared leaves below it, or kNoNode
     const uint32_t *inputs;
     uint32_t n_be_nodes;           // basic events of the joined graph (node ids below are events)
     unsigned int *error;
@@ -368,9 +491,25 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
             const int b = __ffsll((long long)m) - 1;
             double lw_cut = 0.0;
             if (p.cut_comp >= 0) {
-                const double n_cut = cut_count(col, p.W, p.root_row[k], b, p.cut_gate, p.inputs, p.n_be_nodes);
+                const uint32_t root = p.root_row[k], nbn = p.n_be_nodes;
+                const double n_cut = cut_count(col, p.W, root, b, p.cut_gate, p.inputs, nbn);
                 if (!(n_cut >= 1.0)) atomicOr(p.error, 2u);  // too deep, or a failure without a cut set
-                lw_cut = p.cut_logS[k] - log(fmax(n_cut, 1.0));
+                double log_sz = p.cut_logS[k];
+                auto fired = [&](uint32_t x) -> bool { return (col[(uint64_t)x * p.W] >> b) & 1ull; };
+                auto entered = [&](uint32_t x) -> bool {
+                    const uint32_t c = p.companion[x - nbn];
+                    return c != kNoNode && fired(c);
+                };
+                if (entered(root)) {  // a shared leaf with z_i = 1 below the top: S_z(top)
+                    const double sz = tree_eval(
+                        root, p.cut_gate, p.inputs, nbn,
+                        [&](uint32_t x) { return p.shared[x] ? (fired(x) ? 1.0 : 0.0) : p.cut_S[x]; }, entered,
+                        [&](uint32_t x) { return p.cut_S[x]; });
+                    if (!(sz > 0.0)) atomicOr(p.error, 2u);
+                    log_sz = log(fmax(sz, 1e-300));
+                }
+                lw_cut = p.C[(uint64_t)p.cut_comp * p.n_inst + k] + acc[p.cut_comp][b] + log_sz -
+                         log(fmax(n_cut, 1.0));
             }
             double lw = p.cut_comp == 0 ? lw_cut : p.C[k] + acc[0][b];
             if (nc > 1) {
@@ -617,6 +756,19 @@ struct mcg_is_batch {
     uint4 *d_cut_gate = nullptr;
     double *d_cut_S = nullptr, *d_cut_tab = nullptr, *d_cut_logS = nullptr;
     unsigned int *d_cut_error = nullptr;
+    // shared basic events of the cut-set component: companion gates appended
+    // to the graph at creation (the caller's gates are the first n_gates_in)
+    uint32_t n_gates_in = 0;
+    bool companions = false;
+    std::vector<uint32_t> companion;     // per gate of the caller: its companion node, or kNoNode
+    std::vector<unsigned char> shared;   // per basic event
+    std::vector<uint32_t> z_event;       // shared events, tree by tree
+    std::vector<uint64_t> z_thr, cut_q;  // per run: their proposal thresholds; the component's table
+    unsigned char *d_shared = nullptr;
+    uint2 *d_gate_occ = nullptr;
+    uint32_t *d_companion = nullptr, *d_z_begin = nullptr, *d_z_event = nullptr, *d_z_index = nullptr;
+    uint32_t *d_z_occ_begin = nullptr, *d_z_occ = nullptr;
+    uint64_t *d_z_thr = nullptr;
 };
 
 namespace {
@@ -641,6 +793,10 @@ void release_batch(mcg_is_batch *b) {
     cudaFree(b->d_cut_tab);
     cudaFree(b->d_cut_logS);
     cudaFree(b->d_cut_error);
+    for (void *q : {(void *)b->d_shared, (void *)b->d_gate_occ, (void *)b->d_companion, (void *)b->d_z_begin,
+                    (void *)b->d_z_event, (void *)b->d_z_index, (void *)b->d_z_occ_begin, (void *)b->d_z_occ,
+                    (void *)b->d_z_thr})
+        cudaFree(q);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->engine) mcg_destroy(b->engine);
@@ -673,6 +829,76 @@ std::string check_partition(const mcg::Graph &g, const std::vector<uint32_t> &be
     return std::string();
 }
 
+// Companion gates for the cut-set component on trees whose only shared
+// nodes are basic events: for every gate with a shared event's leaf below
+// it, an OR over those leaves and over its child gates' companions, appended
+// after the caller's gates (the tallies stay the trees' tops).  The weights
+// kernel reads a companion's word to see which gates a sample's z_i = 1
+// leaves reach.  Nothing is added when no basic event is shared, when a gate
+// is read by several gates, or when a gate is not AND / OR / ATLEAST /
+// pass-through without complemented inputs (the cut-set component refuses
+// such graphs).
+struct Augmented {
+    std::vector<uint8_t> op;
+    std::vector<uint32_t> k, begin, count, neg, inputs;
+    std::vector<int32_t> pdag;
+    std::vector<uint32_t> companion;  // per caller's gate
+    mcg_graph_desc desc{};
+};
+
+bool add_companions(const mcg_graph_desc &d, Augmented &a) {
+    const uint64_t nb = d.n_be, ng = d.n_gates, nn = nb + ng;
+    std::vector<uint32_t> fanout(nn, 0);
+    for (uint64_t i = 0; i < d.n_inputs; ++i)
+        if (d.inputs[i] < nn) ++fanout[d.inputs[i]];
+    bool any_shared = false;
+    for (uint64_t i = 0; i < nb; ++i) any_shared |= fanout[i] > 1;
+    if (!any_shared) return false;
+    for (uint64_t j = 0; j < ng; ++j) {
+        const uint8_t op = d.gate_op[j];
+        if (fanout[nb + j] > 1 || d.gate_neg_count[j] ||
+            !(op == MCG_AND || op == MCG_OR || op == MCG_ATLEAST || op == MCG_NULL))
+            return false;
+        if ((uint64_t)d.gate_in_begin[j] + d.gate_in_count[j] > d.n_inputs) return false;
+    }
+    a.op.assign(d.gate_op, d.gate_op + ng);
+    a.k.assign(d.gate_k, d.gate_k + ng);
+    a.begin.assign(d.gate_in_begin, d.gate_in_begin + ng);
+    a.count.assign(d.gate_in_count, d.gate_in_count + ng);
+    a.neg.assign(d.gate_neg_count, d.gate_neg_count + ng);
+    a.inputs.assign(d.inputs, d.inputs + d.n_inputs);
+    if (d.gate_pdag_idx) a.pdag.assign(d.gate_pdag_idx, d.gate_pdag_idx + ng);
+    a.companion.assign(ng, kNoNode);
+    for (uint64_t j = 0; j < ng; ++j) {
+        std::vector<uint32_t> in;
+        for (uint32_t c = 0; c < d.gate_in_count[j]; ++c) {
+            const uint32_t x = d.inputs[d.gate_in_begin[j] + c];
+            if (x < nb ? fanout[x] > 1 : (x - nb < j && a.companion[x - nb] != kNoNode))
+                in.push_back(x < nb ? x : a.companion[x - nb]);
+        }
+        if (in.empty()) continue;
+        a.companion[j] = (uint32_t)(nb + a.op.size());
+        a.op.push_back(MCG_OR);
+        a.k.push_back(0);
+        a.begin.push_back((uint32_t)a.inputs.size());
+        a.count.push_back((uint32_t)in.size());
+        a.neg.push_back(0);
+        if (d.gate_pdag_idx) a.pdag.push_back(-1);
+        a.inputs.insert(a.inputs.end(), in.begin(), in.end());
+    }
+    a.desc = d;
+    a.desc.n_gates = (uint32_t)a.op.size();
+    a.desc.gate_op = a.op.data();
+    a.desc.gate_k = a.k.data();
+    a.desc.gate_in_begin = a.begin.data();
+    a.desc.gate_in_count = a.count.data();
+    a.desc.gate_neg_count = a.neg.data();
+    a.desc.inputs = a.inputs.data();
+    a.desc.n_inputs = a.inputs.size();
+    a.desc.gate_pdag_idx = d.gate_pdag_idx ? a.pdag.data() : nullptr;
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -698,7 +924,11 @@ mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_inst, con
     });
     b->n_inst = n_inst;
     b->be_begin.assign(be_begin, be_begin + n_inst + 1);
-    mcg_status st = mcg_create(graph, &run, &b->engine);
+    b->n_gates_in = graph->n_gates;
+    Augmented aug;
+    b->companions = add_companions(*graph, aug);
+    if (b->companions) b->companion = aug.companion;
+    mcg_status st = mcg_create(b->companions ? &aug.desc : graph, &run, &b->engine);
     if (st != MCG_OK) return st;
     const mcg::Graph &g = b->engine->graph;
     const std::string bad = check_partition(g, b->be_begin);
@@ -736,23 +966,42 @@ mcg_status mcg_is_batch_destroy(mcg_is_batch *b) {
 namespace {
 
 // Tables of the cut-set component (see k_cut_force): every gate AND, OR,
-// ATLEAST (k <= 8) or pass-through without complemented inputs, no node read
-// twice (minimal cut sets are then the descents), S(top) > 0 for every tree.
+// ATLEAST (k <= 8) or pass-through without complemented inputs and read by
+// one gate at most; basic events read by several gates are the shared
+// events z of their tree (the graph then carries companion gates); S(top) > 0
+// for every tree.
 mcg_status build_cut_tables(mcg_is_batch *b) {
     const mcg::Graph &g = b->engine->graph;
-    const uint32_t nb = g.n_be, ng = g.n_gates, nn = g.n_nodes();
+    const uint32_t nb = g.n_be, ng_all = g.n_gates, ng = b->n_gates_in, nn = g.n_nodes();
     std::vector<uint32_t> fanout(nn, 0);
-    for (uint32_t x : g.inputs) ++fanout[x];
-    for (uint32_t i = 0; i < nn; ++i)
-        if (fanout[i] > 1)
+    for (uint32_t j = 0; j < ng; ++j)
+        for (uint32_t c = 0; c < g.gate_in_count[j]; ++c) ++fanout[g.inputs[g.gate_in_begin[j] + c]];
+    for (uint32_t i = 0; i < nb + ng; ++i)
+        if (fanout[i] > 1 && (i >= nb || !b->companions))
             return mcg::fail(MCG_ERR_INVALID, "cut-set sampling needs trees: node " + std::to_string(i) +
                                                   " is read by several gates");
-    std::vector<double> S(nn, 0.0), tab;
-    std::vector<uint4> gate(ng);
+    b->shared.assign(nb, 0);
+    for (uint32_t i = 0; i < nb; ++i) b->shared[i] = fanout[i] > 1;
+    // S_0 (shared events at 0) for the tables; S with every event at p for the check
+    std::vector<double> S(nn, 0.0), Sp(nn, 0.0), tab;
+    std::vector<uint4> gate(std::max<uint32_t>(ng_all, 1), make_uint4(0, 0, 0, 0));
     for (uint32_t i = 0; i < nb; ++i) {
         const uint64_t t = g.be_threshold[i];
-        S[i] = t >= (1ull << 32) ? 1.0 : (double)t / 4294967296.0;
+        Sp[i] = t >= (1ull << 32) ? 1.0 : (double)t / 4294967296.0;
+        S[i] = b->shared[i] ? 0.0 : Sp[i];
     }
+    auto elementary = [](const std::vector<double> &v, uint32_t k, std::vector<double> &E) {
+        const uint32_t n = (uint32_t)v.size();  // E[j][r] = e_r(v_j, ..., v_{n-1}), j = n .. 0
+        E.assign((size_t)(n + 1) * (k + 1), 0.0);
+        E[(size_t)n * (k + 1)] = 1.0;
+        for (int c = (int)n - 1; c >= 0; --c)
+            for (uint32_t r = 0; r <= k; ++r) {
+                double e = E[(size_t)(c + 1) * (k + 1) + r];
+                if (r > 0) e += v[c] * E[(size_t)(c + 1) * (k + 1) + r - 1];
+                E[(size_t)c * (k + 1) + r] = e;
+            }
+    };
+    std::vector<double> vals, valp, E, Ep;
     for (uint32_t j = 0; j < ng; ++j) {
         const uint32_t op = g.gate_op[j], n = g.gate_in_count[j], k = g.gate_k[j] & 0xFFu;
         const uint32_t *in = g.inputs.data() + g.gate_in_begin[j];
@@ -762,52 +1011,122 @@ mcg_status build_cut_tables(mcg_is_batch *b) {
         if (op == MCG_ATLEAST && k > (uint32_t)kCutMaxK)
             return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: ATLEAST threshold above 8");
         gate[j] = make_uint4(op | (k << 8), g.gate_in_begin[j], n, (uint32_t)tab.size());
-        double v = 0.0;
+        vals.assign(n, 0.0);
+        valp.assign(n, 0.0);
+        for (uint32_t c = 0; c < n; ++c) vals[c] = S[in[c]], valp[c] = Sp[in[c]];
+        double v = 0.0, vp = 0.0;
         if (op == MCG_AND) {
-            v = 1.0;
-            for (uint32_t c = 0; c < n; ++c) v *= S[in[c]];
+            v = vp = 1.0;
+            for (uint32_t c = 0; c < n; ++c) v *= vals[c], vp *= valp[c];
         } else if (op == MCG_OR) {
-            for (uint32_t c = 0; c < n; ++c) v += S[in[c]];
+            for (uint32_t c = 0; c < n; ++c) v += vals[c], vp += valp[c];
             double cum = 0.0;
             for (uint32_t c = 0; c < n; ++c) {
-                cum += S[in[c]];
+                cum += vals[c];
                 tab.push_back(v > 0 ? cum / v : 1.0);
             }
         } else if (op == MCG_ATLEAST) {
-            // E[j][r] = e_r(S_j, ..., S_{n-1}), j = n .. 0
-            std::vector<double> E((size_t)(n + 1) * (k + 1), 0.0);
-            E[(size_t)n * (k + 1)] = 1.0;
-            for (int c = (int)n - 1; c >= 0; --c) {
-                for (uint32_t r = 0; r <= k; ++r) {
-                    double e = E[(size_t)(c + 1) * (k + 1) + r];
-                    if (r > 0) e += S[in[c]] * E[(size_t)(c + 1) * (k + 1) + r - 1];
-                    E[(size_t)c * (k + 1) + r] = e;
-                }
-            }
+            elementary(vals, k, E);
+            elementary(valp, k, Ep);
             v = E[k];
+            vp = Ep[k];
             tab.insert(tab.end(), E.begin(), E.end());
         } else {  // pass-through
-            v = n ? S[in[n - 1]] : 0.0;
+            v = n ? vals[n - 1] : 0.0;
+            vp = n ? valp[n - 1] : 0.0;
         }
         S[nb + j] = v;
+        Sp[nb + j] = vp;
     }
+    for (uint32_t j = ng; j < ng_all; ++j)  // companions: never entered by the descent or the evaluations
+        gate[j] = make_uint4(MCG_OR, g.gate_in_begin[j], g.gate_in_count[j], 0);
     std::vector<double> logS(b->n_inst);
     for (uint32_t t = 0; t < b->n_inst; ++t) {
-        const double st = S[g.tally_nodes[t]];
+        const double st = Sp[g.tally_nodes[t]];
         if (!(st > 0.0) || !std::isfinite(st))
             return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: tree " + std::to_string(t) + " has no cut set");
-        logS[t] = std::log(st);
+        logS[t] = std::log(S[g.tally_nodes[t]]);  // -inf when every cut set holds a shared event
     }
+    // shared-leaf occurrences in depth-first order from every top: each gate's
+    // subtree holds the range [lo, hi) of them
+    std::vector<uint2> occ_range(std::max<uint32_t>(ng_all, 1), make_uint2(0, 0));
+    std::vector<std::vector<uint32_t>> occ_of(nb);
+    uint32_t pos = 0;
+    for (uint32_t t = 0; t < b->n_inst; ++t) {
+        const uint32_t root = g.tally_nodes[t];
+        if (root < nb) continue;
+        std::vector<std::pair<uint32_t, uint32_t>> st{{root, 0}};
+        occ_range[root - nb].x = pos;
+        while (!st.empty()) {
+            auto &top = st.back();
+            const uint32_t j = top.first - nb;
+            if (top.second < g.gate_in_count[j]) {
+                const uint32_t x = g.inputs[g.gate_in_begin[j] + top.second++];
+                if (x < nb) {
+                    if (b->shared[x]) occ_of[x].push_back(pos++);
+                } else {
+                    occ_range[x - nb].x = pos;
+                    st.push_back({x, 0});
+                }
+            } else {
+                occ_range[j].y = pos;
+                const uint32_t op = g.gate_op[j];
+                if (op == MCG_ATLEAST && occ_range[j].y > occ_range[j].x && g.gate_in_count[j] > (uint32_t)kCutMaxN)
+                    return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: ATLEAST gate " + std::to_string(j) +
+                                                          " above shared events has more than 32 inputs");
+                st.pop_back();
+            }
+        }
+    }
+    std::vector<uint32_t> z_begin(b->n_inst + 1, 0), z_index(nb, 0), z_occ_begin{0}, z_occ;
+    b->z_event.clear();
+    for (uint32_t t = 0; t < b->n_inst; ++t) {
+        z_begin[t] = (uint32_t)b->z_event.size();
+        for (uint32_t i = b->be_begin[t]; i < b->be_begin[t + 1]; ++i) {
+            if (!b->shared[i]) continue;
+            z_index[i] = (uint32_t)b->z_event.size();
+            b->z_event.push_back(i);
+            z_occ.insert(z_occ.end(), occ_of[i].begin(), occ_of[i].end());
+            z_occ_begin.push_back((uint32_t)z_occ.size());
+        }
+    }
+    z_begin[b->n_inst] = (uint32_t)b->z_event.size();
+    std::vector<uint32_t> comp(std::max<uint32_t>(ng, 1), kNoNode);
+    if (b->companions) std::copy(b->companion.begin(), b->companion.end(), comp.begin());
     if (tab.empty()) tab.push_back(0.0);
-    MCG_CUDA(cudaMalloc((void **)&b->d_cut_gate, std::max<uint32_t>(ng, 1) * sizeof(uint4)));
+    const uint64_t nz = std::max<uint64_t>(b->z_event.size(), 1);
+    if (z_occ.empty()) z_occ.push_back(0);
+    MCG_CUDA(cudaMalloc((void **)&b->d_cut_gate, gate.size() * sizeof(uint4)));
     MCG_CUDA(cudaMalloc((void **)&b->d_cut_S, nn * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_cut_tab, tab.size() * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_cut_logS, b->n_inst * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_cut_error, sizeof(unsigned int)));
-    if (ng) MCG_CUDA(cudaMemcpy(b->d_cut_gate, gate.data(), ng * sizeof(uint4), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMalloc((void **)&b->d_shared, std::max<uint32_t>(nb, 1)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_gate_occ, occ_range.size() * sizeof(uint2)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_companion, comp.size() * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_z_begin, z_begin.size() * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_z_event, nz * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_z_index, std::max<uint32_t>(nb, 1) * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_z_occ_begin, z_occ_begin.size() * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_z_occ, z_occ.size() * sizeof(uint32_t)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_z_thr, nz * sizeof(uint64_t)));
+    MCG_CUDA(cudaMemcpy(b->d_cut_gate, gate.data(), gate.size() * sizeof(uint4), cudaMemcpyHostToDevice));
     MCG_CUDA(cudaMemcpy(b->d_cut_S, S.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
     MCG_CUDA(cudaMemcpy(b->d_cut_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
     MCG_CUDA(cudaMemcpy(b->d_cut_logS, logS.data(), b->n_inst * sizeof(double), cudaMemcpyHostToDevice));
+    if (nb) {
+        MCG_CUDA(cudaMemcpy(b->d_shared, b->shared.data(), nb, cudaMemcpyHostToDevice));
+        MCG_CUDA(cudaMemcpy(b->d_z_index, z_index.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    MCG_CUDA(cudaMemcpy(b->d_gate_occ, occ_range.data(), occ_range.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_companion, comp.data(), comp.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_z_begin, z_begin.data(), z_begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (!b->z_event.empty())
+        MCG_CUDA(cudaMemcpy(b->d_z_event, b->z_event.data(), b->z_event.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_z_occ_begin, z_occ_begin.data(), z_occ_begin.size() * sizeof(uint32_t),
+                        cudaMemcpyHostToDevice));
+    MCG_CUDA(cudaMemcpy(b->d_z_occ, z_occ.data(), z_occ.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     b->cut_ready = true;
     return MCG_OK;
 }
@@ -834,8 +1153,9 @@ mcg_status ensure_components(mcg_is_batch *b, uint32_t n_comp) {
 extern "C" {
 
 mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_def, const uint64_t *q_def,
-                            const uint64_t *words_def, uint64_t words_cutset, uint32_t iteration, uint64_t word_begin,
-                            uint64_t word_count, double *tree_sums, double *ce_num, double *kernel_ms) {
+                            const uint64_t *words_def, uint64_t words_cutset, const uint64_t *q_cutset,
+                            uint32_t iteration, uint64_t word_begin, uint64_t word_count, double *tree_sums,
+                            double *ce_num, double *kernel_ms) {
     mcg::clear_error();
     if (!b || !q_thr || !tree_sums) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
     if (n_def + 1 > (uint32_t)kMaxComponents)
@@ -869,14 +1189,22 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
             comp_words.push_back(words_def[c]);
         }
     int cut_comp = -1;
-    if (words_cutset) {  // nominal thresholds plus a forced cut set per sample
+    if (words_cutset) {  // shared events from q_cutset, nominal private events plus a forced cut set per sample
         if (!b->cut_ready) {
             MCG_CUDA(cudaSetDevice(e->device));
             const mcg_status cs = build_cut_tables(b);
             if (cs != MCG_OK) return cs;
         }
+        b->cut_q.assign(g.be_threshold.begin(), g.be_threshold.end());
+        b->z_thr.resize(b->z_event.size());
+        for (size_t j = 0; j < b->z_event.size(); ++j) {
+            const uint32_t i = b->z_event[j];
+            const uint64_t tp = g.be_threshold[i];
+            if (q_cutset && tp != 0 && tp < (1ull << 32)) b->cut_q[i] = q_cutset[i];
+            b->z_thr[j] = b->cut_q[i];
+        }
         cut_comp = (int)comp_q.size();
-        comp_q.push_back(g.be_threshold.data());
+        comp_q.push_back(b->cut_q.data());
         comp_words.push_back(words_cutset);
     }
     if (comp_q.empty()) comp_q.push_back(q_thr), comp_words.push_back(0);
@@ -909,6 +1237,13 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
     for (auto &th : pool) th.join();
     for (unsigned t = 0; t < n_thr; ++t)
         if (bad[t]) return mcg::fail(MCG_ERR_INVALID, why[t]);
+    if (cut_comp >= 0) {  // the forcing kernel draws the shared events itself: the sampler leaves them 0
+        uint4 *cq = b->beq.data() + (uint64_t)cut_comp * nb;
+        for (uint32_t i : b->z_event) cq[i].z = cq[i].w = 0u;
+        if (!b->z_thr.empty())
+            MCG_CUDA(cudaMemcpyAsync(b->d_z_thr, b->z_thr.data(), b->z_thr.size() * sizeof(uint64_t),
+                                     cudaMemcpyHostToDevice, e->stream));
+    }
     if (nb) {
         MCG_CUDA(cudaMemcpyAsync(b->d_be_q, b->beq.data(), nc * nb * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
         MCG_CUDA(cudaMemcpyAsync(b->d_a, b->a.data(), nc * nb * sizeof(double), cudaMemcpyHostToDevice, e->stream));
@@ -936,6 +1271,9 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
     args.cut_comp = cut_comp;
     args.cut_logS = b->d_cut_logS;
     args.cut_gate = b->d_cut_gate;
+    args.cut_S = b->d_cut_S;
+    args.shared = b->d_shared;
+    args.companion = b->d_companion;
     args.inputs = e->d_inputs;
     args.n_be_nodes = g.n_be;
     args.error = b->d_cut_error;
@@ -972,6 +1310,14 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
             ca.inputs = e->d_inputs;
             ca.S = b->d_cut_S;
             ca.tab = b->d_cut_tab;
+            ca.shared = b->d_shared;
+            ca.gate_occ = b->d_gate_occ;
+            ca.z_begin = b->d_z_begin;
+            ca.z_event = b->d_z_event;
+            ca.z_thr = b->d_z_thr;
+            ca.z_index = b->d_z_index;
+            ca.z_occ_begin = b->d_z_occ_begin;
+            ca.z_occ = b->d_z_occ;
             ca.seed = mix64_host(((uint64_t)iteration << 32) ^ 0x5bd1e995u);
             ca.error = b->d_cut_error;
             e->sample_hook = [=](cudaStream_t s, uint64_t *buf, uint64_t W, uint64_t wb) -> mcg_status {
@@ -1007,6 +1353,8 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
     if (cut_error & 2u)
         return mcg::fail(MCG_ERR_STATE, "cut-set count failed (tree deeper than 32 levels, or a failure without "
                                         "a cut set)");
+    if (cut_error & 4u)
+        return mcg::fail(MCG_ERR_STATE, "cut-set descent above shared events failed (tree deeper than 32 levels)");
     if (kernel_ms) {
         float ms = 0.f;
         MCG_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));

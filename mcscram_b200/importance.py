@@ -56,8 +56,8 @@ _capi.register_signatures({
     "mcg_is_batch_create": (C.c_int, [C.POINTER(_capi.GraphDesc), C.c_uint32, C.POINTER(C.c_uint32),
                                       C.POINTER(_capi.RunDesc), C.POINTER(_vp)]),
     "mcg_is_batch_destroy": (C.c_int, [_vp]),
-    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, C.c_uint32, _u64p, _u64p, C.c_uint64, C.c_uint32, C.c_uint64,
-                                   C.c_uint64, _dp, _dp, _dp]),
+    "mcg_is_batch_run": (C.c_int, [_vp, _u64p, C.c_uint32, _u64p, _u64p, C.c_uint64, _u64p, C.c_uint32,
+                                   C.c_uint64, C.c_uint64, _dp, _dp, _dp]),
     "mcg_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_vp)]),
     "mcg_mlp_destroy": (C.c_int, [_vp]),
     "mcg_mlp_set_params": (C.c_int, [_vp, _fp]),
@@ -213,12 +213,18 @@ def _conditioned(pr, cache, nb, n_nodes, roots):
 def cut_set_eligible(g: FlatGraph) -> bool:
     """Whether the cut-set component (mcg_is_batch_run's words_cutset) takes
     this graph: AND/OR/ATLEAST (k <= 8)/pass-through gates, no complemented
-    inputs, no node read twice."""
+    inputs, no gate read by two gates (basic events may be: they are drawn
+    first, and the cut set on the tree conditioned on them)."""
     from .graph import NULL
     ok_ops = np.isin(g.gate_op, [AND, OR, ATLEAST, NULL])
     k_ok = np.where(g.gate_op == ATLEAST, (g.gate_k & 0xFF) <= 8, True)
-    return bool(np.all(ok_ops) and np.all(k_ok) and np.all(g.gate_neg_count == 0) and
-                np.all(np.bincount(g.inputs, minlength=g.n_nodes) <= 1))
+    fan = np.bincount(g.inputs, minlength=g.n_nodes)
+    return bool(np.all(ok_ops) and np.all(k_ok) and np.all(g.gate_neg_count == 0) and np.all(fan[g.n_be:] <= 1))
+
+
+def shared_events(g: FlatGraph) -> np.ndarray:
+    """Basic events read by more than one gate."""
+    return np.bincount(g.inputs, minlength=g.n_nodes)[: g.n_be] > 1
 
 
 def _mode_kids(g: FlatGraph) -> List[int]:
@@ -601,12 +607,14 @@ class BatchedImportanceSampler:
 
     def run(self, q_thresholds: np.ndarray, iteration: int = 1, word_begin: int = 0, word_count: int = 1 << 14,
             ce: bool = False, q_defensive: Optional[np.ndarray] = None, words_defensive=0,
-            words_cutset: int = 0) -> dict:
+            words_cutset: int = 0, q_cutset: Optional[np.ndarray] = None) -> dict:
         """Per-tree sums of one pass.  q_defensive ([n_be] or [n_comp, n_be]
         thresholds) with words_defensive (an int or one per component): the
         main proposal draws the first words, each defensive proposal the next
         words_defensive[c], the cut-set component the last words_cutset, and
-        samples carry the balance-heuristic weight."""
+        samples carry the balance-heuristic weight.  q_cutset ([n_be]
+        thresholds): the cut-set component's proposal for the events read by
+        several gates (default: their nominal thresholds)."""
         q_thresholds = np.ascontiguousarray(q_thresholds, dtype=np.uint64)
         nb = self.union.n_be
         if q_thresholds.shape != (nb,):
@@ -621,9 +629,15 @@ class BatchedImportanceSampler:
         sums = np.zeros((self.n_trees, 4), dtype=np.float64)
         ce_num = np.zeros(max(nb, 1), dtype=np.float64) if ce else None
         ms = C.c_double()
+        qc = None
+        if q_cutset is not None:
+            qc = np.ascontiguousarray(q_cutset, dtype=np.uint64)
+            if qc.shape != (nb,):
+                raise ValueError("one cut-set proposal threshold per event of the joined graph")
         _capi.check(self.lib.mcg_is_batch_run(self.h, _p(q_thresholds, C.c_uint64), n_def,
                                               _p(qd, C.c_uint64) if n_def else None,
                                               _p(wd, C.c_uint64) if n_def else None, int(words_cutset),
+                                              _p(qc, C.c_uint64) if qc is not None else None,
                                               iteration, word_begin, word_count, _p(sums, C.c_double),
                                               _p(ce_num, C.c_double) if ce else None, C.byref(ms)))
         out = {"sum_w": sums[:, 0].copy(), "sum_w2": sums[:, 1].copy(), "hits": sums[:, 2].astype(np.int64),
@@ -834,8 +848,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     if cut:
         bad = [k for k, g in enumerate(graphs) if not cut_set_eligible(g)]
         if bad:
-            raise ValueError(f"cut-set sampling needs trees of AND/OR/ATLEAST gates without shared nodes or "
-                             f"negations; trees {bad[:5]} are not")
+            raise ValueError(f"cut-set sampling needs trees of AND/OR/ATLEAST gates without negations and without "
+                             f"gates read by several gates; trees {bad[:5]} are not")
         q_def = np.zeros((0, full.union.n_be))
     elif defensive_proposal == "modes":
         q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
@@ -849,6 +863,34 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         raise ValueError("defensive_proposal must be 'cutsets', 'modes', 'approx' or 'probe'")
     n_comp = q_def.shape[0]
 
+    # Events read by several gates: the cut-set component draws them first,
+    # from r = the current proposal clipped to [p, 0.5] (their conditional
+    # failure probability given the top is what it should approach; at the
+    # start the independence approximation's estimate of it), and then the cut
+    # set on the tree conditioned on them.
+    shared_u = np.concatenate([shared_events(g) for g in graphs]) if cut else np.zeros(full.union.n_be, bool)
+    has_shared = bool(shared_u.any())
+
+    def z_thr(qv, smp=None):
+        if not has_shared:
+            return None
+        smp = full if smp is None else smp
+        return smp.proposal_thresholds(np.where(shared_u_of(smp), np.clip(qv, p_of(smp), 0.5), p_of(smp)))
+
+    def shared_u_of(smp):
+        return shared_u if smp is full else np.concatenate([shared_u[sl[k]] for k in members])
+
+    def p_of(smp):
+        return p if smp is full else np.concatenate([p[sl[k]] for k in members])
+
+    r0 = None
+    if has_shared:
+        r0 = p.copy()
+        for k, g in enumerate(graphs):
+            m = shared_u[sl[k]]
+            if m.any():
+                r0[sl[k]][m] = np.clip(approximate_importance(g)[1][m], p[sl[k]][m], 0.5)
+
     def def_words(w):  # words per defensive component
         return max(1, int(round(defensive * w / n_comp))) if defensive > 0 and n_comp else 0
 
@@ -861,8 +903,10 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     for r in range(ce_rounds):
         if q is None and cut:  # first round: cut-set samples alone
             res = full.run(full.union.be_threshold, iteration=it, word_count=ce_words, ce=True,
-                           words_cutset=ce_words)
+                           words_cutset=ce_words, q_cutset=z_thr(r0) if has_shared else None)
             q = np.minimum(p * scale[tree_of_event], cap_e)
+            if has_shared:
+                q = np.where(shared_u, r0, q)
         elif q is None:  # first round: the defensive mixture alone
             res = full.run(thr_def[0], iteration=it, word_count=ce_words, ce=True, q_defensive=thr_def,
                            words_defensive=[ce_words // n_comp + (c < ce_words % n_comp) for c in range(n_comp)])
@@ -870,7 +914,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         else:
             res = full.run(full.proposal_thresholds(q), iteration=it, word_count=ce_words, ce=True,
                            q_defensive=thr_def if def_words(ce_words) else None, words_defensive=def_words(ce_words),
-                           words_cutset=cut_words(ce_words))
+                           words_cutset=cut_words(ce_words), q_cutset=z_thr(q) if cut_words(ce_words) else None)
         it += 1
         gpu["ce"] += res["kernel_ms"]
         sw = res["sum_w"][tree_of_event]
@@ -922,7 +966,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
                              for k in members], axis=1)
         res = sampler.run(sampler.proposal_thresholds(qa), iteration=it, word_begin=0, word_count=words,
                           q_defensive=np.stack([sampler.proposal_thresholds(qc) for qc in qd]) if def_words(words)
-                          else None, words_defensive=def_words(words), words_cutset=cut_words(words))
+                          else None, words_defensive=def_words(words), words_cutset=cut_words(words),
+                          q_cutset=z_thr(qa, sampler) if cut_words(words) else None)
         it += 1
         gpu["estimate"] += res["kernel_ms"]
         used += words

@@ -43,6 +43,8 @@ class TreeSpec:
     atleast_k_max_offset: int = 1              # k in [2, n - offset]
     share_be_frac: float = 0.0                 # basic events given >= 2 parents
     share_node_frac: float = 0.0               # nodes (events and gates) given >= 2 parents
+    share_scope: Optional[int] = None          # shared events' parents within the subtree of the first
+                                               # parent's ancestor this many levels up (None: anywhere)
     name: str = "tree"
     extra: dict = field(default_factory=dict)
 
@@ -91,6 +93,67 @@ def _default_layers(n_gates: int, fanin_mean: float) -> int:
     # depth of a balanced tree of n_gates gates with the mean fan-in, plus a margin
     d = int(np.ceil(np.log(max(n_gates, 2)) / np.log(max(fanin_mean, 1.5)))) + 2
     return max(2, min(d, n_gates))
+
+
+def _local_sharing(rng, children, be_req, slots, share_be, B, G, scope):
+    """Slot assignment with every shared event's two occurrences in one
+    neighbourhood: the subtree of the ancestor `scope` levels above the gate
+    of its first occurrence (widened a level at a time when that subtree has
+    no other gate with a free slot).  Gates must have one parent each.
+    Returns (events, slots) in matching order; the other events fill the
+    remaining slots at random."""
+    parent = np.full(G, -1, dtype=np.int64)
+    for g in range(G):
+        for c in children[g]:
+            if c >= B:
+                parent[c - B] = g
+    free_by_gate = {}
+    for s in slots:
+        free_by_gate[int(s)] = free_by_gate.get(int(s), 0) + 1
+
+    def ancestor(g, h):
+        for _ in range(h):
+            if parent[g] < 0:
+                break
+            g = int(parent[g])
+        return g
+
+    def subtree_gates(a):
+        out, todo = [], [a]
+        while todo:
+            g = todo.pop()
+            out.append(g)
+            todo.extend(int(c) - B for c in children[g] if c >= B)
+        return out
+
+    ev, sl = [], []
+    for e in rng.permutation(np.nonzero(share_be)[0]):
+        open_gates = [g for g, n in free_by_gate.items() if n > 0]
+        if len(open_gates) < 2:
+            raise ValueError("no slots left for a shared event")
+        g1 = int(open_gates[rng.integers(len(open_gates))])
+        h = scope
+        while True:
+            cand = [g for g in subtree_gates(ancestor(g1, h)) if g != g1 and free_by_gate.get(g, 0) > 0]
+            if cand or ancestor(g1, h) == ancestor(g1, h + 1):
+                break
+            h += 1
+        if not cand:
+            raise ValueError("no second slot for a shared event")
+        g2 = int(cand[rng.integers(len(cand))])
+        for g in (g1, g2):
+            free_by_gate[g] -= 1
+            ev.append(int(e))
+            sl.append(g)
+    rest_slots = np.repeat(np.array(list(free_by_gate.keys()), dtype=np.int64),
+                           np.array(list(free_by_gate.values()), dtype=np.int64))
+    rng.shuffle(rest_slots)
+    rest_ev = np.nonzero(~share_be)[0]
+    rng.shuffle(rest_ev)
+    if rest_slots.size != rest_ev.size:
+        raise ValueError("slot/requirement mismatch after placing the shared events")
+    return (np.concatenate([np.array(ev, dtype=np.int64), rest_ev]),
+            np.concatenate([np.array(sl, dtype=np.int64), rest_slots]))
 
 
 def generate(spec: TreeSpec) -> FlatGraph:
@@ -235,6 +298,8 @@ def generate(spec: TreeSpec) -> FlatGraph:
     rng.shuffle(slots)
     if slots.size != be_req.size:
         raise ValueError(f"slot/requirement mismatch {slots.size} vs {be_req.size}")
+    if spec.share_scope is not None and share_be.any():
+        be_req, slots = _local_sharing(rng, children, be_req, slots, share_be, B, G, spec.share_scope)
     # assign avoiding duplicate children; repair collisions by swapping
     assign = slots.copy()
     child_sets = [set(ch) for ch in children]

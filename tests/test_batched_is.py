@@ -629,10 +629,262 @@ def test_cut_set_estimates_rare_trees(gpu):
 
 
 @pytest.mark.gpu
-def test_cut_set_component_rejects_shared_nodes(gpu):
+def test_cut_set_component_rejects_shared_gates(gpu):
     from mcscram_b200 import _capi
-    from mcscram_b200.importance import BatchedImportanceSampler
-    g = synth.config1()  # 20 % of its events have two parents
+    from mcscram_b200.importance import BatchedImportanceSampler, cut_set_eligible
+    g = synth.generate(synth.TreeSpec(n_be=40, n_gates=20, mix={AND: 0.5, OR: 0.5}, p_range=(0.01, 0.2), seed=3,
+                                      n_layers=5, share_node_frac=0.3))
+    assert np.any(np.bincount(g.inputs, minlength=g.n_nodes)[g.n_be:] > 1) and not cut_set_eligible(g)
     with BatchedImportanceSampler([g]) as s:
         with pytest.raises(_capi.McgError, match="read by several gates"):
             s.run(s.union.be_threshold, iteration=1, word_count=64, words_cutset=64)
+
+
+# ------------------------------------------- cut-set component with shared basic events
+
+Z_OCC = 32  # occurrences a sample keeps for pruning (the kernel's kZOcc)
+
+
+def _occurrences(u, roots, shared):
+    nb = u.n_be
+    occ_range, occ_of, pos = {}, {}, 0
+    for root in roots:
+        stack = [(int(root), 0)]
+        occ_range[int(root) - nb] = [pos, pos]
+        while stack:
+            node, i = stack[-1]
+            j = node - nb
+            ins = [int(x) for x in u.gate_inputs(j)]
+            if i < len(ins):
+                stack[-1] = (node, i + 1)
+                x = ins[i]
+                if x < nb:
+                    if shared[x]:
+                        occ_of.setdefault(x, []).append(pos)
+                        pos += 1
+                else:
+                    occ_range[x - nb] = [pos, pos]
+                    stack.append((x, 0))
+            else:
+                occ_range[j][1] = pos
+                stack.pop()
+    return occ_range, occ_of
+
+
+def _eval(u, node, leaf, enter, other):
+    """The kernels' AND / OR / ATLEAST recursion (same order of operations)."""
+    nb = u.n_be
+    j = node - nb
+    op, k = int(u.gate_op[j]), int(u.gate_k[j]) & 0xFF
+    acc = 1.0 if op == AND else 0.0
+    dp = [1.0] + [0.0] * 8
+    for x in (int(c) for c in u.gate_inputs(j)):
+        val = leaf(x) if x < nb else (_eval(u, x, leaf, enter, other) if enter(x) else other(x))
+        if op == AND:
+            acc *= val
+        elif op == ATLEAST:
+            for r in range(k, 0, -1):
+                dp[r] += dp[r - 1] * val
+        else:
+            acc += val
+    return dp[k] if op == ATLEAST else acc
+
+
+def _descend_shared(u, S0, tab, shared, occ_range, zlist, zthr, root, base):
+    """Shared events drawn and private events forced for one sample (the
+    library's draws, pruning and arithmetic)."""
+    nb = u.n_be
+    zbase = _mix64(base ^ 0x2545F4914F6CDD1D)
+    z = {}
+    occ, prune = [], True
+    for jj, (e, occs) in enumerate(zlist):
+        z[e] = (_mix64((zbase + (jj + 1) * 0x9E3779B97F4A7C15) & M64) >> 32) < int(zthr[e])
+        if not z[e]:
+            continue
+        for o in occs:
+            if not prune:
+                break
+            if len(occ) == Z_OCC:
+                prune = False
+                break
+            occ.append(o)
+            occ.sort()
+
+    def affected(x):
+        lo, hi = occ_range.get(x - nb, (0, 0))
+        if lo >= hi:
+            return False
+        if not prune:
+            return True
+        return any(lo <= o < hi for o in occ)
+
+    leaf = lambda x: (1.0 if z[x] else 0.0) if shared[x] else S0[x]
+    other = lambda x: S0[x]
+
+    def sz(x):
+        if x < nb:
+            return leaf(x)
+        return _eval(u, x, leaf, affected, other) if affected(x) else S0[x]
+
+    draw = 0
+
+    def unif():
+        nonlocal draw
+        draw += 1
+        return (_mix64((base + draw * 0x9E3779B97F4A7C15) & M64) >> 11) * 2.0 ** -53
+
+    forced = []
+    if not sz(int(root)) > 0:
+        return z, forced
+    stack = [int(root)]
+    while stack:
+        node = stack.pop()
+        if node < nb:
+            if not shared[node]:
+                forced.append(node)
+            continue
+        j = node - nb
+        op, n, k = int(u.gate_op[j]), int(u.gate_in_count[j]), int(u.gate_k[j]) & 0xFF
+        ins = [int(x) for x in u.gate_inputs(j)]
+        cond = affected(node)
+        if op == OR:
+            x = unif()
+            c = 0
+            if not cond:
+                while c + 1 < n and x >= tab[j][c]:
+                    c += 1
+            else:
+                tot = 0.0
+                for i in ins:
+                    tot += sz(i)
+                cum = 0.0
+                while c + 1 < n:
+                    cum += sz(ins[c])
+                    if x * tot < cum:
+                        break
+                    c += 1
+            stack.append(ins[c])
+        elif op == ATLEAST:
+            if cond:
+                v = [sz(i) for i in ins]
+                E = [[0.0] * (k + 1) for _ in range(n + 1)]
+                E[n][0] = 1.0
+                for c in range(n - 1, -1, -1):
+                    for r in range(k + 1):
+                        e = E[c + 1][r]
+                        if r > 0:
+                            e += v[c] * E[c + 1][r - 1]
+                        E[c][r] = e
+            else:
+                v, E = [S0[i] for i in ins], tab[j]
+            r = k
+            for c in range(n):
+                if r == 0:
+                    break
+                take = n - c == r
+                if not take:
+                    take = unif() * E[c][r] < v[c] * E[c + 1][r - 1]
+                if take:
+                    stack.append(ins[c])
+                    r -= 1
+        else:
+            stack.extend(ins)
+    return z, forced
+
+
+def _dag_cut_trees(n=3, n_be=36, n_gates=16, share=0.3, seeds=range(60), n_layers=4):
+    out = []
+    for seed in seeds:
+        try:
+            g = synth.generate(synth.TreeSpec(n_be=n_be, n_gates=n_gates, mix={AND: 0.4, OR: 0.3, ATLEAST: 0.3},
+                                              p_range=(0.01, 0.2), seed=seed, atleast_n=(3, 4), n_layers=n_layers,
+                                              share_be_frac=share))
+        except ValueError:
+            continue
+        fan = np.bincount(g.inputs, minlength=g.n_nodes)
+        if np.all(fan[g.n_be:] <= 1) and np.any(fan[: g.n_be] > 1):
+            out.append(g)
+        if len(out) == n:
+            return out
+    raise AssertionError("no trees with shared events generated")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w_main,w_cut,zscale,n_be", [(0, 256, 12.0, 36), (300, 300, 12.0, 36), (0, 48, 1e6, 110)])
+def test_cut_set_component_with_shared_events_matches_cpu(oracle_mod, gpu, w_main, w_cut, zscale, n_be):
+    """Trees whose shared nodes are basic events: the words after forcing,
+    the hits, sum w, sum w^2 and CE numerators equal a CPU restatement of
+    the component (shared events drawn from their own proposal, the cut set
+    on the conditioned tree).  zscale 1e6 puts many shared events at 0.5, so
+    that samples exceed the pruning list and take the unpruned path."""
+    from mcscram_b200.importance import BatchedImportanceSampler
+    trees = _dag_cut_trees() if n_be < 100 else _dag_cut_trees(n=2, n_be=n_be, n_gates=n_be // 2, share=0.4, n_layers=5)
+    it = 5
+    with BatchedImportanceSampler(trees, chunk_words=256) as s:
+        u, bb, roots = s.union, s.be_begin, s.roots
+        p = u.quantised_probabilities()
+        shared = np.bincount(u.inputs, minlength=u.n_nodes)[: u.n_be] > 1
+        q = probability_threshold(np.minimum(p * 6.0, 0.5))
+        qz = probability_threshold(np.where(shared, np.minimum(p * zscale, 0.5), p))
+        W = w_main + w_cut
+        r = s.run(q, iteration=it, word_count=W, ce=True, words_cutset=w_cut, q_cutset=qz)
+    parts = []
+    if w_main:
+        parts.append(oracle_mod.eval_words(u.with_thresholds(q), it, 0, w_main)[: u.n_be])
+    nom = oracle_mod.eval_words(u, it, w_main, w_cut)[: u.n_be].copy()
+    nom[shared] = 0  # the forcing kernel draws the shared events itself
+    v0 = u.with_thresholds(np.where(shared, 0, u.be_threshold).astype(np.uint64))
+    S0, tab = _cut_tables(v0)
+    occ_range, occ_of = _occurrences(u, roots, shared)
+    seed = _mix64(((it << 32) ^ 0x5bd1e995) & M64)
+    for k, root in enumerate(roots):
+        zlist = [(e, occ_of.get(e, [])) for e in range(int(bb[k]), int(bb[k + 1])) if shared[e]]
+        b0 = _mix64(seed ^ (k << 32))
+        for w in range(w_cut):
+            b1 = _mix64(b0 ^ (w_main + w))
+            for b in range(64):
+                z, forced = _descend_shared(u, S0, tab, shared, occ_range, zlist, qz, int(root), _mix64(b1 ^ b))
+                for e in forced + [e for e, on in z.items() if on]:
+                    nom[e, w] |= np.uint64(1) << np.uint64(b)
+    parts.append(nom)
+    be = np.concatenate(parts, axis=1)
+    bits = _gate_words(u, be)
+    ql = q.astype(np.float64) / TWO32
+    l1 = np.log1p(-p) - np.log1p(-ql)
+    a = np.log(p) - np.log(ql) - l1
+    rz = qz.astype(np.float64) / TWO32
+    lz1 = np.where(shared, np.log1p(-p) - np.log1p(-rz), 0.0)
+    az = np.where(shared, np.log(p) - np.log(rz) - lz1, 0.0)
+    ce = np.zeros(u.n_be)
+    n_long = 0
+    for k, root in enumerate(roots):
+        sl = slice(int(bb[k]), int(bb[k + 1]))
+        top = bits[int(root)]
+        lw_main = l1[sl].sum() + np.einsum("i,iwb->wb", a[sl], bits[sl].astype(np.float64))
+        lw_z = lz1[sl].sum() + np.einsum("i,iwb->wb", az[sl], bits[sl].astype(np.float64))
+        wgt = np.zeros((W, 64))
+        hits = 0
+        for w in range(W):
+            for b in range(64):
+                if not top[w, b]:
+                    continue
+                x = bits[:, w, b]
+                leaf = lambda e: (1.0 if x[e] else 0.0) if shared[e] else S0[e]
+                s_z = _eval(u, int(root), leaf, lambda g: True, lambda g: S0[g])
+                n_cut = _count(u, x, int(root))
+                lw_cut = lw_z[w, b] + np.log(s_z) - np.log(n_cut)
+                if w_main:
+                    lw = -np.logaddexp(np.log(w_main / W) - lw_main[w, b], np.log(w_cut / W) - lw_cut)
+                else:
+                    lw = lw_cut
+                wgt[w, b] = np.exp(lw)
+                hits += 1
+                n_long += int(sum(len(occ_of.get(e, [])) for e in range(sl.start, sl.stop) if x[e] and shared[e])
+                              > Z_OCC)
+        assert r["hits"][k] == hits
+        assert r["sum_w"][k] == pytest.approx(wgt.sum(), rel=1e-10)
+        assert r["sum_w2"][k] == pytest.approx((wgt ** 2).sum(), rel=1e-10)
+        ce[sl] = np.einsum("wb,iwb->i", wgt, bits[sl].astype(np.float64))
+    np.testing.assert_allclose(r["ce_num"], ce, rtol=1e-10, atol=1e-300)
+    if zscale > 1e3:
+        assert n_long > 0  # the unpruned path ran

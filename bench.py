@@ -57,12 +57,14 @@ def parse_args():
                     help="plain workload's tree (config1: the small 200-event tree, for profiling captures)")
     ap.add_argument("--chunk-words", type=int, default=0, help="staged/layered chunk words (0 = engine default)")
     ap.add_argument("--sampler-blocks", type=int, default=0, help="staged: sampler blocks per SM (0 = default)")
-    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis", "converge", "eta"],
+    ap.add_argument("--mlp-rows", type=int, default=1_400_000, help="rows of the mlp workload")
+    ap.add_argument("--workload", default="plain", choices=["plain", "ua", "is", "bis", "converge", "eta", "mlp"],
                     help="plain: the 5,000-event tree (headline); ua: batched uncertainty analysis; "
                          "is: GPU time to 5%% relative error on the 1e-8 tree, learned IS vs plain; "
                          "bis: the same for 1,024 rare-event trees at once with one shared network; "
                          "converge: ComputeTallies to a relative error, waiting vs pipelined convergence loop; "
-                         "eta: combined event-tree pass, every sequence of a 2^n-sequence tree tallied")
+                         "eta: combined event-tree pass, every sequence of a 2^n-sequence tree tallied; "
+                         "mlp: proposal-network training steps at the batched set's row count")
     ap.add_argument("--eta-functional", type=int, default=8, help="functional events of the eta workload's tree")
     ap.add_argument("--converge-rel-err", type=float, default=1e-3)
     ap.add_argument("--converge-words", type=int, default=1 << 14, help="words per pass of the convergence loop")
@@ -75,9 +77,14 @@ def parse_args():
                     help="single: CE rounds + estimate on the one-tree sampler; batched: the batched pipeline "
                          "(cut-set defensive component, one CE round) on a batch of this one tree")
     ap.add_argument("--is-round-words", type=int, default=1 << 20, help="words per CE round (2^26 samples)")
+    ap.add_argument("--is-tree", default="read-once", choices=["read-once", "dag"],
+                    help="the 1e-8 tree: read-once, or with 20%% of its basic events read by two gates")
     ap.add_argument("--is-batch-words", type=int, default=1 << 20)
     ap.add_argument("--plain-words", type=int, default=1 << 23, help="words of the plain-MC rate measurement")
     ap.add_argument("--bis-trees", type=int, default=1024)
+    ap.add_argument("--bis-set", default="shared", choices=["shared", "read-once"],
+                    help="rare-event trees with 20%% of their basic events read by two gates (exact values from "
+                         "tests/golden/config5_dag_exact.json), or read-once trees (exact by recursion)")
     ap.add_argument("--bis-ce-rounds", type=int, default=0, help="CE rounds (0 = the driver's default)")
     ap.add_argument("--bis-ce-words", type=int, default=1 << 13, help="words per tree per CE round")
     ap.add_argument("--bis-est-words", type=int, default=1 << 12, help="words per tree of the first estimate round")
@@ -292,7 +299,7 @@ def run_ua(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
-def measure_is(args, local: int) -> dict:
+def measure_is(args, local: int, tree: str = "read-once") -> dict:
     """GPU time to a 5% relative error (95% confidence) on the 2,000-event tree
     whose exact top-event probability is ~1e-8: the learned-IS pipeline
     (cross-entropy rounds with on-GPU MLP training, then IS batches until the
@@ -305,7 +312,8 @@ def measure_is(args, local: int) -> dict:
     from mcscram_b200.importance import ImportanceSampler, cross_entropy, estimate
 
     torch.cuda.set_device(local)
-    g = synth.config4().with_tallies([])
+    dag = tree == "dag"
+    g = (synth.config4_dag() if dag else synth.config4()).with_tallies([])
     g = g.with_tallies([g.root])
     # plain sampler rate on this tree (staged pipeline, inputs resident)
     stream = torch.cuda.Stream()
@@ -351,17 +359,21 @@ def measure_is(args, local: int) -> dict:
     p_hat = res["estimate"]
     n_req = 1.959963984540054 ** 2 * (1 - p_hat) / (p_hat * 0.05 ** 2) if p_hat > 0 else float("inf")
     plain_s = n_req / plain_rate
-    exact = float(synth.read_once_probability(g)[g.root])
+    if dag:  # committed BDD value (tests/golden/make_dag_exact.py)
+        exact = json.loads((ROOT / "tests" / "golden" / "config5_dag_exact.json").read_text())["config4_dag"]
+    else:
+        exact = float(synth.read_once_probability(g)[g.root])
     se = p_hat * res["rel_err95"] / 1.959963984540054
     return {
         "metric": "GPU time to 5% rel err at P_top~1e-8", "value": is_wall, "unit": "s", "n_gpus": 1,
         "higher_is_better": False, "vs_baseline": None, "dtype": "u64 sampling, fp64 weights, bf16/fp32 MLP",
         "data": "synthetic", "steps": 1, "warmup": args.warmup,
-        "config": {"workload": "2,000-event / 1,200-gate rare-event tree (seed 49), learned IS (CE rounds "
-                               f"{args.is_rounds} x {args.is_round_words * 64} samples) vs plain MC"
-                               if args.is_pipeline == "single" else
-                               "2,000-event / 1,200-gate rare-event tree (seed 49), batched learned IS pipeline on "
-                               "this one tree (cut-set defensive component, one CE round) vs plain MC"},
+        "config": {"workload": (("2,000-event / 1,200-gate rare-event tree with 400 basic events read by two "
+                                 "gates (seed 4)") if dag else "2,000-event / 1,200-gate rare-event tree (seed 49)") +
+                               (f", learned IS (CE rounds {args.is_rounds} x {args.is_round_words * 64} samples) vs "
+                                "plain MC" if args.is_pipeline == "single" else
+                                ", batched learned IS pipeline on this one tree (cut-set defensive component, one "
+                                "CE round) vs plain MC")},
         "is": {"estimate": p_hat, "rel_err95": res["rel_err95"], "samples": res["samples"], "hits": res["hits"],
                "ess": res["ess"], "fallback": res["fallback"], "wall_s": is_wall,
                "gpu_s": (hist.gpu_ms + res["gpu_ms"]) * 1e-3, "ce_rounds": hist.rounds,
@@ -377,7 +389,7 @@ def run_is(args, rank: int, world: int, local: int) -> int:
     2,000-event rare-event tree against plain MC (measure_is)."""
     if rank != 0:
         return 0
-    print(json.dumps(measure_is(args, local)), flush=True)
+    print(json.dumps(measure_is(args, local, args.is_tree)), flush=True)
     return 0
 
 
@@ -407,8 +419,13 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     workers = ProcessPoolExecutor(max_workers=n_workers, mp_context=mp.get_context("spawn"))
     t_gen = time.perf_counter()
     mine_idx = parallel.shard_items(args.bis_trees, world, rank)
-    trees = synth.config5_instances(mine_idx, workers=workers)
+    dag = args.bis_set == "shared"
+    trees = synth.config5_instances(mine_idx, workers=workers, shared=dag)
     t_gen = time.perf_counter() - t_gen
+    if dag:  # exact values of the shared-event set: committed BDD results (null: BDD over its node limit)
+        fx = json.loads((ROOT / "tests" / "golden" / "config5_dag_exact.json").read_text())["config5_dag"]
+        for k, i in enumerate(mine_idx):
+            trees[k].meta["exact_p_top"] = fx[i] if i < len(fx) and fx[i] is not None else float("nan")
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -461,35 +478,42 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     clk = clocks.stop()
     gpu_s = sum(res.gpu_ms.values()) * 1e-3
     z = 1.959963984540054
-    n_req = z * z * (1 - exact) / (exact * 0.05 ** 2)  # plain samples per tree to 5% at 95%
+    p_ref = np.where(np.isfinite(exact), exact, res.estimate)
+    n_req = z * z * (1 - p_ref) / (p_ref * 0.05 ** 2)  # plain samples per tree to 5% at 95%
     nb = np.array([g.n_be for g in trees], dtype=np.float64)
     plain_s = float(np.sum(n_req / 64 * nb / be_word_s))
+    checked = np.isfinite(exact)
+    exact = np.where(checked, exact, res.estimate)
     err = np.abs(res.estimate - exact) / exact
     se = res.estimate * res.rel_err95 / z
-    within3 = np.abs(res.estimate - exact) <= 3 * se
+    within3 = (np.abs(res.estimate - exact) <= 3 * se) & checked
+    within5 = (np.abs(res.estimate - exact) <= 5 * se) & checked
     with np.errstate(divide="ignore", invalid="ignore"):
         zs = np.where(se > 0, (res.estimate - exact) / se, np.inf)
     worst = [{"tree": int(mine_idx[k]), "events": trees[k].n_be, "p_exact": float(exact[k]),
               "est_over_exact": float(res.estimate[k] / exact[k]), "rel_err95": float(res.rel_err95[k]),
               "z": float(zs[k]), "converged": bool(res.converged[k]), "fallback": bool(res.fallback[k])}
-             for k in np.argsort(-np.abs(np.nan_to_num(zs, nan=np.inf)))[:12] if not within3[k]]
+             for k in np.argsort(-np.abs(np.nan_to_num(zs, nan=np.inf)))[:12] if checked[k] and not within3[k]]
     wall_max, gpu_max = wall, gpu_s
     if world > 1:
         wall_max, gpu_max = parallel.allreduce_max([wall, gpu_s])
         counts = parallel.allreduce_tallies(np.array([res.converged.sum(), res.fallback.sum(), within3.sum(),
-                                                      len(trees)], dtype=np.uint64))
+                                                      len(trees), checked.sum(), within5.sum()], dtype=np.uint64))
         plain_s = parallel.allreduce_max([plain_s])[0]
     else:
-        counts = [int(res.converged.sum()), int(res.fallback.sum()), int(within3.sum()), len(trees)]
+        counts = [int(res.converged.sum()), int(res.fallback.sum()), int(within3.sum()), len(trees),
+                  int(checked.sum()), int(within5.sum())]
     if rank == 0:
         print(json.dumps({
             "metric": "GPU time to 5% rel err, batched rare-event trees", "value": wall_max, "unit": "s",
             "n_gpus": world, "steps": 1, "warmup": args.warmup, "higher_is_better": False, "scaling": "strong",
             "vs_baseline": None, "dtype": "u64 sampling, fp64 weights, bf16/fp32 MLP", "data": "synthetic",
-            "config": {"workload": f"batched learned IS: {args.bis_trees} read-once rare-event trees (events "
-                                   "log-uniform [50, 10000], AND-/ATLEAST-heavy, exact P_top log-uniform "
+            "config": {"workload": f"batched learned IS: {args.bis_trees} rare-event trees "
+                                   f"({'20% of basic events read by two gates' if dag else 'read-once'}; events "
+                                   "log-uniform [50, 10000], AND-/ATLEAST-heavy, target P_top log-uniform "
                                    "[1e-10, 1e-5]), one shared 16-64-64-1 proposal network, until 5% rel err "
                                    "(95%) per tree or plain fallback",
+                       "tree_set": args.bis_set,
                        "ce_rounds": sum(1 for r in res.rounds if r["phase"] == "ce"),
                        "ce_samples_per_tree": args.bis_ce_words * 64,
                        "defensive": args.bis_defensive, "defensive_share": args.bis_defensive_share,
@@ -500,6 +524,7 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
             "is": {"wall_s": wall_max, "gpu_s": gpu_max, "gpu_ms_by_phase": res.gpu_ms,
                    "wall_s_by_phase": res.seconds, "trees": int(counts[3]), "converged": int(counts[0]),
                    "fallback": int(counts[1]), "within_3_sigma_of_exact": int(counts[2]),
+                   "checked_against_exact": int(counts[4]), "within_5_sigma_of_exact": int(counts[5]),
                    "median_abs_rel_err_vs_exact": float(np.median(err)), "max_abs_rel_err_vs_exact": float(err.max()),
                    "max_rel_err95": float(res.rel_err95.max()), "samples_total": int(res.samples.sum()),
                    "rounds": len(res.rounds), "converged_outside_3_sigma": int((res.converged & ~within3).sum()),
@@ -514,6 +539,58 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def run_mlp(args, rank: int, world: int, local: int) -> int:
+    """Training of the proposal network at the batched rare-event set's size:
+    `--mlp-rows` rows (1.4 M, the 1,024 trees' events) of 16 features,
+    `--steps` Adam steps timed with CUDA events after `--warmup` steps.  The
+    dense products are 2 x (16x64 + 64x64 + 64) multiply-adds per row
+    forward, twice that backward (activation and weight gradients): 3 x that
+    per row and step in all."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    from mcscram_b200.importance import ProposalMLP
+
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(1)
+    n = args.mlp_rows
+    feats = rng.normal(size=(n, 16)).astype(np.float32)
+    tgt = rng.uniform(0.0, 0.5, n).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    mlp = ProposalMLP(device=local)
+    mlp.train(feats, tgt, w, steps=max(args.warmup, 1), lr=1e-3)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    loss = mlp.train(feats, tgt, w, steps=args.steps, lr=1e-3)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    ms = mlp.last_train_ms / args.steps if getattr(mlp, "last_train_ms", None) else wall * 1e3 / args.steps
+    mlp.close()
+    flops = 3 * 2 * (16 * 64 + 64 * 64 + 64) * n  # per Adam step
+    peak = None
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    if peaks_file.exists():
+        peak = json.loads(peaks_file.read_text()).get("bf16_tflops")
+    achieved = flops / (ms * 1e-3) / 1e12
+    print(json.dumps({
+        "metric": "proposal-network training step", "value": ms, "unit": "ms/step", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "vs_baseline": None,
+        "dtype": "bf16 operands, fp32 accumulation", "data": "synthetic",
+        "config": {"workload": f"16-64-64-1 network, weighted cross-entropy, {n} rows, Adam",
+                   "rows": n, "timing": "CUDA events around the training steps (gradient, reduction, Adam, "
+                                        "weight packing) with rows resident"},
+        "loss": loss, "wall_s": wall,
+        "roofline": {"bound": "tensor", "kernel": "k_mlp_grad", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 GEMM, burst)",
+                     "work_unit": "3 x 2 x 5,184 flops per row and step"},
+        "clocks": clk}), flush=True)
     return 0
 
 
@@ -693,6 +770,8 @@ def main() -> int:
         return run_bis(args, rank, world, local)
     if args.workload == "converge":
         return run_converge(args, rank, world, local)
+    if args.workload == "mlp":
+        return run_mlp(args, rank, world, local)
     if args.workload == "eta":
         return run_eta(args, rank, world, local)
 
@@ -859,12 +938,13 @@ def main() -> int:
         # the metric's second half: learned-IS time to 5 % at P_top ~ 1e-8,
         # after the timed region (its own clocks inside)
         torch.cuda.set_stream(torch.cuda.default_stream())
-        m = measure_is(args, local)
-        line["is"] = {"workload": m["config"]["workload"], "metric": m["metric"], "wall_s": m["value"],
-                      "unit": "s", **{k: v for k, v in m["is"].items() if k != "ce_rounds"},
-                      "plain_samples_per_s": m["plain"]["samples_per_s"],
-                      "plain_seconds_derived": m["plain"]["seconds"], "speedup_vs_plain": m["speedup"],
-                      "clocks": m["clocks"]}
+        for key, tree in (("is", "read-once"), ("is_dag", "dag")):
+            m = measure_is(args, local, tree)
+            line[key] = {"workload": m["config"]["workload"], "metric": m["metric"], "wall_s": m["value"],
+                         "unit": "s", **{k: v for k, v in m["is"].items() if k != "ce_rounds"},
+                         "plain_samples_per_s": m["plain"]["samples_per_s"],
+                         "plain_seconds_derived": m["plain"]["seconds"], "speedup_vs_plain": m["speedup"],
+                         "clocks": m["clocks"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -105,7 +105,9 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_threshold, uint32
 
 /* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
  * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32
- * accumulation), FP32 master weights and Adam state.  Parameter layout
+ * accumulation), FP32 master weights and Adam state.  The gradient runs in
+ * persistent CTAs whose partial gradients are summed in a fixed order, so
+ * the same rows give the same gradient bit for bit.  Parameter layout
  * (5,313 floats): W1[16][64], b1[64], W2[64][64], b2[64], W3[64], b3. */
 typedef struct mcg_mlp mcg_mlp;
 #define MCG_MLP_IN 16
@@ -127,6 +129,9 @@ mcg_status mcg_mlp_grad(mcg_mlp *m, const float *features, const float *targets,
 /* `steps` Adam steps (lr, beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
 mcg_status mcg_mlp_train(mcg_mlp *m, const float *features, const float *targets, const float *weights, uint32_t n,
                          uint32_t steps, float lr, float *loss_out);
+/* Device time of the steps of the last mcg_mlp_train call (CUDA events on
+ * the network's stream, row upload excluded). */
+mcg_status mcg_mlp_train_time(mcg_mlp *m, double *ms);
 
 #ifdef __cplusplus
 }

@@ -2,13 +2,17 @@
 //
 // 16 features -> 64 -> 64 -> 1, ReLU, sigmoid.  Dense products run on the
 // tensor cores with mma.sync.m16n8k16 (BF16 operands, FP32 accumulation);
-// the rank-1 and elementwise steps on CUDA cores.  One CTA of 4 warps owns
-// 64 rows: warp w the rows 16w .. 16w+15 for the row-wise products, and an
-// output-tile slice of the weight gradients (a reduction over the CTA's 64
-// rows); CTAs add their gradients into FP32 buffers atomically.
+// the rank-1 and elementwise steps on CUDA cores.  A CTA of 4 warps works on
+// 64 rows at a time: warp w the rows 16w .. 16w+15 for the row-wise products,
+// and an output-tile slice of the weight gradients (a reduction over the
+// rows).  The gradient kernel is persistent: each CTA walks 64-row tiles
+// with its gradient slices held in the MMA accumulators and registers,
+// writes one partial gradient at the end, and a second kernel sums the
+// partials in CTA order (deterministic, no atomics on global memory).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -163,6 +167,31 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
     z_out[1] = c[2] + b3;  // row m0 + g + 8
 }
 
+__device__ void load_weights(Smem &s, const bf16 *__restrict__ pack, const float *__restrict__ params) {
+    for (int i = threadIdx.x; i < kHid * kIn; i += kThreads) s.w1t[i] = pack[kPackW1t + i];
+    for (int i = threadIdx.x; i < kHid * kHid; i += kThreads) {
+        s.w2t[i] = pack[kPackW2t + i];
+        s.w2[i] = pack[kPackW2 + i];
+    }
+    for (int i = threadIdx.x; i < 8 * kHid; i += kThreads) s.w3t[i] = pack[kPackW3t + i];
+    for (int i = threadIdx.x; i < kHid; i += kThreads) {
+        s.b1[i] = params[kOffB1 + i];
+        s.b2[i] = params[kOffB2 + i];
+        s.w3[i] = params[kOffW3 + i];
+    }
+}
+
+// The tile's rows as BF16 (row-major and feature-major); rows past n are 0.
+__device__ void load_rows(Smem &s, const float *__restrict__ feat, uint32_t n, uint32_t row0) {
+    for (int i = threadIdx.x; i < kRows * kIn; i += kThreads) {
+        const int r = i / kIn, f = i % kIn;
+        const float v = (row0 + r < n) ? feat[(uint64_t)(row0 + r) * kIn + f] : 0.f;
+        const bf16 b = __float2bfloat16(v);
+        s.x[r * kIn + f] = b;
+        s.xt[f * kRows + r] = b;
+    }
+}
+
 __device__ void load_tile(Smem &s, const bf16 *__restrict__ pack, const float *__restrict__ params,
                           const float *__restrict__ feat, uint32_t n, uint32_t row0) {
     for (int i = threadIdx.x; i < kHid * kIn; i += kThreads) s.w1t[i] = pack[kPackW1t + i];
@@ -205,85 +234,89 @@ __global__ void __launch_bounds__(kThreads) k_mlp_forward(const bf16 *__restrict
     }
 }
 
-// Weighted BCE gradient; grad and loss are accumulated (zero them first).
+// Weighted BCE gradient of the rows [0, n): persistent CTAs, CTA b taking
+// tiles b, b + gridDim.x, ...; its gradient (kParams floats, then the loss)
+// goes to partial[b * (kParams + 1) ..] (every entry written once).
 __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ pack, const float *__restrict__ params,
                                                        const float *__restrict__ feat, const float *__restrict__ tgt,
                                                        const float *__restrict__ wts, float inv_wsum, uint32_t n,
-                                                       float *__restrict__ grad, float *__restrict__ loss) {
+                                                       float *__restrict__ partial) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem &s = *reinterpret_cast<Smem *>(smem_raw);
-    const uint32_t row0 = blockIdx.x * kRows;
-    load_tile(s, pack, params, feat, n, row0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    float z[2];
-    forward_rows(s, warp, lane, params[kOffB3], z);
-    // dL/dz = w (q - t) / sum w for the CTA's rows
-    if (t == 0) {
+    const int m0 = warp * 16;
+    load_weights(s, pack, params);
+    if (threadIdx.x == 0) s.loss = 0.f;
+    const float b3 = params[kOffB3];
+    // this CTA's gradient: dW2 rows m0 .. m0 + 15 and dW1 n-tiles 2w, 2w + 1 in
+    // MMA accumulators; W3, b2, b1 (threads c < 64) and b3 (thread 64) in registers
+    float acc2[kHid / 8][4], acc1[2][4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int rl = warp * 16 + g + 8 * h;
-            const uint32_t r = row0 + rl;
-            float d = 0.f;
-            if (r < n) {
-                const float qv = 1.f / (1.f + __expf(-z[h]));
-                const float tv = tgt[r];
-                const float wv = (wts ? wts[r] : 1.f) * inv_wsum;
-                d = wv * (qv - tv);
-                const float qc = fminf(fmaxf(qv, 1e-7f), 1.f - 1e-7f);
-                atomicAdd(&s.loss, -wv * (tv * __logf(qc) + (1.f - tv) * __logf(1.f - qc)));
+    for (int nt = 0; nt < kHid / 8; ++nt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc2[nt][j] = 0.f;
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc1[q][j] = 0.f;
+    float gw3 = 0.f, gb2 = 0.f, gb1 = 0.f, gb3 = 0.f;
+    const uint32_t tiles = (n + kRows - 1) / kRows;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t row0 = tile * kRows;
+        load_rows(s, feat, n, row0);
+        __syncthreads();
+        float z[2];
+        forward_rows(s, warp, lane, b3, z);
+        // dL/dz = w (q - t) / sum w for the tile's rows
+        if (t == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rl = m0 + g + 8 * h;
+                const uint32_t r = row0 + rl;
+                float d = 0.f;
+                if (r < n) {
+                    const float qv = 1.f / (1.f + __expf(-z[h]));
+                    const float tv = tgt[r];
+                    const float wv = (wts ? wts[r] : 1.f) * inv_wsum;
+                    d = wv * (qv - tv);
+                    const float qc = fminf(fmaxf(qv, 1e-7f), 1.f - 1e-7f);
+                    atomicAdd(&s.loss, -wv * (tv * __logf(qc) + (1.f - tv) * __logf(1.f - qc)));
+                }
+                s.dz[rl] = d;
             }
-            s.dz[rl] = d;
         }
-    }
-    __syncthreads();
-    // dH2 = dz W3^T masked; bias and W3 gradients
-    for (int i = threadIdx.x; i < kRows * kHid; i += kThreads) {
-        const int r = i / kHid, c = i % kHid;
-        const float v = s.m2[i] ? s.dz[r] * s.w3[c] : 0.f;
-        const bf16 b = __float2bfloat16(v);
-        s.dh2[i] = b;
-        s.dh2t[c * kRows + r] = b;
-    }
-    __syncthreads();
-    if (threadIdx.x < kHid) {
-        const int c = threadIdx.x;
-        float gw3 = 0.f, gb2 = 0.f;
-        for (int r = 0; r < kRows; ++r) {
-            gw3 += __bfloat162float(s.h2[r * kHid + c]) * s.dz[r];
-            gb2 += s.m2[r * kHid + c] ? s.dz[r] * s.w3[c] : 0.f;
+        __syncthreads();
+        // dH2 = dz W3^T masked
+        for (int i = threadIdx.x; i < kRows * kHid; i += kThreads) {
+            const int r = i / kHid, c = i % kHid;
+            const float v = s.m2[i] ? s.dz[r] * s.w3[c] : 0.f;
+            const bf16 b = __float2bfloat16(v);
+            s.dh2[i] = b;
+            s.dh2t[c * kRows + r] = b;
         }
-        atomicAdd(&grad[kOffW3 + c], gw3);
-        atomicAdd(&grad[kOffB2 + c], gb2);
-    } else if (threadIdx.x == kHid) {
-        float gb3 = 0.f;
-        for (int r = 0; r < kRows; ++r) gb3 += s.dz[r];
-        atomicAdd(&grad[kOffB3], gb3);
-        atomicAdd(loss, s.loss);
-    }
-    // dW2[in][out] = H1^T dH2: M = 64 (in), N = 64 (out), K = 64 rows; warp w: in rows 16w..
-    {
-        const int m0 = warp * 16;
+        __syncthreads();
+        if (threadIdx.x < kHid) {
+            const int c = threadIdx.x;
+            for (int r = 0; r < kRows; ++r) {
+                gw3 += __bfloat162float(s.h2[r * kHid + c]) * s.dz[r];
+                gb2 += s.m2[r * kHid + c] ? s.dz[r] * s.w3[c] : 0.f;
+            }
+        } else if (threadIdx.x == kHid) {
+            for (int r = 0; r < kRows; ++r) gb3 += s.dz[r];
+        }
+        // dW2[in][out] += H1^T dH2: M = 64 (in), N = 64 (out), K = 64 rows; warp w: in rows 16w..
 #pragma unroll
         for (int nt = 0; nt < kHid / 8; ++nt) {
-            float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int kt = 0; kt < kRows / 16; ++kt) {
                 uint32_t a[4], b[2];
                 frag_a(a, s.h1t, kRows, m0, kt * 16, lane);
                 frag_b(b, s.dh2t, kRows, nt * 8, kt * 16, lane);
-                mma16816(c, a, b);
+                mma16816(acc2[nt], a, b);
             }
-            const int col = nt * 8 + 2 * t;
-            atomicAdd(&grad[kOffW2 + (m0 + g) * kHid + col], c[0]);
-            atomicAdd(&grad[kOffW2 + (m0 + g) * kHid + col + 1], c[1]);
-            atomicAdd(&grad[kOffW2 + (m0 + g + 8) * kHid + col], c[2]);
-            atomicAdd(&grad[kOffW2 + (m0 + g + 8) * kHid + col + 1], c[3]);
         }
-    }
-    // dH1 = dH2 W2^T masked: [16 rows x 64 out] x [64 out x 64 in]; B = W2 (in-major) as Bt[in][out]
-    {
-        const int m0 = warp * 16;
+        // dH1 = dH2 W2^T masked: [16 rows x 64 out] x [64 out x 64 in]; B = W2 (in-major) as Bt[in][out]
 #pragma unroll
         for (int nt = 0; nt < kHid / 8; ++nt) {
             float c[4] = {0.f, 0.f, 0.f, 0.f};
@@ -302,32 +335,61 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ 
                 s.dh1t[cc * kRows + r] = __float2bfloat16(v);
             }
         }
-    }
-    __syncthreads();
-    // db1 and dW1[f][h] = X^T dH1: M = 16 (features), N = 64, K = 64 rows; warp w: n-tiles 2w, 2w+1
-    if (threadIdx.x < kHid) {
-        const int c = threadIdx.x;
-        float gb1 = 0.f;
-        for (int r = 0; r < kRows; ++r) gb1 += __bfloat162float(s.dh1t[c * kRows + r]);
-        atomicAdd(&grad[kOffB1 + c], gb1);
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const int nt = warp * 2 + j;
-        float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kt = 0; kt < kRows / 16; ++kt) {
-            uint32_t a[4], b[2];
-            frag_a(a, s.xt, kRows, 0, kt * 16, lane);
-            frag_b(b, s.dh1t, kRows, nt * 8, kt * 16, lane);
-            mma16816(c, a, b);
+        __syncthreads();
+        // db1 and dW1[f][h] += X^T dH1: M = 16 (features), N = 64, K = 64 rows; warp w: n-tiles 2w, 2w+1
+        if (threadIdx.x < kHid) {
+            const int c = threadIdx.x;
+            for (int r = 0; r < kRows; ++r) gb1 += __bfloat162float(s.dh1t[c * kRows + r]);
         }
-        const int col = nt * 8 + 2 * t;
-        atomicAdd(&grad[kOffW1 + g * kHid + col], c[0]);
-        atomicAdd(&grad[kOffW1 + g * kHid + col + 1], c[1]);
-        atomicAdd(&grad[kOffW1 + (g + 8) * kHid + col], c[2]);
-        atomicAdd(&grad[kOffW1 + (g + 8) * kHid + col + 1], c[3]);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int nt = warp * 2 + q;
+#pragma unroll
+            for (int kt = 0; kt < kRows / 16; ++kt) {
+                uint32_t a[4], b[2];
+                frag_a(a, s.xt, kRows, 0, kt * 16, lane);
+                frag_b(b, s.dh1t, kRows, nt * 8, kt * 16, lane);
+                mma16816(acc1[q], a, b);
+            }
+        }
+        __syncthreads();  // the next tile overwrites the rows and activations
     }
+    float *out = partial + (uint64_t)blockIdx.x * (kParams + 1);
+#pragma unroll
+    for (int nt = 0; nt < kHid / 8; ++nt) {
+        const int col = nt * 8 + 2 * t;
+        out[kOffW2 + (m0 + g) * kHid + col] = acc2[nt][0];
+        out[kOffW2 + (m0 + g) * kHid + col + 1] = acc2[nt][1];
+        out[kOffW2 + (m0 + g + 8) * kHid + col] = acc2[nt][2];
+        out[kOffW2 + (m0 + g + 8) * kHid + col + 1] = acc2[nt][3];
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int col = (warp * 2 + q) * 8 + 2 * t;
+        out[kOffW1 + g * kHid + col] = acc1[q][0];
+        out[kOffW1 + g * kHid + col + 1] = acc1[q][1];
+        out[kOffW1 + (g + 8) * kHid + col] = acc1[q][2];
+        out[kOffW1 + (g + 8) * kHid + col + 1] = acc1[q][3];
+    }
+    if (threadIdx.x < kHid) {
+        out[kOffW3 + threadIdx.x] = gw3;
+        out[kOffB2 + threadIdx.x] = gb2;
+        out[kOffB1 + threadIdx.x] = gb1;
+    } else if (threadIdx.x == kHid) {
+        out[kOffB3] = gb3;
+        out[kParams] = s.loss;
+    }
+}
+
+// grad[i] = sum over the CTAs of partial[b][i] in CTA order (i = kParams: the loss).
+__global__ void k_mlp_reduce(const float *__restrict__ partial, uint32_t blocks, float *__restrict__ grad,
+                             float *__restrict__ loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > kParams) return;
+    float v = 0.f;
+    for (uint32_t b = 0; b < blocks; ++b) v += partial[(uint64_t)b * (kParams + 1) + i];
+    if (i < kParams) grad[i] = v;
+    else *loss = v;
 }
 
 // FP32 master weights -> BF16 operand copies.
@@ -370,6 +432,10 @@ struct mcg_mlp {
     float *d_params = nullptr, *d_grad = nullptr, *d_m = nullptr, *d_v = nullptr, *d_loss = nullptr;
     bf16 *d_pack = nullptr;
     float *d_feat = nullptr, *d_tgt = nullptr, *d_w = nullptr, *d_q = nullptr;
+    float *d_partial = nullptr;  // [grad_ctas][kParams + 1] per-CTA gradients and losses
+    uint32_t grad_ctas = 0;      // persistent CTAs of the gradient kernel
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the steps of the last mcg_mlp_train
+    double train_ms = 0.0;
     uint32_t cap = 0;
     uint64_t adam_t = 0;
 };
@@ -398,14 +464,15 @@ mcg_status pack(mcg_mlp *m) {
     return MCG_OK;
 }
 
-// Uploads rows, zeroes the gradient, runs the gradient kernel.
+// The gradient of the uploaded rows into d_grad and d_loss: the persistent
+// gradient kernel, then the reduction of its partials.
 mcg_status grad_pass(mcg_mlp *m, uint32_t n, float inv_wsum, bool has_w) {
-    MCG_CUDA(cudaMemsetAsync(m->d_grad, 0, kParams * sizeof(float), m->stream));
-    MCG_CUDA(cudaMemsetAsync(m->d_loss, 0, sizeof(float), m->stream));
-    const uint32_t blocks = (n + kRows - 1) / kRows;
+    const uint32_t tiles = (n + kRows - 1) / kRows;
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(tiles, m->grad_ctas));
     k_mlp_grad<<<blocks, kThreads, sizeof(Smem), m->stream>>>(m->d_pack, m->d_params, m->d_feat, m->d_tgt,
-                                                             has_w ? m->d_w : nullptr, inv_wsum, n, m->d_grad,
-                                                             m->d_loss);
+                                                             has_w ? m->d_w : nullptr, inv_wsum, n, m->d_partial);
+    MCG_CUDA(cudaGetLastError());
+    k_mlp_reduce<<<(kParams + 1 + 255) / 256, 256, 0, m->stream>>>(m->d_partial, blocks, m->d_grad, m->d_loss);
     MCG_CUDA(cudaGetLastError());
     return MCG_OK;
 }
@@ -451,6 +518,13 @@ mcg_status mcg_mlp_create(int32_t device, uint64_t seed, mcg_mlp **out) {
     MCG_CUDA(cudaMalloc((void **)&m->d_pack, kPackSize * sizeof(bf16)));
     MCG_CUDA(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
     MCG_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
+    int sms = 0, per_sm = 0;
+    MCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    MCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_grad, kThreads, sizeof(Smem)));
+    m->grad_ctas = (uint32_t)std::max(1, sms * std::max(per_sm, 1));
+    MCG_CUDA(cudaMalloc((void **)&m->d_partial, (size_t)m->grad_ctas * (kParams + 1) * sizeof(float)));
+    MCG_CUDA(cudaEventCreate(&m->ev0));
+    MCG_CUDA(cudaEventCreate(&m->ev1));
     // He-style initialisation from a seeded host generator
     std::vector<float> p(kParams, 0.f);
     std::mt19937_64 rng(seed);
@@ -483,6 +557,9 @@ mcg_status mcg_mlp_destroy(mcg_mlp *m) {
     cudaFree(m->d_tgt);
     cudaFree(m->d_w);
     cudaFree(m->d_q);
+    cudaFree(m->d_partial);
+    if (m->ev0) cudaEventDestroy(m->ev0);
+    if (m->ev1) cudaEventDestroy(m->ev1);
     cudaStreamDestroy(m->stream);
     delete m;
     return MCG_OK;
@@ -555,6 +632,7 @@ mcg_status mcg_mlp_train(mcg_mlp *m, const float *features, const float *targets
     float inv = 0.f;
     mcg_status st = upload_rows(m, features, targets, weights, n, inv);
     if (st != MCG_OK) return st;
+    MCG_CUDA(cudaEventRecord(m->ev0, m->stream));
     for (uint32_t s = 0; s < steps; ++s) {
         st = grad_pass(m, n, inv, weights != nullptr);
         if (st != MCG_OK) return st;
@@ -566,10 +644,21 @@ mcg_status mcg_mlp_train(mcg_mlp *m, const float *features, const float *targets
         if (st != MCG_OK) return st;
     }
     MCG_CUDA(cudaGetLastError());
+    MCG_CUDA(cudaEventRecord(m->ev1, m->stream));
     float loss = 0.f;
     MCG_CUDA(cudaMemcpyAsync(&loss, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     MCG_CUDA(cudaStreamSynchronize(m->stream));
+    float ms = 0.f;
+    MCG_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+    m->train_ms = ms;
     if (loss_out) *loss_out = loss;
+    return MCG_OK;
+}
+
+mcg_status mcg_mlp_train_time(mcg_mlp *m, double *ms) {
+    mcg::clear_error();
+    if (!m || !ms) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    *ms = m->train_ms;
     return MCG_OK;
 }
 

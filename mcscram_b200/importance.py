@@ -59,6 +59,7 @@ _capi.register_signatures({
     "mcg_is_batch_run": (C.c_int, [_vp, _u64p, C.c_uint32, _u64p, _u64p, C.c_uint64, _u64p, C.c_uint32,
                                    C.c_uint64, C.c_uint64, _dp, _dp, _dp]),
     "mcg_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_vp)]),
+    "mcg_mlp_train_time": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "mcg_mlp_destroy": (C.c_int, [_vp]),
     "mcg_mlp_set_params": (C.c_int, [_vp, _fp]),
     "mcg_mlp_get_params": (C.c_int, [_vp, _fp]),
@@ -459,6 +460,9 @@ class ProposalMLP:
         _capi.check(self.lib.mcg_mlp_train(self.h, _p(feats, C.c_float), _p(targets, C.c_float),
                                            _p(w, C.c_float) if w is not None else None, feats.shape[0], steps, lr,
                                            C.byref(loss)))
+        ms = C.c_double()
+        _capi.check(self.lib.mcg_mlp_train_time(self.h, C.byref(ms)))
+        self.last_train_ms = float(ms.value)
         return float(loss.value)
 
 

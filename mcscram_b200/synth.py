@@ -540,6 +540,79 @@ def config5_instance(i: int, seed: int = 5) -> FlatGraph:
     raise RuntimeError(f"no feasible draw for instance {i}")
 
 
+def calibrate_rare_approx(g: FlatGraph, target: float, p_floor: float = 1e-9, p_cap: float = 0.5) -> FlatGraph:
+    """calibrate_rare for graphs with shared events: the same rescaling
+    p -> clip(p^gamma, p_floor, p_cap), bisected on the top probability of
+    the independence approximation (importance.approximate_importance), which
+    is not exact on a DAG; meta records the approximate value, the exact one
+    comes from elsewhere (an exact BDD)."""
+    from .importance import approximate_importance
+    base = np.clip(g.quantised_probabilities(), 1e-12, 1.0)
+
+    def top(gamma):
+        p = np.clip(base ** gamma, p_floor, p_cap)
+        thr = probability_threshold(p)
+        h = g.with_thresholds(thr)
+        return float(approximate_importance(h)[0][g.root]), thr
+
+    lo, hi = 0.05, 20.0
+    t_lo, _ = top(lo)
+    t_hi, _ = top(hi)
+    if not (t_hi <= target <= t_lo):
+        raise ValueError(f"target {target:g} outside the reachable range [{t_hi:g}, {t_lo:g}]")
+    thr, t = None, None
+    for _ in range(200):
+        mid = np.sqrt(lo * hi)
+        t, thr = top(mid)
+        if t > 0 and abs(np.log(t / target)) < 0.01:
+            break
+        if t > target:
+            lo = mid
+        else:
+            hi = mid
+    out = g.with_thresholds(thr)
+    out.be_prob = thr.astype(np.float64) / (1 << 32)
+    out.meta = dict(g.meta, target_p_top=target, approx_p_top=float(t))
+    return out
+
+
+def config4_dag(seed: int = 4) -> FlatGraph:
+    """The rare-event tree of config 4 (2,000 basic events, 1,200 gates, 60% AND,
+    30% OR, 10% ATLEAST 2-of-3 .. 3-of-5, 12 layers) with 20% of its basic
+    events read by two gates, each second parent within the subtree of the
+    first parent's parent (so that an exact BDD stays small); probabilities
+    log-uniform in [1e-6, 1e-3] rescaled until the independence approximation
+    gives P_top = 1e-8."""
+    g = generate(TreeSpec(n_be=2000, n_gates=1200, mix={AND: 0.6, OR: 0.3, ATLEAST: 0.1}, p_range=(1e-6, 1e-3),
+                          seed=seed, n_layers=12, atleast_n=(3, 5), share_be_frac=0.2, share_scope=1,
+                          name="config4-dag-2000be-1200g"))
+    return calibrate_rare_approx(g, 1e-8)
+
+
+def config5_dag_instance(i: int, seed: int = 5) -> FlatGraph:
+    """Instance i of the batched rare-event set with shared events: the
+    config5_instance draws (events log-uniform in [50, 10,000], AND-heavy
+    60/30/10 or ATLEAST-heavy 30/30/40 mix, target P_top log-uniform in
+    [1e-10, 1e-5]) with 20% of the basic events read by two gates, the second
+    parent within the subtree of the first parent's parent, calibrated with
+    the independence approximation (calibrate_rare_approx)."""
+    rng = np.random.default_rng([seed, i, 1])
+    and_heavy = i % 2 == 0
+    mix = {AND: 0.6, OR: 0.3, ATLEAST: 0.1} if and_heavy else {AND: 0.3, OR: 0.3, ATLEAST: 0.4}
+    for _ in range(100):
+        nb = int(round(np.exp(rng.uniform(np.log(50), np.log(10000)))))
+        ng = max(4, int(round(nb / (1.6 if and_heavy else 2.0))))
+        target = float(np.exp(rng.uniform(np.log(1e-10), np.log(1e-5))))
+        try:
+            g = generate(TreeSpec(n_be=nb, n_gates=ng, mix=mix, p_range=(1e-6, 1e-3),
+                                  seed=int(rng.integers(1 << 31)), atleast_n=(3, 5), share_be_frac=0.2,
+                                  share_scope=1, name=f"config5-dag-{i}-{nb}be"))
+            return calibrate_rare_approx(g, target)
+        except ValueError:
+            continue
+    raise RuntimeError(f"no feasible draw for instance {i}")
+
+
 def config5(n_instances: int = 1024, seed: int = 5, workers: int = 0, first: int = 0) -> list:
     """Instances first .. first + n_instances - 1 of the batched rare-event set
     (config5_instance).  workers > 1 builds them in that many spawned
@@ -547,19 +620,21 @@ def config5(n_instances: int = 1024, seed: int = 5, workers: int = 0, first: int
     return config5_instances(range(first, first + n_instances), seed, workers)
 
 
-def config5_instances(ids, seed: int = 5, workers=0) -> list:
-    """The batched rare-event instances with the given indices, in order;
-    `workers` > 1 spawned processes, or an executor to run them on."""
+def config5_instances(ids, seed: int = 5, workers=0, shared: bool = False) -> list:
+    """The batched rare-event instances with the given indices, in order
+    (shared: the config5_dag_instance set); `workers` > 1 spawned processes,
+    or an executor to run them on."""
     ids = list(ids)
+    make = config5_dag_instance if shared else config5_instance
     if hasattr(workers, "map"):
         n = getattr(workers, "_max_workers", 1) or 1
-        return list(workers.map(config5_instance, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * n))))
+        return list(workers.map(make, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * n))))
     if workers and workers > 1 and len(ids) > 1:
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
         with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
-            return list(ex.map(config5_instance, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * workers))))
-    return [config5_instance(i, seed) for i in ids]
+            return list(ex.map(make, ids, [seed] * len(ids), chunksize=max(1, len(ids) // (4 * workers))))
+    return [make(i, seed) for i in ids]
 
 
 _MEF_CONNECTIVE = {AND: "and", OR: "or", ATLEAST: "atleast", XOR: "xor", NOT: "not", 5: "nand", 6: "nor"}

@@ -233,6 +233,22 @@ def run_reference(args, rank: int, world: int):
 
 # ----------------------------------------------------------------------------- GPU arm
 
+def pipe_peak_from_profile():
+    """Basic-event words per second of the sampler code with the integer
+    multiply (fmaheavy) pipe saturated, from the committed ncu summary of the
+    sampler kernel (profiles/k_stage_be_config2.txt), at its 1.96 GHz."""
+    p = ROOT / "profiles" / "k_stage_be_config2.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("fmaheavy_saturated_gword_s:"):
+            try:
+                return float(ln.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
 def traffic_from_profile(kernel: str):
     """DRAM bytes per launch of `kernel` at the bench's launch size, from the
     committed ncu summary (profiles/<kernel>_config2.txt), if present."""
@@ -926,6 +942,15 @@ def main() -> int:
             "clocks": clk,
             "program": info,
         }
+        pipe = pipe_peak_from_profile()
+        if pipe and clk.get("sm_mhz"):
+            pk = pipe * clk["sm_mhz"] / 1960.0  # the pipe's rate follows the SM clock
+            line["roofline_pipe"] = {"bound": "fmaheavy (integer multiply) pipe", "kernel": kernel,
+                                     "achieved": achieved / 1e9, "peak": pk, "unit": "Gword/s",
+                                     "frac": achieved / 1e9 / pk,
+                                     "peak_source": "ncu: the sampler kernel's words/s over its fmaheavy pipe "
+                                                    "utilisation (profiles/k_stage_be_config2.txt), scaled to "
+                                                    "the median SM clock of this run"}
         if traffic and hbm_peak:
             line["roofline_hbm"] = {"achieved": traffic / avg_launch_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                                     "frac": traffic / avg_launch_s / 1e9 / hbm_peak}

@@ -66,6 +66,14 @@ __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
+// Row strides (in BF16 elements) of the shared-memory tiles: 16-wide rows
+// padded to 24 (48 B) and 64-wide rows to 72 (144 B).  Rows stay 16-byte
+// aligned for ldmatrix, and a fragment's eight rows start on eight
+// different bank groups, so neither the fragment loads below nor ldmatrix
+// conflict (with 64-element rows every row would start on the same bank).
+constexpr int kLdX = 24;
+constexpr int kLd = 72;
+
 // A fragment of the 16x16 tile at rows m0.., cols k0.. of row-major A (lda).
 __device__ __forceinline__ void frag_a(uint32_t a[4], const bf16 *A, int lda, int m0, int k0, int lane) {
     const int g = lane >> 2, t = lane & 3;
@@ -82,20 +90,50 @@ __device__ __forceinline__ void frag_b(uint32_t b[2], const bf16 *Bt, int ldb, i
     b[1] = *reinterpret_cast<const uint32_t *>(&Bt[(n0 + g) * ldb + k0 + 2 * t + 8]);
 }
 
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// ldmatrix with transposition: 8x8 BF16 tiles whose rows lanes 8j .. 8j + 7
+// address (tile j); each lane receives the tiles' elements in the layout of
+// the transposed tiles' mma fragments.
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t r[4], const bf16 *row) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_addr(row)));
+}
+
+__device__ __forceinline__ void ldsm_x2_trans(uint32_t r[2], const bf16 *row) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(smem_addr(row)));
+}
+
+// A fragment of the 16x16 tile (m0.., k0..) of A = M^T for M stored
+// row-major as M[k][m] (ldm): the tiles (k0, m0), (k0, m0 + 8), (k0 + 8, m0),
+// (k0 + 8, m0 + 8) of M, transposed, are a[0] .. a[3].
+__device__ __forceinline__ void frag_a_t(uint32_t a[4], const bf16 *M, int ldm, int m0, int k0, int lane) {
+    const int tile = lane >> 3, row = lane & 7;
+    ldsm_x4_trans(a, M + (k0 + row + ((tile & 2) ? 8 : 0)) * ldm + m0 + ((tile & 1) ? 8 : 0));
+}
+
+// B fragment of the 16x8 tile (k0.., n0..) of B stored row-major as B[k][n]
+// (ldb): the tiles (k0, n0) and (k0 + 8, n0) of B, transposed.
+__device__ __forceinline__ void frag_b_t(uint32_t b[2], const bf16 *B, int ldb, int n0, int k0, int lane) {
+    const int tile = (lane >> 3) & 1, row = lane & 7;
+    ldsm_x2_trans(b, B + (k0 + row + 8 * tile) * ldb + n0);
+}
+
 struct Smem {
-    bf16 w1t[kHid * kIn];
-    bf16 w2t[kHid * kHid];
-    bf16 w2[kHid * kHid];
-    bf16 w3t[8 * kHid];
-    bf16 x[kRows * kIn];      // row-major
-    bf16 xt[kIn * kRows];     // feature-major
-    bf16 h1[kRows * kHid];    // post-ReLU
-    bf16 h1t[kHid * kRows];
-    bf16 h2[kRows * kHid];
-    bf16 h2t[kHid * kRows];
-    bf16 dh2[kRows * kHid];
-    bf16 dh2t[kHid * kRows];
-    bf16 dh1t[kHid * kRows];
+    bf16 w1t[kHid * kLdX];    // W1t[out][in]
+    bf16 w2t[kHid * kLd];     // W2t[out][in]
+    bf16 w2[kHid * kLd];      // W2[in][out]
+    bf16 w3t[8 * kLd];        // row 0 = W3
+    bf16 x[kRows * kLdX];     // the tile's features, row-major
+    bf16 h1[kRows * kLd];     // post-ReLU activations, row-major
+    bf16 h2[kRows * kLd];
+    bf16 dh2[kRows * kLd];    // gradients of the pre-activations, row-major
+    bf16 dh1[kRows * kLd];
     uint8_t m1[kRows * kHid];  // ReLU masks
     uint8_t m2[kRows * kHid];
     float b1[kHid], b2[kHid], w3[kHid];
@@ -103,29 +141,27 @@ struct Smem {
     float loss;
 };
 
-// Forward for the CTA's rows; writes h1/h2 (+ transposes, masks) and returns
-// z for row r (valid in lanes with (lane & 3) == 0: rows g and g + 8).
+// Forward for the CTA's rows; writes h1/h2 and the masks and returns z for
+// row r (valid in lanes with (lane & 3) == 0: rows g and g + 8).
 __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[2]) {
     const int m0 = warp * 16;
     const int g = lane >> 2, t = lane & 3;
     // layer 1: [16 x 16] x [16 x 64]
     {
         uint32_t a[4];
-        frag_a(a, s.x, kIn, m0, 0, lane);
+        frag_a(a, s.x, kLdX, m0, 0, lane);
 #pragma unroll
         for (int nt = 0; nt < kHid / 8; ++nt) {
             float c[4] = {0.f, 0.f, 0.f, 0.f};
             uint32_t b[2];
-            frag_b(b, s.w1t, kIn, nt * 8, 0, lane);
+            frag_b(b, s.w1t, kLdX, nt * 8, 0, lane);
             mma16816(c, a, b);
             const int col = nt * 8 + 2 * t;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int r = m0 + g + (j >= 2 ? 8 : 0), cc = col + (j & 1);
                 const float v = c[j] + s.b1[cc];
-                const bf16 h = __float2bfloat16(v > 0.f ? v : 0.f);
-                s.h1[r * kHid + cc] = h;
-                s.h1t[cc * kRows + r] = h;
+                s.h1[r * kLd + cc] = __float2bfloat16(v > 0.f ? v : 0.f);
                 s.m1[r * kHid + cc] = v > 0.f;
             }
         }
@@ -138,8 +174,8 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
 #pragma unroll
         for (int kt = 0; kt < kHid / 16; ++kt) {
             uint32_t a[4], b[2];
-            frag_a(a, s.h1, kHid, m0, kt * 16, lane);
-            frag_b(b, s.w2t, kHid, nt * 8, kt * 16, lane);
+            frag_a(a, s.h1, kLd, m0, kt * 16, lane);
+            frag_b(b, s.w2t, kLd, nt * 8, kt * 16, lane);
             mma16816(c, a, b);
         }
         const int col = nt * 8 + 2 * t;
@@ -147,9 +183,7 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
         for (int j = 0; j < 4; ++j) {
             const int r = m0 + g + (j >= 2 ? 8 : 0), cc = col + (j & 1);
             const float v = c[j] + s.b2[cc];
-            const bf16 h = __float2bfloat16(v > 0.f ? v : 0.f);
-            s.h2[r * kHid + cc] = h;
-            s.h2t[cc * kRows + r] = h;
+            s.h2[r * kLd + cc] = __float2bfloat16(v > 0.f ? v : 0.f);
             s.m2[r * kHid + cc] = v > 0.f;
         }
     }
@@ -159,8 +193,8 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
 #pragma unroll
     for (int kt = 0; kt < kHid / 16; ++kt) {
         uint32_t a[4], b[2];
-        frag_a(a, s.h2, kHid, m0, kt * 16, lane);
-        frag_b(b, s.w3t, kHid, 0, kt * 16, lane);
+        frag_a(a, s.h2, kLd, m0, kt * 16, lane);
+        frag_b(b, s.w3t, kLd, 0, kt * 16, lane);
         mma16816(c, a, b);
     }
     z_out[0] = c[0] + b3;  // row m0 + g, column 0 when t == 0
@@ -168,12 +202,12 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
 }
 
 __device__ void load_weights(Smem &s, const bf16 *__restrict__ pack, const float *__restrict__ params) {
-    for (int i = threadIdx.x; i < kHid * kIn; i += kThreads) s.w1t[i] = pack[kPackW1t + i];
+    for (int i = threadIdx.x; i < kHid * kIn; i += kThreads) s.w1t[(i / kIn) * kLdX + i % kIn] = pack[kPackW1t + i];
     for (int i = threadIdx.x; i < kHid * kHid; i += kThreads) {
-        s.w2t[i] = pack[kPackW2t + i];
-        s.w2[i] = pack[kPackW2 + i];
+        s.w2t[(i / kHid) * kLd + i % kHid] = pack[kPackW2t + i];
+        s.w2[(i / kHid) * kLd + i % kHid] = pack[kPackW2 + i];
     }
-    for (int i = threadIdx.x; i < 8 * kHid; i += kThreads) s.w3t[i] = pack[kPackW3t + i];
+    for (int i = threadIdx.x; i < 8 * kHid; i += kThreads) s.w3t[(i / kHid) * kLd + i % kHid] = pack[kPackW3t + i];
     for (int i = threadIdx.x; i < kHid; i += kThreads) {
         s.b1[i] = params[kOffB1 + i];
         s.b2[i] = params[kOffB2 + i];
@@ -181,37 +215,19 @@ __device__ void load_weights(Smem &s, const bf16 *__restrict__ pack, const float
     }
 }
 
-// The tile's rows as BF16 (row-major and feature-major); rows past n are 0.
+// The tile's rows as BF16; rows past n are 0.
 __device__ void load_rows(Smem &s, const float *__restrict__ feat, uint32_t n, uint32_t row0) {
     for (int i = threadIdx.x; i < kRows * kIn; i += kThreads) {
         const int r = i / kIn, f = i % kIn;
         const float v = (row0 + r < n) ? feat[(uint64_t)(row0 + r) * kIn + f] : 0.f;
-        const bf16 b = __float2bfloat16(v);
-        s.x[r * kIn + f] = b;
-        s.xt[f * kRows + r] = b;
+        s.x[r * kLdX + f] = __float2bfloat16(v);
     }
 }
 
 __device__ void load_tile(Smem &s, const bf16 *__restrict__ pack, const float *__restrict__ params,
                           const float *__restrict__ feat, uint32_t n, uint32_t row0) {
-    for (int i = threadIdx.x; i < kHid * kIn; i += kThreads) s.w1t[i] = pack[kPackW1t + i];
-    for (int i = threadIdx.x; i < kHid * kHid; i += kThreads) {
-        s.w2t[i] = pack[kPackW2t + i];
-        s.w2[i] = pack[kPackW2 + i];
-    }
-    for (int i = threadIdx.x; i < 8 * kHid; i += kThreads) s.w3t[i] = pack[kPackW3t + i];
-    for (int i = threadIdx.x; i < kHid; i += kThreads) {
-        s.b1[i] = params[kOffB1 + i];
-        s.b2[i] = params[kOffB2 + i];
-        s.w3[i] = params[kOffW3 + i];
-    }
-    for (int i = threadIdx.x; i < kRows * kIn; i += kThreads) {
-        const int r = i / kIn, f = i % kIn;
-        const float v = (row0 + r < n) ? feat[(uint64_t)(row0 + r) * kIn + f] : 0.f;
-        const bf16 b = __float2bfloat16(v);
-        s.x[r * kIn + f] = b;
-        s.xt[f * kRows + r] = b;
-    }
+    load_weights(s, pack, params);
+    load_rows(s, feat, n, row0);
     if (threadIdx.x == 0) s.loss = 0.f;
     __syncthreads();
 }
@@ -290,16 +306,13 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ 
         // dH2 = dz W3^T masked
         for (int i = threadIdx.x; i < kRows * kHid; i += kThreads) {
             const int r = i / kHid, c = i % kHid;
-            const float v = s.m2[i] ? s.dz[r] * s.w3[c] : 0.f;
-            const bf16 b = __float2bfloat16(v);
-            s.dh2[i] = b;
-            s.dh2t[c * kRows + r] = b;
+            s.dh2[r * kLd + c] = __float2bfloat16(s.m2[i] ? s.dz[r] * s.w3[c] : 0.f);
         }
         __syncthreads();
         if (threadIdx.x < kHid) {
             const int c = threadIdx.x;
             for (int r = 0; r < kRows; ++r) {
-                gw3 += __bfloat162float(s.h2[r * kHid + c]) * s.dz[r];
+                gw3 += __bfloat162float(s.h2[r * kLd + c]) * s.dz[r];
                 gb2 += s.m2[r * kHid + c] ? s.dz[r] * s.w3[c] : 0.f;
             }
         } else if (threadIdx.x == kHid) {
@@ -307,12 +320,13 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ 
         }
         // dW2[in][out] += H1^T dH2: M = 64 (in), N = 64 (out), K = 64 rows; warp w: in rows 16w..
 #pragma unroll
-        for (int nt = 0; nt < kHid / 8; ++nt) {
+        for (int kt = 0; kt < kRows / 16; ++kt) {
+            uint32_t a[4];
+            frag_a_t(a, s.h1, kLd, m0, kt * 16, lane);
 #pragma unroll
-            for (int kt = 0; kt < kRows / 16; ++kt) {
-                uint32_t a[4], b[2];
-                frag_a(a, s.h1t, kRows, m0, kt * 16, lane);
-                frag_b(b, s.dh2t, kRows, nt * 8, kt * 16, lane);
+            for (int nt = 0; nt < kHid / 8; ++nt) {
+                uint32_t b[2];
+                frag_b_t(b, s.dh2, kLd, nt * 8, kt * 16, lane);
                 mma16816(acc2[nt], a, b);
             }
         }
@@ -323,32 +337,31 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ 
 #pragma unroll
             for (int kt = 0; kt < kHid / 16; ++kt) {
                 uint32_t a[4], b[2];
-                frag_a(a, s.dh2, kHid, m0, kt * 16, lane);
-                frag_b(b, s.w2, kHid, nt * 8, kt * 16, lane);
+                frag_a(a, s.dh2, kLd, m0, kt * 16, lane);
+                frag_b(b, s.w2, kLd, nt * 8, kt * 16, lane);
                 mma16816(c, a, b);
             }
             const int col = nt * 8 + 2 * t;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int r = m0 + g + (j >= 2 ? 8 : 0), cc = col + (j & 1);
-                const float v = s.m1[r * kHid + cc] ? c[j] : 0.f;
-                s.dh1t[cc * kRows + r] = __float2bfloat16(v);
+                s.dh1[r * kLd + cc] = __float2bfloat16(s.m1[r * kHid + cc] ? c[j] : 0.f);
             }
         }
         __syncthreads();
         // db1 and dW1[f][h] += X^T dH1: M = 16 (features), N = 64, K = 64 rows; warp w: n-tiles 2w, 2w+1
         if (threadIdx.x < kHid) {
             const int c = threadIdx.x;
-            for (int r = 0; r < kRows; ++r) gb1 += __bfloat162float(s.dh1t[c * kRows + r]);
+            for (int r = 0; r < kRows; ++r) gb1 += __bfloat162float(s.dh1[r * kLd + c]);
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int nt = warp * 2 + q;
+        for (int kt = 0; kt < kRows / 16; ++kt) {
+            uint32_t a[4];
+            frag_a_t(a, s.x, kLdX, 0, kt * 16, lane);
 #pragma unroll
-            for (int kt = 0; kt < kRows / 16; ++kt) {
-                uint32_t a[4], b[2];
-                frag_a(a, s.xt, kRows, 0, kt * 16, lane);
-                frag_b(b, s.dh1t, kRows, nt * 8, kt * 16, lane);
+            for (int q = 0; q < 2; ++q) {
+                uint32_t b[2];
+                frag_b_t(b, s.dh1, kLd, (warp * 2 + q) * 8, kt * 16, lane);
                 mma16816(acc1[q], a, b);
             }
         }

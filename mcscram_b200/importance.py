@@ -223,6 +223,69 @@ def cut_set_eligible(g: FlatGraph) -> bool:
     return bool(np.all(ok_ops) and np.all(k_ok) and np.all(g.gate_neg_count == 0) and np.all(fan[g.n_be:] <= 1))
 
 
+def cut_inclusion(g: FlatGraph) -> np.ndarray:
+    """Expected number of times each basic event is picked by the cut-set
+    descent on the graph read as a tree, every leaf of an event read by m
+    gates at p^(1/m): S(node) bottom-up (leaf value; AND product, OR sum,
+    ATLEAST k-th elementary symmetric sum), then the descent's visit
+    probability top-down (OR: child share S(child)/S(OR); AND: every child;
+    ATLEAST k: P(child in the k-subset) = S_c e_{k-1}(others) / e_k(all)).
+    A cut set that uses all m leaves of a shared event then weighs p once, as
+    it does in the graph, where read as a tree it would weigh p^m; one that
+    uses fewer leaves weighs more than it should.  For events read by several
+    gates the result is a generous estimate of how much of the union of cut
+    sets goes through them: the seed of their proposal in the cut-set
+    component."""
+    nb, ng = g.n_be, g.n_gates
+    S = np.zeros(g.n_nodes)
+    p0 = g.quantised_probabilities()
+    fan = np.maximum(np.bincount(g.inputs, minlength=g.n_nodes)[:nb], 1)
+    S[:nb] = np.where(fan > 1, p0 ** (1.0 / fan), p0)
+    ops = g.gate_op
+    kk = g.gate_k & 0xFF
+
+    def esym(v, k):
+        e = np.zeros(k + 1)
+        e[0] = 1.0
+        for x in v:
+            e[1:] = e[1:] + e[:-1] * x
+        return e
+
+    for j in range(ng):
+        v = S[g.gate_inputs(j)]
+        op = int(ops[j])
+        if op == AND:
+            S[nb + j] = float(np.prod(v))
+        elif op == ATLEAST:
+            S[nb + j] = esym(v, int(kk[j]))[int(kk[j])]
+        elif op == OR:
+            S[nb + j] = float(np.sum(v))
+        else:
+            S[nb + j] = float(v[-1]) if v.size else 0.0
+    visit = np.zeros(g.n_nodes)
+    visit[g.root] = 1.0
+    for j in range(ng - 1, -1, -1):
+        vg = visit[nb + j]
+        if vg == 0.0:
+            continue
+        ins = g.gate_inputs(j).astype(np.int64)
+        v = S[ins]
+        op = int(ops[j])
+        if op == OR:
+            tot = v.sum()
+            if tot > 0:
+                np.add.at(visit, ins, vg * v / tot)
+        elif op == ATLEAST:
+            k = int(kk[j])
+            ek = esym(v, k)[k]
+            if ek > 0:
+                share = np.array([v[c] * esym(np.delete(v, c), k - 1)[k - 1] / ek for c in range(v.size)])
+                np.add.at(visit, ins, vg * share)
+        else:
+            np.add.at(visit, ins, vg)
+    return visit[:nb]
+
+
 def shared_events(g: FlatGraph) -> np.ndarray:
     """Basic events read by more than one gate."""
     return np.bincount(g.inputs, minlength=g.n_nodes)[: g.n_be] > 1
@@ -868,10 +931,12 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     n_comp = q_def.shape[0]
 
     # Events read by several gates: the cut-set component draws them first,
-    # from r = the current proposal clipped to [p, 0.5] (their conditional
-    # failure probability given the top is what it should approach; at the
-    # start the independence approximation's estimate of it), and then the cut
-    # set on the tree conditioned on them.
+    # from r = the current proposal clipped to [max(p, floor), 0.9] (their
+    # conditional failure probability given the top is what it should
+    # approach; at the start cut_inclusion's generous estimate of it, half of
+    # which stays as the floor, so that a cut set of several shared events
+    # that the first samples under-weigh is still drawn), and then the cut set
+    # on the tree conditioned on them.
     shared_u = np.concatenate([shared_events(g) for g in graphs]) if cut else np.zeros(full.union.n_be, bool)
     has_shared = bool(shared_u.any())
 
@@ -879,7 +944,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         if not has_shared:
             return None
         smp = full if smp is None else smp
-        return smp.proposal_thresholds(np.where(shared_u_of(smp), np.clip(qv, p_of(smp), 0.5), p_of(smp)))
+        lo = np.maximum(p_of(smp), r_floor if smp is full else np.concatenate([r_floor[sl[k]] for k in members]))
+        return smp.proposal_thresholds(np.where(shared_u_of(smp), np.clip(qv, lo, 0.9), p_of(smp)))
 
     def shared_u_of(smp):
         return shared_u if smp is full else np.concatenate([shared_u[sl[k]] for k in members])
@@ -888,12 +954,15 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         return p if smp is full else np.concatenate([p[sl[k]] for k in members])
 
     r0 = None
-    if has_shared:
+    r_floor = np.zeros(full.union.n_be)
+    if has_shared:  # seed: the larger of the cut-set descent's inclusion and the approximate conditional
         r0 = p.copy()
         for k, g in enumerate(graphs):
             m = shared_u[sl[k]]
             if m.any():
-                r0[sl[k]][m] = np.clip(approximate_importance(g)[1][m], p[sl[k]][m], 0.5)
+                inc = np.minimum(cut_inclusion(g)[m], 0.9)
+                r_floor[sl[k]][m] = 0.5 * inc
+                r0[sl[k]][m] = np.clip(inc, p[sl[k]][m], 0.9)
 
     def def_words(w):  # words per defensive component
         return max(1, int(round(defensive * w / n_comp))) if defensive > 0 and n_comp else 0
@@ -992,6 +1061,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         first = run_k[(~checked[run_k]) & (rounds_in[run_k] >= fallback_after)]
         checked[first] = True
         bad = first[(H[first] > 0) & (ess[first] < collapse_ratio * H[first]) & ~done[first]]
+        if cut:  # its weights stay below S / pi: more samples, not plain sampling (hopeless at 1e-9)
+            bad = bad[:0]
         for k in bad:
             fallback[k] = True
             q_use[sl[k]] = p[sl[k]]

@@ -196,6 +196,7 @@ struct CutArgs {
     const uint32_t *inputs;
     const double *S;               // per node: S_0
     const double *tab;             // OR: cumulative S_0(child) / S_0(OR); ATLEAST: E[j][r] = e_r(S_j..S_n-1)
+    const unsigned char *tree_ok;  // per tree: drawn by the component (else its samples stay nominal)
     const unsigned char *shared;   // per basic event: read by several gates
     const uint2 *gate_occ;         // per gate: [lo, hi) of the shared-leaf occurrences below it
     const uint32_t *z_begin;       // per tree: its shared events are z_event[z_begin[k] .. z_begin[k + 1])
@@ -279,6 +280,7 @@ __global__ void __launch_bounds__(256) k_cut_force(CutArgs a) {
     const uint64_t wi = item >> 6;
     const uint64_t w = wi % a.W;
     const uint32_t k = (uint32_t)(wi / a.W);
+    if (!a.tree_ok[k]) return;  // a tree the component cannot draw: nominal samples
     uint64_t base = mix64(a.seed ^ ((uint64_t)k << 32));
     base = mix64(base ^ (a.word_begin + w));
     base = mix64(base ^ (uint64_t)b);
@@ -434,6 +436,7 @@ struct IsBatchArgs {
     const double *cut_logS;        // per tree: log S_0(top)
     const uint4 *cut_gate;         // per gate (see CutArgs)
     const double *cut_S;           // per node: S_0
+    const unsigned char *cut_tree_ok;  // per tree: drawn by the component (else its density there is p)
     const unsigned char *shared;   // per basic event: read by several gates
     const uint32_t *companion;     // per gate: node of the OR over the shared leaves below it, or kNoNode
     const uint32_t *inputs;
@@ -490,7 +493,9 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
         for (uint64_t m = top; m; m &= m - 1) {
             const int b = __ffsll((long long)m) - 1;
             double lw_cut = 0.0;
-            if (p.cut_comp >= 0) {
+            if (p.cut_comp >= 0 && !p.cut_tree_ok[k]) {
+                lw_cut = p.C[(uint64_t)p.cut_comp * p.n_inst + k] + acc[p.cut_comp][b];  // nominal: 0
+            } else if (p.cut_comp >= 0) {
                 const uint32_t root = p.root_row[k], nbn = p.n_be_nodes;
                 const double n_cut = cut_count(col, p.W, root, b, p.cut_gate, p.inputs, nbn);
                 if (!(n_cut >= 1.0)) atomicOr(p.error, 2u);  // too deep, or a failure without a cut set
@@ -762,6 +767,9 @@ struct mcg_is_batch {
     bool companions = false;
     std::vector<uint32_t> companion;     // per gate of the caller: its companion node, or kNoNode
     std::vector<unsigned char> shared;   // per basic event
+    std::vector<unsigned char> tree_gates_ok;  // per tree: gates the component takes (companions built for it)
+    std::vector<unsigned char> tree_ok;  // per tree: the cut-set component draws it (else its samples stay nominal)
+    unsigned char *d_tree_ok = nullptr;
     std::vector<uint32_t> z_event;       // shared events, tree by tree
     std::vector<uint64_t> z_thr, cut_q;  // per run: their proposal thresholds; the component's table
     unsigned char *d_shared = nullptr;
@@ -793,7 +801,7 @@ void release_batch(mcg_is_batch *b) {
     cudaFree(b->d_cut_tab);
     cudaFree(b->d_cut_logS);
     cudaFree(b->d_cut_error);
-    for (void *q : {(void *)b->d_shared, (void *)b->d_gate_occ, (void *)b->d_companion, (void *)b->d_z_begin,
+    for (void *q : {(void *)b->d_tree_ok, (void *)b->d_shared, (void *)b->d_gate_occ, (void *)b->d_companion, (void *)b->d_z_begin,
                     (void *)b->d_z_event, (void *)b->d_z_index, (void *)b->d_z_occ_begin, (void *)b->d_z_occ,
                     (void *)b->d_z_thr})
         cudaFree(q);
@@ -829,38 +837,48 @@ std::string check_partition(const mcg::Graph &g, const std::vector<uint32_t> &be
     return std::string();
 }
 
-// Companion gates for the cut-set component on trees whose only shared
-// nodes are basic events: for every gate with a shared event's leaf below
-// it, an OR over those leaves and over its child gates' companions, appended
-// after the caller's gates (the tallies stay the trees' tops).  The weights
-// kernel reads a companion's word to see which gates a sample's z_i = 1
-// leaves reach.  Nothing is added when no basic event is shared, when a gate
-// is read by several gates, or when a gate is not AND / OR / ATLEAST /
-// pass-through without complemented inputs (the cut-set component refuses
-// such graphs).
+// Trees the cut-set component can draw: every gate AND / OR / ATLEAST /
+// pass-through without complemented inputs and read by one gate at most
+// (tree_ok[t]).  For those of them with basic events read by several gates,
+// companion gates: for every gate with a shared event's leaf below it, an OR
+// over those leaves and over its child gates' companions, appended after the
+// caller's gates (the tallies stay the trees' tops).  The weights kernel
+// reads a companion's word to see which gates a sample's z_i = 1 leaves
+// reach.  Returns whether any companion was added.
 struct Augmented {
     std::vector<uint8_t> op;
     std::vector<uint32_t> k, begin, count, neg, inputs;
     std::vector<int32_t> pdag;
     std::vector<uint32_t> companion;  // per caller's gate
+    std::vector<unsigned char> tree_ok;
     mcg_graph_desc desc{};
 };
 
-bool add_companions(const mcg_graph_desc &d, Augmented &a) {
+bool add_companions(const mcg_graph_desc &d, uint32_t n_inst, const uint32_t *be_begin, Augmented &a) {
     const uint64_t nb = d.n_be, ng = d.n_gates, nn = nb + ng;
-    std::vector<uint32_t> fanout(nn, 0);
+    std::vector<uint32_t> fanout(nn, 0), owner(nn, kNoNode);
     for (uint64_t i = 0; i < d.n_inputs; ++i)
         if (d.inputs[i] < nn) ++fanout[d.inputs[i]];
-    bool any_shared = false;
-    for (uint64_t i = 0; i < nb; ++i) any_shared |= fanout[i] > 1;
-    if (!any_shared) return false;
+    for (uint32_t t = 0; t < n_inst; ++t)
+        for (uint32_t i = be_begin[t]; i < be_begin[t + 1]; ++i) owner[i] = t;
+    a.tree_ok.assign(n_inst, 1);
     for (uint64_t j = 0; j < ng; ++j) {
+        uint32_t o = kNoNode;
+        const bool in_range = (uint64_t)d.gate_in_begin[j] + d.gate_in_count[j] <= d.n_inputs;
+        for (uint32_t c = 0; in_range && c < d.gate_in_count[j]; ++c) {
+            const uint32_t x = d.inputs[d.gate_in_begin[j] + c];
+            if (x < nn && owner[x] != kNoNode) o = owner[x];
+        }
+        owner[nb + j] = o;
         const uint8_t op = d.gate_op[j];
-        if (fanout[nb + j] > 1 || d.gate_neg_count[j] ||
-            !(op == MCG_AND || op == MCG_OR || op == MCG_ATLEAST || op == MCG_NULL))
-            return false;
-        if ((uint64_t)d.gate_in_begin[j] + d.gate_in_count[j] > d.n_inputs) return false;
+        if (o != kNoNode && (!in_range || fanout[nb + j] > 1 || d.gate_neg_count[j] ||
+                             !(op == MCG_AND || op == MCG_OR || op == MCG_ATLEAST || op == MCG_NULL)))
+            a.tree_ok[o] = 0;
     }
+    bool any_shared = false;
+    for (uint64_t i = 0; i < nb; ++i) any_shared |= fanout[i] > 1 && owner[i] != kNoNode && a.tree_ok[owner[i]];
+    a.companion.assign(ng, kNoNode);
+    if (!any_shared) return false;
     a.op.assign(d.gate_op, d.gate_op + ng);
     a.k.assign(d.gate_k, d.gate_k + ng);
     a.begin.assign(d.gate_in_begin, d.gate_in_begin + ng);
@@ -868,8 +886,8 @@ bool add_companions(const mcg_graph_desc &d, Augmented &a) {
     a.neg.assign(d.gate_neg_count, d.gate_neg_count + ng);
     a.inputs.assign(d.inputs, d.inputs + d.n_inputs);
     if (d.gate_pdag_idx) a.pdag.assign(d.gate_pdag_idx, d.gate_pdag_idx + ng);
-    a.companion.assign(ng, kNoNode);
     for (uint64_t j = 0; j < ng; ++j) {
+        if (owner[nb + j] == kNoNode || !a.tree_ok[owner[nb + j]]) continue;
         std::vector<uint32_t> in;
         for (uint32_t c = 0; c < d.gate_in_count[j]; ++c) {
             const uint32_t x = d.inputs[d.gate_in_begin[j] + c];
@@ -926,8 +944,9 @@ mcg_status mcg_is_batch_create(const mcg_graph_desc *graph, uint32_t n_inst, con
     b->be_begin.assign(be_begin, be_begin + n_inst + 1);
     b->n_gates_in = graph->n_gates;
     Augmented aug;
-    b->companions = add_companions(*graph, aug);
-    if (b->companions) b->companion = aug.companion;
+    b->companions = add_companions(*graph, n_inst, be_begin, aug);
+    b->companion = aug.companion;
+    b->tree_gates_ok = aug.tree_ok;
     mcg_status st = mcg_create(b->companions ? &aug.desc : graph, &run, &b->engine);
     if (st != MCG_OK) return st;
     const mcg::Graph &g = b->engine->graph;
@@ -973,15 +992,34 @@ namespace {
 mcg_status build_cut_tables(mcg_is_batch *b) {
     const mcg::Graph &g = b->engine->graph;
     const uint32_t nb = g.n_be, ng_all = g.n_gates, ng = b->n_gates_in, nn = g.n_nodes();
-    std::vector<uint32_t> fanout(nn, 0);
+    std::vector<uint32_t> fanout(nn, 0), owner(nn, kNoNode);
     for (uint32_t j = 0; j < ng; ++j)
         for (uint32_t c = 0; c < g.gate_in_count[j]; ++c) ++fanout[g.inputs[g.gate_in_begin[j] + c]];
+    for (uint32_t t = 0; t < b->n_inst; ++t)
+        for (uint32_t i = b->be_begin[t]; i < b->be_begin[t + 1]; ++i) owner[i] = t;
+    for (uint32_t j = 0; j < ng; ++j)
+        for (uint32_t c = 0; c < g.gate_in_count[j]; ++c) {
+            const uint32_t o = owner[g.inputs[g.gate_in_begin[j] + c]];
+            if (o != kNoNode) owner[nb + j] = o;
+        }
+    // Trees the component cannot draw keep nominal samples in its words (their
+    // density there is p); it fails only when it can draw none of them.
+    std::vector<unsigned char> &ok = b->tree_ok;
+    ok.assign(b->n_inst, 1);
+    std::string why;
+    auto reject = [&](uint32_t node, const std::string &msg) {
+        const uint32_t t = owner[node];
+        if (t == kNoNode || !ok[t]) return;
+        ok[t] = 0;
+        if (why.empty()) why = msg;
+    };
+    // a shared basic event needs its tree's companion gates (built when every gate of the tree qualified)
     for (uint32_t i = 0; i < nb + ng; ++i)
-        if (fanout[i] > 1 && (i >= nb || !b->companions))
-            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling needs trees: node " + std::to_string(i) +
-                                                  " is read by several gates");
+        if (fanout[i] > 1 && owner[i] != kNoNode &&
+            (i >= nb || !b->companions || owner[i] >= b->tree_gates_ok.size() || !b->tree_gates_ok[owner[i]]))
+            reject(i, "cut-set sampling needs trees: node " + std::to_string(i) + " is read by several gates");
     b->shared.assign(nb, 0);
-    for (uint32_t i = 0; i < nb; ++i) b->shared[i] = fanout[i] > 1;
+    for (uint32_t i = 0; i < nb; ++i) b->shared[i] = fanout[i] > 1 && owner[i] != kNoNode && ok[owner[i]];
     // S_0 (shared events at 0) for the tables; S with every event at p for the check
     std::vector<double> S(nn, 0.0), Sp(nn, 0.0), tab;
     std::vector<uint4> gate(std::max<uint32_t>(ng_all, 1), make_uint4(0, 0, 0, 0));
@@ -1006,10 +1044,10 @@ mcg_status build_cut_tables(mcg_is_batch *b) {
         const uint32_t op = g.gate_op[j], n = g.gate_in_count[j], k = g.gate_k[j] & 0xFFu;
         const uint32_t *in = g.inputs.data() + g.gate_in_begin[j];
         if (g.gate_neg_count[j] || !(op == MCG_AND || op == MCG_OR || op == MCG_ATLEAST || op == MCG_NULL))
-            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling needs AND/OR/ATLEAST gates without complemented "
-                                              "inputs; gate " + std::to_string(j) + " is not one");
-        if (op == MCG_ATLEAST && k > (uint32_t)kCutMaxK)
-            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: ATLEAST threshold above 8");
+            reject(nb + j, "cut-set sampling needs AND/OR/ATLEAST gates without complemented inputs; gate " +
+                               std::to_string(j) + " is not one");
+        if (op == MCG_ATLEAST && k > (uint32_t)kCutMaxK) reject(nb + j, "cut-set sampling: ATLEAST threshold above 8");
+        if (owner[nb + j] == kNoNode || !ok[owner[nb + j]]) continue;  // its tree keeps nominal samples
         gate[j] = make_uint4(op | (k << 8), g.gate_in_begin[j], n, (uint32_t)tab.size());
         vals.assign(n, 0.0);
         valp.assign(n, 0.0);
@@ -1040,11 +1078,15 @@ mcg_status build_cut_tables(mcg_is_batch *b) {
     }
     for (uint32_t j = ng; j < ng_all; ++j)  // companions: never entered by the descent or the evaluations
         gate[j] = make_uint4(MCG_OR, g.gate_in_begin[j], g.gate_in_count[j], 0);
-    std::vector<double> logS(b->n_inst);
+    std::vector<double> logS(b->n_inst, 0.0);
     for (uint32_t t = 0; t < b->n_inst; ++t) {
+        if (!ok[t]) continue;
         const double st = Sp[g.tally_nodes[t]];
-        if (!(st > 0.0) || !std::isfinite(st))
-            return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: tree " + std::to_string(t) + " has no cut set");
+        if (!(st > 0.0) || !std::isfinite(st)) {
+            ok[t] = 0;
+            if (why.empty()) why = "cut-set sampling: tree " + std::to_string(t) + " has no cut set";
+            continue;
+        }
         logS[t] = std::log(S[g.tally_nodes[t]]);  // -inf when every cut set holds a shared event
     }
     // shared-leaf occurrences in depth-first order from every top: each gate's
@@ -1054,7 +1096,7 @@ mcg_status build_cut_tables(mcg_is_batch *b) {
     uint32_t pos = 0;
     for (uint32_t t = 0; t < b->n_inst; ++t) {
         const uint32_t root = g.tally_nodes[t];
-        if (root < nb) continue;
+        if (root < nb || !ok[t]) continue;
         std::vector<std::pair<uint32_t, uint32_t>> st{{root, 0}};
         occ_range[root - nb].x = pos;
         while (!st.empty()) {
@@ -1071,19 +1113,25 @@ mcg_status build_cut_tables(mcg_is_batch *b) {
             } else {
                 occ_range[j].y = pos;
                 const uint32_t op = g.gate_op[j];
-                if (op == MCG_ATLEAST && occ_range[j].y > occ_range[j].x && g.gate_in_count[j] > (uint32_t)kCutMaxN)
-                    return mcg::fail(MCG_ERR_INVALID, "cut-set sampling: ATLEAST gate " + std::to_string(j) +
-                                                          " above shared events has more than 32 inputs");
+                if (op == MCG_ATLEAST && occ_range[j].y > occ_range[j].x && g.gate_in_count[j] > (uint32_t)kCutMaxN) {
+                    ok[t] = 0;
+                    if (why.empty())
+                        why = "cut-set sampling: ATLEAST gate " + std::to_string(j) +
+                              " above shared events has more than 32 inputs";
+                }
                 st.pop_back();
             }
         }
     }
+    bool any = false;
+    for (uint32_t t = 0; t < b->n_inst; ++t) any |= ok[t] != 0;
+    if (!any) return mcg::fail(MCG_ERR_INVALID, why.empty() ? std::string("cut-set sampling: no tree qualifies") : why);
     std::vector<uint32_t> z_begin(b->n_inst + 1, 0), z_index(nb, 0), z_occ_begin{0}, z_occ;
     b->z_event.clear();
     for (uint32_t t = 0; t < b->n_inst; ++t) {
         z_begin[t] = (uint32_t)b->z_event.size();
         for (uint32_t i = b->be_begin[t]; i < b->be_begin[t + 1]; ++i) {
-            if (!b->shared[i]) continue;
+            if (!b->shared[i] || !ok[t]) continue;
             z_index[i] = (uint32_t)b->z_event.size();
             b->z_event.push_back(i);
             z_occ.insert(z_occ.end(), occ_of[i].begin(), occ_of[i].end());
@@ -1102,6 +1150,8 @@ mcg_status build_cut_tables(mcg_is_batch *b) {
     MCG_CUDA(cudaMalloc((void **)&b->d_cut_logS, b->n_inst * sizeof(double)));
     MCG_CUDA(cudaMalloc((void **)&b->d_cut_error, sizeof(unsigned int)));
     MCG_CUDA(cudaMalloc((void **)&b->d_shared, std::max<uint32_t>(nb, 1)));
+    MCG_CUDA(cudaMalloc((void **)&b->d_tree_ok, b->n_inst));
+    MCG_CUDA(cudaMemcpy(b->d_tree_ok, ok.data(), b->n_inst, cudaMemcpyHostToDevice));
     MCG_CUDA(cudaMalloc((void **)&b->d_gate_occ, occ_range.size() * sizeof(uint2)));
     MCG_CUDA(cudaMalloc((void **)&b->d_companion, comp.size() * sizeof(uint32_t)));
     MCG_CUDA(cudaMalloc((void **)&b->d_z_begin, z_begin.size() * sizeof(uint32_t)));
@@ -1272,6 +1322,7 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
     args.cut_logS = b->d_cut_logS;
     args.cut_gate = b->d_cut_gate;
     args.cut_S = b->d_cut_S;
+    args.cut_tree_ok = b->d_tree_ok;
     args.shared = b->d_shared;
     args.companion = b->d_companion;
     args.inputs = e->d_inputs;
@@ -1310,6 +1361,7 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
             ca.inputs = e->d_inputs;
             ca.S = b->d_cut_S;
             ca.tab = b->d_cut_tab;
+            ca.tree_ok = b->d_tree_ok;
             ca.shared = b->d_shared;
             ca.gate_occ = b->d_gate_occ;
             ca.z_begin = b->d_z_begin;

@@ -907,17 +907,25 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     feats[:, 15] = (np.log10(np.maximum(scale, 1.0)) / 6.0)[tree_of_event]
     mlp = mlp or (ProposalMLP(device=device) if use_network else None)
     cap_e = cap[tree_of_event]
-    if defensive_proposal == "auto":  # cut sets where every tree takes them, modes otherwise
-        defensive_proposal = "cutsets" if all(cut_set_eligible(g) for g in graphs) else "modes"
-    cut = defensive_proposal == "cutsets"
+    eligible = np.array([cut_set_eligible(g) for g in graphs])
+    if defensive_proposal == "auto":  # per tree: cut sets where it takes them, mode proposals where not
+        defensive_proposal = "cutsets" if eligible.all() else ("modes" if not eligible.any() else "mixed")
+    mixed = defensive_proposal == "mixed"
+    cut = defensive_proposal in ("cutsets", "mixed")
     if ce_rounds is None:  # cut-set samples give near-ideal targets at once
-        ce_rounds = 1 if cut else 5
-    if cut:
-        bad = [k for k, g in enumerate(graphs) if not cut_set_eligible(g)]
+        ce_rounds = 1 if defensive_proposal == "cutsets" else 5
+    elig_e = eligible[tree_of_event]
+    if defensive_proposal == "cutsets":
+        bad = [k for k, g in enumerate(graphs) if not eligible[k]]
         if bad:
             raise ValueError(f"cut-set sampling needs trees of AND/OR/ATLEAST gates without negations and without "
                              f"gates read by several gates; trees {bad[:5]} are not")
         q_def = np.zeros((0, full.union.n_be))
+    elif mixed:  # mode proposals for the trees the cut-set component cannot draw, the main proposal
+        # again for the others (their rows follow it round by round)
+        q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
+                        np.maximum(cap_e, mode_cap)[None, :])
+        q_def[:, elig_e] = np.minimum(p * scale[tree_of_event], cap_e)[elig_e][None, :]
     elif defensive_proposal == "modes":
         q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
                         np.maximum(cap_e, mode_cap)[None, :])
@@ -927,7 +935,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     elif defensive_proposal == "probe":
         q_def = np.minimum(p * scale[tree_of_event], cap_e)[None, :]
     else:
-        raise ValueError("defensive_proposal must be 'cutsets', 'modes', 'approx' or 'probe'")
+        raise ValueError("defensive_proposal must be 'auto', 'cutsets', 'mixed', 'modes', 'approx' or 'probe'")
     n_comp = q_def.shape[0]
 
     # Events read by several gates: the cut-set component draws them first,
@@ -937,7 +945,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     # which stays as the floor, so that a cut set of several shared events
     # that the first samples under-weigh is still drawn), and then the cut set
     # on the tree conditioned on them.
-    shared_u = np.concatenate([shared_events(g) for g in graphs]) if cut else np.zeros(full.union.n_be, bool)
+    shared_u = (np.concatenate([shared_events(g) for g in graphs]) & elig_e if cut
+                else np.zeros(full.union.n_be, bool))
     has_shared = bool(shared_u.any())
 
     def z_thr(qv, smp=None):
@@ -974,10 +983,18 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     q = None
     t0 = time.perf_counter()
     for r in range(ce_rounds):
-        if q is None and cut:  # first round: cut-set samples alone
+        if q is None and cut and not mixed:  # first round: cut-set samples alone
             res = full.run(full.union.be_threshold, iteration=it, word_count=ce_words, ce=True,
                            words_cutset=ce_words, q_cutset=z_thr(r0) if has_shared else None)
             q = np.minimum(p * scale[tree_of_event], cap_e)
+            if has_shared:
+                q = np.where(shared_u, r0, q)
+        elif q is None and mixed:  # first round: the mode proposals and the cut-set component, half each
+            half = ce_words // 2
+            res = full.run(thr_def[0], iteration=it, word_count=ce_words, ce=True, q_defensive=thr_def,
+                           words_defensive=[half // n_comp + (c < half % n_comp) for c in range(n_comp)],
+                           words_cutset=ce_words - half, q_cutset=z_thr(r0) if has_shared else None)
+            q = np.where(elig_e, np.minimum(p * scale[tree_of_event], cap_e), q_def.mean(axis=0))
             if has_shared:
                 q = np.where(shared_u, r0, q)
         elif q is None:  # first round: the defensive mixture alone
@@ -1002,6 +1019,9 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         else:
             loss, q = float("nan"), target
         wall["train"] += time.perf_counter() - t1
+        if mixed:  # the cut-set trees' defensive rows follow their main proposal
+            q_def[:, elig_e] = q[elig_e][None, :]
+            thr_def = np.stack([full.proposal_thresholds(qc) for qc in q_def])
         est, rel = _rel95(res["samples"], res["sum_w"], res["sum_w2"])
         rounds.append({"phase": "ce", "round": r, "ms": res["kernel_ms"], "loss": loss,
                        "median_rel95": float(np.median(rel)), "trees_without_hits": int((res["hits"] == 0).sum())})
@@ -1062,7 +1082,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         checked[first] = True
         bad = first[(H[first] > 0) & (ess[first] < collapse_ratio * H[first]) & ~done[first]]
         if cut:  # its weights stay below S / pi: more samples, not plain sampling (hopeless at 1e-9)
-            bad = bad[:0]
+            bad = bad[~eligible[bad]]
         for k in bad:
             fallback[k] = True
             q_use[sl[k]] = p[sl[k]]

@@ -809,21 +809,34 @@ def _dag_cut_trees(n=3, n_be=36, n_gates=16, share=0.3, seeds=range(60), n_layer
     raise AssertionError("no trees with shared events generated")
 
 
+def _tree_with_shared_gates():
+    g = synth.generate(synth.TreeSpec(n_be=30, n_gates=14, mix={AND: 0.5, OR: 0.5}, p_range=(0.01, 0.2), seed=3,
+                                      n_layers=4, share_node_frac=0.3))
+    assert np.any(np.bincount(g.inputs, minlength=g.n_nodes)[g.n_be:] > 1)
+    return g
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("w_main,w_cut,zscale,n_be", [(0, 256, 12.0, 36), (300, 300, 12.0, 36), (0, 48, 1e6, 110)])
-def test_cut_set_component_with_shared_events_matches_cpu(oracle_mod, gpu, w_main, w_cut, zscale, n_be):
+@pytest.mark.parametrize("w_main,w_cut,zscale,n_be,mixed", [(0, 256, 12.0, 36, False), (300, 300, 12.0, 36, False),
+                                                            (0, 48, 1e6, 110, False), (200, 200, 12.0, 36, True)])
+def test_cut_set_component_with_shared_events_matches_cpu(oracle_mod, gpu, w_main, w_cut, zscale, n_be, mixed):
     """Trees whose shared nodes are basic events: the words after forcing,
     the hits, sum w, sum w^2 and CE numerators equal a CPU restatement of
     the component (shared events drawn from their own proposal, the cut set
     on the conditioned tree).  zscale 1e6 puts many shared events at 0.5, so
-    that samples exceed the pruning list and take the unpruned path."""
+    that samples exceed the pruning list and take the unpruned path.  mixed
+    adds a tree with a gate read by two gates, which the component cannot
+    draw: its samples there stay nominal (density p)."""
     from mcscram_b200.importance import BatchedImportanceSampler
     trees = _dag_cut_trees() if n_be < 100 else _dag_cut_trees(n=2, n_be=n_be, n_gates=n_be // 2, share=0.4, n_layers=5)
+    if mixed:
+        trees = trees[:2] + [_tree_with_shared_gates()] + trees[2:]
     it = 5
     with BatchedImportanceSampler(trees, chunk_words=256) as s:
         u, bb, roots = s.union, s.be_begin, s.roots
         p = u.quantised_probabilities()
-        shared = np.bincount(u.inputs, minlength=u.n_nodes)[: u.n_be] > 1
+        drawn = np.array([not (mixed and k == 2) for k in range(len(trees))])
+        shared = (np.bincount(u.inputs, minlength=u.n_nodes)[: u.n_be] > 1) & np.repeat(drawn, np.diff(bb))
         q = probability_threshold(np.minimum(p * 6.0, 0.5))
         qz = probability_threshold(np.where(shared, np.minimum(p * zscale, 0.5), p))
         W = w_main + w_cut
@@ -835,9 +848,11 @@ def test_cut_set_component_with_shared_events_matches_cpu(oracle_mod, gpu, w_mai
     nom[shared] = 0  # the forcing kernel draws the shared events itself
     v0 = u.with_thresholds(np.where(shared, 0, u.be_threshold).astype(np.uint64))
     S0, tab = _cut_tables(v0)
-    occ_range, occ_of = _occurrences(u, roots, shared)
+    occ_range, occ_of = _occurrences(u, roots[drawn], shared)
     seed = _mix64(((it << 32) ^ 0x5bd1e995) & M64)
     for k, root in enumerate(roots):
+        if not drawn[k]:
+            continue
         zlist = [(e, occ_of.get(e, [])) for e in range(int(bb[k]), int(bb[k + 1])) if shared[e]]
         b0 = _mix64(seed ^ (k << 32))
         for w in range(w_cut):
@@ -869,10 +884,13 @@ def test_cut_set_component_with_shared_events_matches_cpu(oracle_mod, gpu, w_mai
                 if not top[w, b]:
                     continue
                 x = bits[:, w, b]
-                leaf = lambda e: (1.0 if x[e] else 0.0) if shared[e] else S0[e]
-                s_z = _eval(u, int(root), leaf, lambda g: True, lambda g: S0[g])
-                n_cut = _count(u, x, int(root))
-                lw_cut = lw_z[w, b] + np.log(s_z) - np.log(n_cut)
+                if drawn[k]:
+                    leaf = lambda e: (1.0 if x[e] else 0.0) if shared[e] else S0[e]
+                    s_z = _eval(u, int(root), leaf, lambda g: True, lambda g: S0[g])
+                    n_cut = _count(u, x, int(root))
+                    lw_cut = lw_z[w, b] + np.log(s_z) - np.log(n_cut)
+                else:
+                    lw_cut = 0.0  # nominal samples: density p
                 if w_main:
                     lw = -np.logaddexp(np.log(w_main / W) - lw_main[w, b], np.log(w_cut / W) - lw_cut)
                 else:
@@ -957,3 +975,26 @@ def test_network_against_the_pipeline_without_it(gpu):
         assert np.all(np.abs(res.estimate - exact) <= 4 * se + 10 * exact ** 2), (net, res.estimate / exact)
         out[net] = np.median(res.rel_err95)
     print(f"median 95% relative error at 2^19 samples per tree: network {out[True]:.4g}, without {out[False]:.4g}")
+
+
+@pytest.mark.gpu
+def test_mixed_batch_chooses_the_defensive_proposal_per_tree(gpu):
+    """A batch of rare DAGs the cut-set component draws and rare trees with
+    gates read by two gates (which it cannot draw): "auto" gives the first
+    the cut-set component and the others mode proposals in the same passes,
+    and every estimate lies within 4 sigma of the exact BDD value."""
+    from oracle import oracle
+    from mcscram_b200.importance import batched_learned_is, cut_set_eligible
+    trees, exact = _small_dag_rare(3)
+    for seed in (7, 8):
+        g = synth.generate(synth.TreeSpec(n_be=120, n_gates=60, mix={AND: 0.5, OR: 0.4, ATLEAST: 0.1},
+                                          p_range=(1e-4, 1e-2), seed=seed, n_layers=6, atleast_n=(3, 4),
+                                          share_node_frac=0.15))
+        g = synth.calibrate_rare_approx(g, 1e-6)
+        assert not cut_set_eligible(g)
+        trees.append(g)
+        exact = np.append(exact, oracle.bdd_probability(g))
+    res = batched_learned_is(trees, target_rel_err=0.05, max_est_words=1 << 22)
+    se = res.estimate * res.rel_err95 / 1.96
+    assert np.all(np.abs(res.estimate - exact) <= 4 * se + 10 * exact ** 2), (res.estimate / exact, res.rel_err95)
+    assert res.converged.sum() >= len(trees) - 1

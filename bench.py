@@ -88,6 +88,8 @@ def parse_args():
     ap.add_argument("--bis-ce-rounds", type=int, default=0, help="CE rounds (0 = the driver's default)")
     ap.add_argument("--bis-ce-words", type=int, default=1 << 13, help="words per tree per CE round")
     ap.add_argument("--bis-est-words", type=int, default=1 << 12, help="words per tree of the first estimate round")
+    ap.add_argument("--bis-max-est-words", type=int, default=1 << 20,
+                    help="estimate words per tree at most (a tree not at 5 %% by then is reported unconverged)")
     ap.add_argument("--bis-train-steps", type=int, default=150)
     ap.add_argument("--bis-plain-trees", type=int, default=64, help="trees of the plain-rate measurement")
     ap.add_argument("--bis-mode-cap", type=float, default=0.5, help="cap of the defensive mode proposals")
@@ -455,7 +457,7 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
                            max_est_words=1 << 12, train_steps=5, workers=workers)
     if args.warmup:
         batched_learned_is(trees, target_rel_err=0.05, device=local, ce_rounds=args.bis_ce_rounds or None,
-                           ce_words=args.bis_ce_words, est_words=args.bis_est_words,
+                           ce_words=args.bis_ce_words, est_words=args.bis_est_words, max_est_words=args.bis_max_est_words,
                            train_steps=args.bis_train_steps, mode_cap=args.bis_mode_cap, workers=workers,
                            defensive_proposal=args.bis_defensive, defensive=args.bis_defensive_share,
                            use_network=not args.bis_no_network,
@@ -484,7 +486,7 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = batched_learned_is(trees, target_rel_err=0.05, device=local, ce_rounds=args.bis_ce_rounds or None,
-                             ce_words=args.bis_ce_words, est_words=args.bis_est_words,
+                             ce_words=args.bis_ce_words, est_words=args.bis_est_words, max_est_words=args.bis_max_est_words,
                              train_steps=args.bis_train_steps, mode_cap=args.bis_mode_cap, workers=workers,
                              defensive_proposal=args.bis_defensive, defensive=args.bis_defensive_share,
                              use_network=not args.bis_no_network,

@@ -223,6 +223,21 @@ def cut_set_eligible(g: FlatGraph) -> bool:
     return bool(np.all(ok_ops) and np.all(k_ok) and np.all(g.gate_neg_count == 0) and np.all(fan[g.n_be:] <= 1))
 
 
+def shared_seed(g: FlatGraph) -> np.ndarray:
+    """A generous estimate of P(x_i = 1 | top) for the basic events read by
+    several gates (others: their p): the largest of cut_inclusion (a shared
+    event's m leaves at p^(1/m)), the same inclusion with the leaves at p,
+    and the independence approximation's conditional marginal.  The first
+    weighs right a cut set that uses all of a shared event's leaves and
+    over-weighs one that uses fewer, the second the other way round."""
+    from .graph import probability_threshold
+    p = g.quantised_probabilities()
+    fan = np.maximum(np.bincount(g.inputs, minlength=g.n_nodes)[: g.n_be], 1)
+    plain = g.with_thresholds(probability_threshold(np.clip(p ** fan, 0.0, 1.0)))
+    est = np.maximum(np.maximum(cut_inclusion(g), cut_inclusion(plain)), approximate_importance(g)[1])
+    return np.where(fan > 1, est, p)
+
+
 def cut_inclusion(g: FlatGraph) -> np.ndarray:
     """Expected number of times each basic event is picked by the cut-set
     descent on the graph read as a tree, every leaf of an event read by m
@@ -964,14 +979,20 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
 
     r0 = None
     r_floor = np.zeros(full.union.n_be)
-    if has_shared:  # seed: the larger of the cut-set descent's inclusion and the approximate conditional
+    explore = np.zeros(full.union.n_be)
+    if has_shared:  # seed: shared_seed, half of which stays as a floor; exploration in the first round
         r0 = p.copy()
         for k, g in enumerate(graphs):
             m = shared_u[sl[k]]
             if m.any():
-                inc = np.minimum(cut_inclusion(g)[m], 0.9)
+                inc = np.minimum(shared_seed(g)[m], 0.9)
                 r_floor[sl[k]][m] = 0.5 * inc
                 r0[sl[k]][m] = np.clip(inc, p[sl[k]][m], 0.9)
+                # every shared event of the tree at least at 2 / (its count): pairs of them that
+                # the seeds miss are drawn together often enough for the first targets to see them
+                explore[sl[k]][m] = min(0.5, 2.0 / m.sum())
+        if ce_rounds is None or ce_rounds < 2:
+            ce_rounds = 2
 
     def def_words(w):  # words per defensive component
         return max(1, int(round(defensive * w / n_comp))) if defensive > 0 and n_comp else 0
@@ -985,7 +1006,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     for r in range(ce_rounds):
         if q is None and cut and not mixed:  # first round: cut-set samples alone
             res = full.run(full.union.be_threshold, iteration=it, word_count=ce_words, ce=True,
-                           words_cutset=ce_words, q_cutset=z_thr(r0) if has_shared else None)
+                           words_cutset=ce_words, q_cutset=z_thr(np.maximum(r0, explore)) if has_shared else None)
             q = np.minimum(p * scale[tree_of_event], cap_e)
             if has_shared:
                 q = np.where(shared_u, r0, q)
@@ -993,7 +1014,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             half = ce_words // 2
             res = full.run(thr_def[0], iteration=it, word_count=ce_words, ce=True, q_defensive=thr_def,
                            words_defensive=[half // n_comp + (c < half % n_comp) for c in range(n_comp)],
-                           words_cutset=ce_words - half, q_cutset=z_thr(r0) if has_shared else None)
+                           words_cutset=ce_words - half,
+                           q_cutset=z_thr(np.maximum(r0, explore)) if has_shared else None)
             q = np.where(elig_e, np.minimum(p * scale[tree_of_event], cap_e), q_def.mean(axis=0))
             if has_shared:
                 q = np.where(shared_u, r0, q)

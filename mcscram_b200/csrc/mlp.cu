@@ -124,9 +124,11 @@ __device__ __forceinline__ void frag_b_t(uint32_t b[2], const bf16 *B, int ldb, 
     ldsm_x2_trans(b, B + (k0 + row + 8 * tile) * ldb + n0);
 }
 
+// ReLU masks are read back from the BF16 activations (h > 0); a positive
+// pre-activation rounds to a positive BF16 value unless it is below the
+// smallest BF16 subnormal's half.
 struct Smem {
-    bf16 w1t[kHid * kLdX];    // W1t[out][in]
-    bf16 w2t[kHid * kLd];     // W2t[out][in]
+    bf16 w1[kIn * kLd];       // W1[in][out]
     bf16 w2[kHid * kLd];      // W2[in][out]
     bf16 w3t[8 * kLd];        // row 0 = W3
     bf16 x[kRows * kLdX];     // the tile's features, row-major
@@ -134,12 +136,12 @@ struct Smem {
     bf16 h2[kRows * kLd];
     bf16 dh2[kRows * kLd];    // gradients of the pre-activations, row-major
     bf16 dh1[kRows * kLd];
-    uint8_t m1[kRows * kHid];  // ReLU masks
-    uint8_t m2[kRows * kHid];
     float b1[kHid], b2[kHid], w3[kHid];
     float dz[kRows];
     float loss;
 };
+
+__device__ __forceinline__ bool relu_on(bf16 h) { return __bfloat162float(h) > 0.f; }
 
 // Forward for the CTA's rows; writes h1/h2 and the masks and returns z for
 // row r (valid in lanes with (lane & 3) == 0: rows g and g + 8).
@@ -154,7 +156,7 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
         for (int nt = 0; nt < kHid / 8; ++nt) {
             float c[4] = {0.f, 0.f, 0.f, 0.f};
             uint32_t b[2];
-            frag_b(b, s.w1t, kLdX, nt * 8, 0, lane);
+            frag_b_t(b, s.w1, kLd, nt * 8, 0, lane);
             mma16816(c, a, b);
             const int col = nt * 8 + 2 * t;
 #pragma unroll
@@ -162,7 +164,6 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
                 const int r = m0 + g + (j >= 2 ? 8 : 0), cc = col + (j & 1);
                 const float v = c[j] + s.b1[cc];
                 s.h1[r * kLd + cc] = __float2bfloat16(v > 0.f ? v : 0.f);
-                s.m1[r * kHid + cc] = v > 0.f;
             }
         }
     }
@@ -175,7 +176,7 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
         for (int kt = 0; kt < kHid / 16; ++kt) {
             uint32_t a[4], b[2];
             frag_a(a, s.h1, kLd, m0, kt * 16, lane);
-            frag_b(b, s.w2t, kLd, nt * 8, kt * 16, lane);
+            frag_b_t(b, s.w2, kLd, nt * 8, kt * 16, lane);
             mma16816(c, a, b);
         }
         const int col = nt * 8 + 2 * t;
@@ -184,7 +185,6 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
             const int r = m0 + g + (j >= 2 ? 8 : 0), cc = col + (j & 1);
             const float v = c[j] + s.b2[cc];
             s.h2[r * kLd + cc] = __float2bfloat16(v > 0.f ? v : 0.f);
-            s.m2[r * kHid + cc] = v > 0.f;
         }
     }
     __syncwarp();
@@ -202,11 +202,11 @@ __device__ void forward_rows(Smem &s, int warp, int lane, float b3, float z_out[
 }
 
 __device__ void load_weights(Smem &s, const bf16 *__restrict__ pack, const float *__restrict__ params) {
-    for (int i = threadIdx.x; i < kHid * kIn; i += kThreads) s.w1t[(i / kIn) * kLdX + i % kIn] = pack[kPackW1t + i];
-    for (int i = threadIdx.x; i < kHid * kHid; i += kThreads) {
-        s.w2t[(i / kHid) * kLd + i % kHid] = pack[kPackW2t + i];
-        s.w2[(i / kHid) * kLd + i % kHid] = pack[kPackW2 + i];
+    for (int i = threadIdx.x; i < kIn * kHid; i += kThreads) {  // W1[f][h] = W1t[h][f]
+        const int f = i / kHid, h = i % kHid;
+        s.w1[f * kLd + h] = pack[kPackW1t + h * kIn + f];
     }
+    for (int i = threadIdx.x; i < kHid * kHid; i += kThreads) s.w2[(i / kHid) * kLd + i % kHid] = pack[kPackW2 + i];
     for (int i = threadIdx.x; i < 8 * kHid; i += kThreads) s.w3t[(i / kHid) * kLd + i % kHid] = pack[kPackW3t + i];
     for (int i = threadIdx.x; i < kHid; i += kThreads) {
         s.b1[i] = params[kOffB1 + i];
@@ -306,14 +306,14 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ 
         // dH2 = dz W3^T masked
         for (int i = threadIdx.x; i < kRows * kHid; i += kThreads) {
             const int r = i / kHid, c = i % kHid;
-            s.dh2[r * kLd + c] = __float2bfloat16(s.m2[i] ? s.dz[r] * s.w3[c] : 0.f);
+            s.dh2[r * kLd + c] = __float2bfloat16(relu_on(s.h2[r * kLd + c]) ? s.dz[r] * s.w3[c] : 0.f);
         }
         __syncthreads();
         if (threadIdx.x < kHid) {
             const int c = threadIdx.x;
             for (int r = 0; r < kRows; ++r) {
                 gw3 += __bfloat162float(s.h2[r * kLd + c]) * s.dz[r];
-                gb2 += s.m2[r * kHid + c] ? s.dz[r] * s.w3[c] : 0.f;
+                gb2 += relu_on(s.h2[r * kLd + c]) ? s.dz[r] * s.w3[c] : 0.f;
             }
         } else if (threadIdx.x == kHid) {
             for (int r = 0; r < kRows; ++r) gb3 += s.dz[r];
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const bf16 *__restrict__ 
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int r = m0 + g + (j >= 2 ? 8 : 0), cc = col + (j & 1);
-                s.dh1[r * kLd + cc] = __float2bfloat16(s.m1[r * kHid + cc] ? c[j] : 0.f);
+                s.dh1[r * kLd + cc] = __float2bfloat16(relu_on(s.h1[r * kLd + cc]) ? c[j] : 0.f);
             }
         }
         __syncthreads();

@@ -969,6 +969,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             return None
         smp = full if smp is None else smp
         lo = np.maximum(p_of(smp), r_floor if smp is full else np.concatenate([r_floor[sl[k]] for k in members]))
+        lo = np.maximum(lo, z_target if smp is full else np.concatenate([z_target[sl[k]] for k in members]))
         return smp.proposal_thresholds(np.where(shared_u_of(smp), np.clip(qv, lo, 0.9), p_of(smp)))
 
     def shared_u_of(smp):
@@ -979,6 +980,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
 
     r0 = None
     r_floor = np.zeros(full.union.n_be)
+    z_target = np.zeros(full.union.n_be)  # the shared events' own cross-entropy targets
     explore = np.zeros(full.union.n_be)
     if has_shared:  # seed: shared_seed, half of which stays as a floor; exploration in the first round
         r0 = p.copy()
@@ -1034,6 +1036,9 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         target = np.where(hit, res["ce_num"] / np.where(hit, sw, 1.0), q)
         target = np.clip(target, 1e-7, cap_e)
         target = smoothing * target + (1.0 - smoothing) * q
+        if has_shared:  # the cut-set component's shared events follow their own targets (the network
+            # smooths across events with alike features and can miss one tree's particular pair)
+            z_target = np.where(shared_u, np.maximum(z_target, target) if r > 0 else target, z_target)
         t1 = time.perf_counter()
         if use_network:
             loss = _train_shared(mlp, feats, target.astype(np.float32), train_steps, lr, weights=row_w)

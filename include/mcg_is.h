@@ -103,6 +103,21 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_threshold, uint32
                             const uint64_t *q_cutset, uint32_t iteration, uint64_t word_begin, uint64_t word_count,
                             double *tree_sums, double *ce_num, double *kernel_ms);
 
+/* Host only.  For the tree rooted at `root` (AND / OR / ATLEAST /
+ * pass-through gates without complemented inputs, each gate read by one gate
+ * at most; basic events may be read by several): *p_top = its cut-set sum S
+ * (event p = threshold / 2^32; AND product; OR sum; ATLEAST k-th elementary
+ * symmetric sum), every basic event counted once per product however many of
+ * its leaves it covers, and posterior[e] ~ P(x_e = 1 | top) = p_e S(top |
+ * x_e = 1) / S for every event e read by several gates (-1 for the others).
+ * S is the rare-event approximation of P(top) (the sum over cut sets).  Below
+ * the lowest common ancestor of a shared event's leaves a node's value is a
+ * polynomial in that event's indicator; more than max_terms monomials at one
+ * gate (0: 4096) gives MCG_ERR_INVALID.  Seeds the cut-set component's
+ * proposal for shared events (no reference counterpart). */
+mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_t root, uint64_t max_terms, double *p_top,
+                                 double *posterior);
+
 /* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
  * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32
  * accumulation), FP32 master weights and Adam state.  The gradient runs in

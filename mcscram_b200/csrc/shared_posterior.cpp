@@ -1,0 +1,231 @@
+// shared_posterior.cpp -- the cut-set sum of a tree with shared basic events
+// and its shared events' conditional probabilities (mcg_shared_posteriors in
+// include/mcg_is.h).
+//
+// For a tree of AND / OR / ATLEAST / pass-through gates (each gate read by one
+// gate at most) the cut-set sum S (event: p; AND: product; OR: sum; ATLEAST
+// k: k-th elementary symmetric sum) approximates P(top) for rare events.  A
+// basic event read by several gates must count once in a product, not once per
+// leaf: below the lowest common ancestor (LCA) of its leaves a node's value is
+// kept as a polynomial in the indicator z_i of each such "open" event (every
+// product reduces z_i^2 to z_i), and at the LCA z_i is replaced by p_i (the
+// polynomial is then affine in z_i, so this is its expectation).  S(top) is
+// the constant left at the top.  P(z_i = 1 | top) ~ p_i S(top | z_i = 1) / S,
+// where S(top | z_i = 1) replaces z_i by 1 at its LCA; only the gates above
+// that LCA change, so each shared event costs one pass up its path.
+#include <algorithm>
+#include <cstdint>
+#include <iterator>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "error.hpp"
+#include "mcg.h"
+#include "mcg_is.h"
+
+namespace {
+
+using Mono = std::vector<uint32_t>;  // sorted shared-event ids
+using Poly = std::map<Mono, double>;
+
+struct PolyLimit {
+    size_t max_terms;
+    bool over = false;
+};
+
+void add_into(Poly &dst, const Poly &src, double scale = 1.0) {
+    for (const auto &t : src) dst[t.first] += scale * t.second;
+}
+
+Mono mono_union(const Mono &a, const Mono &b) {
+    Mono out;
+    out.reserve(a.size() + b.size());
+    std::set_union(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(out));
+    return out;
+}
+
+Poly mul(const Poly &a, const Poly &b, PolyLimit &lim) {
+    Poly out;
+    for (const auto &x : a)
+        for (const auto &y : b) {
+            out[mono_union(x.first, y.first)] += x.second * y.second;
+            if (out.size() > lim.max_terms) {
+                lim.over = true;
+                return out;
+            }
+        }
+    return out;
+}
+
+Poly constant(double c) { return Poly{{Mono{}, c}}; }
+
+// z_i := v in every monomial that holds i
+Poly substitute(const Poly &f, uint32_t i, double v) {
+    Poly out;
+    for (const auto &t : f) {
+        auto it = std::lower_bound(t.first.begin(), t.first.end(), i);
+        if (it != t.first.end() && *it == i) {
+            Mono m = t.first;
+            m.erase(m.begin() + (it - t.first.begin()));
+            out[m] += v * t.second;
+        } else {
+            out[t.first] += t.second;
+        }
+    }
+    return out;
+}
+
+struct Tree {
+    const mcg_graph_desc &g;
+    uint32_t nb;
+    std::vector<uint32_t> parent;                 // per node: reading gate, or kNone
+    std::vector<char> shared;                     // per basic event
+    std::vector<double> p;                        // per basic event
+    std::vector<std::vector<uint32_t>> closes;    // per gate: shared events whose LCA it is
+    std::vector<uint32_t> lca;                    // per basic event (shared)
+    std::vector<Poly> value;                      // per gate: its polynomial after closing
+};
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// The gate's polynomial from its children's (child(x) gives a child's), before closing.
+template <class Child>
+Poly combine(const Tree &t, uint32_t gate, Child child, PolyLimit &lim) {
+    const mcg_graph_desc &g = t.g;
+    const uint32_t j = gate - t.nb;
+    const uint32_t op = g.gate_op[j], n = g.gate_in_count[j], k = g.gate_k[j] & 0xFFu;
+    const uint32_t *in = g.inputs + g.gate_in_begin[j];
+    if (op == MCG_AND) {
+        Poly acc = constant(1.0);
+        for (uint32_t c = 0; c < n && !lim.over; ++c) acc = mul(acc, child(in[c]), lim);
+        return acc;
+    }
+    if (op == MCG_OR) {
+        Poly acc;
+        for (uint32_t c = 0; c < n; ++c) add_into(acc, child(in[c]));
+        return acc;
+    }
+    if (op == MCG_ATLEAST) {  // E[r] = e_r of the children so far
+        std::vector<Poly> E(k + 1);
+        E[0] = constant(1.0);
+        for (uint32_t c = 0; c < n && !lim.over; ++c) {
+            const Poly v = child(in[c]);
+            for (int r = (int)k; r >= 1 && !lim.over; --r) add_into(E[r], mul(E[r - 1], v, lim));
+        }
+        return k == 0 ? constant(1.0) : E[k];
+    }
+    return n ? child(in[n - 1]) : Poly{};  // pass-through
+}
+
+Poly leaf(const Tree &t, uint32_t x) {
+    if (t.shared[x]) return Poly{{Mono{x}, 1.0}};
+    return constant(t.p[x]);
+}
+
+Poly close_all(const Tree &t, uint32_t gate, Poly f, uint32_t keep = kNone, double keep_value = 0.0) {
+    for (uint32_t i : t.closes[gate - t.nb]) f = substitute(f, i, i == keep ? keep_value : t.p[i]);
+    return f;
+}
+
+double constant_term(const Poly &f) {
+    auto it = f.find(Mono{});
+    return it == f.end() ? 0.0 : it->second;
+}
+
+}  // namespace
+
+extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_t root, uint64_t max_terms,
+                                            double *p_top, double *posterior) {
+    mcg::clear_error();
+    if (!graph || !p_top || !posterior) return mcg::fail(MCG_ERR_INVALID, "NULL argument");
+    const mcg_graph_desc &g = *graph;
+    const uint32_t nb = g.n_be, nn = g.n_be + g.n_gates;
+    if (root >= nn) return mcg::fail(MCG_ERR_INVALID, "root out of range");
+    Tree t{g, nb, std::vector<uint32_t>(nn, kNone), std::vector<char>(nb, 0), std::vector<double>(nb, 0.0),
+           std::vector<std::vector<uint32_t>>(g.n_gates), std::vector<uint32_t>(nb, kNone),
+           std::vector<Poly>(g.n_gates)};
+    for (uint32_t i = 0; i < nb; ++i) {
+        const uint64_t th = g.be_threshold[i];
+        t.p[i] = th >= (1ull << 32) ? 1.0 : (double)th / 4294967296.0;
+    }
+    // the gates and leaves below the root, each gate read once
+    std::vector<std::vector<uint32_t>> leaf_parents(nb);
+    std::vector<uint32_t> order;  // gates below the root, children before parents
+    if (root >= nb) {
+        std::vector<std::pair<uint32_t, uint32_t>> st{{root, 0}};
+        while (!st.empty()) {
+            auto &top = st.back();
+            const uint32_t j = top.first - nb;
+            const uint32_t op = g.gate_op[j];
+            if (top.second == 0 && (g.gate_neg_count[j] ||
+                                    !(op == MCG_AND || op == MCG_OR || op == MCG_ATLEAST || op == MCG_NULL)))
+                return mcg::fail(MCG_ERR_INVALID, "AND/OR/ATLEAST/pass-through gates without complemented inputs "
+                                                  "only; gate " + std::to_string(j) + " is not one");
+            if (op == MCG_ATLEAST && (g.gate_k[j] & 0xFFu) > 64)
+                return mcg::fail(MCG_ERR_INVALID, "ATLEAST threshold above 64");
+            if (top.second < g.gate_in_count[j]) {
+                const uint32_t x = g.inputs[g.gate_in_begin[j] + top.second++];
+                if (x >= top.first) return mcg::fail(MCG_ERR_INVALID, "gate input not below the gate");
+                if (x < nb) {
+                    leaf_parents[x].push_back(top.first);
+                } else {
+                    if (t.parent[x] != kNone)
+                        return mcg::fail(MCG_ERR_INVALID, "gate " + std::to_string(x - nb) +
+                                                              " is read by several gates");
+                    t.parent[x] = top.first;
+                    st.push_back({x, 0});
+                }
+            } else {
+                order.push_back(top.first);
+                st.pop_back();
+            }
+        }
+    }
+    std::vector<uint32_t> depth(nn, 0);
+    for (auto it = order.rbegin(); it != order.rend(); ++it)
+        depth[*it] = t.parent[*it] == kNone ? 0 : depth[t.parent[*it]] + 1;
+    auto lca2 = [&](uint32_t a, uint32_t b) {
+        while (depth[a] > depth[b]) a = t.parent[a];
+        while (depth[b] > depth[a]) b = t.parent[b];
+        while (a != b) a = t.parent[a], b = t.parent[b];
+        return a;
+    };
+    for (uint32_t i = 0; i < nb; ++i) {
+        if (leaf_parents[i].size() < 2) continue;
+        t.shared[i] = 1;
+        uint32_t l = leaf_parents[i][0];
+        for (size_t q = 1; q < leaf_parents[i].size(); ++q) l = lca2(l, leaf_parents[i][q]);
+        t.lca[i] = l;
+        t.closes[l - nb].push_back(i);
+    }
+    PolyLimit lim{max_terms ? (size_t)max_terms : (size_t)4096};
+    auto child_value = [&](uint32_t x) -> Poly { return x < nb ? leaf(t, x) : t.value[x - nb]; };
+    for (uint32_t v : order) {
+        t.value[v - nb] = close_all(t, v, combine(t, v, child_value, lim));
+        if (lim.over)
+            return mcg::fail(MCG_ERR_INVALID, "more than " + std::to_string(lim.max_terms) +
+                                                  " terms: too many shared events open below one gate");
+    }
+    const double S = root < nb ? t.p[root] : constant_term(t.value[root - nb]);
+    *p_top = S;
+    for (uint32_t i = 0; i < nb; ++i) posterior[i] = -1.0;
+    if (!(S > 0.0)) return MCG_OK;
+    for (uint32_t i = 0; i < nb; ++i) {
+        if (!t.shared[i]) continue;
+        // S(top | z_i = 1): z_i := 1 at its LCA, then the gates above it again
+        uint32_t v = t.lca[i];
+        Poly f = close_all(t, v, combine(t, v, child_value, lim), i, 1.0);
+        while (t.parent[v] != kNone && !lim.over) {
+            const uint32_t u = t.parent[v], changed = v;
+            const Poly fv = f;
+            f = close_all(t, u, combine(t, u, [&](uint32_t x) -> Poly {
+                return x == changed ? fv : child_value(x);
+            }, lim));
+            v = u;
+        }
+        if (lim.over) return mcg::fail(MCG_ERR_INVALID, "term limit exceeded");
+        posterior[i] = std::min(1.0, t.p[i] * constant_term(f) / S);
+    }
+    return MCG_OK;
+}

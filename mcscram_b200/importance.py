@@ -60,6 +60,8 @@ _capi.register_signatures({
                                    C.c_uint64, C.c_uint64, _dp, _dp, _dp]),
     "mcg_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_vp)]),
     "mcg_mlp_train_time": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "mcg_shared_posteriors": (C.c_int, [C.POINTER(_capi.GraphDesc), C.c_uint32, C.c_uint64, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double)]),
     "mcg_mlp_destroy": (C.c_int, [_vp]),
     "mcg_mlp_set_params": (C.c_int, [_vp, _fp]),
     "mcg_mlp_get_params": (C.c_int, [_vp, _fp]),
@@ -221,6 +223,23 @@ def cut_set_eligible(g: FlatGraph) -> bool:
     k_ok = np.where(g.gate_op == ATLEAST, (g.gate_k & 0xFF) <= 8, True)
     fan = np.bincount(g.inputs, minlength=g.n_nodes)
     return bool(np.all(ok_ops) and np.all(k_ok) and np.all(g.gate_neg_count == 0) and np.all(fan[g.n_be:] <= 1))
+
+
+def shared_posteriors(g: FlatGraph, max_terms: int = 4096):
+    """(S, posterior): the tree's cut-set sum with every shared event counted
+    once per product, and P(x_e = 1 | top) ~ p_e S(top | x_e = 1) / S for the
+    events read by several gates (-1 for the others), from
+    mcg_shared_posteriors; None when a gate holds more than max_terms
+    monomials (too many shared events open below it) or the graph does not
+    qualify."""
+    lib = _capi.load()
+    view = _capi.GraphView(g)
+    post = np.zeros(max(g.n_be, 1), dtype=np.float64)
+    s = C.c_double()
+    rc = lib.mcg_shared_posteriors(C.byref(view.desc), int(g.root), max_terms, C.byref(s), _p(post, C.c_double))
+    if rc != _capi.MCG_OK:
+        return None
+    return float(s.value), post[: g.n_be]
 
 
 def shared_seed(g: FlatGraph) -> np.ndarray:
@@ -749,10 +768,17 @@ class BatchedIsResult:
 def _prepare_one(g: FlatGraph, n_modes: int, importance: bool):
     """Per-tree host inputs of the batched driver: features (the per-tree
     input 15 filled in later) and the uncapped mode proposals, from one
-    independence-approximation pass conditioned on the top and on each mode."""
+    independence-approximation pass conditioned on the top and on each mode;
+    and for a tree with events read by several gates whose gates are each read
+    once, their conditional probabilities given the top (shared_posteriors;
+    None when the tree has no shared event or they cannot be computed)."""
     pr, cond = approximate_importance(g, root=[g.root] + _mode_kids(g))
+    post = None
+    if cut_set_eligible(g) and shared_events(g).any():
+        r = shared_posteriors(g)
+        post = None if r is None else r[1]
     return (event_features(g, instance_scale=1.0, importance=importance, approx=(pr, cond[0])),
-            mode_proposals(g, n_modes, 1.0, approx=(pr, cond)))
+            mode_proposals(g, n_modes, 1.0, approx=(pr, cond)), post)
 
 
 def prepare_trees(graphs, n_modes: int = 4, importance: bool = True, workers=0):
@@ -918,7 +944,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         probe.close()
     wall["probe"] = time.perf_counter() - t0
     # 2. cross-entropy rounds with the shared network
-    feats = np.concatenate([f for f, _ in prepared])
+    feats = np.concatenate([pr[0] for pr in prepared])
     feats[:, 15] = (np.log10(np.maximum(scale, 1.0)) / 6.0)[tree_of_event]
     mlp = mlp or (ProposalMLP(device=device) if use_network else None)
     cap_e = cap[tree_of_event]
@@ -938,11 +964,11 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         q_def = np.zeros((0, full.union.n_be))
     elif mixed:  # mode proposals for the trees the cut-set component cannot draw, the main proposal
         # again for the others (their rows follow it round by round)
-        q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
+        q_def = np.clip(np.concatenate([pr[1] for pr in prepared], axis=1), 1e-7,
                         np.maximum(cap_e, mode_cap)[None, :])
         q_def[:, elig_e] = np.minimum(p * scale[tree_of_event], cap_e)[elig_e][None, :]
     elif defensive_proposal == "modes":
-        q_def = np.clip(np.concatenate([m for _, m in prepared], axis=1), 1e-7,
+        q_def = np.clip(np.concatenate([pr[1] for pr in prepared], axis=1), 1e-7,
                         np.maximum(cap_e, mode_cap)[None, :])
     elif defensive_proposal == "approx":
         q_def = np.concatenate([np.clip(approximate_importance(g)[1], 1e-7, cap[k])
@@ -982,18 +1008,25 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     r_floor = np.zeros(full.union.n_be)
     z_target = np.zeros(full.union.n_be)  # the shared events' own cross-entropy targets
     explore = np.zeros(full.union.n_be)
-    if has_shared:  # seed: shared_seed, half of which stays as a floor; exploration in the first round
+    if has_shared:
+        # seed: their conditional probabilities given the top (shared_posteriors), half of which
+        # stays as a floor; for a tree where those cannot be computed, shared_seed and an
+        # exploration round (every shared event at least at 2 / its count, so that pairs of them
+        # the seeds miss are drawn together often enough for the first targets to see them)
         r0 = p.copy()
+        needs_exploration = False
         for k, g in enumerate(graphs):
             m = shared_u[sl[k]]
-            if m.any():
-                inc = np.minimum(shared_seed(g)[m], 0.9)
-                r_floor[sl[k]][m] = 0.5 * inc
-                r0[sl[k]][m] = np.clip(inc, p[sl[k]][m], 0.9)
-                # every shared event of the tree at least at 2 / (its count): pairs of them that
-                # the seeds miss are drawn together often enough for the first targets to see them
+            if not m.any():
+                continue
+            post = prepared[k][2]
+            inc = np.minimum((post if post is not None else shared_seed(g))[m], 0.9)
+            r_floor[sl[k]][m] = 0.5 * inc
+            r0[sl[k]][m] = np.clip(inc, p[sl[k]][m], 0.9)
+            if post is None:
                 explore[sl[k]][m] = min(0.5, 2.0 / m.sum())
-        if ce_rounds is None or ce_rounds < 2:
+                needs_exploration = True
+        if needs_exploration and (ce_rounds is None or ce_rounds < 2):
             ce_rounds = 2
 
     def def_words(w):  # words per defensive component

@@ -168,14 +168,16 @@ def test_prepare_trees_on_an_executor_equals_serial():
     from concurrent.futures import ThreadPoolExecutor
 
     from mcscram_b200.importance import prepare_trees
-    trees = [synth.config5_instance(i) for i in range(4)]
+    trees = [synth.config5_instance(i) for i in range(3)] + [synth.config5_dag_instance(5)]
     serial = prepare_trees(trees, 4, True, 0)
     with ThreadPoolExecutor(max_workers=2) as ex:
         pooled = prepare_trees(trees, 4, True, ex)
         made = synth.config5_instances([1, 3], workers=ex)
-    for (f0, m0), (f1, m1) in zip(serial, pooled):
+    for (f0, m0, z0), (f1, m1, z1) in zip(serial, pooled):
         assert np.array_equal(f0, f1) and np.array_equal(m0, m1)
-    assert np.array_equal(made[1].be_threshold, trees[3].be_threshold)
+        assert (z0 is None) == (z1 is None) and (z0 is None or np.array_equal(z0, z1))
+    assert serial[0][2] is None and serial[3][2] is not None  # shared-event posteriors for the DAG only
+    assert np.array_equal(made[1].be_threshold, synth.config5_instance(3).be_threshold)
 
 
 def test_mode_proposals_condition_on_top_children():

@@ -234,13 +234,55 @@ __device__ __forceinline__ void count_init(CountFrame &f, uint32_t node, uint32_
     for (int r = 1; r <= kCutMaxK; ++r) f.dp[r] = 0.0;
 }
 
+// No memo: every entered gate is evaluated.
+struct NoMemo {
+    __device__ bool get(uint32_t, double &) const { return false; }
+    __device__ void put(uint32_t, double) {}
+};
+
+// Values of gates already evaluated for one sample (open addressing over
+// kMemoSlots node ids; when full, further values are simply not kept).
+constexpr int kMemoSlots = 32;
+struct GateMemo {
+    uint32_t key[kMemoSlots];
+    double val[kMemoSlots];
+    __device__ void clear() {
+#pragma unroll
+        for (int i = 0; i < kMemoSlots; ++i) key[i] = kNoNode;
+    }
+    __device__ bool get(uint32_t node, double &v) const {
+        uint32_t h = (node * 2654435761u) >> 27;
+        for (int i = 0; i < kMemoSlots; ++i, h = (h + 1) & (kMemoSlots - 1)) {
+            if (key[h] == node) {
+                v = val[h];
+                return true;
+            }
+            if (key[h] == kNoNode) return false;
+        }
+        return false;
+    }
+    __device__ void put(uint32_t node, double v) {
+        uint32_t h = (node * 2654435761u) >> 27;
+        for (int i = 0; i < kMemoSlots; ++i, h = (h + 1) & (kMemoSlots - 1)) {
+            if (key[h] == kNoNode || key[h] == node) {
+                key[h] = node;
+                val[h] = v;
+                return;
+            }
+        }
+    }
+};
+
 // The AND / OR / ATLEAST recursion (product, sum, k-th elementary symmetric
 // sum) from gate `root`: a basic event x gives leaf(x), a gate x is entered
-// when enter(x) holds and gives other(x) otherwise.  Returns -1 when the
-// tree is deeper than the frames hold.
-template <class Leaf, class Enter, class Other>
+// when enter(x) holds and gives other(x) otherwise; memo holds values of
+// gates evaluated before (the same recursion gives the same value).  Returns
+// -1 when the tree is deeper than the frames hold.
+template <class Leaf, class Enter, class Other, class Memo = NoMemo>
 __device__ double tree_eval(uint32_t root, const uint4 *gate, const uint32_t *inputs, uint32_t n_be, Leaf leaf,
-                            Enter enter, Other other) {
+                            Enter enter, Other other, Memo *memo = nullptr) {
+    double known;
+    if (memo && memo->get(root, known)) return known;
     CountFrame st[kCountDepth];
     int sp = 1;
     count_init(st[0], root, gate[root - n_be].x & 0xFFu);
@@ -258,12 +300,17 @@ __device__ double tree_eval(uint32_t root, const uint4 *gate, const uint32_t *in
                 count_deliver(f, op, kk, other(x));
                 continue;
             }
+            if (memo && memo->get(x, known)) {
+                count_deliver(f, op, kk, known);
+                continue;
+            }
             if (sp == kCountDepth) return -1.0;
             count_init(st[sp], x, gate[x - n_be].x & 0xFFu);
             ++sp;
             continue;
         }
         const double v = op == MCG_ATLEAST ? f.dp[kk] : f.acc;
+        if (memo) memo->put(f.node, v);
         if (--sp == 0) return v;
         const uint32_t pop = gate[st[sp - 1].node - n_be].x;
         count_deliver(st[sp - 1], pop & 0xFFu, (pop >> 8) & 0xFFu, v);
@@ -325,10 +372,12 @@ __global__ void __launch_bounds__(256) k_cut_force(CutArgs a) {
     };
     auto leaf = [&](uint32_t x) -> double { return a.shared[x] ? (z_of(a.z_index[x]) ? 1.0 : 0.0) : a.S[x]; };
     auto s0 = [&](uint32_t x) -> double { return a.S[x]; };
+    GateMemo memo;
+    memo.clear();
     auto sz = [&](uint32_t x) -> double {  // S_z of any node
         if (x < n_be) return leaf(x);
         if (!affected(x)) return a.S[x];
-        const double v = tree_eval(x, a.gate, a.inputs, n_be, leaf, affected, s0);
+        const double v = tree_eval(x, a.gate, a.inputs, n_be, leaf, affected, s0, &memo);
         if (v < 0.0) atomicOr(a.error, 4u);
         return v;
     };

@@ -980,23 +980,26 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     n_comp = q_def.shape[0]
 
     # Events read by several gates: the cut-set component draws them first,
-    # from r = the current proposal clipped to [max(p, floor), 0.9] (their
-    # conditional failure probability given the top is what it should
-    # approach; at the start cut_inclusion's generous estimate of it, half of
-    # which stays as the floor, so that a cut set of several shared events
-    # that the first samples under-weigh is still drawn), and then the cut set
-    # on the tree conditioned on them.
+    # from r = their conditional failure probability given the top (the
+    # product proposal's cross-entropy optimum): the posterior of
+    # shared_posteriors where it was computed, else the event's own
+    # cross-entropy target above a floor of half of shared_seed's generous
+    # estimate (so that a cut set of several shared events that the first
+    # samples under-weigh is still drawn), at most 0.9; then the cut set on
+    # the tree conditioned on them.
     shared_u = (np.concatenate([shared_events(g) for g in graphs]) & elig_e if cut
                 else np.zeros(full.union.n_be, bool))
     has_shared = bool(shared_u.any())
 
-    def z_thr(qv, smp=None):
+    def z_thr(rv, smp=None):  # thresholds of the cut-set component: r (per event of the union) on the shared events
         if not has_shared:
             return None
         smp = full if smp is None else smp
-        lo = np.maximum(p_of(smp), r_floor if smp is full else np.concatenate([r_floor[sl[k]] for k in members]))
-        lo = np.maximum(lo, z_target if smp is full else np.concatenate([z_target[sl[k]] for k in members]))
-        return smp.proposal_thresholds(np.where(shared_u_of(smp), np.clip(qv, lo, 0.9), p_of(smp)))
+        rs = rv if smp is full else np.concatenate([rv[sl[k]] for k in members])
+        return smp.proposal_thresholds(np.where(shared_u_of(smp), rs, p_of(smp)))
+
+    def r_now():  # the posterior where computed, else the event's own target above its floor
+        return np.where(post_fixed, r0, np.minimum(np.maximum(np.maximum(p, r_floor), z_target), 0.9))
 
     def shared_u_of(smp):
         return shared_u if smp is full else np.concatenate([shared_u[sl[k]] for k in members])
@@ -1004,16 +1007,21 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     def p_of(smp):
         return p if smp is full else np.concatenate([p[sl[k]] for k in members])
 
-    r0 = None
+    r0 = p.copy()
     r_floor = np.zeros(full.union.n_be)
     z_target = np.zeros(full.union.n_be)  # the shared events' own cross-entropy targets
     explore = np.zeros(full.union.n_be)
+    # Shared events of the trees whose posteriors were computed keep r = the posterior in every
+    # round: it is the cross-entropy optimum of their product proposal, and lifting the many
+    # shared events that hardly matter (posterior ~ p) above p, as noisy targets do, spreads
+    # log(p(z) / r(z)) over a range that grows with their number (sd ~ 11 over 1,665 such events
+    # at r ~ 7 p), which leaves the estimate to a few samples with few of them drawn.
+    post_fixed = np.zeros(full.union.n_be, dtype=bool)
     if has_shared:
         # seed: their conditional probabilities given the top (shared_posteriors), half of which
         # stays as a floor; for a tree where those cannot be computed, shared_seed and an
         # exploration round (every shared event at least at 2 / its count, so that pairs of them
         # the seeds miss are drawn together often enough for the first targets to see them)
-        r0 = p.copy()
         needs_exploration = False
         for k, g in enumerate(graphs):
             m = shared_u[sl[k]]
@@ -1023,6 +1031,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             inc = np.minimum((post if post is not None else shared_seed(g))[m], 0.9)
             r_floor[sl[k]][m] = 0.5 * inc
             r0[sl[k]][m] = np.clip(inc, p[sl[k]][m], 0.9)
+            post_fixed[sl[k]] = m & (post is not None)
             if post is None:
                 explore[sl[k]][m] = min(0.5, 2.0 / m.sum())
                 needs_exploration = True
@@ -1061,17 +1070,18 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         else:
             res = full.run(full.proposal_thresholds(q), iteration=it, word_count=ce_words, ce=True,
                            q_defensive=thr_def if def_words(ce_words) else None, words_defensive=def_words(ce_words),
-                           words_cutset=cut_words(ce_words), q_cutset=z_thr(q) if cut_words(ce_words) else None)
+                           words_cutset=cut_words(ce_words), q_cutset=z_thr(r_now()) if cut_words(ce_words) else None)
         it += 1
         gpu["ce"] += res["kernel_ms"]
         sw = res["sum_w"][tree_of_event]
         hit = sw > 0
         target = np.where(hit, res["ce_num"] / np.where(hit, sw, 1.0), q)
         target = np.clip(target, 1e-7, cap_e)
-        target = smoothing * target + (1.0 - smoothing) * q
         if has_shared:  # the cut-set component's shared events follow their own targets (the network
-            # smooths across events with alike features and can miss one tree's particular pair)
+            # smooths across events with alike features, which lifts the many that hardly matter
+            # and can miss one tree's particular pair)
             z_target = np.where(shared_u, np.maximum(z_target, target) if r > 0 else target, z_target)
+        target = smoothing * target + (1.0 - smoothing) * q
         t1 = time.perf_counter()
         if use_network:
             loss = _train_shared(mlp, feats, target.astype(np.float32), train_steps, lr, weights=row_w)
@@ -1120,7 +1130,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
         res = sampler.run(sampler.proposal_thresholds(qa), iteration=it, word_begin=0, word_count=words,
                           q_defensive=np.stack([sampler.proposal_thresholds(qc) for qc in qd]) if def_words(words)
                           else None, words_defensive=def_words(words), words_cutset=cut_words(words),
-                          q_cutset=z_thr(qa, sampler) if cut_words(words) else None)
+                          q_cutset=z_thr(r_now(), sampler) if cut_words(words) else None)
         it += 1
         gpu["estimate"] += res["kernel_ms"]
         used += words

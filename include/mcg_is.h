@@ -119,8 +119,8 @@ mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_t root, uin
                                  double *posterior);
 
 /* The proposal network: 16 features -> 64 -> 64 -> 1, ReLU, sigmoid output.
- * BF16 weights for the tensor-core products (mma.sync m16n8k16, FP32
- * accumulation), FP32 master weights and Adam state.  The gradient runs in
+ * BF16 weights for the tensor-core products (tcgen05.mma with FP32
+ * accumulators in tensor memory), FP32 master weights and Adam state.  The gradient runs in
  * persistent CTAs whose partial gradients are summed in a fixed order, so
  * the same rows give the same gradient bit for bit.  Parameter layout
  * (5,313 floats): W1[16][64], b1[64], W2[64][64], b2[64], W3[64], b3. */

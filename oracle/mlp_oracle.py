@@ -3,8 +3,10 @@
 Forward pass, weighted binary cross-entropy loss and its gradient for the
 16 -> 64 -> 64 -> 1 network (parameter layout W1[16][64], b1[64], W2[64][64],
 b2[64], W3[64], b3), in float64 numpy.  With bf16=True every operand the GPU
-kernels feed to the tensor cores (features, weights, hidden activations and
-the back-propagated hidden gradients) is first rounded to BF16
+kernels feed to the tensor cores (features, weights, hidden activations, the
+back-propagated hidden gradients and the output gradient dz, which the
+kernels multiply with the hidden activations to get dW3 and sum into the bias
+gradients on the tensor cores) is first rounded to BF16
 (round-to-nearest-even), so the only remaining difference from the kernels
 is FP32 versus FP64 accumulation.
 """
@@ -59,11 +61,10 @@ def loss_and_grad(params, X, t, w=None, bf=False):
     qc = np.clip(q, 1e-7, 1 - 1e-7)
     loss = float(-(ws * (t * np.log(qc) + (1 - t) * np.log(1 - qc))).sum())
     dz = ws * (q - t)
-    gW3 = h2.T @ dz
+    gW3 = h2.T @ r(dz)
     gb3 = dz.sum()
-    dh2 = (pre2 > 0) * np.outer(dz, W3)
+    dh2 = r((pre2 > 0) * np.outer(dz, W3))
     gb2 = dh2.sum(axis=0)
-    dh2 = r(dh2)
     gW2 = h1.T @ dh2
     dh1 = r((pre1 > 0) * (dh2 @ r(W2).T))
     gb1 = dh1.sum(axis=0)

@@ -131,8 +131,6 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
     MCG_CUDA(cudaGetDeviceProperties(&prop, b->device));
     b->ctas_per_sm = run.ctas_per_sm ? run.ctas_per_sm : 4u;
     if (b->ctas_per_sm < 2 || b->ctas_per_sm > 4) return mcg::fail(MCG_ERR_INVALID, "ctas_per_sm must be 2..4");
-    const size_t cap = std::min<size_t>(prop.sharedMemPerBlockOptin,
-                                        prop.sharedMemPerMultiprocessor / b->ctas_per_sm) - 1024;
     b->share = kShare;
     for (const auto &g : b->trees)
         for (size_t i = 0; i < g.gate_op.size(); ++i)
@@ -140,6 +138,16 @@ mcg_status setup(mcg_batch *b, const mcg_run_desc &run) {
                 if (g.gate_in_count[i] <= kShareAtleastMaxIn) b->atleast = true;
                 else b->share = 1;
             }
+    // What one of ctas_per_sm resident CTAs may take: the SM's shared memory
+    // shared out, less the per-block reservation and the kernel's static
+    // shared memory (its work-item slot), so that all of them stay resident.
+    cudaFuncAttributes fa{};
+    MCG_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(batch_kernel(b->ctas_per_sm, b->share,
+                                                                                     b->atleast))));
+    const size_t cap = std::min<size_t>(prop.sharedMemPerBlockOptin,
+                                        prop.sharedMemPerMultiprocessor / b->ctas_per_sm -
+                                            prop.reservedSharedMemPerBlock) -
+                       fa.sharedSizeBytes;
     // a slot holds one word per instance of a work item
     uint32_t budget = (uint32_t)(cap / (kThreads * sizeof(uint64_t) * b->share));
     if (run.smem_slots == MCG_SMEM_SLOTS_NONE) budget = 0;

@@ -105,6 +105,33 @@ def test_config2_windows_bit_exact(capi, oracle_mod, gpu, mode):
             assert np.array_equal(ones, expect), (wb, n)
 
 
+def test_config2_headline_pass(capi, oracle_mod, gpu):
+    """The benchmark's pass (pass 1 over words [0, 2^24) of the 5,000-event
+    tree, strip mode) checked without a full CPU pass: its tallies equal the
+    sum of the two half passes run by other engines (staged, fused), and
+    windows drawn across the whole range equal the oracle's."""
+    g = synth.config2()
+    W = 1 << 24
+    with engine(capi, g, mode=capi.MODE_STRIP) as e:
+        e.run(1, 1, 0, W)
+        full, total = e.tallies()
+        rng = np.random.default_rng(24)
+        for wb in sorted(int(x) for x in rng.integers(0, W - 512, 6)):
+            e.reset_tallies()
+            e.run(1, 1, wb, 512)
+            ones, _ = e.tallies()
+            assert np.array_equal(ones, oracle_mod.tallies(g, 1, 1, wb, 512)), wb
+    assert total == W * 64
+    with engine(capi, g, mode=capi.MODE_STAGED, layered_max_words=1 << 17) as st:
+        st.run(1, 1, 0, W // 2)
+        lo, _ = st.tallies()
+    with engine(capi, g, mode=capi.MODE_FUSED) as f:
+        f.run(1, 1, W // 2, W // 2)
+        hi, _ = f.tallies()
+    assert np.array_equal(full, lo + hi)
+    assert int(full.sum()) > 0
+
+
 def test_config2_fused_equals_layered_large(capi, gpu):
     g = synth.config2()
     W = 1 << 19

@@ -49,7 +49,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-is", action="store_true",
                     help="plain workload: leave out the learned-IS time to accuracy on the 1e-8 tree")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fused kernel CTAs per SM (0 = engine default)")
     ap.add_argument("--peak-words", type=int, default=1 << 22, help="words per register-only sampler launch")
     ap.add_argument("--mode", default="strip", choices=["fused", "staged", "layered", "strip"])
@@ -896,21 +896,26 @@ def main() -> int:
     # end to end: host descriptor -> engine (tables to HBM) -> one pass -> tallies to host
     e2e = None
     if args.e2e_steps > 0:
-        ts = []
+        ts, phases = [], []
         for i in range(args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            with _capi.Engine(g, **eng_kw) as e2:
-                e2.run(1, 1, word_begin, W)
-                ones, total = e2.tallies()
-            ts.append(time.perf_counter() - t0)
+            e2 = _capi.Engine(g, **eng_kw)
+            t1 = time.perf_counter()
+            e2.run(1, 1, word_begin, W)
+            ones, total = e2.tallies()
+            t2 = time.perf_counter()
+            e2.close()
+            t3 = time.perf_counter()
+            ts.append(t3 - t0)
+            phases.append({"create_s": t1 - t0, "pass_and_tallies_s": t2 - t1, "destroy_s": t3 - t2})
         if world > 1:
             ts = parallel.allreduce_max([max(ts)])
         e2e_s = statistics.median(ts)
         h2d = ((info["n_ops"] * 16 if args.mode == "fused" else 0) + g.n_be * 16 + g.n_gates * 20 +
                g.inputs.size * 4 + g.tally_nodes.size * 4)
         e2e = {"value": g.n_gates * samples / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(g.tally_nodes.size * 8), "seconds_per_step": e2e_s}
+               "d2h_bytes_per_step": int(g.tally_nodes.size * 8), "seconds_per_step": e2e_s, "steps": phases}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -82,6 +82,7 @@ def parse_args():
     ap.add_argument("--is-batch-words", type=int, default=1 << 20)
     ap.add_argument("--plain-words", type=int, default=1 << 23, help="words of the plain-MC rate measurement")
     ap.add_argument("--bis-trees", type=int, default=1024)
+    ap.add_argument("--bis-only", default="", help="comma-separated tree indices of the set to run instead")
     ap.add_argument("--bis-set", default="shared", choices=["shared", "read-once"],
                     help="rare-event trees with 20%% of their basic events read by two gates (exact values from "
                          "tests/golden/config5_dag_exact.json), or read-once trees (exact by recursion)")
@@ -437,6 +438,9 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
     workers = ProcessPoolExecutor(max_workers=n_workers, mp_context=mp.get_context("spawn"))
     t_gen = time.perf_counter()
     mine_idx = parallel.shard_items(args.bis_trees, world, rank)
+    if args.bis_only:  # a chosen subset of the set's trees (to profile the slowest ones)
+        only = [int(x) for x in args.bis_only.split(",")]
+        mine_idx = [only[i] for i in parallel.shard_items(len(only), world, rank)]
     dag = args.bis_set == "shared"
     trees = synth.config5_instances(mine_idx, workers=workers, shared=dag)
     t_gen = time.perf_counter() - t_gen
@@ -546,6 +550,10 @@ def run_bis(args, rank: int, world: int, local: int) -> int:
                    "median_abs_rel_err_vs_exact": float(np.median(err)), "max_abs_rel_err_vs_exact": float(err.max()),
                    "max_rel_err95": float(res.rel_err95.max()), "samples_total": int(res.samples.sum()),
                    "rounds": len(res.rounds), "converged_outside_3_sigma": int((res.converged & ~within3).sum()),
+                   "round_log": [[r["phase"], int(r.get("trees", r.get("trees_left", 0))), int(r.get("words", 0)),
+                                  round(float(r["ms"]), 1)] + ([[int(mine_idx[k]) for k in r["tree_ids"]]]
+                                                               if 0 < len(r.get("tree_ids", [])) < 8 else [])
+                                 for r in res.rounds],
                    "outside_3_sigma_rank0": worst},
             "plain": {"event_words_per_s": be_word_s, "measured_on_trees": len(sub), "measured_words": args.plain_words >> 6,
                       "measured_ms": plain_ms, "required_samples_total": float(n_req.sum()), "seconds": plain_s,

@@ -225,34 +225,48 @@ __device__ __forceinline__ void count_deliver(CountFrame &f, uint32_t op, uint32
     }
 }
 
-__device__ __forceinline__ void count_init(CountFrame &f, uint32_t node, uint32_t op) {
+// A frame for `node`; the k-subset sums dp[0 .. k] only for an ATLEAST gate
+// (the only connective that reads them).
+__device__ __forceinline__ void count_init(CountFrame &f, uint32_t node, uint32_t op, uint32_t kk) {
     f.node = node;
     f.j = 0;
     f.acc = op == MCG_AND ? 1.0 : 0.0;
-    f.dp[0] = 1.0;
-#pragma unroll
-    for (int r = 1; r <= kCutMaxK; ++r) f.dp[r] = 0.0;
+    if (op == MCG_ATLEAST) {
+        f.dp[0] = 1.0;
+        for (uint32_t r = 1; r <= kk && r <= (uint32_t)kCutMaxK; ++r) f.dp[r] = 0.0;
+    }
 }
 
 // No memo: every entered gate is evaluated.
 struct NoMemo {
-    __device__ bool get(uint32_t, double &) const { return false; }
+    __device__ bool get(uint32_t, double &) { return false; }
     __device__ void put(uint32_t, double) {}
 };
 
-// Values of gates already evaluated for one sample (open addressing over
-// kMemoSlots node ids; when full, further values are simply not kept).
-constexpr int kMemoSlots = 32;
+// Values of gates already evaluated for one sample: open addressing over
+// kMemoSlots node ids with at most kMemoProbes probes, so a full table costs
+// a few loads per lookup (a sample that sets many shared events evaluates
+// hundreds of gates); values that find no slot are simply not kept.  The
+// slots are cleared on first use, so samples that never evaluate a gate pay
+// nothing.
+constexpr int kMemoBits = 6;
+constexpr int kMemoSlots = 1 << kMemoBits;
+constexpr int kMemoProbes = 8;
 struct GateMemo {
     uint32_t key[kMemoSlots];
     double val[kMemoSlots];
-    __device__ void clear() {
+    bool ready = false;
+    __device__ void clear() { ready = false; }
+    __device__ void prepare() {
+        if (ready) return;
 #pragma unroll
         for (int i = 0; i < kMemoSlots; ++i) key[i] = kNoNode;
+        ready = true;
     }
-    __device__ bool get(uint32_t node, double &v) const {
-        uint32_t h = (node * 2654435761u) >> 27;
-        for (int i = 0; i < kMemoSlots; ++i, h = (h + 1) & (kMemoSlots - 1)) {
+    __device__ bool get(uint32_t node, double &v) {
+        prepare();
+        uint32_t h = (node * 2654435761u) >> (32 - kMemoBits);
+        for (int i = 0; i < kMemoProbes; ++i, h = (h + 1) & (kMemoSlots - 1)) {
             if (key[h] == node) {
                 v = val[h];
                 return true;
@@ -262,8 +276,9 @@ struct GateMemo {
         return false;
     }
     __device__ void put(uint32_t node, double v) {
-        uint32_t h = (node * 2654435761u) >> 27;
-        for (int i = 0; i < kMemoSlots; ++i, h = (h + 1) & (kMemoSlots - 1)) {
+        prepare();
+        uint32_t h = (node * 2654435761u) >> (32 - kMemoBits);
+        for (int i = 0; i < kMemoProbes; ++i, h = (h + 1) & (kMemoSlots - 1)) {
             if (key[h] == kNoNode || key[h] == node) {
                 key[h] = node;
                 val[h] = v;
@@ -285,7 +300,10 @@ __device__ double tree_eval(uint32_t root, const uint4 *gate, const uint32_t *in
     if (memo && memo->get(root, known)) return known;
     CountFrame st[kCountDepth];
     int sp = 1;
-    count_init(st[0], root, gate[root - n_be].x & 0xFFu);
+    {
+        const uint32_t g0 = gate[root - n_be].x;
+        count_init(st[0], root, g0 & 0xFFu, (g0 >> 8) & 0xFFu);
+    }
     for (;;) {
         CountFrame &f = st[sp - 1];
         const uint4 g = gate[f.node - n_be];
@@ -305,7 +323,10 @@ __device__ double tree_eval(uint32_t root, const uint4 *gate, const uint32_t *in
                 continue;
             }
             if (sp == kCountDepth) return -1.0;
-            count_init(st[sp], x, gate[x - n_be].x & 0xFFu);
+            {
+                const uint32_t gx = gate[x - n_be].x;
+                count_init(st[sp], x, gx & 0xFFu, (gx >> 8) & 0xFFu);
+            }
             ++sp;
             continue;
         }
@@ -404,11 +425,16 @@ __global__ void __launch_bounds__(256) k_cut_force(CutArgs a) {
             if (!cond) {
                 while (j + 1 < n && u >= tab[j]) ++j;
             } else {  // shares of S_z: the children's sum, then the first child whose cumulative share passes u
+                double cz[kCutMaxN];  // the children's S_z, kept from the sum (wider gates evaluate twice)
                 double tot = 0.0;
-                for (uint32_t c = 0; c < n; ++c) tot += sz(in[c]);
+                for (uint32_t c = 0; c < n; ++c) {
+                    const double v = sz(in[c]);
+                    if (c < (uint32_t)kCutMaxN) cz[c] = v;
+                    tot += v;
+                }
                 double cum = 0.0;
                 for (; j + 1 < n; ++j) {
-                    cum += sz(in[j]);
+                    cum += j < (uint32_t)kCutMaxN ? cz[j] : sz(in[j]);
                     if (u * tot < cum) break;
                 }
             }

@@ -781,6 +781,15 @@ def _prepare_one(g: FlatGraph, n_modes: int, importance: bool):
             mode_proposals(g, n_modes, 1.0, approx=(pr, cond)), post)
 
 
+def prepare_trees_async(graphs, n_modes: int, importance: bool, executor):
+    """Starts _prepare_one for every tree on an executor (the tasks are
+    submitted now) and returns a function that waits for the results."""
+    n = getattr(executor, "_max_workers", 1) or 1
+    results = executor.map(_prepare_one, graphs, [n_modes] * len(graphs), [importance] * len(graphs),
+                           chunksize=max(1, len(graphs) // (4 * n)))
+    return lambda: list(results)
+
+
 def prepare_trees(graphs, n_modes: int = 4, importance: bool = True, workers=0):
     """_prepare_one for every tree, in `workers` spawned processes when > 1,
     or on `workers` itself when it is an executor (a process pool kept across
@@ -883,7 +892,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
        and reported as a fallback.
     Every round draws fresh Philox counters (its own pass number).  The
     per-tree host inputs (features, mode proposals) are computed by
-    prepare_trees, in `workers` processes, unless given as `prepared`.
+    prepare_trees, in `workers` processes, unless given as `prepared`; when
+    `workers` is an executor they are computed while the probe runs.
     use_network=False takes the smoothed cross-entropy targets themselves as
     the next proposal (the method without the network, for comparison);
     importance_features=False leaves the independence-approximation inputs
@@ -895,8 +905,12 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     wall = {"features": 0.0, "probe": 0.0, "ce": 0.0, "train": 0.0, "estimate": 0.0, "rebuild": 0.0}
     rounds = []
     t0 = time.perf_counter()
+    collect = None
     if prepared is None:
-        prepared = prepare_trees(graphs, n_modes, importance_features, workers)
+        if hasattr(workers, "map"):  # a kept pool: the host inputs are computed while the probe runs
+            collect = prepare_trees_async(graphs, n_modes, importance_features, workers)
+        else:
+            prepared = prepare_trees(graphs, n_modes, importance_features, workers)
     wall["features"] = time.perf_counter() - t0
     t0 = time.perf_counter()
     full = BatchedImportanceSampler(graphs, device=device, chunk_words=chunk_words)
@@ -943,6 +957,10 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
     if probe is not full:
         probe.close()
     wall["probe"] = time.perf_counter() - t0
+    if collect is not None:  # what the host inputs still take after the probe
+        t0 = time.perf_counter()
+        prepared = collect()
+        wall["features"] += time.perf_counter() - t0
     # 2. cross-entropy rounds with the shared network
     feats = np.concatenate([pr[0] for pr in prepared])
     feats[:, 15] = (np.log10(np.maximum(scale, 1.0)) / 6.0)[tree_of_event]
@@ -1160,7 +1178,8 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             H[k] = 0
         converged |= done
         rounds.append({"phase": "estimate", "words": words, "trees": int(run_k.size), "ms": res["kernel_ms"],
-                       "converged": int(converged.sum()), "fallback": int(fallback.sum())})
+                       "converged": int(converged.sum()), "fallback": int(fallback.sum()),
+                       "tree_ids": [int(k) for k in run_k[:8]]})
         say(rounds[-1])
         active = np.nonzero(~converged & ~(fallback & (N >= plain_words * 64)))[0]
         words = min(words * 2, max(max_est_words - used, est_words))

@@ -249,7 +249,7 @@ struct NoMemo {
 // hundreds of gates); values that find no slot are simply not kept.  The
 // slots are cleared on first use, so samples that never evaluate a gate pay
 // nothing.
-constexpr int kMemoBits = 6;
+constexpr int kMemoBits = 8;
 constexpr int kMemoSlots = 1 << kMemoBits;
 constexpr int kMemoProbes = 8;
 struct GateMemo {

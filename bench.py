@@ -277,7 +277,7 @@ def run_ua(args, rank: int, world: int, local: int) -> int:
     torch.cuda.set_device(local)
     trees = synth.config3(args.ua_trees)
     mine = [t.with_tallies([t.root]) for i, t in enumerate(trees) if i % world == rank]
-    with Batch(mine, device=local) as b:
+    with Batch(mine, device=local, ctas_per_sm=args.ctas_per_sm) as b:
         base = [t.be_prob for t in mine]
         for i in range(args.warmup):
             b.uncertainty(base, draws_per_tree=args.ua_draws, words_per_instance=args.ua_words, seed=i)

@@ -349,6 +349,12 @@ def measure_is(args, local: int, tree: str = "read-once") -> dict:
         plain_ms = a.elapsed_time(b)
         ones, total = e.tallies()
     plain_rate = args.plain_words * 64 / (plain_ms * 1e-3)  # samples / s
+    if args.is_pipeline == "batched" and args.warmup:
+        # one untimed run of the pipeline: the first launches of its kernels in
+        # a process load their code and size the per-thread stack
+        from mcscram_b200.importance import batched_learned_is
+        batched_learned_is([g], target_rel_err=0.05, device=local)
+        torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
@@ -400,6 +406,8 @@ def measure_is(args, local: int, tree: str = "read-once") -> dict:
         "plain": {"samples_per_s": plain_rate, "required_samples": n_req, "seconds": plain_s,
                   "measured_words": args.plain_words, "measured_ms": plain_ms,
                   "note": "time derived from the rate measured on this tree"},
+        "warm_up": ("the batched pipeline once untimed on the same tree" if args.is_pipeline == "batched" and
+                    args.warmup else "none"),
         "speedup": plain_s / is_wall, "clocks": clk}
 
 
@@ -984,7 +992,7 @@ def main() -> int:
                          "unit": "s", **{k: v for k, v in m["is"].items() if k != "ce_rounds"},
                          "plain_samples_per_s": m["plain"]["samples_per_s"],
                          "plain_seconds_derived": m["plain"]["seconds"], "speedup_vs_plain": m["speedup"],
-                         "clocks": m["clocks"]}
+                         "warm_up": m["warm_up"], "clocks": m["clocks"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -87,7 +87,8 @@ def parse_args():
                     help="rare-event trees with 20%% of their basic events read by two gates (exact values from "
                          "tests/golden/config5_dag_exact.json), or read-once trees (exact by recursion)")
     ap.add_argument("--bis-ce-rounds", type=int, default=0, help="CE rounds (0 = the driver's default)")
-    ap.add_argument("--bis-ce-words", type=int, default=1 << 13, help="words per tree per CE round")
+    ap.add_argument("--bis-ce-words", type=int, default=1 << 11,
+                    help="words per tree per CE round (2^17 samples: 2^18 and 2^19 measured as accurate, slower)")
     ap.add_argument("--bis-est-words", type=int, default=1 << 12, help="words per tree of the first estimate round")
     ap.add_argument("--bis-max-est-words", type=int, default=1 << 20,
                     help="estimate words per tree at most (a tree not at 5 %% by then is reported unconverged)")

@@ -498,7 +498,8 @@ struct IsBatchArgs {
     const uint64_t *buf;
     uint64_t W;
     uint32_t n_inst;
-    uint32_t strips;               // ceil(W / kWeightThreads)
+    uint32_t strips;               // ceil(W / (kWeightThreads / split))
+    uint32_t split;                // threads per word: 1, 2, 4 or 8
     uint32_t n_comp;               // 1 .. kMaxComponents
     uint32_t n_be;                 // stride of a[] and C[] between components
     const uint32_t *be_begin;      // n_inst + 1
@@ -535,9 +536,12 @@ __global__ void __launch_bounds__(kWeightThreads) k_is_weights_batch(IsBatchArgs
         __syncthreads();
         if (item >= items) break;
         const uint32_t k = (uint32_t)(item / p.strips);
-        const uint64_t w = (item % p.strips) * kWeightThreads + threadIdx.x;
+        // p.split threads share a word, thread q taking its samples [q * 64 / split, (q + 1) * 64 / split)
+        const uint32_t q = threadIdx.x % p.split, per = 64u / p.split;
+        const uint64_t w = (item % p.strips) * (kWeightThreads / p.split) + threadIdx.x / p.split;
         const bool valid = w < p.W;
-        const uint64_t top = valid ? p.buf[(uint64_t)p.root_row[k] * p.W + w] : 0ull;
+        const uint64_t mine = per == 64u ? ~0ull : ((1ull << per) - 1ull) << (q * per);
+        const uint64_t top = valid ? p.buf[(uint64_t)p.root_row[k] * p.W + w] & mine : 0ull;
         if (!__syncthreads_or(top != 0ull)) continue;
         for (uint64_t m = top; m; m &= m - 1) {
             const int b = __ffsll((long long)m) - 1;
@@ -1408,7 +1412,12 @@ mcg_status mcg_is_batch_run(mcg_is_batch *b, const uint64_t *q_thr, uint32_t n_d
         IsBatchArgs p = args;
         p.buf = buf;
         p.W = W;
-        p.strips = (uint32_t)((W + kWeightThreads - 1) / kWeightThreads);
+        // one thread per word, or more where that leaves most SMs idle (a
+        // few trees in a short pass: each sample's cut-set terms are costly)
+        p.split = 1;
+        while (p.split < 8 && (uint64_t)n_inst * ((W * p.split + kWeightThreads - 1) / kWeightThreads) < 4ull * sms)
+            p.split *= 2;
+        p.strips = (uint32_t)((W * p.split + kWeightThreads - 1) / kWeightThreads);
         const uint64_t items = (uint64_t)n_inst * p.strips;
         const uint32_t blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sms * 8));
         cudaError_t err = cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), s);

@@ -783,11 +783,18 @@ def _prepare_one(g: FlatGraph, n_modes: int, importance: bool):
 
 def prepare_trees_async(graphs, n_modes: int, importance: bool, executor):
     """Starts _prepare_one for every tree on an executor (the tasks are
-    submitted now) and returns a function that waits for the results."""
-    n = getattr(executor, "_max_workers", 1) or 1
-    results = executor.map(_prepare_one, graphs, [n_modes] * len(graphs), [importance] * len(graphs),
-                           chunksize=max(1, len(graphs) // (4 * n)))
-    return lambda: list(results)
+    submitted now, one tree each, the largest first so that no worker is left
+    with several of them at the end) and returns a function that waits for
+    the results, in the order of `graphs`."""
+    order = sorted(range(len(graphs)), key=lambda k: -graphs[k].n_be)
+    futures = [executor.submit(_prepare_one, graphs[k], n_modes, importance) for k in order]
+
+    def collect():
+        out = [None] * len(graphs)
+        for k, f in zip(order, futures):
+            out[k] = f.result()
+        return out
+    return collect
 
 
 def prepare_trees(graphs, n_modes: int = 4, importance: bool = True, workers=0):

@@ -771,14 +771,17 @@ def _prepare_one(g: FlatGraph, n_modes: int, importance: bool):
     independence-approximation pass conditioned on the top and on each mode;
     and for a tree with events read by several gates whose gates are each read
     once, their conditional probabilities given the top (shared_posteriors;
-    None when the tree has no shared event or they cannot be computed)."""
+    None when the tree has no shared event or they cannot be computed), and
+    where they cannot be computed the heuristic seed (shared_seed; else None)."""
     pr, cond = approximate_importance(g, root=[g.root] + _mode_kids(g))
-    post = None
+    post = seed = None
     if cut_set_eligible(g) and shared_events(g).any():
         r = shared_posteriors(g)
         post = None if r is None else r[1]
+        if post is None:
+            seed = shared_seed(g)
     return (event_features(g, instance_scale=1.0, importance=importance, approx=(pr, cond[0])),
-            mode_proposals(g, n_modes, 1.0, approx=(pr, cond)), post)
+            mode_proposals(g, n_modes, 1.0, approx=(pr, cond)), post, seed)
 
 
 def prepare_trees_async(graphs, n_modes: int, importance: bool, executor):
@@ -1053,7 +1056,7 @@ def batched_learned_is(graphs, target_rel_err: float = 0.05, mlp: Optional[Propo
             if not m.any():
                 continue
             post = prepared[k][2]
-            inc = np.minimum((post if post is not None else shared_seed(g))[m], 0.9)
+            inc = np.minimum((post if post is not None else prepared[k][3])[m], 0.9)
             r_floor[sl[k]][m] = 0.5 * inc
             r0[sl[k]][m] = np.clip(inc, p[sl[k]][m], 0.9)
             post_fixed[sl[k]] = m & (post is not None)

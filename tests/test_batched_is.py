@@ -173,10 +173,12 @@ def test_prepare_trees_on_an_executor_equals_serial():
     with ThreadPoolExecutor(max_workers=2) as ex:
         pooled = prepare_trees(trees, 4, True, ex)
         made = synth.config5_instances([1, 3], workers=ex)
-    for (f0, m0, z0), (f1, m1, z1) in zip(serial, pooled):
+    for (f0, m0, z0, s0), (f1, m1, z1, s1) in zip(serial, pooled):
         assert np.array_equal(f0, f1) and np.array_equal(m0, m1)
         assert (z0 is None) == (z1 is None) and (z0 is None or np.array_equal(z0, z1))
+        assert (s0 is None) == (s1 is None) and (s0 is None or np.array_equal(s0, s1))
     assert serial[0][2] is None and serial[3][2] is not None  # shared-event posteriors for the DAG only
+    assert serial[3][3] is None  # the heuristic seed only where the posteriors cannot be computed
     assert np.array_equal(made[1].be_threshold, synth.config5_instance(3).be_threshold)
 
 

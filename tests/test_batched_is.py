@@ -182,6 +182,25 @@ def test_prepare_trees_on_an_executor_equals_serial():
     assert np.array_equal(made[1].be_threshold, synth.config5_instance(3).be_threshold)
 
 
+def test_prepare_trees_async_keeps_the_order_of_the_trees():
+    """The pipeline submits the trees largest first and collects them back in
+    the caller's order: the same inputs as the serial path, tree for tree."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from mcscram_b200.importance import prepare_trees, prepare_trees_async
+    trees = [synth.config5_dag_instance(i) for i in (5, 0, 3)] + [synth.config5_instance(2)]
+    assert len({t.n_be for t in trees}) == len(trees)  # distinct sizes: the submission order differs
+    serial = prepare_trees(trees, 4, True, 0)
+    with ThreadPoolExecutor(max_workers=3) as ex:
+        collect = prepare_trees_async(trees, 4, True, ex)
+        pooled = collect()
+    assert len(pooled) == len(trees)
+    for a, b in zip(serial, pooled):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        for x, y in zip(a[2:], b[2:]):
+            assert (x is None) == (y is None) and (x is None or np.array_equal(x, y))
+
+
 def test_mode_proposals_condition_on_top_children():
     from mcscram_b200.importance import approximate_importance, mode_proposals
     g = synth.config5_instance(0)

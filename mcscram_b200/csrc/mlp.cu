@@ -762,7 +762,7 @@ mcg_status ensure_rows(mcg_mlp *m, uint32_t n) {
     return MCG_OK;
 }
 
-// After a synchronised call: did a kernel give up on a tensor-core or copy wait?
+// After a synchronised call: did one of its kernels give up on a tensor-core or copy wait?
 mcg_status check_waits(mcg_mlp *m) {
     int err = 0;
     MCG_CUDA(cudaMemcpy(&err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -792,9 +792,12 @@ mcg_status grad_pass(mcg_mlp *m, uint32_t n, float inv_wsum, bool has_w) {
     return MCG_OK;
 }
 
+// The call's rows to the device; also clears the wait-timeout flag, so that
+// check_waits reports this call's kernels only.
 mcg_status upload_rows(mcg_mlp *m, const float *feat, const float *tgt, const float *w, uint32_t n, float &inv_wsum) {
     mcg_status st = ensure_rows(m, n);
     if (st != MCG_OK) return st;
+    MCG_CUDA(cudaMemsetAsync(m->d_err, 0, sizeof(int), m->stream));
     MCG_CUDA(cudaMemcpyAsync(m->d_feat, feat, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice, m->stream));
     if (tgt) MCG_CUDA(cudaMemcpyAsync(m->d_tgt, tgt, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, m->stream));
     double ws = 0.0;

@@ -209,34 +209,6 @@ struct CutArgs {
     unsigned int *error;
 };
 
-struct CountFrame {
-    uint32_t node, j;
-    double acc;
-    double dp[kCutMaxK + 1];
-};
-
-__device__ __forceinline__ void count_deliver(CountFrame &f, uint32_t op, uint32_t kk, double v) {
-    if (op == MCG_AND) {
-        f.acc *= v;
-    } else if (op == MCG_ATLEAST) {
-        for (int r = (int)kk; r >= 1; --r) f.dp[r] += f.dp[r - 1] * v;
-    } else {
-        f.acc += v;
-    }
-}
-
-// A frame for `node`; the k-subset sums dp[0 .. k] only for an ATLEAST gate
-// (the only connective that reads them).
-__device__ __forceinline__ void count_init(CountFrame &f, uint32_t node, uint32_t op, uint32_t kk) {
-    f.node = node;
-    f.j = 0;
-    f.acc = op == MCG_AND ? 1.0 : 0.0;
-    if (op == MCG_ATLEAST) {
-        f.dp[0] = 1.0;
-        for (uint32_t r = 1; r <= kk && r <= (uint32_t)kCutMaxK; ++r) f.dp[r] = 0.0;
-    }
-}
-
 // No memo: every entered gate is evaluated.
 struct NoMemo {
     __device__ bool get(uint32_t, double &) { return false; }
@@ -292,49 +264,79 @@ struct GateMemo {
 // sum) from gate `root`: a basic event x gives leaf(x), a gate x is entered
 // when enter(x) holds and gives other(x) otherwise; memo holds values of
 // gates evaluated before (the same recursion gives the same value).  Returns
-// -1 when the tree is deeper than the frames hold.
+// -1 when the tree is deeper than the frames hold.  The frame being worked
+// on (node, next input, accumulator, gate record) stays in registers; only
+// the suspended ancestors and the ATLEAST k-subset sums are in local memory.
 template <class Leaf, class Enter, class Other, class Memo = NoMemo>
 __device__ double tree_eval(uint32_t root, const uint4 *gate, const uint32_t *inputs, uint32_t n_be, Leaf leaf,
                             Enter enter, Other other, Memo *memo = nullptr) {
     double known;
     if (memo && memo->get(root, known)) return known;
-    CountFrame st[kCountDepth];
-    int sp = 1;
-    {
-        const uint32_t g0 = gate[root - n_be].x;
-        count_init(st[0], root, g0 & 0xFFu, (g0 >> 8) & 0xFFu);
-    }
+    struct Suspended {
+        uint32_t node, j;
+        double acc;
+    };
+    Suspended st[kCountDepth];
+    double dp[kCountDepth][kCutMaxK + 1];  // the k-subset sums of an ATLEAST frame at each depth
+    int sp = 0;                            // depth of the current frame
+    uint32_t node = root, j = 0;
+    uint4 g = gate[root - n_be];
+    uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu;
+    double acc = op == MCG_AND ? 1.0 : 0.0;
+    auto start = [&]() {  // the k-subset sums of a new ATLEAST frame at depth sp
+        if (op == MCG_ATLEAST) {
+            dp[sp][0] = 1.0;
+            for (uint32_t r = 1; r <= kk && r <= (uint32_t)kCutMaxK; ++r) dp[sp][r] = 0.0;
+        }
+    };
+    auto deliver = [&](double v) {
+        if (op == MCG_AND) {
+            acc *= v;
+        } else if (op == MCG_ATLEAST) {
+            for (int r = (int)kk; r >= 1; --r) dp[sp][r] += dp[sp][r - 1] * v;
+        } else {
+            acc += v;
+        }
+    };
+    start();
     for (;;) {
-        CountFrame &f = st[sp - 1];
-        const uint4 g = gate[f.node - n_be];
-        const uint32_t op = g.x & 0xFFu, kk = (g.x >> 8) & 0xFFu;
-        if (f.j < g.z) {
-            const uint32_t x = inputs[g.y + f.j++];
+        if (j < g.z) {
+            const uint32_t x = inputs[g.y + j++];
             if (x < n_be) {
-                count_deliver(f, op, kk, leaf(x));
+                deliver(leaf(x));
                 continue;
             }
             if (!enter(x)) {
-                count_deliver(f, op, kk, other(x));
+                deliver(other(x));
                 continue;
             }
             if (memo && memo->get(x, known)) {
-                count_deliver(f, op, kk, known);
+                deliver(known);
                 continue;
             }
-            if (sp == kCountDepth) return -1.0;
-            {
-                const uint32_t gx = gate[x - n_be].x;
-                count_init(st[sp], x, gx & 0xFFu, (gx >> 8) & 0xFFu);
-            }
+            if (sp + 1 == kCountDepth) return -1.0;
+            st[sp] = Suspended{node, j, acc};
             ++sp;
+            node = x;
+            j = 0;
+            g = gate[x - n_be];
+            op = g.x & 0xFFu;
+            kk = (g.x >> 8) & 0xFFu;
+            acc = op == MCG_AND ? 1.0 : 0.0;
+            start();
             continue;
         }
-        const double v = op == MCG_ATLEAST ? f.dp[kk] : f.acc;
-        if (memo) memo->put(f.node, v);
-        if (--sp == 0) return v;
-        const uint32_t pop = gate[st[sp - 1].node - n_be].x;
-        count_deliver(st[sp - 1], pop & 0xFFu, (pop >> 8) & 0xFFu, v);
+        const double v = op == MCG_ATLEAST ? dp[sp][kk] : acc;
+        if (memo) memo->put(node, v);
+        if (sp == 0) return v;
+        --sp;
+        node = st[sp].node;
+        j = st[sp].j;
+        acc = st[sp].acc;
+        g = gate[node - n_be];
+        op = g.x & 0xFFu;
+        kk = (g.x >> 8) & 0xFFu;
+        deliver(v);
     }
 }
 

@@ -11,8 +11,12 @@
 // product reduces z_i^2 to z_i), and at the LCA z_i is replaced by p_i (the
 // polynomial is then affine in z_i, so this is its expectation).  S(top) is
 // the constant left at the top.  P(z_i = 1 | top) ~ p_i S(top | z_i = 1) / S,
-// where S(top | z_i = 1) replaces z_i by 1 at its LCA; only the gates above
-// that LCA change, so each shared event costs one pass up its path.
+// where S(top | z_i = 1) replaces z_i by 1 at its LCA.  Every connective is
+// linear in each input in this ring, and the substitutions at the LCAs above
+// are ring homomorphisms, so the change D at the LCA reaches the top as the
+// full evaluation of D * adj(LCA): one top-down pass of adjoints (the
+// product of the partial derivatives along the path, with the events no
+// longer open below evaluated at their p) serves every shared event.
 #include <algorithm>
 #include <cstdint>
 #include <iterator>
@@ -133,6 +137,65 @@ double constant_term(const Poly &f) {
     return it == f.end() ? 0.0 : it->second;
 }
 
+// z_j := p_j for every event j not in `keep` (sorted).
+Poly evaluate_except(const Tree &t, const Poly &f, const std::vector<uint32_t> &keep) {
+    Poly out;
+    for (const auto &term : f) {
+        Mono m;
+        double c = term.second;
+        for (uint32_t j : term.first) {
+            if (std::binary_search(keep.begin(), keep.end(), j)) m.push_back(j);
+            else c *= t.p[j];
+        }
+        out[m] += c;
+    }
+    return out;
+}
+
+// The value with every z_j := p_j.
+double evaluate_all(const Tree &t, const Poly &f) {
+    double s = 0.0;
+    for (const auto &term : f) {
+        double c = term.second;
+        for (uint32_t j : term.first) c *= t.p[j];
+        s += c;
+    }
+    return s;
+}
+
+// d(gate) / d(input q) from the other inputs' values: the product of the
+// others (AND), 1 (OR), the (k - 1)-th elementary symmetric sum of the
+// others (ATLEAST k), 1 for a pass-through gate's last input and 0 for its
+// others.  Every connective is linear in each input (z^2 = z keeps the
+// product in the same ring), so a change D of input q changes the gate by
+// D times this.
+template <class Child>
+Poly partial(const Tree &t, uint32_t gate, uint32_t q, Child child, PolyLimit &lim) {
+    const mcg_graph_desc &g = t.g;
+    const uint32_t j = gate - t.nb;
+    const uint32_t op = g.gate_op[j], n = g.gate_in_count[j], k = g.gate_k[j] & 0xFFu;
+    const uint32_t *in = g.inputs + g.gate_in_begin[j];
+    if (op == MCG_AND) {
+        Poly acc = constant(1.0);
+        for (uint32_t c = 0; c < n && !lim.over; ++c)
+            if (c != q) acc = mul(acc, child(in[c]), lim);
+        return acc;
+    }
+    if (op == MCG_OR) return constant(1.0);
+    if (op == MCG_ATLEAST) {
+        if (k == 0) return Poly{};
+        std::vector<Poly> E(k);  // e_r of the other inputs, r < k
+        E[0] = constant(1.0);
+        for (uint32_t c = 0; c < n && !lim.over; ++c) {
+            if (c == q) continue;
+            const Poly v = child(in[c]);
+            for (int r = (int)k - 1; r >= 1 && !lim.over; --r) add_into(E[r], mul(E[r - 1], v, lim));
+        }
+        return E[k - 1];
+    }
+    return q + 1 == n ? constant(1.0) : Poly{};  // pass-through
+}
+
 }  // namespace
 
 extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_t root, uint64_t max_terms,
@@ -211,21 +274,53 @@ extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_
     *p_top = S;
     for (uint32_t i = 0; i < nb; ++i) posterior[i] = -1.0;
     if (!(S > 0.0)) return MCG_OK;
+    // The events open at each gate: a leaf below it, their LCA above it.
+    std::vector<std::vector<uint32_t>> open(g.n_gates);
+    for (uint32_t v : order) {
+        const uint32_t j = v - nb;
+        std::vector<uint32_t> o;
+        for (uint32_t q = 0; q < g.gate_in_count[j]; ++q) {
+            const uint32_t x = g.inputs[g.gate_in_begin[j] + q];
+            if (x < nb) {
+                if (t.shared[x]) o.push_back(x);
+            } else {
+                o.insert(o.end(), open[x - nb].begin(), open[x - nb].end());
+            }
+        }
+        std::sort(o.begin(), o.end());
+        o.erase(std::unique(o.begin(), o.end()), o.end());
+        std::vector<uint32_t> closing = t.closes[j];
+        std::sort(closing.begin(), closing.end());
+        std::set_difference(o.begin(), o.end(), closing.begin(), closing.end(), std::back_inserter(open[j]));
+    }
+    // Adjoints, top down: a change D of a gate's closed value changes S(top)
+    // by the full evaluation of D * adj(gate).  adj(child) = adj(gate) *
+    // d(gate)/d(child), with every event not open at the child set to its p
+    // (D below that child holds only events open there).  The closings above
+    // are ring homomorphisms that leave the factors from higher up unchanged,
+    // so they commute with these products.
+    std::vector<Poly> adj(g.n_gates);
+    if (root >= nb) adj[root - nb] = constant(1.0);
+    for (auto it = order.rbegin(); it != order.rend() && !lim.over; ++it) {
+        const uint32_t u = *it, j = u - nb;
+        if (adj[j].empty()) continue;  // the top does not depend on this gate
+        for (uint32_t q = 0; q < g.gate_in_count[j] && !lim.over; ++q) {
+            const uint32_t c = g.inputs[g.gate_in_begin[j] + q];
+            if (c < nb) continue;
+            const Poly d = partial(t, u, q, child_value, lim);
+            adj[c - nb] = evaluate_except(t, mul(adj[j], d, lim), open[c - nb]);
+        }
+    }
+    if (lim.over) return mcg::fail(MCG_ERR_INVALID, "term limit exceeded");
     for (uint32_t i = 0; i < nb; ++i) {
         if (!t.shared[i]) continue;
-        // S(top | z_i = 1): z_i := 1 at its LCA, then the gates above it again
-        uint32_t v = t.lca[i];
-        Poly f = close_all(t, v, combine(t, v, child_value, lim), i, 1.0);
-        while (t.parent[v] != kNone && !lim.over) {
-            const uint32_t u = t.parent[v], changed = v;
-            const Poly fv = f;
-            f = close_all(t, u, combine(t, u, [&](uint32_t x) -> Poly {
-                return x == changed ? fv : child_value(x);
-            }, lim));
-            v = u;
-        }
+        // S(top | z_i = 1) = S + the change of z_i := 1 (instead of p_i) at its LCA, carried up by the adjoint
+        const uint32_t v = t.lca[i];
+        Poly d = close_all(t, v, combine(t, v, child_value, lim), i, 1.0);
+        add_into(d, t.value[v - nb], -1.0);
+        const double delta = evaluate_all(t, mul(d, adj[v - nb], lim));
         if (lim.over) return mcg::fail(MCG_ERR_INVALID, "term limit exceeded");
-        posterior[i] = std::min(1.0, t.p[i] * constant_term(f) / S);
+        posterior[i] = std::min(1.0, t.p[i] * (S + delta) / S);
     }
     return MCG_OK;
 }

@@ -301,6 +301,7 @@ extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_
     // so they commute with these products.
     std::vector<Poly> adj(g.n_gates);
     if (root >= nb) adj[root - nb] = constant(1.0);
+    // (a product over the limit sends every event to the per-path fallback below)
     for (auto it = order.rbegin(); it != order.rend() && !lim.over; ++it) {
         const uint32_t u = *it, j = u - nb;
         if (adj[j].empty()) continue;  // the top does not depend on this gate
@@ -311,16 +312,33 @@ extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_
             adj[c - nb] = evaluate_except(t, mul(adj[j], d, lim), open[c - nb]);
         }
     }
-    if (lim.over) return mcg::fail(MCG_ERR_INVALID, "term limit exceeded");
-    for (uint32_t i = 0; i < nb; ++i) {
+    for (uint32_t i = 0; i < nb && !lim.over; ++i) {
         if (!t.shared[i]) continue;
         // S(top | z_i = 1) = S + the change of z_i := 1 (instead of p_i) at its LCA, carried up by the adjoint
         const uint32_t v = t.lca[i];
         Poly d = close_all(t, v, combine(t, v, child_value, lim), i, 1.0);
         add_into(d, t.value[v - nb], -1.0);
         const double delta = evaluate_all(t, mul(d, adj[v - nb], lim));
-        if (lim.over) return mcg::fail(MCG_ERR_INVALID, "term limit exceeded");
         posterior[i] = std::min(1.0, t.p[i] * (S + delta) / S);
+    }
+    if (!lim.over) return MCG_OK;
+    // The adjoints hold more terms than the limit where the gates' own values
+    // did not: S(top | z_i = 1) by re-evaluating the gates above each LCA.
+    lim.over = false;
+    for (uint32_t i = 0; i < nb; ++i) {
+        if (!t.shared[i]) continue;
+        uint32_t v = t.lca[i];
+        Poly f = close_all(t, v, combine(t, v, child_value, lim), i, 1.0);
+        while (t.parent[v] != kNone && !lim.over) {
+            const uint32_t u = t.parent[v], changed = v;
+            const Poly fv = f;
+            f = close_all(t, u, combine(t, u, [&](uint32_t x) -> Poly {
+                return x == changed ? fv : child_value(x);
+            }, lim));
+            v = u;
+        }
+        if (lim.over) return mcg::fail(MCG_ERR_INVALID, "term limit exceeded");
+        posterior[i] = std::min(1.0, t.p[i] * constant_term(f) / S);
     }
     return MCG_OK;
 }

@@ -88,3 +88,104 @@ def test_refuses_gates_read_twice():
     g = synth.generate(synth.TreeSpec(n_be=30, n_gates=14, mix={AND: 0.5, OR: 0.5}, p_range=(0.01, 0.2), seed=3,
                                       n_layers=4, share_node_frac=0.3))
     assert shared_posteriors(g) is None
+
+
+def _ring_posteriors(g):
+    """The definition restated: node values as polynomials in the indicators
+    of the shared events still open (dict of frozenset -> coefficient, z^2 =
+    z), every event set to its p at the lowest common ancestor of its
+    leaves, and S(top | z_i = 1) by evaluating the whole tree again with z_i
+    set to 1 there instead."""
+    nb = g.n_be
+    p = g.quantised_probabilities()
+    parent = {}
+    leaf_parents = {}
+    for j in range(g.n_gates):
+        for x in g.gate_inputs(j):
+            x = int(x)
+            if x < nb:
+                leaf_parents.setdefault(x, []).append(nb + j)
+            else:
+                parent[x] = nb + j
+
+    def ancestors(v):
+        out = [v]
+        while v in parent:
+            v = parent[v]
+            out.append(v)
+        return out
+
+    shared = [e for e, ps in leaf_parents.items() if len(ps) > 1]
+    lca = {}
+    for e in shared:
+        common = set(ancestors(leaf_parents[e][0]))
+        for q in leaf_parents[e][1:]:
+            common &= set(ancestors(q))
+        lca[e] = min(common, key=lambda v: len(ancestors(v)) * -1)  # the deepest common ancestor
+    closes = {}
+    for e, v in lca.items():
+        closes.setdefault(v, []).append(e)
+
+    def mul(a, b):
+        out = {}
+        for ma, ca in a.items():
+            for mb, cb in b.items():
+                m = ma | mb
+                out[m] = out.get(m, 0.0) + ca * cb
+        return out
+
+    def add(a, b):
+        out = dict(a)
+        for m, c in b.items():
+            out[m] = out.get(m, 0.0) + c
+        return out
+
+    def top_value(fixed=None):
+        val = {}
+        for j in range(g.n_gates):
+            kids = []
+            for x in g.gate_inputs(j):
+                x = int(x)
+                kids.append(({frozenset([x]): 1.0} if x in lca else {frozenset(): float(p[x])}) if x < nb
+                            else val[x])
+            op, k = int(g.gate_op[j]), int(g.gate_k[j]) & 0xFF
+            if op == AND:
+                f = {frozenset(): 1.0}
+                for v in kids:
+                    f = mul(f, v)
+            elif op == OR:
+                f = {}
+                for v in kids:
+                    f = add(f, v)
+            else:
+                e = [{frozenset(): 1.0}] + [{} for _ in range(k)]
+                for v in kids:
+                    for r in range(k, 0, -1):
+                        e[r] = add(e[r], mul(e[r - 1], v))
+                f = e[k]
+            for ev in closes.get(nb + j, []):
+                val_e = 1.0 if ev == fixed else float(p[ev])
+                g2 = {}
+                for m, c in f.items():
+                    if ev in m:
+                        m, c = m - {ev}, c * val_e
+                    g2[m] = g2.get(m, 0.0) + c
+                f = g2
+            val[nb + j] = f
+        return val[g.root].get(frozenset(), 0.0)
+
+    S = top_value()
+    return S, {e: float(p[e]) * top_value(e) / S for e in shared}
+
+
+@pytest.mark.parametrize("i", [5, 25, 33, 37, 51])
+def test_posteriors_equal_the_definition_on_small_dags(i):
+    """The one-pass adjoint computation against the definition (the tree
+    evaluated again for every shared event), on small rare DAGs of AND, OR
+    and ATLEAST gates: equal to rounding."""
+    g = synth.config5_dag_instance(i)
+    S, post = shared_posteriors(g)
+    S_ref, ref = _ring_posteriors(g)
+    assert ref and S == pytest.approx(S_ref, rel=1e-12)
+    for e, v in ref.items():
+        assert post[e] == pytest.approx(min(v, 1.0), rel=1e-10, abs=1e-300), e

@@ -92,6 +92,7 @@ struct Tree {
 };
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr size_t kAdjointLimitFactor = 16;
 
 // The gate's polynomial from its children's (child(x) gives a child's), before closing.
 template <class Child>
@@ -301,7 +302,11 @@ extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_
     // so they commute with these products.
     std::vector<Poly> adj(g.n_gates);
     if (root >= nb) adj[root - nb] = constant(1.0);
-    // (a product over the limit sends every event to the per-path fallback below)
+    // The adjoints may hold more terms than the gates' values; they get
+    // kAdjointLimitFactor times the limit (a product over it sends every event
+    // to the per-path fallback below, which is far slower on such trees).
+    const size_t gate_limit = lim.max_terms;
+    lim.max_terms = gate_limit * kAdjointLimitFactor;
     for (auto it = order.rbegin(); it != order.rend() && !lim.over; ++it) {
         const uint32_t u = *it, j = u - nb;
         if (adj[j].empty()) continue;  // the top does not depend on this gate
@@ -322,9 +327,10 @@ extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_
         posterior[i] = std::min(1.0, t.p[i] * (S + delta) / S);
     }
     if (!lim.over) return MCG_OK;
-    // The adjoints hold more terms than the limit where the gates' own values
-    // did not: S(top | z_i = 1) by re-evaluating the gates above each LCA.
+    // The adjoints hold more terms than their limit where the gates' own
+    // values did not: S(top | z_i = 1) by re-evaluating the gates above each LCA.
     lim.over = false;
+    lim.max_terms = gate_limit;
     for (uint32_t i = 0; i < nb; ++i) {
         if (!t.shared[i]) continue;
         uint32_t v = t.lca[i];

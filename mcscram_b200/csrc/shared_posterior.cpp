@@ -18,6 +18,7 @@
 // product of the partial derivatives along the path, with the events no
 // longer open below evaluated at their p) serves every shared event.
 #include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <iterator>
 #include <map>
@@ -306,7 +307,7 @@ extern "C" mcg_status mcg_shared_posteriors(const mcg_graph_desc *graph, uint32_
     // kAdjointLimitFactor times the limit (a product over it sends every event
     // to the per-path fallback below, which is far slower on such trees).
     const size_t gate_limit = lim.max_terms;
-    lim.max_terms = gate_limit * kAdjointLimitFactor;
+    lim.max_terms = gate_limit > SIZE_MAX / kAdjointLimitFactor ? SIZE_MAX : gate_limit * kAdjointLimitFactor;
     for (auto it = order.rbegin(); it != order.rend() && !lim.over; ++it) {
         const uint32_t u = *it, j = u - nb;
         if (adj[j].empty()) continue;  // the top does not depend on this gate
